@@ -1,0 +1,370 @@
+#!/usr/bin/env python
+"""Benchmark of the pseudo-CT path: voxels/s at 222x222x112, 10 atlases, NH=11.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One step = one pass of the path (patch SSD -> exp weights -> weighted CT fusion) over one
+synthetic subject (seeded generator; the reference's subject data is not public): one
+pct_synthesize_device call on inputs resident in HBM. Timed with CUDA events on the launching
+stream, W warm-up steps, K timed steps, barrier + synchronize on both sides, max over ranks.
+Under torchrun each rank processes its own subject (weak scaling, no data-path collective).
+
+`e2e` times the drop-in host-pointer entry point (pct_synthesize): pinned host inputs copied
+in, the path, the volume copied out, every step.
+
+`--impl reference` times the reference's own OpenMP CPU routine
+(MultiAtlasPatchBasedSegmentationOpenMP, compiled unmodified into oracle/_ref) on all host
+threads over a bounded slab of the same workload, extrapolated to the full volume by its
+measured candidates/s (the per-voxel work is identical everywhere).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+# Workload: config 1 at the metric's window (222x222x112, 10 atlases, NH=11, sigma 2.5, beta 1).
+NX, NY, NZ, NUM, NH = 222, 222, 112, 10, 11
+SIGMA, BETA = 2.5, 1.0
+N_BLOBS = 60
+METRIC = "pseudo-CT voxels/s at 222x222x112, 10 atlases, NH=11"
+UNIT = "voxels/s"
+# Algorithmic FP32 lane-operations per candidate (voxel, atlas, offset): 1 sub + 1 mul for the
+# squared difference, 6 adds for the separable 3x3x3 box sum, 1 scale, 1 FMA + 1 add for the two
+# accumulators; plus 1 MUFU ex2.
+OPS_PER_CANDIDATE = 11
+FP32_LANES_PER_SM = 128
+MUFU_LANES_PER_SM = 16
+PROFILE_SUMMARY = REPO / "profiles" / "fuse_plain_nh11_222x222x112_10atlas.md"
+
+
+def interior(n: int, nh: int) -> int:
+    return max(0, n - 2 * ((nh - 1) // 2 + 1))
+
+
+def candidates(nx=NX, ny=NY, nz=NZ, num=NUM, nh=NH) -> int:
+    return interior(nx, nh) * interior(ny, nh) * interior(nz, nh) * num * nh ** 3
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks/throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+        self._t = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-i", str(self.gpu), "-lms", "200"], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+            time.sleep(0.3)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self._t:
+            self._t.join(timeout=2)
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks() -> dict:
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text())
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0, "fallback": True}
+
+
+def profiled_traffic() -> float | None:
+    """Per-launch DRAM bytes of the fusion kernel from the committed ncu summary, if any."""
+    if not PROFILE_SUMMARY.exists():
+        return None
+    for line in PROFILE_SUMMARY.read_text().splitlines():
+        if line.strip().startswith("dram_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+# ---------------------------------------------------------------------------------- CPU side
+
+def cpu_reference_rate(target_s: float, threads: int = 0) -> dict:
+    """Times the reference's OpenMP routine on a z/x-cropped slab of the workload (1 interior
+    z-plane, enough interior x-rows for about target_s seconds); returns candidates/s."""
+    import oracle
+    import pseudoctimaging_b200 as pct
+
+    lo = (NH - 1) // 2 + 1
+    sub_nz = 2 * lo + 1
+    s = pct.synth_subject(NX, NY, sub_nz, NUM, n_blobs=N_BLOBS, seed=1)
+    label = pct.normalize_labels(s.atlas_ct)
+    div = pct.div_from(SIGMA, BETA)
+
+    def run(xrows: int) -> tuple[float, int]:
+        nx = 2 * lo + xrows
+        img = np.ascontiguousarray(s.img[:, :nx, :])
+        mri = np.ascontiguousarray(s.atlas_mri[:, :, :nx, :])
+        lab = np.ascontiguousarray(label[:, :, :nx, :])
+        t = time.perf_counter()
+        oracle.fuse_reference(img, mri, lab, NH, div, multicore=True, threads=threads)
+        dt = time.perf_counter() - t
+        return dt, candidates(nx, NY, sub_nz, NUM, NH)
+
+    dt, c = run(2)  # calibration
+    rate = c / dt
+    rows = int(max(2, min(interior(NX, NH), round(target_s * rate / candidates(2 * lo + 1, NY, sub_nz, NUM, NH)))))
+    dt, c = run(rows)
+    cores = threads if threads > 0 else oracle.reference().pctref_max_threads()
+    return {"cand_per_s": c / dt, "seconds": dt, "candidates": c, "cores": cores,
+            "sample": f"{NY}x{rows}x1 interior voxels (slab {2 * lo + rows}x{NY}x{sub_nz} of the "
+                      f"222x222x112 config-1 subject, seed 1), {NUM} atlases, NH={NH}"}
+
+
+def run_reference_arm(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle
+
+    if not oracle.has_reference():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/libpctref.so was not built (reference sources absent at build time)"}))
+        return
+    full = candidates()
+    step_s = []
+    last = None
+    for i in range(args.warmup + args.steps):
+        r = cpu_reference_rate(args.ref_step_seconds)
+        if i >= args.warmup:
+            step_s.append(full / r["cand_per_s"])
+            last = r
+    t = statistics.median(step_s)
+    value = NX * NY * NZ / t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded blobs/displacement generator, config 1)",
+        "config": {"workload": "222x222x112 subject, 10 atlases, NH=11, sigma 2.5, beta 1; "
+                               "each step a bounded slab, extrapolated by candidates/s",
+                   "nh": NH, "atlases": NUM, "volume": [NX, NY, NZ]},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": last["cores"], "kind": "reference",
+                         "sample": last["sample"], "cand_per_s": last["cand_per_s"]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------------- GPU side
+
+def run_b200_arm(args) -> None:
+    import torch
+    import torch.distributed as dist
+
+    import pseudoctimaging_b200 as pct
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    s = pct.synth_subject(NX, NY, NZ, NUM, n_blobs=N_BLOBS, seed=1 + rank)
+    label = pct.normalize_labels(s.atlas_ct)
+    div = pct.div_from(SIGMA, BETA)
+    d_img = torch.from_numpy(s.img).to(dev)
+    d_mri = torch.from_numpy(s.atlas_mri).to(dev)
+    d_lab = torch.from_numpy(label).to(dev)
+    d_out = torch.zeros_like(d_img)
+    h = pct.Handle(local)
+    stream = torch.cuda.current_stream(dev)
+    sptr = stream.cuda_stream
+
+    def step():
+        h.synthesize_device(d_img.data_ptr(), d_mri.data_ptr(), d_lab.data_ptr(),
+                            d_out.data_ptr(), NX, NY, NZ, NUM, NH, div, pct.EXEC_B200_FP32, sptr)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    value = world * NX * NY * NZ / (ms / 1e3)
+
+    # End to end through the drop-in host-pointer entry point, pinned host buffers.
+    p_img = torch.from_numpy(s.img).pin_memory()
+    p_mri = torch.from_numpy(s.atlas_mri).pin_memory()
+    p_lab = torch.from_numpy(label).pin_memory()
+    p_out = torch.empty_like(p_img).pin_memory()
+    h.set_stream(sptr)
+
+    def e2e_step():
+        pct.lib.pct_synthesize(h.ptr, p_img.data_ptr(), p_mri.data_ptr(), p_lab.data_ptr(),
+                               p_out.data_ptr(), NX, NY, NZ, NUM, NH, div, pct.EXEC_B200_FP32)
+
+    e2e_steps = max(1, min(args.steps, 5))
+    e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+    te = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_ms = float(te.item())
+    assert np.array_equal(np.isnan(p_out.numpy()), np.isnan(d_out.cpu().numpy()))
+    h.set_stream(None)
+
+    clocks = clk.summary()
+    peaks = measured_peaks()
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    mhz = clocks["sm_mhz"] or peaks.get("sm_max_mhz", 1965.0)
+    cand = candidates()
+    fp32_peak = sms * FP32_LANES_PER_SM * mhz * 1e6  # lane-ops/s at the sampled clock
+    mufu_peak = sms * MUFU_LANES_PER_SM * mhz * 1e6
+    achieved = cand * OPS_PER_CANDIDATE / (ms / 1e3)
+    traffic = profiled_traffic()
+    hbm_achieved = (traffic / (ms / 1e3) / 1e9) if traffic else None
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded blobs/displacement generator, config 1; one subject per GPU)",
+        "config": {"workload": "222x222x112 subject, 10 atlases, NH=11, sigma 2.5, beta 1, "
+                               "plain FP32 kernel (EXEC_CHOICE 3)",
+                   "nh": NH, "atlases": NUM, "volume": [NX, NY, NZ],
+                   "l2": "inputs larger than L2 (21 volumes, 464 MB per subject)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "candidates_per_s": world * cand / (ms / 1e3),
+        "gpu_launches": args.steps * 1,
+        "roofline": {
+            "bound": "fp32", "unit": "TFLOP/s",
+            "achieved": achieved / 1e12, "peak": fp32_peak / 1e12, "frac": achieved / fp32_peak,
+            "traffic": traffic,
+            "note": (f"{OPS_PER_CANDIDATE} FP32 lane-ops per candidate x {cand:.3e} candidates per "
+                     f"launch; peak = {sms} SMs x {FP32_LANES_PER_SM} FP32 lanes x sampled SM clock "
+                     f"{mhz:.0f} MHz; MUFU ex2 roof {cand / mufu_peak * 1e3:.2f} ms"),
+            "mufu_frac": (cand / (ms / 1e3)) / mufu_peak,
+            "hbm": {"achieved_gbs": hbm_achieved, "peak_gbs": peaks.get("hbm_gbs"),
+                    "frac": (hbm_achieved / peaks["hbm_gbs"]) if hbm_achieved else None},
+        },
+        "e2e": {"value": world * NX * NY * NZ / (e2e_ms / 1e3), "unit": UNIT,
+                "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": int(4 * NX * NY * NZ * (1 + 2 * NUM)),
+                "d2h_bytes_per_step": int(4 * NX * NY * NZ)},
+        "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+    }
+    h.close()
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = cpu_reference_rate(args.cpu_seconds)
+        cpu_value = NX * NY * NZ / (cand / r["cand_per_s"])
+        line["cpu_baseline"] = {"value": cpu_value, "unit": UNIT, "cores": r["cores"],
+                                "kind": "reference", "sample": r["sample"],
+                                "seconds": r["seconds"], "cand_per_s": r["cand_per_s"]}
+    if rank == 0:
+        print(json.dumps(line))
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0,
+                    help="CPU-baseline sample length (rank 0, N=1 only)")
+    ap.add_argument("--ref-step-seconds", type=float, default=4.0,
+                    help="length of each reference-arm step")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_b200_arm(args)
+
+
+if __name__ == "__main__":
+    main()

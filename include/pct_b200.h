@@ -1,0 +1,171 @@
+/*
+ * pct_b200: B200-native (sm_100a) patch-based multi-atlas pseudo-CT synthesis.
+ *
+ * C ABI over libpct_b200.so. Plain pointers and sizes only; every call returns PCT_OK (0) or a
+ * negative pct_status. Reference paths below are relative to the
+ * EduardoAlcainBallesteros/PseudoCTImaging tree.
+ *
+ * Volume layout (unchanged from the reference, PatchBasedPseudoCT.cu:853-890): row-major
+ * [atlas][z][x][y] with y contiguous; voxel (z,x,y) of atlas a is at a*N + z*nx*ny + x*ny + y,
+ * N = nx*ny*nz. nx is MATLAB's first dimension (rows), ny its second (cols).
+ *
+ * Threading: a pct_handle is used by one host thread at a time. Different handles are
+ * independent (no globals, unlike the reference's nx/ny/nz/num/nh).
+ */
+#ifndef PCT_B200_H
+#define PCT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PCT_ABI_VERSION 1
+
+typedef enum pct_status {
+  PCT_OK = 0,
+  PCT_ERR_INVALID_ARG = -1,   /* null pointer, bad size, even/too-small NH, ... */
+  PCT_ERR_CUDA = -2,          /* a CUDA runtime call failed (see pct_last_error_message) */
+  PCT_ERR_OUT_OF_MEMORY = -3, /* device allocation failed or exceeded the handle's cap */
+  PCT_ERR_UNSUPPORTED = -4,   /* exec_choice or NH this build does not provide */
+  PCT_ERR_NO_DEVICE = -5,     /* bad device index, or no sm_100 device */
+  PCT_ERR_TIMEOUT = -6,       /* a bounded device-side wait gave up */
+  PCT_ERR_INTERNAL = -7
+} pct_status;
+
+/*
+ * EXEC_CHOICE values. 0/1/2 are the reference's GPU choices (PatchBasedPseudoCT.cu:71-78:
+ * GM=0, GM2=1, SM=2, GpuTestTime=4); all three compute the same function, so this library runs
+ * them on its plain FP32 kernel. The new choices sit in the slots the reference leaves free.
+ */
+typedef enum pct_exec_choice {
+  PCT_EXEC_GM = 0,
+  PCT_EXEC_GM2 = 1,
+  PCT_EXEC_SM = 2,
+  PCT_EXEC_B200_FP32 = 3, /* plain FP32 sm_100a kernel */
+  PCT_EXEC_TC_FP16 = 5,   /* tensor-core FP16 correlation + top-k FP32 rescoring */
+  PCT_EXEC_TC_BF16 = 6,   /* tensor-core BF16 correlation + top-k FP32 rescoring */
+  PCT_EXEC_LEARNED = 7,   /* learned proposal + FP32 rescoring */
+  PCT_EXEC_BATCHED = 8    /* many subjects in one persistent launch */
+} pct_exec_choice;
+
+typedef struct pct_handle pct_handle;
+
+/* Library / error helpers. */
+int pct_abi_version(void);
+const char *pct_strerror(int status);
+/* Message of the last failure on this handle ("" if none). Valid until the next call. */
+const char *pct_last_error_message(const pct_handle *h);
+
+/*
+ * Handle lifecycle. Replaces the per-call cudaSetDevice/cudaMalloc/cudaFree of
+ * MultiPatchBasedSegmentationGpu (PatchBasedPseudoCT.cu:1687-1693,1744 and main's
+ * cudaSetDevice at :1988): device buffers are cached on the handle and reused across calls.
+ */
+int pct_create(int device, pct_handle **out);
+int pct_destroy(pct_handle *h);
+/* Stream used by the host-pointer calls (pct_synthesize, pct_run_pipeline); NULL restores the
+ * handle's own stream. The calls still synchronise on it before returning. */
+int pct_set_stream(pct_handle *h, void *stream);
+/* Cap on the bytes the handle may allocate (0 = unlimited). Exceeding it returns
+ * PCT_ERR_OUT_OF_MEMORY without calling the allocator. */
+int pct_set_memory_limit(pct_handle *h, size_t bytes);
+
+/*
+ * Drop-in for MultiPatchBasedSegmentationGpu (PatchBasedPseudoCT.cu:1635-1750).
+ * img [N], atlas [num*N], atlas_label [num*N] (already label-normalised, as the reference's
+ * main does before the call, PatchBasedPseudoCT.cu:2009-2020) and label_segmentation [N] are
+ * HOST buffers owned by the caller. The sizes come in as arguments instead of the reference's
+ * globals nx, ny, nz, num, nh (PatchBasedPseudoCT.cu:652-654). div = 2*27*beta*sigma^2
+ * (PatchBasedPseudoCT.cu:2154). As in the reference, the whole output volume is written:
+ * interior voxels get product/sum_weight or NaN, border voxels 0 (the reference zeroes its
+ * device buffer, :1693, and copies all of it back, :1742). Synchronous.
+ */
+int pct_synthesize(pct_handle *h, const float *img, const float *atlas, const float *atlas_label,
+                   float *label_segmentation, int nx, int ny, int nz, int num_atlas, int nh,
+                   double div, int exec_choice);
+
+/*
+ * Same computation on DEVICE buffers already resident on the handle's device, enqueued on
+ * `stream` (a cudaStream_t; NULL = the handle's own stream). Only interior voxels of d_out are
+ * written; border voxels keep whatever the caller put there. Asynchronous: errors from the
+ * launch are returned, errors during execution surface at the next synchronising call.
+ */
+int pct_synthesize_device(pct_handle *h, const float *d_img, const float *d_atlas,
+                          const float *d_atlas_label, float *d_out, int nx, int ny, int nz,
+                          int num_atlas, int nh, double div, int exec_choice, void *stream);
+
+/* In-place CT -> label scale L' = 255*((L+1024)/4095) on a device buffer of n floats
+ * (PatchBasedPseudoCT.cu:2009-2020, NewPatchedBrainPureC.cpp:1583-1593). */
+int pct_normalize_labels_device(pct_handle *h, float *d_label, size_t n, void *stream);
+
+/*
+ * Post-processing after the path, on a device volume in label scale:
+ * RegularizationStep (NewPatchedBrainPureC.cpp:1059-1106; PatchBasedPseudoCT.cu:1501-1595):
+ * every interior NaN becomes the median of the non-NaN values of its 3x3x3 neighbourhood,
+ * filled in the reference's sequential z,x,y order (a voxel sees the fills of voxels before it).
+ * nh gives the interior, as in the reference. *fills (optional) receives the number of fills.
+ */
+int pct_regularize_device(pct_handle *h, float *d_vol, int nx, int ny, int nz, int nh,
+                          int64_t *fills, void *stream);
+
+/* RoundMatrix then the HU map round(4095*(v/255)) - 1024 over all n voxels
+ * (NewPatchedBrainPureC.cpp:1221-1227,1732-1738; PatchBasedPseudoCT.cu:2173-2179). */
+int pct_finalize_hu_device(pct_handle *h, float *d_vol, size_t n, void *stream);
+
+/*
+ * The reference's main() flow for one subject (PatchBasedPseudoCT.cu:2009-2020,2152-2180), on
+ * host buffers: label normalisation of atlas_ct_hu (copied, not modified), the path
+ * (exec_choice), then, if `regularize` is non-zero, RegularizationStep, RoundMatrix and the
+ * map back to HU. out receives N floats (HU if regularize, else label scale).
+ */
+int pct_run_pipeline(pct_handle *h, const float *img, const float *atlas_mri,
+                     const float *atlas_ct_hu, float *out, int nx, int ny, int nz, int num_atlas,
+                     int nh, double sigma, double beta, int exec_choice, int regularize);
+
+/*
+ * FP64 comparison of two device volumes over the interior of an NH window, in HU
+ * (HU = v*4095/255 - 1024 applied to both). NaN in exactly one of the two counts as a mask
+ * mismatch and is excluded from the error sums; NaN in both is skipped.
+ */
+typedef struct pct_error_stats {
+  double mae_hu;          /* mean |a-b| in HU over voxels finite in both */
+  double max_abs_hu;      /* max |a-b| in HU */
+  double max_rel;         /* max |a-b| / max(|b|, 1e-30), label scale */
+  int64_t compared;       /* voxels finite in both */
+  int64_t nan_mismatch;   /* NaN in exactly one */
+  int64_t nan_both;       /* NaN in both */
+} pct_error_stats;
+int pct_error_stats_device(pct_handle *h, const float *d_a, const float *d_b, int nx, int ny,
+                           int nz, int nh, pct_error_stats *stats, void *stream);
+
+/*
+ * Seeded synthetic subject (host). Input MRI = sum of n_blobs Gaussian blobs (amplitude
+ * U[amp_lo,amp_hi], isotropic std U[std_lo,std_hi] voxels) + N(0, mri_noise). Atlas a: the
+ * noise-free input resampled (trilinear) through a smooth random displacement field whose
+ * largest displacement is max_disp voxels, + fresh N(0, mri_noise); its CT is a fixed
+ * piecewise-linear MRI->HU map of that resampled image, clipped to [-1000, 2000], + N(0,
+ * ct_noise). Deterministic in `seed` regardless of thread count. Any output pointer may be NULL.
+ */
+typedef struct pct_synth_params {
+  int nx, ny, nz, num_atlas;
+  int n_blobs;
+  float amp_lo, amp_hi;
+  float std_lo, std_hi;
+  float mri_noise;
+  float ct_noise;
+  float max_disp;
+  uint64_t seed;
+} pct_synth_params;
+int pct_synth_default_params(pct_synth_params *p, int nx, int ny, int nz, int num_atlas,
+                             int n_blobs, uint64_t seed);
+int pct_synth_generate(const pct_synth_params *p, float *img, float *atlas_mri,
+                       float *atlas_ct_hu);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PCT_B200_H */

@@ -1,0 +1,430 @@
+// C ABI of libpct_b200.so (declared in include/pct_b200.h).
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <new>
+#include <string>
+
+#include "pct_b200.h"
+#include "pct_internal.h"
+
+namespace {
+
+struct DevBuf {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace
+
+struct pct_handle {
+  int device = 0;
+  cudaStream_t stream = nullptr;       // the handle's own stream
+  cudaStream_t user_stream = nullptr;  // set by pct_set_stream for host-pointer calls
+  size_t mem_limit = 0;  // 0 = unlimited
+  size_t allocated = 0;
+  DevBuf img, atlas, label, out, scratch;
+  std::string last_error;
+};
+
+namespace {
+
+int fail(pct_handle *h, int status, const std::string &msg) {
+  if (h) h->last_error = msg;
+  return status;
+}
+
+int cuda_fail(pct_handle *h, cudaError_t e, const char *what) {
+  std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+  if (e == cudaErrorMemoryAllocation) return fail(h, PCT_ERR_OUT_OF_MEMORY, m);
+  return fail(h, PCT_ERR_CUDA, m);
+}
+
+#define PCT_CUDA(h, call)                                    \
+  do {                                                       \
+    cudaError_t pct_e_ = (call);                             \
+    if (pct_e_ != cudaSuccess) return cuda_fail(h, pct_e_, #call); \
+  } while (0)
+
+// Grow-only device buffer owned by the handle, subject to the handle's memory cap.
+int ensure(pct_handle *h, DevBuf &b, size_t bytes) {
+  if (b.bytes >= bytes) return PCT_OK;
+  const size_t others = h->allocated - b.bytes;
+  if (h->mem_limit && others + bytes > h->mem_limit)
+    return fail(h, PCT_ERR_OUT_OF_MEMORY,
+                "allocation of " + std::to_string(bytes) + " bytes exceeds the handle's memory limit");
+  if (b.ptr) {
+    cudaFree(b.ptr);
+    h->allocated -= b.bytes;
+    b.ptr = nullptr;
+    b.bytes = 0;
+  }
+  void *p = nullptr;
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return cuda_fail(h, e, "cudaMalloc");
+  }
+  b.ptr = p;
+  b.bytes = bytes;
+  h->allocated += bytes;
+  return PCT_OK;
+}
+
+int check_choice(pct_handle *h, int exec_choice) {
+  switch (exec_choice) {
+    case PCT_EXEC_GM:
+    case PCT_EXEC_GM2:
+    case PCT_EXEC_SM:
+    case PCT_EXEC_B200_FP32:
+      return PCT_OK;
+    case PCT_EXEC_TC_FP16:
+    case PCT_EXEC_TC_BF16:
+    case PCT_EXEC_LEARNED:
+    case PCT_EXEC_BATCHED:
+      return fail(h, PCT_ERR_UNSUPPORTED,
+                  "exec_choice " + std::to_string(exec_choice) + " is not available in this build");
+    default:
+      return fail(h, PCT_ERR_INVALID_ARG, "unknown exec_choice " + std::to_string(exec_choice));
+  }
+}
+
+int check_shape(pct_handle *h, int nx, int ny, int nz, int num, int nh, double div,
+                pct::Geometry *g) {
+  if (nx <= 0 || ny <= 0 || nz <= 0 || num <= 0)
+    return fail(h, PCT_ERR_INVALID_ARG, "volume sizes and atlas count must be positive");
+  if (nh < 3 || (nh % 2) == 0)
+    return fail(h, PCT_ERR_INVALID_ARG, "NH must be odd and >= 3, got " + std::to_string(nh));
+  if (nh > 11)
+    return fail(h, PCT_ERR_UNSUPPORTED, "NH > 11 is not compiled in (NH in 3..11)");
+  const long long nvox = (long long)nx * ny * nz;
+  if (nvox >= (1LL << 31))
+    return fail(h, PCT_ERR_INVALID_ARG, "volume has 2^31 or more voxels");
+  if (!(div > 0.0) || !isfinite(div))
+    return fail(h, PCT_ERR_INVALID_ARG, "div must be positive and finite");
+  if (!pct::make_geometry(nx, ny, nz, num, nh, g))
+    return fail(h, PCT_ERR_INVALID_ARG, "bad geometry");
+  return PCT_OK;
+}
+
+int select_device(pct_handle *h) {
+  PCT_CUDA(h, cudaSetDevice(h->device));
+  return PCT_OK;
+}
+
+// ---- FP64 error reduction -------------------------------------------------------------------
+
+struct ErrAccum {
+  double sum_abs;
+  unsigned long long max_abs_bits;  // non-negative doubles order like their bit patterns
+  unsigned long long max_rel_bits;
+  unsigned long long compared, nan_mismatch, nan_both;
+};
+
+__global__ void error_stats_kernel(const float *__restrict__ a, const float *__restrict__ b, int nx,
+                                   int ny, int nz, int lo, ErrAccum *acc) {
+  const int ix = nx - 2 * lo, iy = ny - 2 * lo, iz = nz - 2 * lo;
+  const long long total = (long long)ix * iy * iz;
+  double s = 0.0, mabs = 0.0, mrel = 0.0;
+  unsigned long long cmp = 0, mis = 0, both = 0;
+  const double to_hu = 4095.0 / 255.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int y = (int)(i % iy) + lo;
+    const long long r = i / iy;
+    const int x = (int)(r % ix) + lo;
+    const int z = (int)(r / ix) + lo;
+    const long long k = (long long)z * nx * ny + (long long)x * ny + y;
+    const float va = a[k], vb = b[k];
+    const bool na = isnan(va), nb = isnan(vb);
+    if (na && nb) { ++both; continue; }
+    if (na || nb) { ++mis; continue; }
+    const double d = fabs((double)va - (double)vb);
+    s += d * to_hu;
+    mabs = fmax(mabs, d * to_hu);
+    mrel = fmax(mrel, d / fmax(fabs((double)vb), 1e-30));
+    ++cmp;
+  }
+  // Warp then block reduction, one atomic set per block.
+  for (int o = 16; o > 0; o >>= 1) {
+    s += __shfl_down_sync(0xffffffffu, s, o);
+    mabs = fmax(mabs, __shfl_down_sync(0xffffffffu, mabs, o));
+    mrel = fmax(mrel, __shfl_down_sync(0xffffffffu, mrel, o));
+    cmp += __shfl_down_sync(0xffffffffu, cmp, o);
+    mis += __shfl_down_sync(0xffffffffu, mis, o);
+    both += __shfl_down_sync(0xffffffffu, both, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&acc->sum_abs, s);
+    atomicMax(&acc->max_abs_bits, (unsigned long long)__double_as_longlong(mabs));
+    atomicMax(&acc->max_rel_bits, (unsigned long long)__double_as_longlong(mrel));
+    atomicAdd(&acc->compared, cmp);
+    atomicAdd(&acc->nan_mismatch, mis);
+    atomicAdd(&acc->nan_both, both);
+  }
+}
+
+}  // namespace
+
+namespace pct {
+
+bool make_geometry(int nx, int ny, int nz, int num, int nh, Geometry *g) {
+  if (!g || nh < 1 || (nh % 2) == 0) return false;
+  g->nx = nx;
+  g->ny = ny;
+  g->nz = nz;
+  g->num = num;
+  g->nh = nh;
+  g->hw = (nh - 1) / 2;
+  g->lo = g->hw + 1;
+  g->ix = nx - 2 * g->lo;
+  g->iy = ny - 2 * g->lo;
+  g->iz = nz - 2 * g->lo;
+  return true;
+}
+
+}  // namespace pct
+
+extern "C" {
+
+int pct_abi_version(void) { return PCT_ABI_VERSION; }
+
+const char *pct_strerror(int status) {
+  switch (status) {
+    case PCT_OK: return "ok";
+    case PCT_ERR_INVALID_ARG: return "invalid argument";
+    case PCT_ERR_CUDA: return "CUDA runtime error";
+    case PCT_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case PCT_ERR_UNSUPPORTED: return "unsupported configuration";
+    case PCT_ERR_NO_DEVICE: return "no usable sm_100 device";
+    case PCT_ERR_TIMEOUT: return "device-side wait timed out";
+    case PCT_ERR_INTERNAL: return "internal error";
+    default: return "unknown status";
+  }
+}
+
+const char *pct_last_error_message(const pct_handle *h) { return h ? h->last_error.c_str() : ""; }
+
+int pct_create(int device, pct_handle **out) {
+  if (!out) return PCT_ERR_INVALID_ARG;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
+    cudaGetLastError();
+    return PCT_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= count) return PCT_ERR_NO_DEVICE;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return PCT_ERR_NO_DEVICE;
+  if (prop.major != 10) return PCT_ERR_NO_DEVICE;  // kernels are built for sm_100a only
+  pct_handle *h = new (std::nothrow) pct_handle();
+  if (!h) return PCT_ERR_OUT_OF_MEMORY;
+  h->device = device;
+  if (cudaSetDevice(device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    delete h;
+    return PCT_ERR_CUDA;
+  }
+  *out = h;
+  return PCT_OK;
+}
+
+int pct_destroy(pct_handle *h) {
+  if (!h) return PCT_ERR_INVALID_ARG;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (DevBuf *b : {&h->img, &h->atlas, &h->label, &h->out, &h->scratch})
+    if (b->ptr) cudaFree(b->ptr);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return PCT_OK;
+}
+
+int pct_set_stream(pct_handle *h, void *stream) {
+  if (!h) return PCT_ERR_INVALID_ARG;
+  h->user_stream = static_cast<cudaStream_t>(stream);
+  return PCT_OK;
+}
+
+int pct_set_memory_limit(pct_handle *h, size_t bytes) {
+  if (!h) return PCT_ERR_INVALID_ARG;
+  h->mem_limit = bytes;
+  return PCT_OK;
+}
+
+int pct_synthesize_device(pct_handle *h, const float *d_img, const float *d_atlas,
+                          const float *d_atlas_label, float *d_out, int nx, int ny, int nz,
+                          int num_atlas, int nh, double div, int exec_choice, void *stream) {
+  if (!h) return PCT_ERR_INVALID_ARG;
+  h->last_error.clear();
+  if (!d_img || !d_atlas || !d_atlas_label || !d_out)
+    return fail(h, PCT_ERR_INVALID_ARG, "null device pointer");
+  int st = check_choice(h, exec_choice);
+  if (st) return st;
+  pct::Geometry g;
+  st = check_shape(h, nx, ny, nz, num_atlas, nh, div, &g);
+  if (st) return st;
+  st = select_device(h);
+  if (st) return st;
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+  PCT_CUDA(h, pct::launch_fuse_plain(g, d_img, d_atlas, d_atlas_label, d_out, div, s));
+  return PCT_OK;
+}
+
+int pct_synthesize(pct_handle *h, const float *img, const float *atlas, const float *atlas_label,
+                   float *label_segmentation, int nx, int ny, int nz, int num_atlas, int nh,
+                   double div, int exec_choice) {
+  if (!h) return PCT_ERR_INVALID_ARG;
+  h->last_error.clear();
+  if (!img || !atlas || !atlas_label || !label_segmentation)
+    return fail(h, PCT_ERR_INVALID_ARG, "null host pointer");
+  int st = check_choice(h, exec_choice);
+  if (st) return st;
+  pct::Geometry g;
+  st = check_shape(h, nx, ny, nz, num_atlas, nh, div, &g);
+  if (st) return st;
+  st = select_device(h);
+  if (st) return st;
+  const size_t vol = (size_t)g.nvox() * sizeof(float);
+  const size_t vols = vol * (size_t)num_atlas;
+  if ((st = ensure(h, h->img, vol)) || (st = ensure(h, h->atlas, vols)) ||
+      (st = ensure(h, h->label, vols)) || (st = ensure(h, h->out, vol)))
+    return st;
+  cudaStream_t s = h->user_stream ? h->user_stream : h->stream;
+  PCT_CUDA(h, cudaMemcpyAsync(h->img.ptr, img, vol, cudaMemcpyHostToDevice, s));
+  PCT_CUDA(h, cudaMemcpyAsync(h->atlas.ptr, atlas, vols, cudaMemcpyHostToDevice, s));
+  PCT_CUDA(h, cudaMemcpyAsync(h->label.ptr, atlas_label, vols, cudaMemcpyHostToDevice, s));
+  PCT_CUDA(h, cudaMemsetAsync(h->out.ptr, 0, vol, s));
+  PCT_CUDA(h, pct::launch_fuse_plain(g, static_cast<const float *>(h->img.ptr),
+                                     static_cast<const float *>(h->atlas.ptr),
+                                     static_cast<const float *>(h->label.ptr),
+                                     static_cast<float *>(h->out.ptr), div, s));
+  PCT_CUDA(h, cudaMemcpyAsync(label_segmentation, h->out.ptr, vol, cudaMemcpyDeviceToHost, s));
+  PCT_CUDA(h, cudaStreamSynchronize(s));
+  return PCT_OK;
+}
+
+int pct_normalize_labels_device(pct_handle *h, float *d_label, size_t n, void *stream) {
+  if (!h) return PCT_ERR_INVALID_ARG;
+  h->last_error.clear();
+  if (!d_label && n) return fail(h, PCT_ERR_INVALID_ARG, "null device pointer");
+  int st = select_device(h);
+  if (st) return st;
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+  PCT_CUDA(h, pct::launch_normalize_labels(d_label, n, s));
+  return PCT_OK;
+}
+
+int pct_finalize_hu_device(pct_handle *h, float *d_vol, size_t n, void *stream) {
+  if (!h) return PCT_ERR_INVALID_ARG;
+  h->last_error.clear();
+  if (!d_vol && n) return fail(h, PCT_ERR_INVALID_ARG, "null device pointer");
+  int st = select_device(h);
+  if (st) return st;
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+  PCT_CUDA(h, pct::launch_finalize_hu(d_vol, n, s));
+  return PCT_OK;
+}
+
+int pct_regularize_device(pct_handle *h, float *d_vol, int nx, int ny, int nz, int nh,
+                          int64_t *fills, void *stream) {
+  if (!h) return PCT_ERR_INVALID_ARG;
+  h->last_error.clear();
+  if (!d_vol) return fail(h, PCT_ERR_INVALID_ARG, "null device pointer");
+  if (nx <= 0 || ny <= 0 || nz <= 0 || nh < 1 || (nh % 2) == 0)
+    return fail(h, PCT_ERR_INVALID_ARG, "bad volume shape or NH");
+  if ((long long)nx * ny * nz >= (1LL << 31))
+    return fail(h, PCT_ERR_INVALID_ARG, "volume has 2^31 or more voxels");
+  int st = select_device(h);
+  if (st) return st;
+  if ((st = ensure(h, h->scratch, pct::regularize_scratch_bytes((long long)nx * ny * nz)))) return st;
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+  long long f = 0;
+  int rounds = 0;
+  PCT_CUDA(h, pct::launch_regularize(d_vol, nx, ny, nz, nh, h->scratch.ptr, s, &f, &rounds));
+  if (fills) *fills = f;
+  return PCT_OK;
+}
+
+int pct_run_pipeline(pct_handle *h, const float *img, const float *atlas_mri,
+                     const float *atlas_ct_hu, float *out, int nx, int ny, int nz, int num_atlas,
+                     int nh, double sigma, double beta, int exec_choice, int regularize) {
+  if (!h) return PCT_ERR_INVALID_ARG;
+  h->last_error.clear();
+  if (!img || !atlas_mri || !atlas_ct_hu || !out)
+    return fail(h, PCT_ERR_INVALID_ARG, "null host pointer");
+  // div = 2*27*beta*sigma^2 (PatchBasedPseudoCT.cu:2154).
+  const double div = 2.0 * 27.0 * beta * (sigma * sigma);
+  int st = check_choice(h, exec_choice);
+  if (st) return st;
+  pct::Geometry g;
+  st = check_shape(h, nx, ny, nz, num_atlas, nh, div, &g);
+  if (st) return st;
+  st = select_device(h);
+  if (st) return st;
+  const size_t vol = (size_t)g.nvox() * sizeof(float);
+  const size_t vols = vol * (size_t)num_atlas;
+  if ((st = ensure(h, h->img, vol)) || (st = ensure(h, h->atlas, vols)) ||
+      (st = ensure(h, h->label, vols)) || (st = ensure(h, h->out, vol)))
+    return st;
+  if (regularize && (st = ensure(h, h->scratch, pct::regularize_scratch_bytes(g.nvox())))) return st;
+  cudaStream_t s = h->user_stream ? h->user_stream : h->stream;
+  float *d_img = static_cast<float *>(h->img.ptr), *d_atlas = static_cast<float *>(h->atlas.ptr);
+  float *d_label = static_cast<float *>(h->label.ptr), *d_out = static_cast<float *>(h->out.ptr);
+  PCT_CUDA(h, cudaMemcpyAsync(d_img, img, vol, cudaMemcpyHostToDevice, s));
+  PCT_CUDA(h, cudaMemcpyAsync(d_atlas, atlas_mri, vols, cudaMemcpyHostToDevice, s));
+  PCT_CUDA(h, cudaMemcpyAsync(d_label, atlas_ct_hu, vols, cudaMemcpyHostToDevice, s));
+  PCT_CUDA(h, pct::launch_normalize_labels(d_label, vols / sizeof(float), s));
+  PCT_CUDA(h, cudaMemsetAsync(d_out, 0, vol, s));
+  PCT_CUDA(h, pct::launch_fuse_plain(g, d_img, d_atlas, d_label, d_out, div, s));
+  if (regularize) {
+    long long f = 0;
+    int rounds = 0;
+    PCT_CUDA(h, pct::launch_regularize(d_out, nx, ny, nz, nh, h->scratch.ptr, s, &f, &rounds));
+    PCT_CUDA(h, pct::launch_finalize_hu(d_out, (size_t)g.nvox(), s));
+  }
+  PCT_CUDA(h, cudaMemcpyAsync(out, d_out, vol, cudaMemcpyDeviceToHost, s));
+  PCT_CUDA(h, cudaStreamSynchronize(s));
+  return PCT_OK;
+}
+
+int pct_error_stats_device(pct_handle *h, const float *d_a, const float *d_b, int nx, int ny,
+                           int nz, int nh, pct_error_stats *stats, void *stream) {
+  if (!h) return PCT_ERR_INVALID_ARG;
+  h->last_error.clear();
+  if (!d_a || !d_b || !stats) return fail(h, PCT_ERR_INVALID_ARG, "null pointer");
+  if (nx <= 0 || ny <= 0 || nz <= 0 || nh < 1 || (nh % 2) == 0)
+    return fail(h, PCT_ERR_INVALID_ARG, "bad volume shape or NH");
+  int st = select_device(h);
+  if (st) return st;
+  if ((st = ensure(h, h->scratch, sizeof(ErrAccum)))) return st;
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+  ErrAccum *acc = static_cast<ErrAccum *>(h->scratch.ptr);
+  PCT_CUDA(h, cudaMemsetAsync(acc, 0, sizeof(ErrAccum), s));
+  const int lo = (nh - 1) / 2 + 1;
+  memset(stats, 0, sizeof(*stats));
+  if (nx > 2 * lo && ny > 2 * lo && nz > 2 * lo) {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+    error_stats_kernel<<<sms * 4, 256, 0, s>>>(d_a, d_b, nx, ny, nz, lo, acc);
+    PCT_CUDA(h, cudaGetLastError());
+  }
+  ErrAccum host;
+  PCT_CUDA(h, cudaMemcpyAsync(&host, acc, sizeof(host), cudaMemcpyDeviceToHost, s));
+  PCT_CUDA(h, cudaStreamSynchronize(s));
+  double mabs, mrel;
+  memcpy(&mabs, &host.max_abs_bits, sizeof(double));
+  memcpy(&mrel, &host.max_rel_bits, sizeof(double));
+  stats->compared = (int64_t)host.compared;
+  stats->nan_mismatch = (int64_t)host.nan_mismatch;
+  stats->nan_both = (int64_t)host.nan_both;
+  stats->mae_hu = host.compared ? host.sum_abs / (double)host.compared : 0.0;
+  stats->max_abs_hu = mabs;
+  stats->max_rel = mrel;
+  return PCT_OK;
+}
+
+}  // extern "C"
