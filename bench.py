@@ -210,6 +210,49 @@ def run_reference_arm(args) -> None:
 
 # ---------------------------------------------------------------------------------- GPU side
 
+def measure_e2e(h, s, label, div, sptr, stream, steps, world, dev) -> dict:
+    """The drop-in host-pointer entry point (pct_synthesize) on pinned host buffers: every step
+    copies the subject in, runs the path and copies the volume out, on `stream`."""
+    import torch
+    import torch.distributed as dist
+
+    import pseudoctimaging_b200 as pct
+
+    p_img = torch.from_numpy(s.img).pin_memory()
+    p_mri = torch.from_numpy(s.atlas_mri).pin_memory()
+    p_lab = torch.from_numpy(label).pin_memory()
+    p_out = torch.empty_like(p_img).pin_memory()
+    nz, nx, ny = s.img.shape
+    h.set_stream(sptr)
+
+    def e2e_step():
+        st = pct.lib.pct_synthesize(h.ptr, p_img.data_ptr(), p_mri.data_ptr(), p_lab.data_ptr(),
+                                    p_out.data_ptr(), nx, ny, nz, NUM, NH, div, pct.EXEC_B200_FP32)
+        if st != 0:
+            raise pct.PctError(st, "pct_synthesize")
+
+    e2e_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    h.set_stream(None)
+    nvox = nx * ny * nz
+    return {"value": world * nvox / (ms / 1e3), "unit": UNIT, "ms_per_step": ms,
+            "steps": steps, "h2d_bytes_per_step": int(4 * nvox * (1 + 2 * NUM)),
+            "d2h_bytes_per_step": int(4 * nvox), "out": p_out}
+
+
 def run_b200_arm(args) -> None:
     import torch
     import torch.distributed as dist
@@ -223,8 +266,7 @@ def run_b200_arm(args) -> None:
     dev = torch.device("cuda", local)
     if world > 1:
         import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=dev)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
 
     def barrier():
         if world > 1:
@@ -238,7 +280,8 @@ def run_b200_arm(args) -> None:
     d_lab = torch.from_numpy(label).to(dev)
     d_out = torch.zeros_like(d_img)
     h = pct.Handle(local)
-    stream = torch.cuda.current_stream(dev)
+    stream = torch.cuda.Stream(dev)  # a real stream handle, so events and kernels share it
+    torch.cuda.set_stream(stream)
     sptr = stream.cuda_stream
 
     def step():
@@ -264,36 +307,15 @@ def run_b200_arm(args) -> None:
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms = float(t.item())
-    value = world * NX * NY * NZ / (ms / 1e3)
+    nvox = NX * NY * NZ
+    value = world * nvox / (ms / 1e3)
 
-    # End to end through the drop-in host-pointer entry point, pinned host buffers.
-    p_img = torch.from_numpy(s.img).pin_memory()
-    p_mri = torch.from_numpy(s.atlas_mri).pin_memory()
-    p_lab = torch.from_numpy(label).pin_memory()
-    p_out = torch.empty_like(p_img).pin_memory()
-    h.set_stream(sptr)
-
-    def e2e_step():
-        pct.lib.pct_synthesize(h.ptr, p_img.data_ptr(), p_mri.data_ptr(), p_lab.data_ptr(),
-                               p_out.data_ptr(), NX, NY, NZ, NUM, NH, div, pct.EXEC_B200_FP32)
-
-    e2e_steps = max(1, min(args.steps, 5))
-    e2e_step()
-    torch.cuda.synchronize()
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(e2e_steps):
-        e2e_step()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1) / e2e_steps
-    te = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_ms = float(te.item())
-    assert np.array_equal(np.isnan(p_out.numpy()), np.isnan(d_out.cpu().numpy()))
-    h.set_stream(None)
+    e2e = None
+    if not args.no_e2e:
+        e2e = measure_e2e(h, s, label, div, sptr, stream, max(1, min(args.steps, 5)), world, dev)
+        out = e2e.pop("out")
+        assert np.array_equal(np.isnan(out.numpy()), np.isnan(d_out.cpu().numpy())), \
+            "host-pointer and device-pointer runs disagree"
 
     clocks = clk.summary()
     peaks = measured_peaks()
@@ -303,7 +325,7 @@ def run_b200_arm(args) -> None:
     fp32_peak = sms * FP32_LANES_PER_SM * mhz * 1e6  # lane-ops/s at the sampled clock
     mufu_peak = sms * MUFU_LANES_PER_SM * mhz * 1e6
     achieved = cand * OPS_PER_CANDIDATE / (ms / 1e3)
-    traffic = profiled_traffic()
+    traffic = profiled_traffic() if NZ == 112 else None
     hbm_achieved = (traffic / (ms / 1e3) / 1e9) if traffic else None
 
     line = {
@@ -311,10 +333,11 @@ def run_b200_arm(args) -> None:
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded blobs/displacement generator, config 1; one subject per GPU)",
-        "config": {"workload": "222x222x112 subject, 10 atlases, NH=11, sigma 2.5, beta 1, "
+        "config": {"workload": f"{NX}x{NY}x{NZ} subject, 10 atlases, NH=11, sigma 2.5, beta 1, "
                                "plain FP32 kernel (EXEC_CHOICE 3)",
                    "nh": NH, "atlases": NUM, "volume": [NX, NY, NZ],
-                   "l2": "inputs larger than L2 (21 volumes, 464 MB per subject)",
+                   "l2": f"inputs larger than L2 ({1 + 2 * NUM} volumes, "
+                         f"{4 * nvox * (1 + 2 * NUM) / 1e6:.0f} MB per subject)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "candidates_per_s": world * cand / (ms / 1e3),
         "gpu_launches": args.steps * 1,
@@ -329,10 +352,7 @@ def run_b200_arm(args) -> None:
             "hbm": {"achieved_gbs": hbm_achieved, "peak_gbs": peaks.get("hbm_gbs"),
                     "frac": (hbm_achieved / peaks["hbm_gbs"]) if hbm_achieved else None},
         },
-        "e2e": {"value": world * NX * NY * NZ / (e2e_ms / 1e3), "unit": UNIT,
-                "ms_per_step": e2e_ms,
-                "h2d_bytes_per_step": int(4 * NX * NY * NZ * (1 + 2 * NUM)),
-                "d2h_bytes_per_step": int(4 * NX * NY * NZ)},
+        "e2e": e2e,
         "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
     }
     h.close()
@@ -340,7 +360,7 @@ def run_b200_arm(args) -> None:
         dist.destroy_process_group()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_reference_rate(args.cpu_seconds)
-        cpu_value = NX * NY * NZ / (cand / r["cand_per_s"])
+        cpu_value = nvox / (cand / r["cand_per_s"])
         line["cpu_baseline"] = {"value": cpu_value, "unit": UNIT, "cores": r["cores"],
                                 "kind": "reference", "sample": r["sample"],
                                 "seconds": r["seconds"], "cand_per_s": r["cand_per_s"]}
@@ -349,17 +369,22 @@ def run_b200_arm(args) -> None:
 
 
 def main() -> None:
+    global NZ
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-pointer end-to-end leg")
+    ap.add_argument("--nz", type=int, default=NZ,
+                    help="z extent of the subject (default 112; smaller only for profiling runs)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
                     help="CPU-baseline sample length (rank 0, N=1 only)")
     ap.add_argument("--ref-step-seconds", type=float, default=4.0,
                     help="length of each reference-arm step")
     args = ap.parse_args()
+    NZ = args.nz
     if args.impl == "reference":
         run_reference_arm(args)
     else:

@@ -11,6 +11,8 @@
  *
  * Threading: a pct_handle is used by one host thread at a time. Different handles are
  * independent (no globals, unlike the reference's nx/ny/nz/num/nh).
+ *
+ * Streams: every `void *stream` argument is a cudaStream_t; NULL means the CUDA default stream.
  */
 #ifndef PCT_B200_H
 #define PCT_B200_H
@@ -89,8 +91,8 @@ int pct_synthesize(pct_handle *h, const float *img, const float *atlas, const fl
 
 /*
  * Same computation on DEVICE buffers already resident on the handle's device, enqueued on
- * `stream` (a cudaStream_t; NULL = the handle's own stream). Only interior voxels of d_out are
- * written; border voxels keep whatever the caller put there. Asynchronous: errors from the
+ * `stream` (a cudaStream_t; NULL = the CUDA default stream, as everywhere in this header). Only
+ * interior voxels of d_out are written; border voxels keep whatever the caller put there. Asynchronous: errors from the
  * launch are returned, errors during execution surface at the next synchronising call.
  */
 int pct_synthesize_device(pct_handle *h, const float *d_img, const float *d_atlas,

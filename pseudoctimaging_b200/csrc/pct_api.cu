@@ -269,7 +269,7 @@ int pct_synthesize_device(pct_handle *h, const float *d_img, const float *d_atla
   if (st) return st;
   st = select_device(h);
   if (st) return st;
-  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
   PCT_CUDA(h, pct::launch_fuse_plain(g, d_img, d_atlas, d_atlas_label, d_out, div, s));
   return PCT_OK;
 }
@@ -313,7 +313,7 @@ int pct_normalize_labels_device(pct_handle *h, float *d_label, size_t n, void *s
   if (!d_label && n) return fail(h, PCT_ERR_INVALID_ARG, "null device pointer");
   int st = select_device(h);
   if (st) return st;
-  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
   PCT_CUDA(h, pct::launch_normalize_labels(d_label, n, s));
   return PCT_OK;
 }
@@ -324,7 +324,7 @@ int pct_finalize_hu_device(pct_handle *h, float *d_vol, size_t n, void *stream) 
   if (!d_vol && n) return fail(h, PCT_ERR_INVALID_ARG, "null device pointer");
   int st = select_device(h);
   if (st) return st;
-  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
   PCT_CUDA(h, pct::launch_finalize_hu(d_vol, n, s));
   return PCT_OK;
 }
@@ -341,7 +341,7 @@ int pct_regularize_device(pct_handle *h, float *d_vol, int nx, int ny, int nz, i
   int st = select_device(h);
   if (st) return st;
   if ((st = ensure(h, h->scratch, pct::regularize_scratch_bytes((long long)nx * ny * nz)))) return st;
-  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
   long long f = 0;
   int rounds = 0;
   PCT_CUDA(h, pct::launch_regularize(d_vol, nx, ny, nz, nh, h->scratch.ptr, s, &f, &rounds));
@@ -401,7 +401,7 @@ int pct_error_stats_device(pct_handle *h, const float *d_a, const float *d_b, in
   int st = select_device(h);
   if (st) return st;
   if ((st = ensure(h, h->scratch, sizeof(ErrAccum)))) return st;
-  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
   ErrAccum *acc = static_cast<ErrAccum *>(h->scratch.ptr);
   PCT_CUDA(h, cudaMemsetAsync(acc, 0, sizeof(ErrAccum), s));
   const int lo = (nh - 1) / 2 + 1;

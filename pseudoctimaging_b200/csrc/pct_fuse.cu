@@ -42,6 +42,14 @@ __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a
 __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 
+// Output rule of NewPatchedBrainPureC.cpp:1325-1331 in FP32: product/sum_weight when both
+// exceed DBL_EPSILON in magnitude, else NaN (the C NAN bit pattern).
+__device__ __forceinline__ float fuse_result(float product, float sum_weight) {
+  return (fabsf(product) > kDblEpsilonF && fabsf(sum_weight) > kDblEpsilonF)
+             ? __fdiv_rn(product, sum_weight)
+             : __int_as_float(0x7fc00000);
+}
+
 struct FuseParams {
   const float *img;
   const float *atlas;
@@ -68,19 +76,27 @@ __global__ void __launch_bounds__(128) fuse_plain_kernel(const FuseParams p) {
   const int tz = t / p.tiles_x;
 
   const int lo = HW + 1;
-  const int y0 = lo + ty * kOutY, x0 = lo + tx * RX, z0 = lo + tz * (2 * TZ);
+  const int y0 = lo + ty * kOutY, x0 = lo + tx * RX;
   const int y = y0 - 1 + lane;
-  // Clamp every coordinate the tile touches to [HW, n-1-HW] so that +-HW stays in the volume.
-  // Clamped lanes/rows/planes only feed outputs beyond the interior, which are never stored.
+  // y and x are never slid across offsets, so lanes and rows past the interior are simply
+  // clamped to [HW, n-1-HW] (keeping +-HW inside the volume); they only feed outputs that are
+  // never stored. z IS slid (dw ring buffer), which needs consecutive planes: a half that would
+  // run past the interior is shifted back inside it instead, and then stores only the planes it
+  // owns (those at or after its unshifted start), so every voxel is written exactly once.
+  // The launcher guarantees at least TZ interior planes, so a shifted half starts at >= lo.
   const int yc = min(y, p.ny - 1 - HW);
   int rowoff[NR];
 #pragma unroll
   for (int r = 0; r < NR; ++r) rowoff[r] = min(x0 - 1 + r, p.nx - 1 - HW) * p.ny + yc;
+  int zs[2], zown[2];
   int planeoff[2][NQ];
 #pragma unroll
-  for (int h = 0; h < 2; ++h)
+  for (int h = 0; h < 2; ++h) {
+    zown[h] = lo + tz * (2 * TZ) + h * TZ;
+    zs[h] = min(zown[h], p.nz - lo - TZ);
 #pragma unroll
-    for (int q = 0; q < NQ; ++q) planeoff[h][q] = min(z0 + h * TZ - 1 + q, p.nz - 1 - HW) * p.nxy;
+    for (int q = 0; q < NQ; ++q) planeoff[h][q] = (zs[h] - 1 + q) * p.nxy;
+  }
 
   // Input patch values, negated so that D = (A + In)^2, paired over the two z-halves.
   float2 In[NQ][NR];
@@ -207,20 +223,62 @@ __global__ void __launch_bounds__(128) fuse_plain_kernel(const FuseParams p) {
     for (int h = 0; h < 2; ++h)
 #pragma unroll
       for (int q = 0; q < TZ; ++q) {
-        const int z = z0 + h * TZ + q;
-        if (z >= p.nz - lo) continue;
+        const int z = zs[h] + q;
+        if (z < zown[h] || z >= p.nz - lo) continue;
 #pragma unroll
         for (int r = 0; r < RX; ++r) {
           const int x = x0 + r;
           if (x >= p.nx - lo) continue;
           const float pr = h ? P[q][r].y : P[q][r].x;
           const float sw = h ? W[q][r].y : W[q][r].x;
-          const float v = (fabsf(pr) > kDblEpsilonF && fabsf(sw) > kDblEpsilonF)
-                              ? __fdiv_rn(pr, sw)
-                              : __int_as_float(0x7fc00000);
-          p.out[(long long)z * p.nxy + (long long)x * p.ny + y] = v;
+          p.out[(long long)z * p.nxy + (long long)x * p.ny + y] = fuse_result(pr, sw);
         }
       }
+  }
+}
+
+// Direct form for volumes with fewer interior z-planes than one tile half: one thread per
+// interior voxel, every candidate's 27-tap SSD summed directly in FP32. Same arithmetic
+// contract as the tiled kernel, no sliding windows, no tile constraints.
+template <int HW>
+__global__ void __launch_bounds__(128) fuse_direct_kernel(const FuseParams p) {
+  const int lo = HW + 1;
+  const int ix = p.nx - 2 * lo, iy = p.ny - 2 * lo, iz = p.nz - 2 * lo;
+  const long long total = (long long)ix * iy * iz;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int y = (int)(i % iy) + lo;
+    const long long rest = i / iy;
+    const int x = (int)(rest % ix) + lo;
+    const int z = (int)(rest / ix) + lo;
+    const int c = z * p.nxy + x * p.ny + y;
+    float in[27];
+    int k = 0;
+    for (int a = -1; a <= 1; ++a)
+      for (int b = -1; b <= 1; ++b)
+        for (int e = -1; e <= 1; ++e) in[k++] = __ldg(p.img + c + a * p.nxy + b * p.ny + e);
+    float pr = 0.f, sw = 0.f;
+    for (int at = 0; at < p.num; ++at) {
+      const float *A = p.atlas + (long long)at * p.nvox;
+      const float *L = p.label + (long long)at * p.nvox;
+      for (int dw = -HW; dw <= HW; ++dw)
+        for (int du = -HW; du <= HW; ++du)
+          for (int dv = -HW; dv <= HW; ++dv) {
+            const int cc = c + dw * p.nxy + du * p.ny + dv;
+            float ssd = 0.f;
+            k = 0;
+            for (int a = -1; a <= 1; ++a)
+              for (int b = -1; b <= 1; ++b)
+                for (int e = -1; e <= 1; ++e) {
+                  const float d = in[k++] - __ldg(A + cc + a * p.nxy + b * p.ny + e);
+                  ssd = fmaf(d, d, ssd);
+                }
+            const float w = ex2_approx(ssd * p.neg_k);
+            pr = fmaf(w, __ldg(L + cc), pr);
+            sw += w;
+          }
+    }
+    p.out[c] = fuse_result(pr, sw);
   }
 }
 
@@ -235,6 +293,16 @@ template <int HW>
 cudaError_t launch_hw(const Geometry &g, const FuseParams &base, cudaStream_t stream) {
   constexpr int RX = TileShape<HW>::RX, TZ = TileShape<HW>::TZ;
   FuseParams p = base;
+  if (g.iz < TZ) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long long total = (long long)g.ix * g.iy * g.iz;
+    const long long want = (total + kThreads - 1) / kThreads;
+    const unsigned blocks = (unsigned)(want < (long long)sms * 16 ? want : (long long)sms * 16);
+    fuse_direct_kernel<HW><<<blocks, kThreads, 0, stream>>>(p);
+    return cudaGetLastError();
+  }
   p.tiles_y = (g.iy + kOutY - 1) / kOutY;
   p.tiles_x = (g.ix + RX - 1) / RX;
   p.tiles_z = (g.iz + 2 * TZ - 1) / (2 * TZ);
