@@ -53,7 +53,13 @@ def interior(n: int, nh: int) -> int:
     return max(0, n - 2 * ((nh - 1) // 2 + 1))
 
 
-def candidates(nx=NX, ny=NY, nz=NZ, num=NUM, nh=NH) -> int:
+def candidates(nx=None, ny=None, nz=None, num=None, nh=None) -> int:
+    """Candidates (voxel, atlas, offset) of one pass; defaults are the current workload."""
+    nx = NX if nx is None else nx
+    ny = NY if ny is None else ny
+    nz = NZ if nz is None else nz
+    num = NUM if num is None else num
+    nh = NH if nh is None else nh
     return interior(nx, nh) * interior(ny, nh) * interior(nz, nh) * num * nh ** 3
 
 
@@ -325,7 +331,7 @@ def run_b200_arm(args) -> None:
     fp32_peak = sms * FP32_LANES_PER_SM * mhz * 1e6  # lane-ops/s at the sampled clock
     mufu_peak = sms * MUFU_LANES_PER_SM * mhz * 1e6
     achieved = cand * OPS_PER_CANDIDATE / (ms / 1e3)
-    traffic = profiled_traffic() if NZ == 112 else None
+    traffic = profiled_traffic() if (NZ == 112 and NH == 11) else None
     hbm_achieved = (traffic / (ms / 1e3) / 1e9) if traffic else None
 
     line = {
@@ -333,7 +339,7 @@ def run_b200_arm(args) -> None:
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded blobs/displacement generator, config 1; one subject per GPU)",
-        "config": {"workload": f"{NX}x{NY}x{NZ} subject, 10 atlases, NH=11, sigma 2.5, beta 1, "
+        "config": {"workload": f"{NX}x{NY}x{NZ} subject, 10 atlases, NH={NH}, sigma 2.5, beta 1, "
                                "plain FP32 kernel (EXEC_CHOICE 3)",
                    "nh": NH, "atlases": NUM, "volume": [NX, NY, NZ],
                    "l2": f"inputs larger than L2 ({1 + 2 * NUM} volumes, "
@@ -369,7 +375,7 @@ def run_b200_arm(args) -> None:
 
 
 def main() -> None:
-    global NZ
+    global NZ, NH, METRIC
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
@@ -377,6 +383,8 @@ def main() -> None:
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-pointer end-to-end leg")
+    ap.add_argument("--nh", type=int, default=NH, choices=[3, 5, 7, 9, 11],
+                    help="search window (default 11, the metric's; 7 and 9 are config-1 sweeps)")
     ap.add_argument("--nz", type=int, default=NZ,
                     help="z extent of the subject (default 112; smaller only for profiling runs)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
@@ -385,6 +393,8 @@ def main() -> None:
                     help="length of each reference-arm step")
     args = ap.parse_args()
     NZ = args.nz
+    NH = args.nh
+    METRIC = f"pseudo-CT voxels/s at {NX}x{NY}x{NZ}, 10 atlases, NH={NH}"
     if args.impl == "reference":
         run_reference_arm(args)
     else:

@@ -99,6 +99,14 @@ int pct_synthesize_device(pct_handle *h, const float *d_img, const float *d_atla
                           const float *d_atlas_label, float *d_out, int nx, int ny, int nz,
                           int num_atlas, int nh, double div, int exec_choice, void *stream);
 
+/*
+ * Waits for `stream` to drain, then reports (and clears) the status of this handle's
+ * asynchronous kernels: PCT_OK, or PCT_ERR_TIMEOUT if a bounded device-side wait gave up (the
+ * kernel then stopped early and its output is incomplete). pct_synthesize and pct_run_pipeline
+ * check this themselves.
+ */
+int pct_device_status(pct_handle *h, void *stream);
+
 /* In-place CT -> label scale L' = 255*((L+1024)/4095) on a device buffer of n floats
  * (PatchBasedPseudoCT.cu:2009-2020, NewPatchedBrainPureC.cpp:1583-1593). */
 int pct_normalize_labels_device(pct_handle *h, float *d_label, size_t n, void *stream);

@@ -82,6 +82,7 @@ SIGNATURES = {
     "pct_set_stream": (_I, [_P, _P]),
     "pct_synthesize": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _D, _I]),
     "pct_synthesize_device": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _D, _I, _P]),
+    "pct_device_status": (_I, [_P, _P]),
     "pct_normalize_labels_device": (_I, [_P, _P, _SZ, _P]),
     "pct_regularize_device": (_I, [_P, _P, _I, _I, _I, _I, ctypes.POINTER(ctypes.c_int64), _P]),
     "pct_finalize_hu_device": (_I, [_P, _P, _SZ, _P]),
@@ -97,7 +98,7 @@ def load_library(path: os.PathLike | str | None = None) -> ctypes.CDLL:
     p = pathlib.Path(path) if path else LIB_PATH
     if not p.exists():
         raise ImportError(
-            f"{p} is missing: build it with `python -m pseudoctimaging_b200.build` "
+            f"{p} is missing: build it with `python pseudoctimaging_b200/build.py` "
             "(the CUDA library is required; there is no CPU fallback)")
     lib = ctypes.CDLL(str(p))
     for name, (res, args) in SIGNATURES.items():
@@ -206,6 +207,10 @@ class Handle:
         self._check(lib.pct_synthesize_device(self._h, d_img, d_atlas, d_label, d_out, nx, ny, nz,
                                               num, nh, float(div), exec_choice, stream or None),
                     "pct_synthesize_device")
+
+    def device_status(self, stream: int = 0) -> None:
+        """Drains `stream` and raises PctError if a kernel's bounded wait gave up."""
+        self._check(lib.pct_device_status(self._h, stream or None), "pct_device_status")
 
     def normalize_labels_device(self, d_label: int, n: int, stream: int = 0) -> None:
         self._check(lib.pct_normalize_labels_device(self._h, d_label, n, stream or None),

@@ -1,6 +1,8 @@
 """Builds libpct_b200.so and the drop-in CLI in-tree for sm_100a with nvcc.
 
-    python -m pseudoctimaging_b200.build [--force] [--verbose]
+    python pseudoctimaging_b200/build.py [--force] [--verbose] [--ptxas-info]
+
+(run it as a script: importing the package loads the library this builds)
 
 Objects go to pseudoctimaging_b200/_build/, the library to pseudoctimaging_b200/lib/ and the CLI
 to pseudoctimaging_b200/bin/. Built files are git-ignored but stay inside the repository so they
@@ -29,7 +31,7 @@ HOST_CXX = shutil.which("g++", path="/usr/bin") or "g++"
 COMMON = ["-O3", "-std=c++17", "-lineinfo", f"-ccbin={HOST_CXX}", "-Xcompiler", "-fPIC",
           f"-I{INCLUDE}", f"-I{CSRC}"]
 # Sources that make up the shared library; the CLI main is linked separately against it.
-LIB_SOURCES = ["pct_api.cu", "pct_fuse.cu", "pct_pointwise.cu", "pct_regularize.cu",
+LIB_SOURCES = ["pct_api.cu", "pct_fuse_tma.cu", "pct_pointwise.cu", "pct_regularize.cu",
                "pct_synth.cpp"]
 CLI_SOURCES = ["pct_cli.cpp"]
 

@@ -1,6 +1,7 @@
 // C ABI of libpct_b200.so (declared in include/pct_b200.h).
 #include <cuda_runtime.h>
 #include <math.h>
+#include <stdint.h>
 #include <stdio.h>
 #include <string.h>
 
@@ -26,6 +27,9 @@ struct pct_handle {
   size_t mem_limit = 0;  // 0 = unlimited
   size_t allocated = 0;
   DevBuf img, atlas, label, out, scratch;
+  DevBuf err;      // device status word written by kernels with bounded waits
+  DevBuf partial;  // per-atlas-group partial sums of the fusion kernel
+  DevBuf stage;    // contiguous host->device staging before the pitched repack
   std::string last_error;
 };
 
@@ -111,6 +115,54 @@ int check_shape(pct_handle *h, int nx, int ny, int nz, int num, int nh, double d
 
 int select_device(pct_handle *h) {
   PCT_CUDA(h, cudaSetDevice(h->device));
+  return PCT_OK;
+}
+
+// Zeroes the device status word and enqueues the TMA-staged fusion kernel.
+int launch_fusion(pct_handle *h, const pct::Geometry &g, const pct::SlabInputs &in, float *d_out,
+                  double div, cudaStream_t s) {
+  int st = ensure(h, h->err, 16);
+  if (st) return st;
+  int *err = static_cast<int *>(h->err.ptr);
+  const size_t pbytes = pct::fuse_tma_partial_bytes(g);
+  if (pbytes && (st = ensure(h, h->partial, pbytes))) return st;
+  PCT_CUDA(h, cudaMemsetAsync(err, 0, sizeof(int), s));
+  PCT_CUDA(h, pct::launch_fuse_tma(g, in, d_out, div, static_cast<float *>(h->partial.ptr), err, s));
+  return PCT_OK;
+}
+
+// Reads (and clears) the device status word after `s` has drained.
+int read_device_status(pct_handle *h, cudaStream_t s) {
+  if (!h->err.ptr) return PCT_OK;
+  int v = 0;
+  PCT_CUDA(h, cudaMemcpyAsync(&v, h->err.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
+  PCT_CUDA(h, cudaStreamSynchronize(s));
+  if (v != 0) {
+    PCT_CUDA(h, cudaMemsetAsync(h->err.ptr, 0, sizeof(int), s));
+    PCT_CUDA(h, cudaStreamSynchronize(s));
+    return fail(h, PCT_ERR_TIMEOUT, "a bounded device-side wait gave up (code " + std::to_string(v) + ")");
+  }
+  return PCT_OK;
+}
+
+// Copies host atlas volumes [num*nz*nx][ny] into a pitched device stack for TMA: one
+// contiguous host->device copy (full PCIe/C2C rate) into a staging buffer, then an on-device
+// repack. When ny is already a multiple of 4 the copy lands in place.
+int stage_pitched_h2d(pct_handle *h, DevBuf &buf, const float *src, const pct::Geometry &g,
+                      cudaStream_t s) {
+  const int pitch = pct::slab_pitch(g.ny);
+  const size_t rows = (size_t)g.num * g.nz * g.nx;
+  int st = ensure(h, buf, rows * pitch * sizeof(float));
+  if (st) return st;
+  const size_t bytes = rows * g.ny * sizeof(float);
+  if (pitch == g.ny) {
+    PCT_CUDA(h, cudaMemcpyAsync(buf.ptr, src, bytes, cudaMemcpyHostToDevice, s));
+    return PCT_OK;
+  }
+  if ((st = ensure(h, h->stage, bytes))) return st;
+  PCT_CUDA(h, cudaMemcpyAsync(h->stage.ptr, src, bytes, cudaMemcpyHostToDevice, s));
+  PCT_CUDA(h, pct::launch_pitch_copy(static_cast<const float *>(h->stage.ptr),
+                                     static_cast<float *>(buf.ptr), (long long)rows, g.ny, pitch, s));
   return PCT_OK;
 }
 
@@ -236,7 +288,8 @@ int pct_destroy(pct_handle *h) {
   if (!h) return PCT_ERR_INVALID_ARG;
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
-  for (DevBuf *b : {&h->img, &h->atlas, &h->label, &h->out, &h->scratch})
+  for (DevBuf *b : {&h->img, &h->atlas, &h->label, &h->out, &h->scratch, &h->err, &h->partial,
+                    &h->stage})
     if (b->ptr) cudaFree(b->ptr);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -270,8 +323,22 @@ int pct_synthesize_device(pct_handle *h, const float *d_img, const float *d_atla
   st = select_device(h);
   if (st) return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  PCT_CUDA(h, pct::launch_fuse_plain(g, d_img, d_atlas, d_atlas_label, d_out, div, s));
-  return PCT_OK;
+  pct::SlabInputs in{d_img, d_atlas, d_atlas_label, g.ny};
+  const bool aligned = (g.ny % 4 == 0) && (reinterpret_cast<uintptr_t>(d_atlas) % 16 == 0) &&
+                       (reinterpret_cast<uintptr_t>(d_atlas_label) % 16 == 0);
+  if (!aligned) {  // TMA needs 16-byte row strides: stage a pitched copy on the handle
+    const int pitch = pct::slab_pitch(g.ny);
+    const long long rows = (long long)g.num * g.nz * g.nx;
+    const size_t bytes = (size_t)rows * pitch * sizeof(float);
+    if ((st = ensure(h, h->atlas, bytes)) || (st = ensure(h, h->label, bytes))) return st;
+    PCT_CUDA(h, pct::launch_pitch_copy(d_atlas, static_cast<float *>(h->atlas.ptr), rows, g.ny,
+                                       pitch, s));
+    PCT_CUDA(h, pct::launch_pitch_copy(d_atlas_label, static_cast<float *>(h->label.ptr), rows,
+                                       g.ny, pitch, s));
+    in = pct::SlabInputs{d_img, static_cast<const float *>(h->atlas.ptr),
+                         static_cast<const float *>(h->label.ptr), pitch};
+  }
+  return launch_fusion(h, g, in, d_out, div, s);
 }
 
 int pct_synthesize(pct_handle *h, const float *img, const float *atlas, const float *atlas_label,
@@ -289,22 +356,27 @@ int pct_synthesize(pct_handle *h, const float *img, const float *atlas, const fl
   st = select_device(h);
   if (st) return st;
   const size_t vol = (size_t)g.nvox() * sizeof(float);
-  const size_t vols = vol * (size_t)num_atlas;
-  if ((st = ensure(h, h->img, vol)) || (st = ensure(h, h->atlas, vols)) ||
-      (st = ensure(h, h->label, vols)) || (st = ensure(h, h->out, vol)))
-    return st;
+  if ((st = ensure(h, h->img, vol)) || (st = ensure(h, h->out, vol))) return st;
   cudaStream_t s = h->user_stream ? h->user_stream : h->stream;
   PCT_CUDA(h, cudaMemcpyAsync(h->img.ptr, img, vol, cudaMemcpyHostToDevice, s));
-  PCT_CUDA(h, cudaMemcpyAsync(h->atlas.ptr, atlas, vols, cudaMemcpyHostToDevice, s));
-  PCT_CUDA(h, cudaMemcpyAsync(h->label.ptr, atlas_label, vols, cudaMemcpyHostToDevice, s));
+  if ((st = stage_pitched_h2d(h, h->atlas, atlas, g, s)) ||
+      (st = stage_pitched_h2d(h, h->label, atlas_label, g, s)))
+    return st;
   PCT_CUDA(h, cudaMemsetAsync(h->out.ptr, 0, vol, s));
-  PCT_CUDA(h, pct::launch_fuse_plain(g, static_cast<const float *>(h->img.ptr),
-                                     static_cast<const float *>(h->atlas.ptr),
-                                     static_cast<const float *>(h->label.ptr),
-                                     static_cast<float *>(h->out.ptr), div, s));
+  pct::SlabInputs in{static_cast<const float *>(h->img.ptr), static_cast<const float *>(h->atlas.ptr),
+                     static_cast<const float *>(h->label.ptr), pct::slab_pitch(g.ny)};
+  if ((st = launch_fusion(h, g, in, static_cast<float *>(h->out.ptr), div, s))) return st;
   PCT_CUDA(h, cudaMemcpyAsync(label_segmentation, h->out.ptr, vol, cudaMemcpyDeviceToHost, s));
   PCT_CUDA(h, cudaStreamSynchronize(s));
-  return PCT_OK;
+  return read_device_status(h, s);
+}
+
+int pct_device_status(pct_handle *h, void *stream) {
+  if (!h) return PCT_ERR_INVALID_ARG;
+  h->last_error.clear();
+  int st = select_device(h);
+  if (st) return st;
+  return read_device_status(h, static_cast<cudaStream_t>(stream));
 }
 
 int pct_normalize_labels_device(pct_handle *h, float *d_label, size_t n, void *stream) {
@@ -366,20 +438,23 @@ int pct_run_pipeline(pct_handle *h, const float *img, const float *atlas_mri,
   st = select_device(h);
   if (st) return st;
   const size_t vol = (size_t)g.nvox() * sizeof(float);
-  const size_t vols = vol * (size_t)num_atlas;
-  if ((st = ensure(h, h->img, vol)) || (st = ensure(h, h->atlas, vols)) ||
-      (st = ensure(h, h->label, vols)) || (st = ensure(h, h->out, vol)))
-    return st;
+  if ((st = ensure(h, h->img, vol)) || (st = ensure(h, h->out, vol))) return st;
   if (regularize && (st = ensure(h, h->scratch, pct::regularize_scratch_bytes(g.nvox())))) return st;
   cudaStream_t s = h->user_stream ? h->user_stream : h->stream;
-  float *d_img = static_cast<float *>(h->img.ptr), *d_atlas = static_cast<float *>(h->atlas.ptr);
-  float *d_label = static_cast<float *>(h->label.ptr), *d_out = static_cast<float *>(h->out.ptr);
+  float *d_img = static_cast<float *>(h->img.ptr), *d_out = static_cast<float *>(h->out.ptr);
   PCT_CUDA(h, cudaMemcpyAsync(d_img, img, vol, cudaMemcpyHostToDevice, s));
-  PCT_CUDA(h, cudaMemcpyAsync(d_atlas, atlas_mri, vols, cudaMemcpyHostToDevice, s));
-  PCT_CUDA(h, cudaMemcpyAsync(d_label, atlas_ct_hu, vols, cudaMemcpyHostToDevice, s));
-  PCT_CUDA(h, pct::launch_normalize_labels(d_label, vols / sizeof(float), s));
+  if ((st = stage_pitched_h2d(h, h->atlas, atlas_mri, g, s)) ||
+      (st = stage_pitched_h2d(h, h->label, atlas_ct_hu, g, s)))
+    return st;
+  const int pitch = pct::slab_pitch(g.ny);
+  // Label normalisation over the whole pitched stack (padding columns are never read).
+  PCT_CUDA(h, pct::launch_normalize_labels(static_cast<float *>(h->label.ptr),
+                                           (size_t)g.num * g.nz * g.nx * pitch, s));
   PCT_CUDA(h, cudaMemsetAsync(d_out, 0, vol, s));
-  PCT_CUDA(h, pct::launch_fuse_plain(g, d_img, d_atlas, d_label, d_out, div, s));
+  pct::SlabInputs in{d_img, static_cast<const float *>(h->atlas.ptr),
+                     static_cast<const float *>(h->label.ptr), pitch};
+  if ((st = launch_fusion(h, g, in, d_out, div, s))) return st;
+  if ((st = read_device_status(h, s))) return st;
   if (regularize) {
     long long f = 0;
     int rounds = 0;

@@ -1,0 +1,641 @@
+// Plain FP32 patch-based multi-atlas fusion for sm_100a, atlas slabs staged by TMA.
+//
+// Same arithmetic contract as the reference (MultiAtlasPatchBasedSegmentationOpenMP +
+// PatchSimilarity, NewPatchedBrainPureC.cpp:1184-1212,1350-1449), in FP32:
+//     SSD(x,d) = sum_{p in 3x3x3} (I(x+p) - A_a(x+d+p))^2,   w = exp(-SSD/div)
+//     out(x)   = sum_{a,d} w*L_a(x+d) / sum_{a,d} w            (NaN rule of :1325-1331)
+//
+// Work decomposition
+//  * A warp owns 30 (y) x RX (x) x 2*TZ (z) output voxels. Lanes run along the contiguous y
+//    axis (lanes 1..30 own outputs, lanes 0/31 carry the y-halo). For one offset d the SSD of
+//    all voxels is a 3x3x3 box sum of D_d = (I - A_d)^2: each lane box-sums its RX+2 rows x
+//    TZ+2 planes in registers along x and z, and the y-box is two warp shuffles.
+//  * The thread's two z-halves are packed into float2 and run on the paired FP32 instructions
+//    (add/mul/fma .f32x2): same lane throughput as scalar FP32, half the issue slots.
+//  * dw is the innermost offset loop: stepping dw shifts the atlas planes by one, so the atlas
+//    window (TZ+2 planes x RX+2 rows per half) lives in registers as a ring and each step reads
+//    one new plane. The step loop is unrolled one ring period at a time (not the whole window)
+//    to keep the kernel inside the instruction cache.
+//  * A CTA is 4 warps stacked along x. Its atlas MRI and atlas CT rows (one x-row = a z x y
+//    slab) sit in two shared-memory rings indexed by x. Each du step needs one new row of each;
+//    one thread issues it with cp.async.bulk.tensor (TMA, no multicast) one step ahead, and the
+//    step's readers wait on an mbarrier (transaction-count completion, ping-pong pair). Every
+//    per-thread shared-memory read is one LDS with an immediate offset.
+//  * TMA zero-fills coordinates outside the volume, so tiles need no clamping: out-of-volume
+//    rows/planes/lanes only ever feed voxels outside the interior, which are never stored.
+//  * CTAs are persistent over the tile list.
+//  * Every mbarrier wait is bounded (globaltimer); on timeout the CTA records an error code,
+//    stops at the next CTA barrier, drains its own in-flight copies (bounded) and returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cmath>
+
+#include "pct_internal.h"
+
+namespace pct {
+namespace {
+
+constexpr int kOutY = 30;
+constexpr int kWarps = 4;
+constexpr int kThreads = kWarps * 32;
+constexpr float kDblEpsilonF = 2.220446049250313080847e-16f;
+
+// ---------------------------------------------------------------- PTX wrappers (sm_90+/sm_100)
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbarrier_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Orders this thread's earlier generic-proxy shared-memory accesses before later async-proxy
+// (TMA) accesses.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Waits for phase `parity` of the barrier, giving up after timeout_ns. Never spins unbounded.
+__device__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, uint64_t timeout_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (;;) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (global_ns() - t0 > timeout_ns) return false;
+  }
+}
+
+// 4-D tiled TMA load (no multicast) into this CTA's shared memory, completing on `bar`.
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap *map, uint32_t bar,
+                                            int c0, int c1, int c2, int c3) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
+      : "memory");
+}
+
+__device__ __forceinline__ float lds_f32(uint32_t addr) {
+  float v;
+  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(addr));
+  return v;
+}
+
+__device__ __forceinline__ float ex2_approx(float x) {
+  float r;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+__device__ __forceinline__ float fuse_result(float product, float sum_weight) {
+  return (fabsf(product) > kDblEpsilonF && fabsf(sum_weight) > kDblEpsilonF)
+             ? __fdiv_rn(product, sum_weight)
+             : __int_as_float(0x7fc00000);
+}
+
+// ---------------------------------------------------------------- geometry of one variant
+
+template <int HW, int RX, int TZ>
+struct Cfg {
+  static constexpr int NQ = TZ + 2;          // D planes per half
+  static constexpr int NR = RX + 2;          // D rows per warp
+  static constexpr int NS = 2 * HW + 1;      // offsets per axis
+  static constexpr int XC = kWarps * RX;     // output rows per CTA
+  // y extent of a slab row: lanes span 32 positions, +-HW for dv, +2 for the 16-byte
+  // alignment of the TMA start coordinate (tile starts are 30*ty, i.e. 0 or 2 mod 4).
+  static constexpr int YB = (34 + 2 * HW + 3) / 4 * 4;
+  static constexpr int ZA = 2 * TZ + 2 + 2 * HW;  // atlas MRI planes per slab row
+  static constexpr int ZL = 2 * TZ + 2 * HW;      // atlas CT planes per slab row
+  static constexpr int RA = XC + 3;               // MRI ring: XC+2 rows in use + 1 prefetch
+  static constexpr int RL = XC + 1;               // CT ring: XC rows in use + 1 prefetch
+  static constexpr uint32_t ROW_A = ZA * YB * 4;  // TMA transaction bytes per row
+  static constexpr uint32_t ROW_L = ZL * YB * 4;
+  static constexpr uint32_t SLOT_A = (ROW_A + 127) / 128 * 128;
+  static constexpr uint32_t SLOT_L = (ROW_L + 127) / 128 * 128;
+  static constexpr uint32_t PLANE = YB * 4;       // bytes between planes of a slab row
+  static constexpr int SMEM = 128 + 128 + RA * SLOT_A + RL * SLOT_L;  // + alignment slack
+  static constexpr int NCH = (NS + NQ - 1) / NQ;  // ring periods per dw sweep
+  static constexpr int OFF = NCH * NQ - NS;       // virtual steps skipped in the first period
+};
+
+struct TmaParams {
+  const float *img;
+  float *out;
+  int nx, ny, nz, num;
+  int nxy;
+  float neg_k;  // -log2(e)/div
+  int tiles_y, tiles_x, tiles_z, ntiles;
+  int groups;         // atlas groups per tile; items = groups * ntiles (group-major)
+  int atlases_per_group;
+  float *partial;     // groups > 1: [groups][2][nvox] partial (product, sum_weight) sums
+  long long nvox;
+  int *err;           // device status word (0 = ok)
+  unsigned long long timeout_ns;
+};
+
+// One dw sweep (all dw for fixed atlas, du, dv) of the thread's voxels.
+template <int HW, int RX, int TZ>
+__device__ __forceinline__ void sweep_dw(const float2 (&In)[TZ + 2][RX + 2], float2 (&P)[TZ][RX],
+                                         float2 (&W)[TZ][RX], const uint32_t (&rowA)[RX + 2],
+                                         const uint32_t (&rowL)[RX], const float2 negk2) {
+  using C = Cfg<HW, RX, TZ>;
+  constexpr int NQ = C::NQ, NR = C::NR;
+  float2 Aw[NQ][NR];  // logical plane q at virtual step v lives in slot (q + v) % NQ
+#pragma unroll
+  for (int q = 0; q < NQ - 1; ++q)
+#pragma unroll
+    for (int r = 0; r < NR; ++r)
+      Aw[(q + C::OFF) % NQ][r] = make_float2(lds_f32(rowA[r] + q * C::PLANE),
+                                             lds_f32(rowA[r] + (TZ + q) * C::PLANE));
+#pragma unroll 1
+  for (int c = 0; c < C::NCH; ++c) {
+#pragma unroll
+    for (int jj = 0; jj < NQ; ++jj) {
+      if (jj < C::OFF && c == 0) continue;
+      const uint32_t so = (uint32_t)(c * NQ + jj - C::OFF) * C::PLANE;  // real step s = dw + HW
+      {
+        constexpr int qn = NQ - 1;
+        const int sn = (qn + jj) % NQ;
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+          Aw[sn][r] = make_float2(lds_f32(rowA[r] + so + qn * C::PLANE),
+                                  lds_f32(rowA[r] + so + (TZ + qn) * C::PLANE));
+      }
+      // x-box of D = (A - I)^2 per plane
+      float2 g[NQ][RX];
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) {
+        const int sq = (q + jj) % NQ;
+        float2 D[NR];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+          const float2 d = add2(Aw[sq][r], In[q][r]);
+          D[r] = mul2(d, d);
+        }
+#pragma unroll
+        for (int x = 0; x < RX; x += 2) {
+          if (x + 1 < RX) {
+            const float2 mid = add2(D[x + 1], D[x + 2]);
+            g[q][x] = add2(D[x], mid);
+            g[q][x + 1] = add2(mid, D[x + 3]);
+          } else {
+            g[q][x] = add2(add2(D[x], D[x + 1]), D[x + 2]);
+          }
+        }
+      }
+      // z-box, y-box (warp shuffles), weight, accumulate
+#pragma unroll
+      for (int x = 0; x < RX; ++x) {
+#pragma unroll
+        for (int q = 0; q < TZ; q += 2) {
+          float2 S[2];
+          if (q + 1 < TZ) {
+            const float2 mid = add2(g[q + 1][x], g[q + 2][x]);
+            S[0] = add2(g[q][x], mid);
+            S[1] = add2(mid, g[q + 3][x]);
+          } else {
+            S[0] = add2(add2(g[q][x], g[q + 1][x]), g[q + 2][x]);
+          }
+#pragma unroll
+          for (int k = 0; k < 2; ++k) {
+            if (q + k >= TZ) break;
+            const float2 cc = S[k];
+            const float2 lft = make_float2(__shfl_up_sync(0xffffffffu, cc.x, 1),
+                                           __shfl_up_sync(0xffffffffu, cc.y, 1));
+            const float2 rgt = make_float2(__shfl_down_sync(0xffffffffu, cc.x, 1),
+                                           __shfl_down_sync(0xffffffffu, cc.y, 1));
+            const float2 e = mul2(add2(add2(cc, lft), rgt), negk2);
+            const float2 w = make_float2(ex2_approx(e.x), ex2_approx(e.y));
+            const float2 lab = make_float2(lds_f32(rowL[x] + so + (q + k) * C::PLANE),
+                                           lds_f32(rowL[x] + so + (TZ + q + k) * C::PLANE));
+            P[q + k][x] = fma2(w, lab, P[q + k][x]);
+            W[q + k][x] = add2(W[q + k][x], w);
+          }
+        }
+      }
+    }
+  }
+}
+
+template <int HW, int RX, int TZ>
+__global__ void __launch_bounds__(kThreads, 1)
+    fuse_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmL,
+                    const TmaParams p) {
+  using C = Cfg<HW, RX, TZ>;
+  constexpr int NQ = C::NQ, NR = C::NR, NS = C::NS;
+  extern __shared__ unsigned char smem_raw[];
+  const uint32_t base = (smem_u32(smem_raw) + 127u) & ~127u;
+  const uint32_t bar0 = base, bar1 = base + 8;
+  volatile int *abort_flag =
+      reinterpret_cast<volatile int *>(smem_raw + (base + 16 - smem_u32(smem_raw)));
+  const uint32_t ringA = base + 128;
+  const uint32_t ringL = ringA + C::RA * C::SLOT_A;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) {
+    mbar_init(bar0, 1);
+    mbar_init(bar1, 1);
+    *abort_flag = 0;
+    fence_mbarrier_init();
+  }
+  __syncthreads();
+
+  const int lo = HW + 1;
+  const float2 negk2 = make_float2(p.neg_k, p.neg_k);
+  const int T = p.atlases_per_group * NS;  // du steps per item (atlas-major)
+  uint32_t gstep = 0;         // steps taken by this CTA: barrier gstep&1, phase (gstep>>1)&1
+  bool aborted = false;
+  bool armed_next = false;    // thread 0: a prefetch is in flight on barrier (gstep+1)&1
+
+  const int nitems = p.ntiles * p.groups;
+  for (int item = blockIdx.x; item < nitems && !aborted; item += gridDim.x) {
+    const int grp = item / p.ntiles;
+    const int a_first = grp * p.atlases_per_group;
+    int t = item - grp * p.ntiles;
+    const int ty = t % p.tiles_y;
+    t /= p.tiles_y;
+    const int txc = t % p.tiles_x;
+    const int tz = t / p.tiles_x;
+    const int y0 = lo + ty * kOutY, X0 = lo + txc * C::XC, z0 = lo + tz * (2 * TZ);
+    const int y = y0 - 1 + lane;
+    const int yb = y0 - 1 - HW;      // first y of the slab (>= 0)
+    const int e = yb & 3;
+    const int ybox = yb - e;         // TMA start, 16-byte aligned
+    const int xw = X0 + warp * RX;   // this warp's first output row
+    const int xA = X0 - 1 - HW, zA = z0 - 1 - HW;  // MRI slab origin (row k=0)
+    const int xL = X0 - HW, zL = z0 - HW;          // CT slab origin
+    const uint32_t lane_off = (uint32_t)(lane + HW + e) * 4u;
+
+    // Input patch values (negated: D = (A + In)^2), zero outside the volume.
+    float2 In[NQ][NR];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q)
+#pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        float v[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int zz = z0 + h * TZ - 1 + q, xx = xw - 1 + r;
+          v[h] = (zz < p.nz && xx < p.nx && y < p.ny)
+                     ? -__ldg(p.img + (long long)zz * p.nxy + (long long)xx * p.ny + y)
+                     : 0.f;
+        }
+        In[q][r] = make_float2(v[0], v[1]);
+      }
+    float2 P[TZ][RX], W[TZ][RX];
+#pragma unroll
+    for (int q = 0; q < TZ; ++q)
+#pragma unroll
+      for (int r = 0; r < RX; ++r) {
+        P[q][r] = make_float2(0.f, 0.f);
+        W[q][r] = make_float2(0.f, 0.f);
+      }
+
+    for (int i = 0; i < T; ++i, ++gstep) {
+      const int ai = i / NS, j = i - ai * NS;
+      const int a = a_first + ai;
+      __syncthreads();  // every warp is done with step i-1: its ring rows may be refilled
+      if (*abort_flag) {
+        aborted = true;
+        break;
+      }
+      if (tid == 0) {
+        fence_proxy_async_smem();
+        if (j == 0) {  // atlas start: the whole window for this step
+          const uint32_t b = (gstep & 1) ? bar1 : bar0;
+          mbar_arrive_expect_tx(b, (C::XC + 2) * C::ROW_A + C::XC * C::ROW_L);
+          for (int k = 0; k < C::XC + 2; ++k)
+            tma_load_4d(ringA + (k % C::RA) * C::SLOT_A, &tmA, b, ybox, xA + k, zA, a);
+          for (int k = 0; k < C::XC; ++k)
+            tma_load_4d(ringL + (k % C::RL) * C::SLOT_L, &tmL, b, ybox, xL + k, zL, a);
+        }
+        armed_next = false;
+        if (j + 1 < NS) {  // prefetch the one new row of each ring for step i+1
+          const uint32_t b = ((gstep + 1) & 1) ? bar1 : bar0;
+          mbar_arrive_expect_tx(b, C::ROW_A + C::ROW_L);
+          const int ka = j + C::XC + 2, kl = j + C::XC;
+          tma_load_4d(ringA + (ka % C::RA) * C::SLOT_A, &tmA, b, ybox, xA + ka, zA, a);
+          tma_load_4d(ringL + (kl % C::RL) * C::SLOT_L, &tmL, b, ybox, xL + kl, zL, a);
+          armed_next = true;
+        }
+      }
+      const bool ok = mbar_wait_bounded((gstep & 1) ? bar1 : bar0, (gstep >> 1) & 1, p.timeout_ns);
+      if (!__all_sync(0xffffffffu, ok)) {
+        if (lane == 0) {
+          atomicExch(p.err, 1);
+          *abort_flag = 1;
+        }
+        continue;  // the next CTA barrier sees the flag
+      }
+      // Ring rows of this thread for step (a, du = j - HW).
+      uint32_t rowA[NR], rowL[RX];
+#pragma unroll
+      for (int r = 0; r < NR; ++r)
+        rowA[r] = ringA + (uint32_t)((warp * RX + r + j) % C::RA) * C::SLOT_A + lane_off;
+#pragma unroll
+      for (int r = 0; r < RX; ++r)
+        rowL[r] = ringL + (uint32_t)((warp * RX + r + j) % C::RL) * C::SLOT_L + lane_off;
+#pragma unroll 1
+      for (int dv = -HW; dv <= HW; ++dv) {
+        uint32_t ra[NR], rl[RX];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) ra[r] = rowA[r] + (uint32_t)(dv * 4);
+#pragma unroll
+        for (int r = 0; r < RX; ++r) rl[r] = rowL[r] + (uint32_t)(dv * 4);
+        sweep_dw<HW, RX, TZ>(In, P, W, ra, rl, negk2);
+      }
+    }
+    if (aborted) break;
+    __syncthreads();  // a timeout in the tile's last step is seen here
+    if (*abort_flag) {
+      aborted = true;
+      break;
+    }
+
+    if (lane >= 1 && lane <= kOutY && y < p.ny - lo) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int q = 0; q < TZ; ++q) {
+          const int z = z0 + h * TZ + q;
+          if (z >= p.nz - lo) continue;
+#pragma unroll
+          for (int r = 0; r < RX; ++r) {
+            const int x = xw + r;
+            if (x >= p.nx - lo) continue;
+            const float pr = h ? P[q][r].y : P[q][r].x;
+            const float sw = h ? W[q][r].y : W[q][r].x;
+            const long long v = (long long)z * p.nxy + (long long)x * p.ny + y;
+            if (p.groups == 1) {
+              p.out[v] = fuse_result(pr, sw);
+            } else {
+              p.partial[(2LL * grp) * p.nvox + v] = pr;
+              p.partial[(2LL * grp + 1) * p.nvox + v] = sw;
+            }
+          }
+        }
+    }
+  }
+  // After an abort, let this CTA's own outstanding copies land (bounded) before exiting: those
+  // of the step whose wait timed out (gstep-1) and the prefetch armed during it, if any.
+  if (aborted && tid == 0) {
+    const uint32_t s = gstep - 1;
+    mbar_wait_bounded((s & 1) ? bar1 : bar0, (s >> 1) & 1, p.timeout_ns);
+    if (armed_next) mbar_wait_bounded((gstep & 1) ? bar1 : bar0, (gstep >> 1) & 1, p.timeout_ns);
+  }
+}
+
+// ---------------------------------------------------------------- host side
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void *ptr = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
+  }
+  return fn;
+}
+
+// 4-D map over a pitched volume stack [num][nz][nx][pitch], box = one x-row slab of
+// `box_z` planes x `box_y` columns. Out-of-volume elements read as zero.
+cudaError_t make_slab_map(CUtensorMap *map, const float *base, int nx, int ny, int nz, int num,
+                          int pitch, int box_y, int box_z) {
+  auto fn = encode_fn();
+  if (!fn) return cudaErrorNotSupported;
+  const cuuint64_t dims[4] = {(cuuint64_t)ny, (cuuint64_t)nx, (cuuint64_t)nz, (cuuint64_t)num};
+  const cuuint64_t strides[3] = {(cuuint64_t)pitch * 4, (cuuint64_t)pitch * 4 * nx,
+                                 (cuuint64_t)pitch * 4 * nx * nz};
+  const cuuint32_t box[4] = {(cuuint32_t)box_y, 1u, (cuuint32_t)box_z, 1u};
+  const cuuint32_t estr[4] = {1u, 1u, 1u, 1u};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float *>(base), dims, strides,
+                  box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+// Sums the per-group partial (product, sum_weight) of every interior voxel in group order and
+// applies the output rule, so the result does not depend on which CTA ran which group.
+__global__ void combine_groups_kernel(const float *__restrict__ partial, int groups, int nx, int ny,
+                                      int nz, int lo, long long nvox, float *__restrict__ out) {
+  const int ix = nx - 2 * lo, iy = ny - 2 * lo, iz = nz - 2 * lo;
+  const long long total = (long long)ix * iy * iz;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int y = (int)(i % iy) + lo;
+    const long long r = i / iy;
+    const int x = (int)(r % ix) + lo;
+    const int z = (int)(r / ix) + lo;
+    const long long v = (long long)z * nx * ny + (long long)x * ny + y;
+    float pr = 0.f, sw = 0.f;
+    for (int g = 0; g < groups; ++g) {
+      pr += partial[(2LL * g) * nvox + v];
+      sw += partial[(2LL * g + 1) * nvox + v];
+    }
+    out[v] = fuse_result(pr, sw);
+  }
+}
+
+cudaError_t launch_combine_groups(const Geometry &g, const float *partial, int groups, float *out,
+                                  cudaStream_t stream) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  combine_groups_kernel<<<sms * 8, 256, 0, stream>>>(partial, groups, g.nx, g.ny, g.nz, g.lo,
+                                                     g.nvox(), out);
+  return cudaGetLastError();
+}
+
+// Register tile (x rows RX, z planes per half TZ) per window size: the largest that compiles to
+// at most 255 registers without spilling.
+template <int HW> struct Shape { static constexpr int RX = 3, TZ = 4; };
+template <> struct Shape<2> { static constexpr int RX = 3, TZ = 3; };
+template <> struct Shape<1> { static constexpr int RX = 4, TZ = 2; };
+
+// Picks the number of atlas groups (a divisor of num) so that the work items fill the
+// persistent grid's rounds: the first group count reaching 97% round occupancy, else the best.
+int choose_groups(int ntiles, int num, int slots) {
+  int best = 1;
+  double best_eff = 0.0;
+  for (int g = 1; g <= num; ++g) {
+    if (num % g) continue;
+    const double rounds = (double)ntiles * g / slots;
+    const double eff = rounds / std::ceil(rounds);
+    if (eff >= 0.97) return g;
+    if (eff > best_eff + 1e-9) {
+      best_eff = eff;
+      best = g;
+    }
+  }
+  return best;
+}
+
+template <int HW>
+struct Plan {
+  int blocks, groups, ntiles, tiles_y, tiles_x, tiles_z;
+};
+
+template <int HW>
+cudaError_t plan_hw(const Geometry &g, Plan<HW> *pl) {
+  constexpr int RX = Shape<HW>::RX, TZ = Shape<HW>::TZ;
+  using C = Cfg<HW, RX, TZ>;
+  auto kern = fuse_tma_kernel<HW, RX, TZ>;
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM)) !=
+      cudaSuccess)
+    return e;
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, C::SMEM)) !=
+      cudaSuccess)
+    return e;
+  if (per_sm < 1) return cudaErrorLaunchOutOfResources;
+  pl->tiles_y = (g.iy + kOutY - 1) / kOutY;
+  pl->tiles_x = (g.ix + C::XC - 1) / C::XC;
+  pl->tiles_z = (g.iz + 2 * TZ - 1) / (2 * TZ);
+  pl->ntiles = pl->tiles_y * pl->tiles_x * pl->tiles_z;
+  const int slots = sms * per_sm;
+  pl->groups = choose_groups(pl->ntiles, g.num, slots);
+  const long long items = (long long)pl->ntiles * pl->groups;
+  pl->blocks = (int)(items < slots ? items : slots);
+  return cudaSuccess;
+}
+
+template <int HW>
+cudaError_t launch_hw(const Geometry &g, const SlabInputs &in, float *out, double div,
+                      float *partial, int *err, cudaStream_t stream) {
+  constexpr int RX = Shape<HW>::RX, TZ = Shape<HW>::TZ;
+  using C = Cfg<HW, RX, TZ>;
+  Plan<HW> pl;
+  cudaError_t e = plan_hw<HW>(g, &pl);
+  if (e != cudaSuccess) return e;
+  if (pl.groups > 1 && !partial) return cudaErrorInvalidValue;
+  CUtensorMap tmA, tmL;
+  if ((e = make_slab_map(&tmA, in.atlas, g.nx, g.ny, g.nz, g.num, in.pitch, C::YB, C::ZA)) !=
+      cudaSuccess)
+    return e;
+  if ((e = make_slab_map(&tmL, in.label, g.nx, g.ny, g.nz, g.num, in.pitch, C::YB, C::ZL)) !=
+      cudaSuccess)
+    return e;
+  TmaParams p{};
+  p.img = in.img;
+  p.out = out;
+  p.nx = g.nx;
+  p.ny = g.ny;
+  p.nz = g.nz;
+  p.num = g.num;
+  p.nxy = g.nx * g.ny;
+  p.neg_k = (float)(-1.4426950408889634 / div);
+  p.tiles_y = pl.tiles_y;
+  p.tiles_x = pl.tiles_x;
+  p.tiles_z = pl.tiles_z;
+  p.ntiles = pl.ntiles;
+  p.groups = pl.groups;
+  p.atlases_per_group = g.num / pl.groups;
+  p.partial = partial;
+  p.nvox = g.nvox();
+  p.err = err;
+  p.timeout_ns = 2000000000ull;  // 2 s per wait; a step's copies land in microseconds
+  fuse_tma_kernel<HW, RX, TZ><<<pl.blocks, kThreads, C::SMEM, stream>>>(tmA, tmL, p);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (pl.groups > 1) return launch_combine_groups(g, partial, pl.groups, out, stream);
+  return cudaSuccess;
+}
+
+template <int HW>
+size_t partial_bytes_hw(const Geometry &g) {
+  Plan<HW> pl;
+  if (plan_hw<HW>(g, &pl) != cudaSuccess || pl.groups <= 1) return 0;
+  return (size_t)pl.groups * 2 * (size_t)g.nvox() * sizeof(float);
+}
+
+}  // namespace
+
+size_t fuse_tma_partial_bytes(const Geometry &g) {
+  if (g.ix <= 0 || g.iy <= 0 || g.iz <= 0) return 0;
+  switch (g.hw) {
+    case 1: return partial_bytes_hw<1>(g);
+    case 2: return partial_bytes_hw<2>(g);
+    case 3: return partial_bytes_hw<3>(g);
+    case 4: return partial_bytes_hw<4>(g);
+    case 5: return partial_bytes_hw<5>(g);
+    default: return 0;
+  }
+}
+
+cudaError_t launch_fuse_tma(const Geometry &g, const SlabInputs &in, float *out, double div,
+                            float *partial, int *err, cudaStream_t stream) {
+  if (g.ix <= 0 || g.iy <= 0 || g.iz <= 0) return cudaSuccess;
+  switch (g.hw) {
+    case 1: return launch_hw<1>(g, in, out, div, partial, err, stream);
+    case 2: return launch_hw<2>(g, in, out, div, partial, err, stream);
+    case 3: return launch_hw<3>(g, in, out, div, partial, err, stream);
+    case 4: return launch_hw<4>(g, in, out, div, partial, err, stream);
+    case 5: return launch_hw<5>(g, in, out, div, partial, err, stream);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+namespace {
+__global__ void pitch_copy_kernel(const float *__restrict__ src, float *__restrict__ dst,
+                                  long long rows, int ny, int pitch) {
+  const long long total = rows * ny;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long r = i / ny;
+    const int c = (int)(i - r * ny);
+    dst[r * pitch + c] = src[i];
+  }
+}
+}  // namespace
+
+cudaError_t launch_pitch_copy(const float *src, float *dst, long long rows, int ny, int pitch,
+                              cudaStream_t stream) {
+  if (rows <= 0) return cudaSuccess;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  pitch_copy_kernel<<<sms * 8, 256, 0, stream>>>(src, dst, rows, ny, pitch);
+  return cudaGetLastError();
+}
+
+}  // namespace pct

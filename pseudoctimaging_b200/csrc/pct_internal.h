@@ -17,12 +17,29 @@ struct Geometry {
 
 bool make_geometry(int nx, int ny, int nz, int num, int nh, Geometry *g);
 
-// Plain FP32 fusion (the path's hot loop). Writes interior voxels of out only.
-cudaError_t launch_fuse_plain(const Geometry &g, const float *img, const float *atlas,
-                              const float *label, float *out, double div, cudaStream_t stream);
+// Inputs of the TMA-staged kernel: the input MRI in the reference layout, and the atlas MRI and
+// CT stacks [num][nz][nx][pitch] with pitch >= ny, pitch % 4 == 0 and 16-byte aligned bases
+// (TMA needs 16-byte row strides).
+struct SlabInputs {
+  const float *img;
+  const float *atlas;
+  const float *label;
+  int pitch;
+};
 
-// Number of kernel launches launch_fuse_plain issues for this geometry.
-int fuse_plain_launches(const Geometry &g);
+// TMA-staged plain FP32 fusion. Writes interior voxels of out only. *err (device) is set to a
+// non-zero code if a bounded wait gave up; the caller zeroes it beforehand. When the planner
+// splits the atlases into groups (to fill the persistent grid), `partial` must point to
+// fuse_tma_partial_bytes(g) bytes of device scratch; otherwise it may be null.
+size_t fuse_tma_partial_bytes(const Geometry &g);
+cudaError_t launch_fuse_tma(const Geometry &g, const SlabInputs &in, float *out, double div,
+                            float *partial, int *err, cudaStream_t stream);
+
+// dst[r*pitch + c] = src[r*ny + c] for r < rows, c < ny.
+cudaError_t launch_pitch_copy(const float *src, float *dst, long long rows, int ny, int pitch,
+                              cudaStream_t stream);
+
+inline int slab_pitch(int ny) { return (ny + 3) / 4 * 4; }
 
 // NaN median fill (synchronous on `stream`: it reads back a counter after each round).
 // scratch must hold regularize_scratch_bytes(nx*ny*nz) bytes.
