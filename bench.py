@@ -46,7 +46,7 @@ UNIT = "voxels/s"
 OPS_PER_CANDIDATE = 11
 FP32_LANES_PER_SM = 128
 MUFU_LANES_PER_SM = 16
-PROFILE_SUMMARY = REPO / "profiles" / "fuse_plain_nh11_222x222x112_10atlas.md"
+PROFILE_SUMMARY = REPO / "profiles" / "fuse_tma_nh11_222x222x112_10atlas.md"
 
 
 def interior(n: int, nh: int) -> int:
