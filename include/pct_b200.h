@@ -34,7 +34,8 @@ typedef enum pct_status {
   PCT_ERR_UNSUPPORTED = -4,   /* exec_choice or NH this build does not provide */
   PCT_ERR_NO_DEVICE = -5,     /* bad device index, or no sm_100 device */
   PCT_ERR_TIMEOUT = -6,       /* a bounded device-side wait gave up */
-  PCT_ERR_INTERNAL = -7
+  PCT_ERR_INTERNAL = -7,
+  PCT_ERR_TOO_LARGE = -8      /* input larger than a fixed-size entry point accepts */
 } pct_status;
 
 /*
@@ -120,6 +121,21 @@ int pct_normalize_labels_device(pct_handle *h, float *d_label, size_t n, void *s
  */
 int pct_regularize_device(pct_handle *h, float *d_vol, int nx, int ny, int nz, int nh,
                           int64_t *fills, void *stream);
+
+/*
+ * Allocation-free variant of pct_regularize_device, for callers that may not allocate GPU memory
+ * while running (for example applications whose device memory belongs to their own pool
+ * allocator, or latency-critical loops that forbid allocation after start-up). No counterpart in
+ * the reference. Same result as pct_regularize_device; needs no handle and calls no allocator:
+ * its scratch is a fixed 64 MiB array inside the library, held by every GPU that loads the
+ * library until the process exits. Volumes of more than 2^23 voxels (8,388,608) are rejected
+ * with PCT_ERR_TOO_LARGE. Runs on the current device; its first call on a device looks up the
+ * array's device address, so make that first call before any stream capture. Calls share the
+ * array: calls whose work overlaps on the GPU race and must be issued one after another.
+ * Synchronous on `stream`.
+ */
+int pct_regularize_device_noalloc(float *d_vol, int nx, int ny, int nz, int nh, int64_t *fills,
+                                  void *stream);
 
 /* RoundMatrix then the HU map round(4095*(v/255)) - 1024 over all n voxels
  * (NewPatchedBrainPureC.cpp:1221-1227,1732-1738; PatchBasedPseudoCT.cu:2173-2179). */

@@ -37,7 +37,7 @@ PCT_OK = 0
 STATUS = {
     0: "PCT_OK", -1: "PCT_ERR_INVALID_ARG", -2: "PCT_ERR_CUDA", -3: "PCT_ERR_OUT_OF_MEMORY",
     -4: "PCT_ERR_UNSUPPORTED", -5: "PCT_ERR_NO_DEVICE", -6: "PCT_ERR_TIMEOUT",
-    -7: "PCT_ERR_INTERNAL",
+    -7: "PCT_ERR_INTERNAL", -8: "PCT_ERR_TOO_LARGE",
 }
 
 
@@ -85,6 +85,8 @@ SIGNATURES = {
     "pct_device_status": (_I, [_P, _P]),
     "pct_normalize_labels_device": (_I, [_P, _P, _SZ, _P]),
     "pct_regularize_device": (_I, [_P, _P, _I, _I, _I, _I, ctypes.POINTER(ctypes.c_int64), _P]),
+    "pct_regularize_device_noalloc": (_I, [_P, _I, _I, _I, _I, ctypes.POINTER(ctypes.c_int64),
+                                            _P]),
     "pct_finalize_hu_device": (_I, [_P, _P, _SZ, _P]),
     "pct_run_pipeline": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _D, _D, _I, _I]),
     "pct_error_stats_device": (_I, [_P, _P, _P, _I, _I, _I, _I, ctypes.POINTER(ErrorStats), _P]),

@@ -253,6 +253,7 @@ const char *pct_strerror(int status) {
     case PCT_ERR_NO_DEVICE: return "no usable sm_100 device";
     case PCT_ERR_TIMEOUT: return "device-side wait timed out";
     case PCT_ERR_INTERNAL: return "internal error";
+    case PCT_ERR_TOO_LARGE: return "input larger than this entry point's fixed scratch accepts";
     default: return "unknown status";
   }
 }
