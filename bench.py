@@ -323,6 +323,7 @@ def run_b200_arm(args) -> None:
         assert np.array_equal(np.isnan(out.numpy()), np.isnan(d_out.cpu().numpy())), \
             "host-pointer and device-pointer runs disagree"
 
+    plan = pct.query_plan(NX, NY, NZ, NUM, NH, local)
     clocks = clk.summary()
     peaks = measured_peaks()
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
@@ -346,7 +347,8 @@ def run_b200_arm(args) -> None:
                          f"{4 * nvox * (1 + 2 * NUM) / 1e6:.0f} MB per subject)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "candidates_per_s": world * cand / (ms / 1e3),
-        "gpu_launches": args.steps * 1,
+        "gpu_launches": args.steps * plan["launches"],
+        "plan": plan,
         "roofline": {
             "bound": "fp32", "unit": "TFLOP/s",
             "achieved": achieved / 1e12, "peak": fp32_peak / 1e12, "frac": achieved / fp32_peak,

@@ -108,6 +108,23 @@ int pct_synthesize_device(pct_handle *h, const float *d_img, const float *d_atla
  */
 int pct_device_status(pct_handle *h, void *stream);
 
+/*
+ * How pct_synthesize_device would run a given shape on `device` (no work is done): the kernel
+ * launches it issues (fusion, pitched repack copies when ny % 4 != 0 or buffers are not 16-byte
+ * aligned — assumed aligned here —, the atlas-group combine), the number of atlas groups, the
+ * register tile and the persistent grid.
+ */
+typedef struct pct_plan {
+  int launches;        /* kernel launches per call */
+  int groups;          /* atlas groups (work items per tile) */
+  int tiles;           /* output tiles */
+  int ctas;            /* persistent CTAs launched */
+  int tile_rows;       /* RX: x rows per warp */
+  int tile_planes;     /* TZ: z planes per half-tile */
+  size_t scratch_bytes;/* device scratch for the group partial sums */
+} pct_plan;
+int pct_query_plan(int device, int nx, int ny, int nz, int num_atlas, int nh, pct_plan *plan);
+
 /* In-place CT -> label scale L' = 255*((L+1024)/4095) on a device buffer of n floats
  * (PatchBasedPseudoCT.cu:2009-2020, NewPatchedBrainPureC.cpp:1583-1593). */
 int pct_normalize_labels_device(pct_handle *h, float *d_label, size_t n, void *stream);

@@ -66,6 +66,15 @@ class SynthParams(ctypes.Structure):
                 ("max_disp", ctypes.c_float), ("seed", ctypes.c_uint64)]
 
 
+class Plan(ctypes.Structure):
+    _fields_ = [("launches", ctypes.c_int), ("groups", ctypes.c_int), ("tiles", ctypes.c_int),
+                ("ctas", ctypes.c_int), ("tile_rows", ctypes.c_int),
+                ("tile_planes", ctypes.c_int), ("scratch_bytes", ctypes.c_size_t)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _P = ctypes.c_void_p
 _I = ctypes.c_int
 _D = ctypes.c_double
@@ -83,6 +92,7 @@ SIGNATURES = {
     "pct_synthesize": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _D, _I]),
     "pct_synthesize_device": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _D, _I, _P]),
     "pct_device_status": (_I, [_P, _P]),
+    "pct_query_plan": (_I, [_I, _I, _I, _I, _I, _I, ctypes.POINTER(Plan)]),
     "pct_normalize_labels_device": (_I, [_P, _P, _SZ, _P]),
     "pct_regularize_device": (_I, [_P, _P, _I, _I, _I, _I, ctypes.POINTER(ctypes.c_int64), _P]),
     "pct_regularize_device_noalloc": (_I, [_P, _I, _I, _I, _I, ctypes.POINTER(ctypes.c_int64),
@@ -111,6 +121,15 @@ def load_library(path: os.PathLike | str | None = None) -> ctypes.CDLL:
 
 
 lib = load_library()
+
+
+def query_plan(nx: int, ny: int, nz: int, num: int, nh: int, device: int = 0) -> dict:
+    """How the device entry point would run this shape (launches, atlas groups, tiles, grid)."""
+    p = Plan()
+    st = lib.pct_query_plan(device, nx, ny, nz, num, nh, ctypes.byref(p))
+    if st != PCT_OK:
+        raise PctError(st, "pct_query_plan")
+    return p.as_dict()
 
 
 def div_from(sigma: float, beta: float) -> float:

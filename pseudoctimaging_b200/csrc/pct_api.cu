@@ -372,6 +372,38 @@ int pct_synthesize(pct_handle *h, const float *img, const float *atlas, const fl
   return read_device_status(h, s);
 }
 
+int pct_query_plan(int device, int nx, int ny, int nz, int num_atlas, int nh, pct_plan *plan) {
+  if (!plan) return PCT_ERR_INVALID_ARG;
+  memset(plan, 0, sizeof(*plan));
+  pct::Geometry g;
+  int st = check_shape(nullptr, nx, ny, nz, num_atlas, nh, 1.0, &g);
+  if (st) return st;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+    cudaGetLastError();
+    return PCT_ERR_NO_DEVICE;
+  }
+  int prev = 0;
+  cudaGetDevice(&prev);
+  if (cudaSetDevice(device) != cudaSuccess) return PCT_ERR_NO_DEVICE;
+  pct::FusePlanInfo info;
+  const cudaError_t e = pct::fuse_tma_plan(g, &info);
+  cudaSetDevice(prev);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return PCT_ERR_CUDA;
+  }
+  const bool work = g.ix > 0 && g.iy > 0 && g.iz > 0;
+  plan->groups = info.groups;
+  plan->tiles = info.tiles;
+  plan->ctas = info.ctas;
+  plan->tile_rows = info.rx;
+  plan->tile_planes = info.tz;
+  plan->scratch_bytes = info.partial_bytes;
+  plan->launches = work ? 1 + (ny % 4 != 0 ? 2 : 0) + (info.groups > 1 ? 1 : 0) : 0;
+  return PCT_OK;
+}
+
 int pct_device_status(pct_handle *h, void *stream) {
   if (!h) return PCT_ERR_INVALID_ARG;
   h->last_error.clear();

@@ -582,6 +582,21 @@ cudaError_t launch_hw(const Geometry &g, const SlabInputs &in, float *out, doubl
 }
 
 template <int HW>
+cudaError_t plan_info_hw(const Geometry &g, FusePlanInfo *info) {
+  Plan<HW> pl;
+  cudaError_t e = plan_hw<HW>(g, &pl);
+  if (e != cudaSuccess) return e;
+  info->groups = pl.groups;
+  info->tiles = pl.ntiles;
+  info->ctas = pl.blocks;
+  info->rx = Shape<HW>::RX;
+  info->tz = Shape<HW>::TZ;
+  info->partial_bytes =
+      pl.groups > 1 ? (size_t)pl.groups * 2 * (size_t)g.nvox() * sizeof(float) : 0;
+  return cudaSuccess;
+}
+
+template <int HW>
 size_t partial_bytes_hw(const Geometry &g) {
   Plan<HW> pl;
   if (plan_hw<HW>(g, &pl) != cudaSuccess || pl.groups <= 1) return 0;
@@ -599,6 +614,19 @@ size_t fuse_tma_partial_bytes(const Geometry &g) {
     case 4: return partial_bytes_hw<4>(g);
     case 5: return partial_bytes_hw<5>(g);
     default: return 0;
+  }
+}
+
+cudaError_t fuse_tma_plan(const Geometry &g, FusePlanInfo *info) {
+  *info = FusePlanInfo{0, 0, 0, 0, 0, 0};
+  if (g.ix <= 0 || g.iy <= 0 || g.iz <= 0) return cudaSuccess;
+  switch (g.hw) {
+    case 1: return plan_info_hw<1>(g, info);
+    case 2: return plan_info_hw<2>(g, info);
+    case 3: return plan_info_hw<3>(g, info);
+    case 4: return plan_info_hw<4>(g, info);
+    case 5: return plan_info_hw<5>(g, info);
+    default: return cudaErrorInvalidValue;
   }
 }
 

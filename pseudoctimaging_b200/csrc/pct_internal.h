@@ -32,6 +32,11 @@ struct SlabInputs {
 // splits the atlases into groups (to fill the persistent grid), `partial` must point to
 // fuse_tma_partial_bytes(g) bytes of device scratch; otherwise it may be null.
 size_t fuse_tma_partial_bytes(const Geometry &g);
+struct FusePlanInfo {
+  int groups, tiles, ctas, rx, tz;
+  size_t partial_bytes;
+};
+cudaError_t fuse_tma_plan(const Geometry &g, FusePlanInfo *info);
 cudaError_t launch_fuse_tma(const Geometry &g, const SlabInputs &in, float *out, double div,
                             float *partial, int *err, cudaStream_t stream);
 
