@@ -185,6 +185,37 @@ int pct_error_stats_device(pct_handle *h, const float *d_a, const float *d_b, in
                            int nz, int nh, pct_error_stats *stats, void *stream);
 
 /*
+ * Volume files of the drop-in command line (host, no GPU). MatrixIO text format of the reference
+ * (MatrixIO<T>::Read/Store, PatchBasedPseudoCT.cu:679-809): header lines num, rows (nx), cols
+ * (ny), depth (nz), then the values in [num][depth][rows][cols] order. dims[] = {num, rows, cols,
+ * depth}. pct_matrixio_read expects n = the product of the header. The raw form is a plain
+ * float32 dump of the same layout.
+ */
+int pct_matrixio_dims(const char *path, int dims[4]);
+int pct_matrixio_read(const char *path, float *out, size_t n);
+int pct_matrixio_write(const char *path, const float *data, int num, int rows, int cols, int depth);
+int pct_raw_read(const char *path, float *out, size_t n);
+int pct_raw_write(const char *path, const float *data, size_t n);
+
+/*
+ * Normalised cross-correlation of two device volumes over the interior of an NH window, counting
+ * only voxels finite in both (FP64 sums); the quality measure the reference reports for its
+ * pseudo-CTs against the real CT (imgs/Correlation.png). *ncc is NaN if fewer than two voxels
+ * qualify or either volume is constant there. *count (optional) receives the voxels used.
+ */
+int pct_ncc_device(pct_handle *h, const float *d_a, const float *d_b, int nx, int ny, int nz,
+                   int nh, double *ncc, int64_t *count, void *stream);
+
+/*
+ * Testing hook for failure detection (no GPU fault involved): the next fusion launch on this
+ * handle has its first CTA withhold the copies its first wait expects, so that bounded wait runs
+ * out after timeout_ms; the CTA records the timeout and stops, and the call reports
+ * PCT_ERR_TIMEOUT (pct_device_status for the asynchronous entry point). One-shot. The device
+ * context stays usable.
+ */
+int pct_test_wait_timeout(pct_handle *h, double timeout_ms);
+
+/*
  * Seeded synthetic subject (host). Input MRI = sum of n_blobs Gaussian blobs (amplitude
  * U[amp_lo,amp_hi], isotropic std U[std_lo,std_hi] voxels) + N(0, mri_noise). Atlas a: the
  * noise-free input resampled (trilinear) through a smooth random displacement field whose

@@ -100,6 +100,14 @@ SIGNATURES = {
     "pct_finalize_hu_device": (_I, [_P, _P, _SZ, _P]),
     "pct_run_pipeline": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _D, _D, _I, _I]),
     "pct_error_stats_device": (_I, [_P, _P, _P, _I, _I, _I, _I, ctypes.POINTER(ErrorStats), _P]),
+    "pct_matrixio_dims": (_I, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)]),
+    "pct_matrixio_read": (_I, [ctypes.c_char_p, _P, _SZ]),
+    "pct_matrixio_write": (_I, [ctypes.c_char_p, _P, _I, _I, _I, _I]),
+    "pct_raw_read": (_I, [ctypes.c_char_p, _P, _SZ]),
+    "pct_raw_write": (_I, [ctypes.c_char_p, _P, _SZ]),
+    "pct_ncc_device": (_I, [_P, _P, _P, _I, _I, _I, _I, ctypes.POINTER(ctypes.c_double),
+                            ctypes.POINTER(ctypes.c_int64), _P]),
+    "pct_test_wait_timeout": (_I, [_P, _D]),
     "pct_synth_default_params": (_I, [ctypes.POINTER(SynthParams), _I, _I, _I, _I, _I,
                                       ctypes.c_uint64]),
     "pct_synth_generate": (_I, [ctypes.POINTER(SynthParams), _P, _P, _P]),
@@ -255,6 +263,17 @@ class Handle:
                                                stream or None), "pct_error_stats_device")
         return st.as_dict()
 
+    def ncc_device(self, d_a: int, d_b: int, nx: int, ny: int, nz: int, nh: int,
+                   stream: int = 0) -> tuple[float, int]:
+        v, n = ctypes.c_double(0.0), ctypes.c_int64(0)
+        self._check(lib.pct_ncc_device(self._h, d_a, d_b, nx, ny, nz, nh, ctypes.byref(v),
+                                       ctypes.byref(n), stream or None), "pct_ncc_device")
+        return v.value, n.value
+
+    def test_wait_timeout(self, timeout_ms: float) -> None:
+        """Arms the one-shot bounded-wait test of the next fusion launch."""
+        self._check(lib.pct_test_wait_timeout(self._h, float(timeout_ms)), "pct_test_wait_timeout")
+
     def run_pipeline(self, img, atlas_mri, atlas_ct_hu, nh: int, sigma: float, beta: float,
                      exec_choice: int = EXEC_B200_FP32, regularize: bool = True) -> np.ndarray:
         img = _f32c(img, "img")
@@ -291,6 +310,31 @@ def run_pipeline(img, atlas_mri, atlas_ct_hu, nh: int, sigma: float = 1.0, beta:
                  exec_choice: int = EXEC_B200_FP32, regularize: bool = True) -> np.ndarray:
     return default_handle().run_pipeline(img, atlas_mri, atlas_ct_hu, nh, sigma, beta,
                                          exec_choice, regularize)
+
+
+def read_matrixio(path) -> np.ndarray:
+    """A MatrixIO text volume as float32 [num][depth][rows][cols] (= [num][nz][nx][ny])."""
+    dims = (ctypes.c_int * 4)()
+    st = lib.pct_matrixio_dims(str(path).encode(), dims)
+    if st != PCT_OK:
+        raise PctError(st, f"pct_matrixio_dims({path})")
+    num, rows, cols, depth = dims
+    out = np.empty((num, depth, rows, cols), np.float32)
+    st = lib.pct_matrixio_read(str(path).encode(), _ptr(out), out.size)
+    if st != PCT_OK:
+        raise PctError(st, f"pct_matrixio_read({path})")
+    return out
+
+
+def write_matrixio(path, vol) -> None:
+    """Writes [num][nz][nx][ny] (or [nz][nx][ny]) float32 data in the MatrixIO text format."""
+    v = np.ascontiguousarray(vol, np.float32)
+    if v.ndim == 3:
+        v = v[None]
+    num, depth, rows, cols = v.shape
+    st = lib.pct_matrixio_write(str(path).encode(), _ptr(v), num, rows, cols, depth)
+    if st != PCT_OK:
+        raise PctError(st, f"pct_matrixio_write({path})")
 
 
 @dataclass

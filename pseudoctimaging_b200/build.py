@@ -23,7 +23,7 @@ REPO = PKG.parent
 CSRC = PKG / "csrc"
 OBJ = PKG / "_build"
 LIB = PKG / "lib" / "libpct_b200.so"
-CLI = PKG / "bin" / "PatchBasedPseudoCT_b200"
+CLI = PKG / "bin" / "PatchBasedPseudoCT_b200"  # the drop-in command line
 INCLUDE = REPO / "include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -32,7 +32,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", f"-ccbin={HOST_CXX}", "-Xcompiler", 
           f"-I{INCLUDE}", f"-I{CSRC}"]
 # Sources that make up the shared library; the CLI main is linked separately against it.
 LIB_SOURCES = ["pct_api.cu", "pct_fuse_tma.cu", "pct_pointwise.cu", "pct_regularize.cu",
-               "pct_noalloc.cu", "pct_synth.cpp"]
+               "pct_noalloc.cu", "pct_synth.cpp", "pct_io.cpp"]
 CLI_SOURCES = ["pct_cli.cpp"]
 
 

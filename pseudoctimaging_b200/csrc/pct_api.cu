@@ -30,6 +30,7 @@ struct pct_handle {
   DevBuf err;      // device status word written by kernels with bounded waits
   DevBuf partial;  // per-atlas-group partial sums of the fusion kernel
   DevBuf stage;    // contiguous host->device staging before the pitched repack
+  unsigned long long wait_test_ns = 0;  // one-shot testing hook, see pct_test_wait_timeout
   std::string last_error;
 };
 
@@ -127,7 +128,10 @@ int launch_fusion(pct_handle *h, const pct::Geometry &g, const pct::SlabInputs &
   const size_t pbytes = pct::fuse_tma_partial_bytes(g);
   if (pbytes && (st = ensure(h, h->partial, pbytes))) return st;
   PCT_CUDA(h, cudaMemsetAsync(err, 0, sizeof(int), s));
-  PCT_CUDA(h, pct::launch_fuse_tma(g, in, d_out, div, static_cast<float *>(h->partial.ptr), err, s));
+  const pct::WaitTest wt{h->wait_test_ns};
+  h->wait_test_ns = 0;
+  PCT_CUDA(h, pct::launch_fuse_tma(g, in, d_out, div, static_cast<float *>(h->partial.ptr), err, wt,
+                                   s));
   return PCT_OK;
 }
 
@@ -215,6 +219,47 @@ __global__ void error_stats_kernel(const float *__restrict__ a, const float *__r
     atomicAdd(&acc->compared, cmp);
     atomicAdd(&acc->nan_mismatch, mis);
     atomicAdd(&acc->nan_both, both);
+  }
+}
+
+// Normalised cross-correlation of two volumes over the interior voxels finite in both, from FP64
+// sums (n, sum a, sum b, sum a^2, sum b^2, sum ab).
+struct NccAccum {
+  double s[5];
+  unsigned long long n;
+};
+
+__global__ void ncc_kernel(const float *__restrict__ a, const float *__restrict__ b, int nx, int ny,
+                           int nz, int lo, NccAccum *acc) {
+  const int ix = nx - 2 * lo, iy = ny - 2 * lo, iz = nz - 2 * lo;
+  const long long total = (long long)ix * iy * iz;
+  double s[5] = {0, 0, 0, 0, 0};
+  unsigned long long n = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int y = (int)(i % iy) + lo;
+    const long long r = i / iy;
+    const int x = (int)(r % ix) + lo;
+    const int z = (int)(r / ix) + lo;
+    const long long k = (long long)z * nx * ny + (long long)x * ny + y;
+    const double va = a[k], vb = b[k];
+    if (isnan(va) || isnan(vb)) continue;
+    s[0] += va;
+    s[1] += vb;
+    s[2] += va * va;
+    s[3] += vb * vb;
+    s[4] += va * vb;
+    ++n;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+    for (int j = 0; j < 5; ++j) s[j] += __shfl_down_sync(0xffffffffu, s[j], o);
+    n += __shfl_down_sync(0xffffffffu, n, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+    for (int j = 0; j < 5; ++j) atomicAdd(&acc->s[j], s[j]);
+    atomicAdd(&acc->n, n);
   }
 }
 
@@ -496,6 +541,44 @@ int pct_run_pipeline(pct_handle *h, const float *img, const float *atlas_mri,
   }
   PCT_CUDA(h, cudaMemcpyAsync(out, d_out, vol, cudaMemcpyDeviceToHost, s));
   PCT_CUDA(h, cudaStreamSynchronize(s));
+  return PCT_OK;
+}
+
+int pct_ncc_device(pct_handle *h, const float *d_a, const float *d_b, int nx, int ny, int nz,
+                   int nh, double *ncc, int64_t *count, void *stream) {
+  if (!h) return PCT_ERR_INVALID_ARG;
+  h->last_error.clear();
+  if (!d_a || !d_b || !ncc) return fail(h, PCT_ERR_INVALID_ARG, "null pointer");
+  if (nx <= 0 || ny <= 0 || nz <= 0 || nh < 1 || (nh % 2) == 0)
+    return fail(h, PCT_ERR_INVALID_ARG, "bad volume shape or NH");
+  int st = select_device(h);
+  if (st) return st;
+  if ((st = ensure(h, h->scratch, sizeof(NccAccum)))) return st;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  NccAccum *acc = static_cast<NccAccum *>(h->scratch.ptr);
+  PCT_CUDA(h, cudaMemsetAsync(acc, 0, sizeof(NccAccum), s));
+  const int lo = (nh - 1) / 2 + 1;
+  if (nx > 2 * lo && ny > 2 * lo && nz > 2 * lo) {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+    ncc_kernel<<<sms * 4, 256, 0, s>>>(d_a, d_b, nx, ny, nz, lo, acc);
+    PCT_CUDA(h, cudaGetLastError());
+  }
+  NccAccum host;
+  PCT_CUDA(h, cudaMemcpyAsync(&host, acc, sizeof(host), cudaMemcpyDeviceToHost, s));
+  PCT_CUDA(h, cudaStreamSynchronize(s));
+  if (count) *count = (int64_t)host.n;
+  const double n = (double)host.n;
+  const double cov = host.s[4] - host.s[0] * host.s[1] / (n > 0 ? n : 1);
+  const double va = host.s[2] - host.s[0] * host.s[0] / (n > 0 ? n : 1);
+  const double vb = host.s[3] - host.s[1] * host.s[1] / (n > 0 ? n : 1);
+  *ncc = (host.n > 1 && va > 0 && vb > 0) ? cov / sqrt(va * vb) : NAN;
+  return PCT_OK;
+}
+
+int pct_test_wait_timeout(pct_handle *h, double timeout_ms) {
+  if (!h || !(timeout_ms > 0) || timeout_ms > 60000) return PCT_ERR_INVALID_ARG;
+  h->wait_test_ns = (unsigned long long)(timeout_ms * 1e6);
   return PCT_OK;
 }
 

@@ -166,6 +166,7 @@ struct TmaParams {
   long long nvox;
   int *err;           // device status word (0 = ok)
   unsigned long long timeout_ns;
+  int withhold_cta;   // testing hook: this CTA withholds its first copies (-1 = none)
 };
 
 // One dw sweep (all dw for fixed atlas, du, dv) of the thread's voxels.
@@ -336,7 +337,9 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
       if (tid == 0) {
         fence_proxy_async_smem();
-        if (j == 0) {  // atlas start: the whole window for this step
+        // Testing hook: withhold the first window of this CTA so that the wait below runs out.
+        const bool withhold = (int)blockIdx.x == p.withhold_cta && gstep == 0;
+        if (j == 0 && !withhold) {  // atlas start: the whole window for this step
           const uint32_t b = (gstep & 1) ? bar1 : bar0;
           mbar_arrive_expect_tx(b, (C::XC + 2) * C::ROW_A + C::XC * C::ROW_L);
           for (int k = 0; k < C::XC + 2; ++k)
@@ -542,7 +545,7 @@ cudaError_t plan_hw(const Geometry &g, Plan<HW> *pl) {
 
 template <int HW>
 cudaError_t launch_hw(const Geometry &g, const SlabInputs &in, float *out, double div,
-                      float *partial, int *err, cudaStream_t stream) {
+                      float *partial, int *err, const WaitTest &wt, cudaStream_t stream) {
   constexpr int RX = Shape<HW>::RX, TZ = Shape<HW>::TZ;
   using C = Cfg<HW, RX, TZ>;
   Plan<HW> pl;
@@ -575,6 +578,11 @@ cudaError_t launch_hw(const Geometry &g, const SlabInputs &in, float *out, doubl
   p.nvox = g.nvox();
   p.err = err;
   p.timeout_ns = 2000000000ull;  // 2 s per wait; a step's copies land in microseconds
+  p.withhold_cta = -1;
+  if (wt.timeout_ns) {
+    p.timeout_ns = wt.timeout_ns;
+    p.withhold_cta = 0;
+  }
   fuse_tma_kernel<HW, RX, TZ><<<pl.blocks, kThreads, C::SMEM, stream>>>(tmA, tmL, p);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (pl.groups > 1) return launch_combine_groups(g, partial, pl.groups, out, stream);
@@ -631,14 +639,14 @@ cudaError_t fuse_tma_plan(const Geometry &g, FusePlanInfo *info) {
 }
 
 cudaError_t launch_fuse_tma(const Geometry &g, const SlabInputs &in, float *out, double div,
-                            float *partial, int *err, cudaStream_t stream) {
+                            float *partial, int *err, const WaitTest &wt, cudaStream_t stream) {
   if (g.ix <= 0 || g.iy <= 0 || g.iz <= 0) return cudaSuccess;
   switch (g.hw) {
-    case 1: return launch_hw<1>(g, in, out, div, partial, err, stream);
-    case 2: return launch_hw<2>(g, in, out, div, partial, err, stream);
-    case 3: return launch_hw<3>(g, in, out, div, partial, err, stream);
-    case 4: return launch_hw<4>(g, in, out, div, partial, err, stream);
-    case 5: return launch_hw<5>(g, in, out, div, partial, err, stream);
+    case 1: return launch_hw<1>(g, in, out, div, partial, err, wt, stream);
+    case 2: return launch_hw<2>(g, in, out, div, partial, err, wt, stream);
+    case 3: return launch_hw<3>(g, in, out, div, partial, err, wt, stream);
+    case 4: return launch_hw<4>(g, in, out, div, partial, err, wt, stream);
+    case 5: return launch_hw<5>(g, in, out, div, partial, err, wt, stream);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -31,6 +31,12 @@ struct SlabInputs {
 // non-zero code if a bounded wait gave up; the caller zeroes it beforehand. When the planner
 // splits the atlases into groups (to fill the persistent grid), `partial` must point to
 // fuse_tma_partial_bytes(g) bytes of device scratch; otherwise it may be null.
+// Testing hook for the bounded waits: when timeout_ns != 0, the first CTA withholds its first
+// copies, so its wait runs out after timeout_ns and the launch reports a timeout.
+struct WaitTest {
+  unsigned long long timeout_ns;
+};
+
 size_t fuse_tma_partial_bytes(const Geometry &g);
 struct FusePlanInfo {
   int groups, tiles, ctas, rx, tz;
@@ -38,7 +44,7 @@ struct FusePlanInfo {
 };
 cudaError_t fuse_tma_plan(const Geometry &g, FusePlanInfo *info);
 cudaError_t launch_fuse_tma(const Geometry &g, const SlabInputs &in, float *out, double div,
-                            float *partial, int *err, cudaStream_t stream);
+                            float *partial, int *err, const WaitTest &wt, cudaStream_t stream);
 
 // dst[r*pitch + c] = src[r*ny + c] for r < rows, c < ny.
 cudaError_t launch_pitch_copy(const float *src, float *dst, long long rows, int ny, int pitch,
