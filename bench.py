@@ -376,6 +376,76 @@ def run_b200_arm(args) -> None:
         print(json.dumps(line))
 
 
+def config3_specs(n: int = 16, seed: int = 3) -> list[tuple[int, int, int, int, int]]:
+    """Config 3: subjects of uneven size (x, y in 96..222, z in 64..112), 5..20 atlases, NH in
+    {7, 9, 11}, drawn from a seeded generator: (nx, ny, nz, num_atlas, nh)."""
+    rng = np.random.default_rng(seed)
+    return [(int(rng.integers(96, 223)), int(rng.integers(96, 223)), int(rng.integers(64, 113)),
+             int(rng.integers(5, 21)), int(rng.choice([7, 9, 11]))) for _ in range(n)]
+
+
+def run_batch_arm(args) -> None:
+    """Config 3: all subjects in one persistent launch captured in a CUDA graph, tile set chosen
+    by the autotuner; one step = one graph replay over every subject."""
+    import tempfile
+
+    import torch
+
+    import pseudoctimaging_b200 as pct
+
+    dev = torch.device("cuda", 0)
+    specs = config3_specs(args.batch_subjects)
+    subs, keep = [], []
+    nvox = cand = 0
+    for i, (nx, ny, nz, num, nh) in enumerate(specs):
+        s = pct.synth_subject(nx, ny, nz, num, n_blobs=N_BLOBS, seed=100 + i)
+        lab = pct.normalize_labels(s.atlas_ct)
+        d = [torch.from_numpy(x).to(dev) for x in (s.img, s.atlas_mri, lab)]
+        out = torch.zeros_like(d[0])
+        keep.append((d, out))
+        subs.append(pct.SubjectDesc(img=d[0].data_ptr(), atlas=d[1].data_ptr(),
+                                    atlas_label=d[2].data_ptr(), out=out.data_ptr(), nx=nx, ny=ny,
+                                    nz=nz, num_atlas=num, nh=nh, div=pct.div_from(SIGMA, BETA)))
+        nvox += nx * ny * nz
+        cand += candidates(nx, ny, nz, num, nh)
+        del s
+    h = pct.Handle(0)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    cache = os.path.join(tempfile.gettempdir(), "pct_b200_tune.jsonl")
+    chosen, tune_ms = h.autotune(subs, cache)
+    g = h.batch_graph(subs, stream.cuda_stream)
+    for _ in range(args.warmup):
+        g.launch(stream.cuda_stream)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            g.launch(stream.cuda_stream)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    g.status(stream.cuda_stream)
+    ms = ev0.elapsed_time(ev1) / args.steps
+    clocks = clk.summary()
+    line = {
+        "metric": f"pseudo-CT voxels/s, config 3 batch ({len(specs)} subjects, one persistent "
+                  "launch in a CUDA graph)",
+        "value": nvox / (ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator, config 3)",
+        "config": {"workload": "config 3 batch", "subjects": specs,
+                   "voxels": nvox, "candidates": cand, "tile_set": chosen,
+                   "autotune_ms_per_set": tune_ms},
+        "candidates_per_s": cand / (ms / 1e3),
+        "gpu_launches": args.steps * 1,
+        "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+    }
+    g.close()
+    h.close()
+    print(json.dumps(line))
+
+
 def main() -> None:
     global NZ, NH, METRIC
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
@@ -383,6 +453,9 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--workload", choices=["single", "batch"], default="single",
+                    help="single: config 1 subject (the metric); batch: config 3 subjects")
+    ap.add_argument("--batch-subjects", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-pointer end-to-end leg")
     ap.add_argument("--nh", type=int, default=NH, choices=[3, 5, 7, 9, 11],
@@ -399,6 +472,8 @@ def main() -> None:
     METRIC = f"pseudo-CT voxels/s at {NX}x{NY}x{NZ}, 10 atlases, NH={NH}"
     if args.impl == "reference":
         run_reference_arm(args)
+    elif args.workload == "batch":
+        run_batch_arm(args)
     else:
         run_b200_arm(args)
 

@@ -125,6 +125,51 @@ typedef struct pct_plan {
 } pct_plan;
 int pct_query_plan(int device, int nx, int ny, int nz, int num_atlas, int nh, pct_plan *plan);
 
+/*
+ * Batched form (EXEC_CHOICE 8): many subjects of uneven size, atlas count and NH in one
+ * persistent kernel launch. Each subject's buffers are DEVICE buffers in the reference layout
+ * (labels already normalised); only interior voxels of `out` are written. NH must be 7, 9 or 11.
+ * The reference processes one subject per call (MultiPatchBasedSegmentationGpu); this has no
+ * direct counterpart there.
+ */
+typedef struct pct_subject {
+  const float *img;          /* [nz][nx][ny] */
+  const float *atlas;        /* [num_atlas][nz][nx][ny] */
+  const float *atlas_label;  /* [num_atlas][nz][nx][ny], normalised */
+  float *out;                /* [nz][nx][ny] */
+  int nx, ny, nz, num_atlas, nh;
+  double div;
+} pct_subject;
+
+/* One persistent launch over all subjects, enqueued on `stream` (asynchronous; errors of the
+ * bounded waits surface through pct_device_status). */
+int pct_synthesize_batch(pct_handle *h, const pct_subject *subjects, int n, void *stream);
+
+/* The same batch captured once into a CUDA graph (pitched staging copies, status reset, the
+ * persistent kernel) for repeated execution on the same buffers: pct_batch_launch replays it on
+ * `stream`, pct_batch_status drains `stream` and reports PCT_OK or PCT_ERR_TIMEOUT.
+ * pct_batch_create drains `stream` (NULL: the device) before it captures on the handle's own
+ * stream. The batch owns its device buffers; it must be destroyed before its handle. */
+typedef struct pct_batch pct_batch;
+int pct_batch_create(pct_handle *h, const pct_subject *subjects, int n, void *stream,
+                     pct_batch **out);
+int pct_batch_launch(pct_batch *b, void *stream);
+int pct_batch_status(pct_batch *b, void *stream);
+int pct_batch_destroy(pct_batch *b);
+
+/*
+ * Register-tile sets compiled into the library (x rows and z planes per warp for each NH). The
+ * autotuner times every set on the given batch (one warm-up and two timed runs each), keeps the
+ * fastest on the handle (used by every later call on it) and appends the result to the JSON-lines
+ * cache `cache_path` (NULL: no cache) keyed by device name and batch shape; a cached entry is
+ * reused without timing (ms_per_set then reads -1). ms_per_set has pct_tile_sets() entries.
+ */
+int pct_tile_sets(void);
+int pct_set_tile_set(pct_handle *h, int set);
+int pct_get_tile_set(const pct_handle *h);
+int pct_autotune(pct_handle *h, const pct_subject *subjects, int n, const char *cache_path,
+                 double *ms_per_set, int *chosen);
+
 /* In-place CT -> label scale L' = 255*((L+1024)/4095) on a device buffer of n floats
  * (PatchBasedPseudoCT.cu:2009-2020, NewPatchedBrainPureC.cpp:1583-1593). */
 int pct_normalize_labels_device(pct_handle *h, float *d_label, size_t n, void *stream);

@@ -66,6 +66,14 @@ class SynthParams(ctypes.Structure):
                 ("max_disp", ctypes.c_float), ("seed", ctypes.c_uint64)]
 
 
+class SubjectDesc(ctypes.Structure):
+    """pct_subject: one subject of a batch (device pointers)."""
+    _fields_ = [("img", ctypes.c_void_p), ("atlas", ctypes.c_void_p),
+                ("atlas_label", ctypes.c_void_p), ("out", ctypes.c_void_p),
+                ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("num_atlas", ctypes.c_int), ("nh", ctypes.c_int), ("div", ctypes.c_double)]
+
+
 class Plan(ctypes.Structure):
     _fields_ = [("launches", ctypes.c_int), ("groups", ctypes.c_int), ("tiles", ctypes.c_int),
                 ("ctas", ctypes.c_int), ("tile_rows", ctypes.c_int),
@@ -93,6 +101,16 @@ SIGNATURES = {
     "pct_synthesize_device": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _D, _I, _P]),
     "pct_device_status": (_I, [_P, _P]),
     "pct_query_plan": (_I, [_I, _I, _I, _I, _I, _I, ctypes.POINTER(Plan)]),
+    "pct_synthesize_batch": (_I, [_P, ctypes.POINTER(SubjectDesc), _I, _P]),
+    "pct_batch_create": (_I, [_P, ctypes.POINTER(SubjectDesc), _I, _P, ctypes.POINTER(_P)]),
+    "pct_batch_launch": (_I, [_P, _P]),
+    "pct_batch_status": (_I, [_P, _P]),
+    "pct_batch_destroy": (_I, [_P]),
+    "pct_tile_sets": (_I, []),
+    "pct_set_tile_set": (_I, [_P, _I]),
+    "pct_get_tile_set": (_I, [_P]),
+    "pct_autotune": (_I, [_P, ctypes.POINTER(SubjectDesc), _I, ctypes.c_char_p,
+                          ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]),
     "pct_normalize_labels_device": (_I, [_P, _P, _SZ, _P]),
     "pct_regularize_device": (_I, [_P, _P, _I, _I, _I, _I, ctypes.POINTER(ctypes.c_int64), _P]),
     "pct_regularize_device_noalloc": (_I, [_P, _I, _I, _I, _I, ctypes.POINTER(ctypes.c_int64),
@@ -263,6 +281,40 @@ class Handle:
                                                stream or None), "pct_error_stats_device")
         return st.as_dict()
 
+    @staticmethod
+    def _subjects(subjects) -> "ctypes.Array":
+        arr = (SubjectDesc * len(subjects))()
+        for i, sd in enumerate(subjects):
+            arr[i] = sd if isinstance(sd, SubjectDesc) else SubjectDesc(**sd)
+        return arr
+
+    def synthesize_batch(self, subjects, stream: int = 0) -> None:
+        """One persistent launch over `subjects` (SubjectDesc or dicts of its fields)."""
+        arr = self._subjects(subjects)
+        self._check(lib.pct_synthesize_batch(self._h, arr, len(arr), stream or None),
+                    "pct_synthesize_batch")
+
+    def batch_graph(self, subjects, stream: int = 0) -> "BatchGraph":
+        return BatchGraph(self, subjects, stream)
+
+    def set_tile_set(self, k: int) -> None:
+        self._check(lib.pct_set_tile_set(self._h, k), "pct_set_tile_set")
+
+    @property
+    def tile_set(self) -> int:
+        return lib.pct_get_tile_set(self._h)
+
+    def autotune(self, subjects, cache_path=None) -> tuple[int, list[float]]:
+        """Times every compiled tile set on the batch; keeps the fastest on this handle."""
+        arr = self._subjects(subjects)
+        n = lib.pct_tile_sets()
+        ms = (ctypes.c_double * n)()
+        chosen = ctypes.c_int(-1)
+        path = str(cache_path).encode() if cache_path else None
+        self._check(lib.pct_autotune(self._h, arr, len(arr), path, ms, ctypes.byref(chosen)),
+                    "pct_autotune")
+        return chosen.value, list(ms)
+
     def ncc_device(self, d_a: int, d_b: int, nx: int, ny: int, nz: int, nh: int,
                    stream: int = 0) -> tuple[float, int]:
         v, n = ctypes.c_double(0.0), ctypes.c_int64(0)
@@ -286,6 +338,39 @@ class Handle:
                                          _ptr(out), nx, ny, nz, num, nh, float(sigma), float(beta),
                                          exec_choice, int(bool(regularize))), "pct_run_pipeline")
         return out
+
+
+class BatchGraph:
+    """A batch captured into a CUDA graph (pct_batch_create); launch() replays it."""
+
+    def __init__(self, handle: Handle, subjects, stream: int = 0):
+        self._handle = handle
+        self._arr = Handle._subjects(subjects)
+        b = _P()
+        handle._check(lib.pct_batch_create(handle._h, self._arr, len(self._arr), stream or None,
+                                           ctypes.byref(b)), "pct_batch_create")
+        self._b = b
+
+    def launch(self, stream: int = 0) -> None:
+        st = lib.pct_batch_launch(self._b, stream or None)
+        if st != PCT_OK:
+            raise PctError(st, "pct_batch_launch")
+
+    def status(self, stream: int = 0) -> None:
+        st = lib.pct_batch_status(self._b, stream or None)
+        if st != PCT_OK:
+            raise PctError(st, "pct_batch_status")
+
+    def close(self) -> None:
+        if getattr(self, "_b", None) and self._b.value:
+            lib.pct_batch_destroy(self._b)
+            self._b = _P()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 _default_handle: Handle | None = None
@@ -368,7 +453,7 @@ def synth_subject(nx: int, ny: int, nz: int, num_atlas: int, n_blobs: int = 20, 
 
 __all__ = [
     "EXEC_GM", "EXEC_GM2", "EXEC_SM", "EXEC_B200_FP32", "EXEC_TC_FP16", "EXEC_TC_BF16",
-    "EXEC_LEARNED", "EXEC_BATCHED", "Handle", "PctError", "ErrorStats", "SynthParams", "Subject",
+    "EXEC_LEARNED", "EXEC_BATCHED", "Handle", "BatchGraph", "SubjectDesc", "Plan", "PctError", "ErrorStats", "SynthParams", "Subject",
     "lib", "load_library", "div_from", "normalize_labels", "multi_patch_based_segmentation_gpu",
     "run_pipeline", "synth_subject", "default_handle", "LIB_PATH", "SIGNATURES",
 ]

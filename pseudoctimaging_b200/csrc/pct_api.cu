@@ -5,8 +5,10 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "pct_b200.h"
 #include "pct_internal.h"
@@ -31,6 +33,8 @@ struct pct_handle {
   DevBuf partial;  // per-atlas-group partial sums of the fusion kernel
   DevBuf stage;    // contiguous host->device staging before the pitched repack
   unsigned long long wait_test_ns = 0;  // one-shot testing hook, see pct_test_wait_timeout
+  int tile_set = 0;                     // register-tile set (pct_autotune / pct_set_tile_set)
+  DevBuf batch_stage, batch_meta;       // pct_synthesize_batch: pitched stacks, subject table
   std::string last_error;
 };
 
@@ -85,10 +89,12 @@ int check_choice(pct_handle *h, int exec_choice) {
     case PCT_EXEC_SM:
     case PCT_EXEC_B200_FP32:
       return PCT_OK;
+    case PCT_EXEC_BATCHED:
+      return fail(h, PCT_ERR_UNSUPPORTED,
+                  "exec_choice 8 (batched) runs through pct_synthesize_batch / pct_batch_create");
     case PCT_EXEC_TC_FP16:
     case PCT_EXEC_TC_BF16:
     case PCT_EXEC_LEARNED:
-    case PCT_EXEC_BATCHED:
       return fail(h, PCT_ERR_UNSUPPORTED,
                   "exec_choice " + std::to_string(exec_choice) + " is not available in this build");
     default:
@@ -125,13 +131,13 @@ int launch_fusion(pct_handle *h, const pct::Geometry &g, const pct::SlabInputs &
   int st = ensure(h, h->err, 16);
   if (st) return st;
   int *err = static_cast<int *>(h->err.ptr);
-  const size_t pbytes = pct::fuse_tma_partial_bytes(g);
+  const size_t pbytes = pct::fuse_tma_partial_bytes(g, h->tile_set);
   if (pbytes && (st = ensure(h, h->partial, pbytes))) return st;
   PCT_CUDA(h, cudaMemsetAsync(err, 0, sizeof(int), s));
   const pct::WaitTest wt{h->wait_test_ns};
   h->wait_test_ns = 0;
   PCT_CUDA(h, pct::launch_fuse_tma(g, in, d_out, div, static_cast<float *>(h->partial.ptr), err, wt,
-                                   s));
+                                   h->tile_set, s));
   return PCT_OK;
 }
 
@@ -335,7 +341,7 @@ int pct_destroy(pct_handle *h) {
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   for (DevBuf *b : {&h->img, &h->atlas, &h->label, &h->out, &h->scratch, &h->err, &h->partial,
-                    &h->stage})
+                    &h->stage, &h->batch_stage, &h->batch_meta})
     if (b->ptr) cudaFree(b->ptr);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -432,7 +438,7 @@ int pct_query_plan(int device, int nx, int ny, int nz, int num_atlas, int nh, pc
   cudaGetDevice(&prev);
   if (cudaSetDevice(device) != cudaSuccess) return PCT_ERR_NO_DEVICE;
   pct::FusePlanInfo info;
-  const cudaError_t e = pct::fuse_tma_plan(g, &info);
+  const cudaError_t e = pct::fuse_tma_plan(g, 0, &info);
   cudaSetDevice(prev);
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -615,6 +621,307 @@ int pct_error_stats_device(pct_handle *h, const float *d_a, const float *d_b, in
   stats->mae_hu = host.compared ? host.sum_abs / (double)host.compared : 0.0;
   stats->max_abs_hu = mabs;
   stats->max_rel = mrel;
+  return PCT_OK;
+}
+
+}  // extern "C"
+
+// ---- batched form, CUDA graph, autotuner ----------------------------------------------------
+
+struct pct_batch {
+  pct_handle *h = nullptr;
+  DevBuf stage, meta, err;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  size_t bytes = 0;
+};
+
+namespace {
+
+int check_subjects(pct_handle *h, const pct_subject *subs, int n, std::vector<pct::Geometry> &geo) {
+  if (!subs || n <= 0) return fail(h, PCT_ERR_INVALID_ARG, "no subjects");
+  geo.resize(n);
+  for (int i = 0; i < n; ++i) {
+    const pct_subject &s = subs[i];
+    if (!s.img || !s.atlas || !s.atlas_label || !s.out)
+      return fail(h, PCT_ERR_INVALID_ARG, "subject " + std::to_string(i) + ": null device pointer");
+    int st = check_shape(h, s.nx, s.ny, s.nz, s.num_atlas, s.nh, s.div, &geo[i]);
+    if (st) return st;
+    if (s.nh != 7 && s.nh != 9 && s.nh != 11)
+      return fail(h, PCT_ERR_UNSUPPORTED, "batched form: NH must be 7, 9 or 11");
+  }
+  return PCT_OK;
+}
+
+// Bytes of pitched staging the batch needs (subjects whose stacks are not TMA-ready).
+size_t batch_stage_bytes(const pct_subject *subs, int n) {
+  size_t total = 0;
+  for (int i = 0; i < n; ++i) {
+    const pct_subject &s = subs[i];
+    const bool ready = (s.ny % 4 == 0) && (reinterpret_cast<uintptr_t>(s.atlas) % 16 == 0) &&
+                       (reinterpret_cast<uintptr_t>(s.atlas_label) % 16 == 0);
+    if (!ready)
+      total += 2 * (size_t)s.num_atlas * s.nz * s.nx * pct::slab_pitch(s.ny) * sizeof(float) + 256;
+  }
+  return total;
+}
+
+// Enqueues the repacks of the subjects that need them into `stage` and fills `in`.
+int stage_batch(pct_handle *h, const pct_subject *subs, int n, const std::vector<pct::Geometry> &geo,
+                void *stage, std::vector<pct::BatchSubjectIn> &in, cudaStream_t s) {
+  in.resize(n);
+  unsigned char *p = static_cast<unsigned char *>(stage);
+  for (int i = 0; i < n; ++i) {
+    const pct_subject &sb = subs[i];
+    const bool ready = (sb.ny % 4 == 0) && (reinterpret_cast<uintptr_t>(sb.atlas) % 16 == 0) &&
+                       (reinterpret_cast<uintptr_t>(sb.atlas_label) % 16 == 0);
+    pct::SlabInputs si{sb.img, sb.atlas, sb.atlas_label, sb.ny};
+    if (!ready) {
+      const int pitch = pct::slab_pitch(sb.ny);
+      const long long rows = (long long)sb.num_atlas * sb.nz * sb.nx;
+      const size_t bytes = (size_t)rows * pitch * sizeof(float);
+      float *a = reinterpret_cast<float *>(p);
+      float *l = reinterpret_cast<float *>(p + bytes);
+      p += 2 * bytes + 256 - (2 * bytes) % 256;
+      PCT_CUDA(h, pct::launch_pitch_copy(sb.atlas, a, rows, sb.ny, pitch, s));
+      PCT_CUDA(h, pct::launch_pitch_copy(sb.atlas_label, l, rows, sb.ny, pitch, s));
+      si = pct::SlabInputs{sb.img, a, l, pitch};
+    }
+    in[i] = pct::BatchSubjectIn{geo[i], si, sb.out, sb.div};
+  }
+  return PCT_OK;
+}
+
+int run_batch_once(pct_handle *h, const pct_subject *subs, int n, int set, cudaStream_t s) {
+  std::vector<pct::Geometry> geo;
+  int st = check_subjects(h, subs, n, geo);
+  if (st) return st;
+  st = select_device(h);
+  if (st) return st;
+  if ((st = ensure(h, h->batch_stage, batch_stage_bytes(subs, n) + 256)) ||
+      (st = ensure(h, h->batch_meta, pct::batch_scratch_bytes(n))) || (st = ensure(h, h->err, 16)))
+    return st;
+  std::vector<pct::BatchSubjectIn> in;
+  if ((st = stage_batch(h, subs, n, geo, h->batch_stage.ptr, in, s))) return st;
+  int *err = static_cast<int *>(h->err.ptr);
+  PCT_CUDA(h, cudaMemsetAsync(err, 0, sizeof(int), s));
+  pct::BatchSetup setup;
+  PCT_CUDA(h, pct::prepare_batch(in.data(), n, set, h->batch_meta.ptr, err, s, &setup));
+  PCT_CUDA(h, pct::launch_prepared_batch(setup, s));
+  return PCT_OK;
+}
+
+std::string batch_signature(const pct_subject *subs, int n) {
+  std::vector<std::string> parts;
+  for (int i = 0; i < n; ++i)
+    parts.push_back(std::to_string(subs[i].nx) + "x" + std::to_string(subs[i].ny) + "x" +
+                    std::to_string(subs[i].nz) + "a" + std::to_string(subs[i].num_atlas) + "n" +
+                    std::to_string(subs[i].nh));
+  std::sort(parts.begin(), parts.end());
+  std::string sig;
+  for (auto &p : parts) sig += (sig.empty() ? "" : ",") + p;
+  return sig;
+}
+
+// Tuning cache: one JSON object per line {"device": ..., "signature": ..., "set": k, "ms": [...]}.
+bool cache_lookup(const char *path, const std::string &device, const std::string &sig, int *set) {
+  if (!path) return false;
+  FILE *f = fopen(path, "r");
+  if (!f) return false;
+  char line[1 << 16];
+  bool found = false;
+  const std::string kd = "\"device\": \"" + device + "\"", ks = "\"signature\": \"" + sig + "\"";
+  while (fgets(line, sizeof(line), f)) {
+    const std::string l(line);
+    if (l.find(kd) == std::string::npos || l.find(ks) == std::string::npos) continue;
+    const size_t p = l.find("\"set\": ");
+    if (p == std::string::npos) continue;
+    const int v = atoi(l.c_str() + p + 7);
+    if (v >= 0 && v < pct::kTileSets) {
+      *set = v;
+      found = true;  // the last matching line wins
+    }
+  }
+  fclose(f);
+  return found;
+}
+
+void cache_store(const char *path, const std::string &device, const std::string &sig, int set,
+                 const double *ms) {
+  if (!path) return;
+  FILE *f = fopen(path, "a");
+  if (!f) return;
+  fprintf(f, "{\"device\": \"%s\", \"signature\": \"%s\", \"set\": %d, \"ms\": [", device.c_str(),
+          sig.c_str(), set);
+  for (int k = 0; k < pct::kTileSets; ++k) fprintf(f, "%s%.4f", k ? ", " : "", ms[k]);
+  fprintf(f, "]}\n");
+  fclose(f);
+}
+
+}  // namespace
+
+extern "C" {
+
+int pct_tile_sets(void) { return pct::kTileSets; }
+
+int pct_set_tile_set(pct_handle *h, int set) {
+  if (!h) return PCT_ERR_INVALID_ARG;
+  if (set < 0 || set >= pct::kTileSets) return fail(h, PCT_ERR_INVALID_ARG, "no such tile set");
+  h->tile_set = set;
+  return PCT_OK;
+}
+
+int pct_get_tile_set(const pct_handle *h) { return h ? h->tile_set : PCT_ERR_INVALID_ARG; }
+
+int pct_synthesize_batch(pct_handle *h, const pct_subject *subjects, int n, void *stream) {
+  if (!h) return PCT_ERR_INVALID_ARG;
+  h->last_error.clear();
+  return run_batch_once(h, subjects, n, h->tile_set, static_cast<cudaStream_t>(stream));
+}
+
+int pct_batch_create(pct_handle *h, const pct_subject *subjects, int n, void *stream,
+                     pct_batch **out) {
+  if (!h || !out) return PCT_ERR_INVALID_ARG;
+  h->last_error.clear();
+  *out = nullptr;
+  std::vector<pct::Geometry> geo;
+  int st = check_subjects(h, subjects, n, geo);
+  if (st) return st;
+  if ((st = select_device(h))) return st;
+  pct_batch *b = new (std::nothrow) pct_batch();
+  if (!b) return PCT_ERR_OUT_OF_MEMORY;
+  b->h = h;
+  // Capture on the handle's own (non-blocking) stream: the legacy default stream cannot be
+  // captured, and the graph does not depend on the stream it was captured on. The caller's
+  // stream is drained first so the batch sees the inputs it has enqueued.
+  if (stream && cudaStreamSynchronize(static_cast<cudaStream_t>(stream)) != cudaSuccess) {
+    delete b;
+    return fail(h, PCT_ERR_CUDA, "cudaStreamSynchronize");
+  }
+  if (!stream) cudaDeviceSynchronize();
+  cudaStream_t s = h->stream;
+  auto cleanup = [&](int code) {
+    pct_batch_destroy(b);
+    return code;
+  };
+  // The batch owns its buffers, so the graph's pointers stay valid whatever the handle does next.
+  if ((st = ensure(h, b->stage, batch_stage_bytes(subjects, n) + 256)) ||
+      (st = ensure(h, b->meta, pct::batch_scratch_bytes(n))) || (st = ensure(h, b->err, 16)))
+    return cleanup(st);
+  b->bytes = b->stage.bytes + b->meta.bytes + b->err.bytes;
+  std::vector<pct::BatchSubjectIn> in;
+  pct::BatchSetup setup;
+  // Subject table and tensor maps are uploaded once, before capture.
+  {
+    std::vector<pct::BatchSubjectIn> probe;
+    if ((st = stage_batch(h, subjects, n, geo, b->stage.ptr, probe, s))) return cleanup(st);
+    cudaError_t e = pct::prepare_batch(probe.data(), n, h->tile_set, b->meta.ptr,
+                                       static_cast<int *>(b->err.ptr), s, &setup);
+    if (e != cudaSuccess) return cleanup(cuda_fail(h, e, "prepare_batch"));
+  }
+  // Capture: repacks, status reset, the persistent kernel.
+  cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return cleanup(cuda_fail(h, e, "cudaStreamBeginCapture"));
+  st = stage_batch(h, subjects, n, geo, b->stage.ptr, in, s);
+  if (!st) {
+    e = cudaMemsetAsync(b->err.ptr, 0, sizeof(int), s);
+    if (e == cudaSuccess) e = pct::launch_prepared_batch(setup, s);
+  }
+  cudaGraph_t g = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(s, &g);
+  if (st) {
+    if (g) cudaGraphDestroy(g);
+    return cleanup(st);
+  }
+  if (e != cudaSuccess || ee != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return cleanup(cuda_fail(h, e != cudaSuccess ? e : ee, "batch capture"));
+  }
+  b->graph = g;
+  e = cudaGraphInstantiate(&b->exec, g, 0);
+  if (e != cudaSuccess) return cleanup(cuda_fail(h, e, "cudaGraphInstantiate"));
+  *out = b;
+  return PCT_OK;
+}
+
+int pct_batch_launch(pct_batch *b, void *stream) {
+  if (!b || !b->exec) return PCT_ERR_INVALID_ARG;
+  if (cudaSetDevice(b->h->device) != cudaSuccess) return PCT_ERR_CUDA;
+  const cudaError_t e = cudaGraphLaunch(b->exec, static_cast<cudaStream_t>(stream));
+  return e == cudaSuccess ? PCT_OK : cuda_fail(b->h, e, "cudaGraphLaunch");
+}
+
+int pct_batch_status(pct_batch *b, void *stream) {
+  if (!b) return PCT_ERR_INVALID_ARG;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int v = 0;
+  if (cudaMemcpyAsync(&v, b->err.ptr, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return PCT_ERR_CUDA;
+  return v ? PCT_ERR_TIMEOUT : PCT_OK;
+}
+
+int pct_batch_destroy(pct_batch *b) {
+  if (!b) return PCT_ERR_INVALID_ARG;
+  if (b->h) cudaSetDevice(b->h->device);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  for (DevBuf *d : {&b->stage, &b->meta, &b->err})
+    if (d->ptr) {
+      cudaFree(d->ptr);
+      if (b->h) b->h->allocated -= d->bytes;
+    }
+  delete b;
+  return PCT_OK;
+}
+
+int pct_autotune(pct_handle *h, const pct_subject *subjects, int n, const char *cache_path,
+                 double *ms_per_set, int *chosen) {
+  if (!h) return PCT_ERR_INVALID_ARG;
+  h->last_error.clear();
+  std::vector<pct::Geometry> geo;
+  int st = check_subjects(h, subjects, n, geo);
+  if (st) return st;
+  if ((st = select_device(h))) return st;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, h->device) != cudaSuccess) return PCT_ERR_CUDA;
+  const std::string device = prop.name, sig = batch_signature(subjects, n);
+  int set = 0;
+  if (cache_lookup(cache_path, device, sig, &set)) {
+    h->tile_set = set;
+    if (chosen) *chosen = set;
+    if (ms_per_set)
+      for (int k = 0; k < pct::kTileSets; ++k) ms_per_set[k] = -1.0;  // not re-measured
+    return PCT_OK;
+  }
+  cudaStream_t s = h->stream;
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+    return fail(h, PCT_ERR_CUDA, "cudaEventCreate");
+  double ms[pct::kTileSets];
+  int best = 0;
+  for (int k = 0; k < pct::kTileSets && !st; ++k) {
+    st = run_batch_once(h, subjects, n, k, s);  // warm-up
+    if (!st) cudaEventRecord(e0, s);
+    for (int r = 0; r < 2 && !st; ++r) st = run_batch_once(h, subjects, n, k, s);
+    if (!st) {
+      cudaEventRecord(e1, s);
+      cudaEventSynchronize(e1);
+      float t = 0;
+      cudaEventElapsedTime(&t, e0, e1);
+      ms[k] = t / 2.0;
+      if (ms[k] < ms[best]) best = k;
+      st = read_device_status(h, s);
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st) return st;
+  h->tile_set = best;
+  if (chosen) *chosen = best;
+  if (ms_per_set)
+    for (int k = 0; k < pct::kTileSets; ++k) ms_per_set[k] = ms[k];
+  cache_store(cache_path, device, sig, best, ms);
   return PCT_OK;
 }
 

@@ -31,7 +31,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <cmath>
+#include <vector>
 
 #include "pct_internal.h"
 
@@ -153,17 +155,23 @@ struct Cfg {
   static constexpr int OFF = NCH * NQ - NS;       // virtual steps skipped in the first period
 };
 
-struct TmaParams {
-  const float *img;
-  float *out;
-  int nx, ny, nz, num;
-  int nxy;
-  float neg_k;  // -log2(e)/div
-  int tiles_y, tiles_x, tiles_z, ntiles;
-  int groups;         // atlas groups per tile; items = groups * ntiles (group-major)
-  int atlases_per_group;
+// One subject as the kernels see it.
+struct SubjectView {
+  const float *img;   // input MRI, reference layout
+  float *out;         // fused output, reference layout (interior written)
   float *partial;     // groups > 1: [groups][2][nvox] partial (product, sum_weight) sums
+  const CUtensorMap *tmA, *tmL;  // atlas MRI / CT slab maps (param or global space)
+  int nx, ny, nz, nxy;
   long long nvox;
+  float neg_k;        // -log2(e)/div
+  int tiles_y, tiles_x, ntiles;
+  int groups, atlases_per_group;  // items = groups * ntiles (group-major)
+  int hw;             // half window of this subject (batched kernel dispatch)
+  int item_begin;     // first global item of this subject (batched kernel)
+};
+
+struct TmaParams {
+  SubjectView sv;
   int *err;           // device status word (0 = ok)
   unsigned long long timeout_ns;
   int withhold_cta;   // testing hook: this CTA withholds its first copies (-1 = none)
@@ -253,173 +261,251 @@ __device__ __forceinline__ void sweep_dw(const float2 (&In)[TZ + 2][RX + 2], flo
   }
 }
 
+// Pipeline state of one CTA, carried across its work items.
+struct Pipe {
+  uint32_t base;              // 128-byte aligned start of the dynamic shared memory
+  uint32_t gstep;             // steps taken: barrier gstep&1, phase (gstep>>1)&1
+  bool armed_next;            // thread 0: a prefetch is in flight on barrier (gstep+1)&1
+  volatile int *abort_flag;
+};
+
+// Processes work item `item` (tile x atlas group) of subject `sv` with register tile (RX, TZ).
+// Returns false when a bounded wait gave up (the CTA must stop).
 template <int HW, int RX, int TZ>
-__global__ void __launch_bounds__(kThreads, 1)
-    fuse_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmL,
-                    const TmaParams p) {
+__device__ __forceinline__ bool run_item(const SubjectView &sv, int item, Pipe &pp, int *err,
+                                         unsigned long long timeout_ns, int withhold_cta) {
   using C = Cfg<HW, RX, TZ>;
   constexpr int NQ = C::NQ, NR = C::NR, NS = C::NS;
-  extern __shared__ unsigned char smem_raw[];
-  const uint32_t base = (smem_u32(smem_raw) + 127u) & ~127u;
-  const uint32_t bar0 = base, bar1 = base + 8;
-  volatile int *abort_flag =
-      reinterpret_cast<volatile int *>(smem_raw + (base + 16 - smem_u32(smem_raw)));
-  const uint32_t ringA = base + 128;
+  const uint32_t bar0 = pp.base, bar1 = pp.base + 8;
+  const uint32_t ringA = pp.base + 128;
   const uint32_t ringL = ringA + C::RA * C::SLOT_A;
-
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  if (tid == 0) {
-    mbar_init(bar0, 1);
-    mbar_init(bar1, 1);
-    *abort_flag = 0;
+  const int lo = HW + 1;
+  const float2 negk2 = make_float2(sv.neg_k, sv.neg_k);
+  const int T = sv.atlases_per_group * NS;  // du steps per item (atlas-major)
+
+  const int grp = item / sv.ntiles;
+  const int a_first = grp * sv.atlases_per_group;
+  int t = item - grp * sv.ntiles;
+  const int ty = t % sv.tiles_y;
+  t /= sv.tiles_y;
+  const int txc = t % sv.tiles_x;
+  const int tz = t / sv.tiles_x;
+  const int y0 = lo + ty * kOutY, X0 = lo + txc * C::XC, z0 = lo + tz * (2 * TZ);
+  const int y = y0 - 1 + lane;
+  const int yb = y0 - 1 - HW;      // first y of the slab (>= 0)
+  const int e = yb & 3;
+  const int ybox = yb - e;         // TMA start, 16-byte aligned
+  const int xw = X0 + warp * RX;   // this warp's first output row
+  const int xA = X0 - 1 - HW, zA = z0 - 1 - HW;  // MRI slab origin (row k=0)
+  const int xL = X0 - HW, zL = z0 - HW;          // CT slab origin
+  const uint32_t lane_off = (uint32_t)(lane + HW + e) * 4u;
+
+  // Input patch values (negated: D = (A + In)^2), zero outside the volume.
+  float2 In[NQ][NR];
+#pragma unroll
+  for (int q = 0; q < NQ; ++q)
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      float v[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int zz = z0 + h * TZ - 1 + q, xx = xw - 1 + r;
+        v[h] = (zz < sv.nz && xx < sv.nx && y < sv.ny)
+                   ? -__ldg(sv.img + (long long)zz * sv.nxy + (long long)xx * sv.ny + y)
+                   : 0.f;
+      }
+      In[q][r] = make_float2(v[0], v[1]);
+    }
+  float2 P[TZ][RX], W[TZ][RX];
+#pragma unroll
+  for (int q = 0; q < TZ; ++q)
+#pragma unroll
+    for (int r = 0; r < RX; ++r) {
+      P[q][r] = make_float2(0.f, 0.f);
+      W[q][r] = make_float2(0.f, 0.f);
+    }
+
+  for (int i = 0; i < T; ++i, ++pp.gstep) {
+    const int ai = i / NS, j = i - ai * NS;
+    const int a = a_first + ai;
+    __syncthreads();  // every warp is done with step i-1: its ring rows may be refilled
+    if (*pp.abort_flag) return false;
+    const uint32_t gstep = pp.gstep;
+    if (tid == 0) {
+      fence_proxy_async_smem();
+      // Testing hook: withhold the first window of this CTA so that the wait below runs out.
+      const bool withhold = (int)blockIdx.x == withhold_cta && gstep == 0;
+      if (j == 0 && !withhold) {  // atlas start: the whole window for this step
+        const uint32_t b = (gstep & 1) ? bar1 : bar0;
+        mbar_arrive_expect_tx(b, (C::XC + 2) * C::ROW_A + C::XC * C::ROW_L);
+        for (int k = 0; k < C::XC + 2; ++k)
+          tma_load_4d(ringA + (k % C::RA) * C::SLOT_A, sv.tmA, b, ybox, xA + k, zA, a);
+        for (int k = 0; k < C::XC; ++k)
+          tma_load_4d(ringL + (k % C::RL) * C::SLOT_L, sv.tmL, b, ybox, xL + k, zL, a);
+      }
+      pp.armed_next = false;
+      if (j + 1 < NS) {  // prefetch the one new row of each ring for step i+1
+        const uint32_t b = ((gstep + 1) & 1) ? bar1 : bar0;
+        mbar_arrive_expect_tx(b, C::ROW_A + C::ROW_L);
+        const int ka = j + C::XC + 2, kl = j + C::XC;
+        tma_load_4d(ringA + (ka % C::RA) * C::SLOT_A, sv.tmA, b, ybox, xA + ka, zA, a);
+        tma_load_4d(ringL + (kl % C::RL) * C::SLOT_L, sv.tmL, b, ybox, xL + kl, zL, a);
+        pp.armed_next = true;
+      }
+    }
+    const bool ok = mbar_wait_bounded((gstep & 1) ? bar1 : bar0, (gstep >> 1) & 1, timeout_ns);
+    if (!__all_sync(0xffffffffu, ok)) {
+      if (lane == 0) {
+        atomicExch(err, 1);
+        *pp.abort_flag = 1;
+      }
+      continue;  // the next CTA barrier sees the flag
+    }
+    // Ring rows of this thread for step (a, du = j - HW).
+    uint32_t rowA[NR], rowL[RX];
+#pragma unroll
+    for (int r = 0; r < NR; ++r)
+      rowA[r] = ringA + (uint32_t)((warp * RX + r + j) % C::RA) * C::SLOT_A + lane_off;
+#pragma unroll
+    for (int r = 0; r < RX; ++r)
+      rowL[r] = ringL + (uint32_t)((warp * RX + r + j) % C::RL) * C::SLOT_L + lane_off;
+#pragma unroll 1
+    for (int dv = -HW; dv <= HW; ++dv) {
+      uint32_t ra[NR], rl[RX];
+#pragma unroll
+      for (int r = 0; r < NR; ++r) ra[r] = rowA[r] + (uint32_t)(dv * 4);
+#pragma unroll
+      for (int r = 0; r < RX; ++r) rl[r] = rowL[r] + (uint32_t)(dv * 4);
+      sweep_dw<HW, RX, TZ>(In, P, W, ra, rl, negk2);
+    }
+  }
+  __syncthreads();  // a timeout in the item's last step is seen here
+  if (*pp.abort_flag) return false;
+
+  if (lane >= 1 && lane <= kOutY && y < sv.ny - lo) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+      for (int q = 0; q < TZ; ++q) {
+        const int z = z0 + h * TZ + q;
+        if (z >= sv.nz - lo) continue;
+#pragma unroll
+        for (int r = 0; r < RX; ++r) {
+          const int x = xw + r;
+          if (x >= sv.nx - lo) continue;
+          const float pr = h ? P[q][r].y : P[q][r].x;
+          const float sw = h ? W[q][r].y : W[q][r].x;
+          const long long v = (long long)z * sv.nxy + (long long)x * sv.ny + y;
+          if (sv.groups == 1) {
+            sv.out[v] = fuse_result(pr, sw);
+          } else {
+            sv.partial[(2LL * grp) * sv.nvox + v] = pr;
+            sv.partial[(2LL * grp + 1) * sv.nvox + v] = sw;
+          }
+        }
+      }
+  }
+  return true;
+}
+
+__device__ __forceinline__ Pipe pipe_init(unsigned char *smem_raw) {
+  Pipe pp;
+  pp.base = (smem_u32(smem_raw) + 127u) & ~127u;
+  pp.gstep = 0;
+  pp.armed_next = false;
+  pp.abort_flag =
+      reinterpret_cast<volatile int *>(smem_raw + (pp.base + 16 - smem_u32(smem_raw)));
+  if (threadIdx.x == 0) {
+    mbar_init(pp.base, 1);
+    mbar_init(pp.base + 8, 1);
+    *pp.abort_flag = 0;
     fence_mbarrier_init();
   }
   __syncthreads();
+  return pp;
+}
 
-  const int lo = HW + 1;
-  const float2 negk2 = make_float2(p.neg_k, p.neg_k);
-  const int T = p.atlases_per_group * NS;  // du steps per item (atlas-major)
-  uint32_t gstep = 0;         // steps taken by this CTA: barrier gstep&1, phase (gstep>>1)&1
-  bool aborted = false;
-  bool armed_next = false;    // thread 0: a prefetch is in flight on barrier (gstep+1)&1
+// After an abort, let this CTA's own outstanding copies land (bounded) before exiting: those of
+// the step whose wait timed out (gstep-1) and the prefetch armed during it, if any.
+__device__ __forceinline__ void pipe_drain(const Pipe &pp, unsigned long long timeout_ns) {
+  if (threadIdx.x != 0) return;
+  const uint32_t bar0 = pp.base, bar1 = pp.base + 8;
+  const uint32_t s = pp.gstep - 1;
+  mbar_wait_bounded((s & 1) ? bar1 : bar0, (s >> 1) & 1, timeout_ns);
+  if (pp.armed_next)
+    mbar_wait_bounded((pp.gstep & 1) ? bar1 : bar0, (pp.gstep >> 1) & 1, timeout_ns);
+}
 
-  const int nitems = p.ntiles * p.groups;
-  for (int item = blockIdx.x; item < nitems && !aborted; item += gridDim.x) {
-    const int grp = item / p.ntiles;
-    const int a_first = grp * p.atlases_per_group;
-    int t = item - grp * p.ntiles;
-    const int ty = t % p.tiles_y;
-    t /= p.tiles_y;
-    const int txc = t % p.tiles_x;
-    const int tz = t / p.tiles_x;
-    const int y0 = lo + ty * kOutY, X0 = lo + txc * C::XC, z0 = lo + tz * (2 * TZ);
-    const int y = y0 - 1 + lane;
-    const int yb = y0 - 1 - HW;      // first y of the slab (>= 0)
-    const int e = yb & 3;
-    const int ybox = yb - e;         // TMA start, 16-byte aligned
-    const int xw = X0 + warp * RX;   // this warp's first output row
-    const int xA = X0 - 1 - HW, zA = z0 - 1 - HW;  // MRI slab origin (row k=0)
-    const int xL = X0 - HW, zL = z0 - HW;          // CT slab origin
-    const uint32_t lane_off = (uint32_t)(lane + HW + e) * 4u;
-
-    // Input patch values (negated: D = (A + In)^2), zero outside the volume.
-    float2 In[NQ][NR];
-#pragma unroll
-    for (int q = 0; q < NQ; ++q)
-#pragma unroll
-      for (int r = 0; r < NR; ++r) {
-        float v[2];
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int zz = z0 + h * TZ - 1 + q, xx = xw - 1 + r;
-          v[h] = (zz < p.nz && xx < p.nx && y < p.ny)
-                     ? -__ldg(p.img + (long long)zz * p.nxy + (long long)xx * p.ny + y)
-                     : 0.f;
-        }
-        In[q][r] = make_float2(v[0], v[1]);
-      }
-    float2 P[TZ][RX], W[TZ][RX];
-#pragma unroll
-    for (int q = 0; q < TZ; ++q)
-#pragma unroll
-      for (int r = 0; r < RX; ++r) {
-        P[q][r] = make_float2(0.f, 0.f);
-        W[q][r] = make_float2(0.f, 0.f);
-      }
-
-    for (int i = 0; i < T; ++i, ++gstep) {
-      const int ai = i / NS, j = i - ai * NS;
-      const int a = a_first + ai;
-      __syncthreads();  // every warp is done with step i-1: its ring rows may be refilled
-      if (*abort_flag) {
-        aborted = true;
-        break;
-      }
-      if (tid == 0) {
-        fence_proxy_async_smem();
-        // Testing hook: withhold the first window of this CTA so that the wait below runs out.
-        const bool withhold = (int)blockIdx.x == p.withhold_cta && gstep == 0;
-        if (j == 0 && !withhold) {  // atlas start: the whole window for this step
-          const uint32_t b = (gstep & 1) ? bar1 : bar0;
-          mbar_arrive_expect_tx(b, (C::XC + 2) * C::ROW_A + C::XC * C::ROW_L);
-          for (int k = 0; k < C::XC + 2; ++k)
-            tma_load_4d(ringA + (k % C::RA) * C::SLOT_A, &tmA, b, ybox, xA + k, zA, a);
-          for (int k = 0; k < C::XC; ++k)
-            tma_load_4d(ringL + (k % C::RL) * C::SLOT_L, &tmL, b, ybox, xL + k, zL, a);
-        }
-        armed_next = false;
-        if (j + 1 < NS) {  // prefetch the one new row of each ring for step i+1
-          const uint32_t b = ((gstep + 1) & 1) ? bar1 : bar0;
-          mbar_arrive_expect_tx(b, C::ROW_A + C::ROW_L);
-          const int ka = j + C::XC + 2, kl = j + C::XC;
-          tma_load_4d(ringA + (ka % C::RA) * C::SLOT_A, &tmA, b, ybox, xA + ka, zA, a);
-          tma_load_4d(ringL + (kl % C::RL) * C::SLOT_L, &tmL, b, ybox, xL + kl, zL, a);
-          armed_next = true;
-        }
-      }
-      const bool ok = mbar_wait_bounded((gstep & 1) ? bar1 : bar0, (gstep >> 1) & 1, p.timeout_ns);
-      if (!__all_sync(0xffffffffu, ok)) {
-        if (lane == 0) {
-          atomicExch(p.err, 1);
-          *abort_flag = 1;
-        }
-        continue;  // the next CTA barrier sees the flag
-      }
-      // Ring rows of this thread for step (a, du = j - HW).
-      uint32_t rowA[NR], rowL[RX];
-#pragma unroll
-      for (int r = 0; r < NR; ++r)
-        rowA[r] = ringA + (uint32_t)((warp * RX + r + j) % C::RA) * C::SLOT_A + lane_off;
-#pragma unroll
-      for (int r = 0; r < RX; ++r)
-        rowL[r] = ringL + (uint32_t)((warp * RX + r + j) % C::RL) * C::SLOT_L + lane_off;
-#pragma unroll 1
-      for (int dv = -HW; dv <= HW; ++dv) {
-        uint32_t ra[NR], rl[RX];
-#pragma unroll
-        for (int r = 0; r < NR; ++r) ra[r] = rowA[r] + (uint32_t)(dv * 4);
-#pragma unroll
-        for (int r = 0; r < RX; ++r) rl[r] = rowL[r] + (uint32_t)(dv * 4);
-        sweep_dw<HW, RX, TZ>(In, P, W, ra, rl, negk2);
-      }
-    }
-    if (aborted) break;
-    __syncthreads();  // a timeout in the tile's last step is seen here
-    if (*abort_flag) {
-      aborted = true;
-      break;
-    }
-
-    if (lane >= 1 && lane <= kOutY && y < p.ny - lo) {
-#pragma unroll
-      for (int h = 0; h < 2; ++h)
-#pragma unroll
-        for (int q = 0; q < TZ; ++q) {
-          const int z = z0 + h * TZ + q;
-          if (z >= p.nz - lo) continue;
-#pragma unroll
-          for (int r = 0; r < RX; ++r) {
-            const int x = xw + r;
-            if (x >= p.nx - lo) continue;
-            const float pr = h ? P[q][r].y : P[q][r].x;
-            const float sw = h ? W[q][r].y : W[q][r].x;
-            const long long v = (long long)z * p.nxy + (long long)x * p.ny + y;
-            if (p.groups == 1) {
-              p.out[v] = fuse_result(pr, sw);
-            } else {
-              p.partial[(2LL * grp) * p.nvox + v] = pr;
-              p.partial[(2LL * grp + 1) * p.nvox + v] = sw;
-            }
-          }
-        }
+// One subject, persistent over its work items.
+template <int HW, int RX, int TZ>
+__global__ void __launch_bounds__(kThreads, 1)
+    fuse_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmL,
+                    TmaParams p) {
+  extern __shared__ unsigned char smem_raw[];
+  Pipe pp = pipe_init(smem_raw);
+  p.sv.tmA = &tmA;
+  p.sv.tmL = &tmL;
+  const int nitems = p.sv.ntiles * p.sv.groups;
+  for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+    if (!run_item<HW, RX, TZ>(p.sv, item, pp, p.err, p.timeout_ns, p.withhold_cta)) {
+      pipe_drain(pp, p.timeout_ns);
+      return;
     }
   }
-  // After an abort, let this CTA's own outstanding copies land (bounded) before exiting: those
-  // of the step whose wait timed out (gstep-1) and the prefetch armed during it, if any.
-  if (aborted && tid == 0) {
-    const uint32_t s = gstep - 1;
-    mbar_wait_bounded((s & 1) ? bar1 : bar0, (s >> 1) & 1, p.timeout_ns);
-    if (armed_next) mbar_wait_bounded((gstep & 1) ? bar1 : bar0, (gstep >> 1) & 1, p.timeout_ns);
+}
+
+// Register tiles (x rows RX, z planes per half TZ) by half window, in two sets the autotuner
+// chooses between. Each compiles to at most 255 registers without spilling more than a few bytes.
+template <int SET, int HW> struct TileOf { static constexpr int RX = 3, TZ = 4; };
+template <> struct TileOf<0, 2> { static constexpr int RX = 3, TZ = 3; };
+template <> struct TileOf<0, 1> { static constexpr int RX = 4, TZ = 2; };
+template <> struct TileOf<1, 5> { static constexpr int RX = 3, TZ = 3; };
+template <> struct TileOf<1, 4> { static constexpr int RX = 4, TZ = 2; };
+template <> struct TileOf<1, 3> { static constexpr int RX = 4, TZ = 2; };
+template <> struct TileOf<1, 2> { static constexpr int RX = 3, TZ = 3; };
+template <> struct TileOf<1, 1> { static constexpr int RX = 4, TZ = 2; };
+template <int SET, int HW>
+constexpr int smem_of() {
+  return Cfg<HW, TileOf<SET, HW>::RX, TileOf<SET, HW>::TZ>::SMEM;
+}
+template <int SET>
+constexpr int batch_smem() {
+  return smem_of<SET, 5>() > smem_of<SET, 4>()
+             ? (smem_of<SET, 5>() > smem_of<SET, 3>() ? smem_of<SET, 5>() : smem_of<SET, 3>())
+             : (smem_of<SET, 4>() > smem_of<SET, 3>() ? smem_of<SET, 4>() : smem_of<SET, 3>());
+}
+
+struct BatchParams {
+  const SubjectView *subjects;  // device array, sorted by half window (largest first)
+  int nsub;
+  int total_items;
+  int *err;
+  unsigned long long timeout_ns;
+};
+
+// Many subjects (uneven sizes, atlas counts and NH in {7, 9, 11}), one persistent launch: work
+// items of all subjects are numbered consecutively; each CTA walks the list with a grid stride
+// and dispatches every item to the tile code of its subject's window.
+template <int SET>
+__global__ void __launch_bounds__(kThreads, 1) fuse_batch_kernel(const BatchParams bp) {
+  extern __shared__ unsigned char smem_raw[];
+  Pipe pp = pipe_init(smem_raw);
+  int s = 0;
+  for (int item = blockIdx.x; item < bp.total_items; item += gridDim.x) {
+    while (s + 1 < bp.nsub && bp.subjects[s + 1].item_begin <= item) ++s;
+    const SubjectView &sv = bp.subjects[s];
+    const int local = item - sv.item_begin;
+    bool ok = true;
+    switch (sv.hw) {
+      case 5: ok = run_item<5, TileOf<SET, 5>::RX, TileOf<SET, 5>::TZ>(sv, local, pp, bp.err, bp.timeout_ns, -1); break;
+      case 4: ok = run_item<4, TileOf<SET, 4>::RX, TileOf<SET, 4>::TZ>(sv, local, pp, bp.err, bp.timeout_ns, -1); break;
+      default: ok = run_item<3, TileOf<SET, 3>::RX, TileOf<SET, 3>::TZ>(sv, local, pp, bp.err, bp.timeout_ns, -1); break;
+    }
+    if (!ok) {
+      pipe_drain(pp, bp.timeout_ns);
+      return;
+    }
   }
 }
 
@@ -487,12 +573,6 @@ cudaError_t launch_combine_groups(const Geometry &g, const float *partial, int g
   return cudaGetLastError();
 }
 
-// Register tile (x rows RX, z planes per half TZ) per window size: the largest that compiles to
-// at most 255 registers without spilling.
-template <int HW> struct Shape { static constexpr int RX = 3, TZ = 4; };
-template <> struct Shape<2> { static constexpr int RX = 3, TZ = 3; };
-template <> struct Shape<1> { static constexpr int RX = 4, TZ = 2; };
-
 // Picks the number of atlas groups (a divisor of num) so that the work items fill the
 // persistent grid's rounds: the first group count reaching 97% round occupancy, else the best.
 int choose_groups(int ntiles, int num, int slots) {
@@ -511,45 +591,72 @@ int choose_groups(int ntiles, int num, int slots) {
   return best;
 }
 
-template <int HW>
+int sm_count() {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms;
+}
+
 struct Plan {
-  int blocks, groups, ntiles, tiles_y, tiles_x, tiles_z;
+  int blocks, groups, ntiles, tiles_y, tiles_x, tiles_z, rx, tz;
 };
 
-template <int HW>
-cudaError_t plan_hw(const Geometry &g, Plan<HW> *pl) {
-  constexpr int RX = Shape<HW>::RX, TZ = Shape<HW>::TZ;
+template <int SET, int HW>
+cudaError_t plan_hw(const Geometry &g, Plan *pl) {
+  constexpr int RX = TileOf<SET, HW>::RX, TZ = TileOf<SET, HW>::TZ;
   using C = Cfg<HW, RX, TZ>;
   auto kern = fuse_tma_kernel<HW, RX, TZ>;
   cudaError_t e;
   if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM)) !=
       cudaSuccess)
     return e;
-  int dev = 0, sms = 148, per_sm = 1;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int per_sm = 1;
   if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, C::SMEM)) !=
       cudaSuccess)
     return e;
   if (per_sm < 1) return cudaErrorLaunchOutOfResources;
+  pl->rx = RX;
+  pl->tz = TZ;
   pl->tiles_y = (g.iy + kOutY - 1) / kOutY;
   pl->tiles_x = (g.ix + C::XC - 1) / C::XC;
   pl->tiles_z = (g.iz + 2 * TZ - 1) / (2 * TZ);
   pl->ntiles = pl->tiles_y * pl->tiles_x * pl->tiles_z;
-  const int slots = sms * per_sm;
+  const int slots = sm_count() * per_sm;
   pl->groups = choose_groups(pl->ntiles, g.num, slots);
   const long long items = (long long)pl->ntiles * pl->groups;
   pl->blocks = (int)(items < slots ? items : slots);
   return cudaSuccess;
 }
 
-template <int HW>
+SubjectView subject_view(const Geometry &g, const SlabInputs &in, float *out, double div,
+                         float *partial, const Plan &pl) {
+  SubjectView sv{};
+  sv.img = in.img;
+  sv.out = out;
+  sv.partial = partial;
+  sv.nx = g.nx;
+  sv.ny = g.ny;
+  sv.nz = g.nz;
+  sv.nxy = g.nx * g.ny;
+  sv.nvox = g.nvox();
+  sv.neg_k = (float)(-1.4426950408889634 / div);
+  sv.tiles_y = pl.tiles_y;
+  sv.tiles_x = pl.tiles_x;
+  sv.ntiles = pl.ntiles;
+  sv.groups = pl.groups;
+  sv.atlases_per_group = g.num / pl.groups;
+  sv.hw = g.hw;
+  return sv;
+}
+
+template <int SET, int HW>
 cudaError_t launch_hw(const Geometry &g, const SlabInputs &in, float *out, double div,
                       float *partial, int *err, const WaitTest &wt, cudaStream_t stream) {
-  constexpr int RX = Shape<HW>::RX, TZ = Shape<HW>::TZ;
+  constexpr int RX = TileOf<SET, HW>::RX, TZ = TileOf<SET, HW>::TZ;
   using C = Cfg<HW, RX, TZ>;
-  Plan<HW> pl;
-  cudaError_t e = plan_hw<HW>(g, &pl);
+  Plan pl;
+  cudaError_t e = plan_hw<SET, HW>(g, &pl);
   if (e != cudaSuccess) return e;
   if (pl.groups > 1 && !partial) return cudaErrorInvalidValue;
   CUtensorMap tmA, tmL;
@@ -560,22 +667,7 @@ cudaError_t launch_hw(const Geometry &g, const SlabInputs &in, float *out, doubl
       cudaSuccess)
     return e;
   TmaParams p{};
-  p.img = in.img;
-  p.out = out;
-  p.nx = g.nx;
-  p.ny = g.ny;
-  p.nz = g.nz;
-  p.num = g.num;
-  p.nxy = g.nx * g.ny;
-  p.neg_k = (float)(-1.4426950408889634 / div);
-  p.tiles_y = pl.tiles_y;
-  p.tiles_x = pl.tiles_x;
-  p.tiles_z = pl.tiles_z;
-  p.ntiles = pl.ntiles;
-  p.groups = pl.groups;
-  p.atlases_per_group = g.num / pl.groups;
-  p.partial = partial;
-  p.nvox = g.nvox();
+  p.sv = subject_view(g, in, out, div, partial, pl);
   p.err = err;
   p.timeout_ns = 2000000000ull;  // 2 s per wait; a step's copies land in microseconds
   p.withhold_cta = -1;
@@ -589,66 +681,180 @@ cudaError_t launch_hw(const Geometry &g, const SlabInputs &in, float *out, doubl
   return cudaSuccess;
 }
 
-template <int HW>
-cudaError_t plan_info_hw(const Geometry &g, FusePlanInfo *info) {
-  Plan<HW> pl;
-  cudaError_t e = plan_hw<HW>(g, &pl);
+template <int SET>
+cudaError_t plan_set(const Geometry &g, Plan *pl) {
+  switch (g.hw) {
+    case 1: return plan_hw<SET, 1>(g, pl);
+    case 2: return plan_hw<SET, 2>(g, pl);
+    case 3: return plan_hw<SET, 3>(g, pl);
+    case 4: return plan_hw<SET, 4>(g, pl);
+    case 5: return plan_hw<SET, 5>(g, pl);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t plan_any(const Geometry &g, int set, Plan *pl) {
+  return set == 1 ? plan_set<1>(g, pl) : plan_set<0>(g, pl);
+}
+
+template <int SET>
+cudaError_t launch_set(const Geometry &g, const SlabInputs &in, float *out, double div,
+                       float *partial, int *err, const WaitTest &wt, cudaStream_t stream) {
+  switch (g.hw) {
+    case 1: return launch_hw<SET, 1>(g, in, out, div, partial, err, wt, stream);
+    case 2: return launch_hw<SET, 2>(g, in, out, div, partial, err, wt, stream);
+    case 3: return launch_hw<SET, 3>(g, in, out, div, partial, err, wt, stream);
+    case 4: return launch_hw<SET, 4>(g, in, out, div, partial, err, wt, stream);
+    case 5: return launch_hw<SET, 5>(g, in, out, div, partial, err, wt, stream);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+// Slab box sizes of one subject under a tile set (for its tensor maps in the batch).
+template <int SET, int HW>
+void boxes_hw(int *yb, int *za, int *zl) {
+  using C = Cfg<HW, TileOf<SET, HW>::RX, TileOf<SET, HW>::TZ>;
+  *yb = C::YB;
+  *za = C::ZA;
+  *zl = C::ZL;
+}
+
+template <int SET>
+cudaError_t batch_plan(int hw, const Geometry &g, Plan *pl, int *yb, int *za, int *zl) {
+  cudaError_t e;
+  switch (hw) {
+    case 5: e = plan_hw<SET, 5>(g, pl); boxes_hw<SET, 5>(yb, za, zl); break;
+    case 4: e = plan_hw<SET, 4>(g, pl); boxes_hw<SET, 4>(yb, za, zl); break;
+    case 3: e = plan_hw<SET, 3>(g, pl); boxes_hw<SET, 3>(yb, za, zl); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return e;
+}
+
+template <int SET>
+cudaError_t launch_batch_set(const BatchSubjectIn *subs, int n, void *dev_scratch, int *err,
+                             cudaStream_t stream, BatchSetup *setup) {
+  // Order subjects by window (largest first), so CTAs working at the same time mostly run the
+  // same tile code.
+  std::vector<int> order(n);
+  for (int i = 0; i < n; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return subs[a].geom.hw > subs[b].geom.hw; });
+  std::vector<SubjectView> views(n);
+  std::vector<CUtensorMap> maps(2 * (size_t)n);
+  int total = 0;
+  cudaError_t e;
+  for (int k = 0; k < n; ++k) {
+    const BatchSubjectIn &b = subs[order[k]];
+    Plan pl;
+    int yb, za, zl;
+    if ((e = batch_plan<SET>(b.geom.hw, b.geom, &pl, &yb, &za, &zl)) != cudaSuccess) return e;
+    pl.groups = 1;  // many subjects fill the grid; no partial sums
+    if ((e = make_slab_map(&maps[2 * k], b.in.atlas, b.geom.nx, b.geom.ny, b.geom.nz, b.geom.num,
+                           b.in.pitch, yb, za)) != cudaSuccess)
+      return e;
+    if ((e = make_slab_map(&maps[2 * k + 1], b.in.label, b.geom.nx, b.geom.ny, b.geom.nz,
+                           b.geom.num, b.in.pitch, yb, zl)) != cudaSuccess)
+      return e;
+    SubjectView sv = subject_view(b.geom, b.in, b.out, b.div, nullptr, pl);
+    sv.item_begin = total;
+    total += (b.geom.ix > 0 && b.geom.iy > 0 && b.geom.iz > 0) ? pl.ntiles : 0;
+    views[k] = sv;
+  }
+  // Device copies: maps first (64-byte aligned), then the subject views pointing at them.
+  unsigned char *base = static_cast<unsigned char *>(dev_scratch);
+  CUtensorMap *d_maps = reinterpret_cast<CUtensorMap *>(base);
+  SubjectView *d_views = reinterpret_cast<SubjectView *>(base + maps.size() * sizeof(CUtensorMap));
+  for (int k = 0; k < n; ++k) {
+    views[k].tmA = d_maps + 2 * k;
+    views[k].tmL = d_maps + 2 * k + 1;
+  }
+  if ((e = cudaMemcpyAsync(d_maps, maps.data(), maps.size() * sizeof(CUtensorMap),
+                           cudaMemcpyHostToDevice, stream)) != cudaSuccess)
+    return e;
+  if ((e = cudaMemcpyAsync(d_views, views.data(), views.size() * sizeof(SubjectView),
+                           cudaMemcpyHostToDevice, stream)) != cudaSuccess)
+    return e;
+  // Host copies must outlive the asynchronous transfers.
+  if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return e;
+
+  constexpr int smem = batch_smem<SET>();
+  auto kern = fuse_batch_kernel<SET>;
+  if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) !=
+      cudaSuccess)
+    return e;
+  int per_sm = 1;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem)) !=
+      cudaSuccess)
+    return e;
+  if (per_sm < 1) return cudaErrorLaunchOutOfResources;
+  const int slots = sm_count() * per_sm;
+  setup->params_ready = true;
+  setup->items = total;
+  setup->blocks = total < slots ? total : slots;
+  setup->smem = smem;
+  setup->set = SET;
+  setup->bp_subjects = d_views;
+  setup->bp_nsub = n;
+  setup->bp_err = err;
+  return cudaSuccess;
+}
+
+}  // namespace
+
+size_t batch_scratch_bytes(int n) {
+  return 2 * (size_t)n * sizeof(CUtensorMap) + (size_t)n * sizeof(SubjectView) + 256;
+}
+
+cudaError_t prepare_batch(const BatchSubjectIn *subs, int n, int set, void *dev_scratch, int *err,
+                          cudaStream_t stream, BatchSetup *setup) {
+  for (int i = 0; i < n; ++i)
+    if (subs[i].geom.hw < 3 || subs[i].geom.hw > 5) return cudaErrorInvalidValue;
+  return set == 1 ? launch_batch_set<1>(subs, n, dev_scratch, err, stream, setup)
+                  : launch_batch_set<0>(subs, n, dev_scratch, err, stream, setup);
+}
+
+cudaError_t launch_prepared_batch(const BatchSetup &setup, cudaStream_t stream) {
+  if (!setup.params_ready) return cudaErrorInvalidValue;
+  if (setup.items == 0) return cudaSuccess;
+  BatchParams bp{static_cast<const SubjectView *>(setup.bp_subjects), setup.bp_nsub, setup.items,
+                 setup.bp_err, 2000000000ull};
+  if (setup.set == 1)
+    fuse_batch_kernel<1><<<setup.blocks, kThreads, setup.smem, stream>>>(bp);
+  else
+    fuse_batch_kernel<0><<<setup.blocks, kThreads, setup.smem, stream>>>(bp);
+  return cudaGetLastError();
+}
+
+size_t fuse_tma_partial_bytes(const Geometry &g, int set) {
+  if (g.ix <= 0 || g.iy <= 0 || g.iz <= 0) return 0;
+  Plan pl;
+  if (plan_any(g, set, &pl) != cudaSuccess || pl.groups <= 1) return 0;
+  return (size_t)pl.groups * 2 * (size_t)g.nvox() * sizeof(float);
+}
+
+cudaError_t fuse_tma_plan(const Geometry &g, int set, FusePlanInfo *info) {
+  *info = FusePlanInfo{0, 0, 0, 0, 0, 0};
+  if (g.ix <= 0 || g.iy <= 0 || g.iz <= 0) return cudaSuccess;
+  Plan pl;
+  cudaError_t e = plan_any(g, set, &pl);
   if (e != cudaSuccess) return e;
   info->groups = pl.groups;
   info->tiles = pl.ntiles;
   info->ctas = pl.blocks;
-  info->rx = Shape<HW>::RX;
-  info->tz = Shape<HW>::TZ;
+  info->rx = pl.rx;
+  info->tz = pl.tz;
   info->partial_bytes =
       pl.groups > 1 ? (size_t)pl.groups * 2 * (size_t)g.nvox() * sizeof(float) : 0;
   return cudaSuccess;
 }
 
-template <int HW>
-size_t partial_bytes_hw(const Geometry &g) {
-  Plan<HW> pl;
-  if (plan_hw<HW>(g, &pl) != cudaSuccess || pl.groups <= 1) return 0;
-  return (size_t)pl.groups * 2 * (size_t)g.nvox() * sizeof(float);
-}
-
-}  // namespace
-
-size_t fuse_tma_partial_bytes(const Geometry &g) {
-  if (g.ix <= 0 || g.iy <= 0 || g.iz <= 0) return 0;
-  switch (g.hw) {
-    case 1: return partial_bytes_hw<1>(g);
-    case 2: return partial_bytes_hw<2>(g);
-    case 3: return partial_bytes_hw<3>(g);
-    case 4: return partial_bytes_hw<4>(g);
-    case 5: return partial_bytes_hw<5>(g);
-    default: return 0;
-  }
-}
-
-cudaError_t fuse_tma_plan(const Geometry &g, FusePlanInfo *info) {
-  *info = FusePlanInfo{0, 0, 0, 0, 0, 0};
-  if (g.ix <= 0 || g.iy <= 0 || g.iz <= 0) return cudaSuccess;
-  switch (g.hw) {
-    case 1: return plan_info_hw<1>(g, info);
-    case 2: return plan_info_hw<2>(g, info);
-    case 3: return plan_info_hw<3>(g, info);
-    case 4: return plan_info_hw<4>(g, info);
-    case 5: return plan_info_hw<5>(g, info);
-    default: return cudaErrorInvalidValue;
-  }
-}
-
 cudaError_t launch_fuse_tma(const Geometry &g, const SlabInputs &in, float *out, double div,
-                            float *partial, int *err, const WaitTest &wt, cudaStream_t stream) {
+                            float *partial, int *err, const WaitTest &wt, int set,
+                            cudaStream_t stream) {
   if (g.ix <= 0 || g.iy <= 0 || g.iz <= 0) return cudaSuccess;
-  switch (g.hw) {
-    case 1: return launch_hw<1>(g, in, out, div, partial, err, wt, stream);
-    case 2: return launch_hw<2>(g, in, out, div, partial, err, wt, stream);
-    case 3: return launch_hw<3>(g, in, out, div, partial, err, wt, stream);
-    case 4: return launch_hw<4>(g, in, out, div, partial, err, wt, stream);
-    case 5: return launch_hw<5>(g, in, out, div, partial, err, wt, stream);
-    default: return cudaErrorInvalidValue;
-  }
+  return set == 1 ? launch_set<1>(g, in, out, div, partial, err, wt, stream)
+                  : launch_set<0>(g, in, out, div, partial, err, wt, stream);
 }
 
 namespace {

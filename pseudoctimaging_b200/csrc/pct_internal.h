@@ -37,14 +37,38 @@ struct WaitTest {
   unsigned long long timeout_ns;
 };
 
-size_t fuse_tma_partial_bytes(const Geometry &g);
+// Tile-shape sets compiled into the library (chosen per handle, see pct_autotune).
+constexpr int kTileSets = 2;
+size_t fuse_tma_partial_bytes(const Geometry &g, int set);
 struct FusePlanInfo {
   int groups, tiles, ctas, rx, tz;
   size_t partial_bytes;
 };
-cudaError_t fuse_tma_plan(const Geometry &g, FusePlanInfo *info);
+cudaError_t fuse_tma_plan(const Geometry &g, int set, FusePlanInfo *info);
 cudaError_t launch_fuse_tma(const Geometry &g, const SlabInputs &in, float *out, double div,
-                            float *partial, int *err, const WaitTest &wt, cudaStream_t stream);
+                            float *partial, int *err, const WaitTest &wt, int set,
+                            cudaStream_t stream);
+
+// Batched form: many subjects (NH 7/9/11), one persistent launch.
+struct BatchSubjectIn {
+  Geometry geom;
+  SlabInputs in;   // pitched atlas stacks (TMA-ready)
+  float *out;
+  double div;
+};
+struct BatchSetup {
+  bool params_ready = false;
+  int items = 0, blocks = 0, smem = 0, set = 0;
+  void *bp_subjects = nullptr;
+  int bp_nsub = 0;
+  int *bp_err = nullptr;
+};
+size_t batch_scratch_bytes(int n);
+// Plans the batch and uploads its subject table and tensor maps to dev_scratch (synchronous).
+cudaError_t prepare_batch(const BatchSubjectIn *subs, int n, int set, void *dev_scratch, int *err,
+                          cudaStream_t stream, BatchSetup *setup);
+// Enqueues the persistent batch kernel (graph-capturable: no host work beyond the launch).
+cudaError_t launch_prepared_batch(const BatchSetup &setup, cudaStream_t stream);
 
 // dst[r*pitch + c] = src[r*ny + c] for r < rows, c < ny.
 cudaError_t launch_pitch_copy(const float *src, float *dst, long long rows, int ny, int pitch,
