@@ -170,6 +170,52 @@ int pct_get_tile_set(const pct_handle *h);
 int pct_autotune(pct_handle *h, const pct_subject *subjects, int n, const char *cache_path,
                  double *ms_per_set, int *chosen);
 
+/*
+ * Learned-proposal form (EXEC_CHOICE 7), training side. The model is a small 3D CNN over the
+ * co-located 9x9x9 patches of the input MRI and one atlas MRI (conv 2->16, 3 x conv 16->16, all
+ * 3x3x3 valid + ReLU, then three linear heads 16->11 scoring dw, du and dv); it proposes, per
+ * (voxel, atlas), the 32 offsets of the 11^3 window with the largest p_w*p_u*p_v. No counterpart
+ * in the reference. Weights are BF16 for the forward pass, with FP32 master weights and Adam.
+ *
+ * A training set is a list of samples (subject, atlas, voxel) over device-resident subjects; its
+ * targets are computed on the GPU from the plain method: the exact FP32 SSD of all 11^3 offsets,
+ * the 32 smallest, turned into one distribution per axis (the share of the 32 with each dw, du,
+ * dv). Every sample voxel must be at least 6 voxels from each face of its volume.
+ */
+typedef struct pct_model pct_model;
+typedef struct pct_train_set pct_train_set;
+typedef struct pct_train_subject {
+  const float *img;    /* device [nz][nx][ny] input MRI */
+  const float *atlas;  /* device [num_atlas][nz][nx][ny] atlas MRIs */
+  int nx, ny, nz, num_atlas;
+} pct_train_subject;
+
+int pct_model_num_params(void);
+/* Deterministic He-normal initialisation from `seed`. */
+int pct_model_create(int device, uint64_t seed, pct_model **out);
+int pct_model_destroy(pct_model *m);
+const char *pct_model_last_error(const pct_model *m);
+/* FP32 master weights in and out (pct_model_num_params floats); setting resets Adam. With
+ * inference_precision != 0 the BF16 weights the kernels use are returned (as floats). */
+int pct_model_set_params(pct_model *m, const float *params);
+int pct_model_get_params(pct_model *m, float *params, int inference_precision);
+
+/* samples: host array [n][3] of (subject index, atlas index, flat voxel index). */
+int pct_train_set_create(int device, const pct_train_subject *subjects, int nsub,
+                         const int *samples, int n, pct_train_set **out);
+/* Per-axis targets [n][33] and the plain method's top-32 offsets [n][32] (index
+ * (dw+5)*121 + (du+5)*11 + (dv+5)); either pointer may be NULL. */
+int pct_train_set_targets(pct_train_set *ts, float *targets, int16_t *top);
+int pct_train_set_destroy(pct_train_set *ts);
+
+/* Mean gradient and loss of samples [begin, begin+count) without updating the model. */
+int pct_model_gradients(pct_model *m, pct_train_set *ts, int begin, int count, float *grad,
+                        float *loss);
+/* `steps` Adam steps on consecutive batches of the (caller-shuffled) samples, wrapping around
+ * at the end of the set; *mean_loss receives the mean per-sample loss over those steps. */
+int pct_model_train(pct_model *m, pct_train_set *ts, int batch, int steps, float lr,
+                    float *mean_loss);
+
 /* In-place CT -> label scale L' = 255*((L+1024)/4095) on a device buffer of n floats
  * (PatchBasedPseudoCT.cu:2009-2020, NewPatchedBrainPureC.cpp:1583-1593). */
 int pct_normalize_labels_device(pct_handle *h, float *d_label, size_t n, void *stream);

@@ -74,6 +74,12 @@ class SubjectDesc(ctypes.Structure):
                 ("num_atlas", ctypes.c_int), ("nh", ctypes.c_int), ("div", ctypes.c_double)]
 
 
+class TrainSubject(ctypes.Structure):
+    """pct_train_subject: a device-resident subject for building a training set."""
+    _fields_ = [("img", ctypes.c_void_p), ("atlas", ctypes.c_void_p), ("nx", ctypes.c_int),
+                ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("num_atlas", ctypes.c_int)]
+
+
 class Plan(ctypes.Structure):
     _fields_ = [("launches", ctypes.c_int), ("groups", ctypes.c_int), ("tiles", ctypes.c_int),
                 ("ctas", ctypes.c_int), ("tile_rows", ctypes.c_int),
@@ -126,6 +132,18 @@ SIGNATURES = {
     "pct_ncc_device": (_I, [_P, _P, _P, _I, _I, _I, _I, ctypes.POINTER(ctypes.c_double),
                             ctypes.POINTER(ctypes.c_int64), _P]),
     "pct_test_wait_timeout": (_I, [_P, _D]),
+    "pct_model_num_params": (_I, []),
+    "pct_model_create": (_I, [_I, ctypes.c_uint64, ctypes.POINTER(_P)]),
+    "pct_model_destroy": (_I, [_P]),
+    "pct_model_last_error": (ctypes.c_char_p, [_P]),
+    "pct_model_set_params": (_I, [_P, _P]),
+    "pct_model_get_params": (_I, [_P, _P, _I]),
+    "pct_train_set_create": (_I, [_I, ctypes.POINTER(TrainSubject), _I, _P, _I,
+                                  ctypes.POINTER(_P)]),
+    "pct_train_set_targets": (_I, [_P, _P, _P]),
+    "pct_train_set_destroy": (_I, [_P]),
+    "pct_model_gradients": (_I, [_P, _P, _I, _I, _P, ctypes.POINTER(ctypes.c_float)]),
+    "pct_model_train": (_I, [_P, _P, _I, _I, ctypes.c_float, ctypes.POINTER(ctypes.c_float)]),
     "pct_synth_default_params": (_I, [ctypes.POINTER(SynthParams), _I, _I, _I, _I, _I,
                                       ctypes.c_uint64]),
     "pct_synth_generate": (_I, [ctypes.POINTER(SynthParams), _P, _P, _P]),
