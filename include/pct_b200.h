@@ -216,6 +216,33 @@ int pct_model_gradients(pct_model *m, pct_train_set *ts, int begin, int count, f
 int pct_model_train(pct_model *m, pct_train_set *ts, int batch, int steps, float lr,
                     float *mean_loss);
 
+/*
+ * Learned-proposal form, inference side. pct_attach_model makes EXEC_CHOICE 7 available on the
+ * handle's pct_synthesize / pct_synthesize_device / pct_run_pipeline calls (NH must be 11; the
+ * model must live on the handle's device and outlive its use; m = NULL detaches). Per atlas and
+ * per row segment of 30 interior voxels along y, the network's per-axis offset probabilities
+ * of the segment's voxels are summed; the 4 most probable offsets per axis are kept and, of their
+ * 64 combinations, the 32 whose per-axis ranks sum to at most 4 (ties: lower offset first). Only
+ * those 32 offsets get the exact FP32 SSD and a weight. A voxel whose own probability mass
+ * (p_w*p_u*p_v summed over the 32) is below `conf_threshold` falls back to all 11^3 offsets for
+ * that atlas. conf_threshold = 0 never falls back; a threshold above 1 always does (every
+ * candidate, as the plain method). Output: the same interior, border and NaN rule as the plain
+ * method (voxels 6 or more from every face). No counterpart in the reference.
+ */
+int pct_attach_model(pct_handle *h, pct_model *m, float conf_threshold);
+/* Counters of the handle's last learned run (synchronises the stream that run used): the
+ * (voxel, atlas) pairs that took the full search, and the offsets evaluated summed over warp
+ * rows (one row = 30 output voxels of one atlas; the plain method evaluates 1331 per row).
+ * Either pointer may be NULL. */
+int pct_learned_stats(pct_handle *h, uint64_t *fallback_pairs, uint64_t *row_offsets);
+/* Testing hook: for one (input, atlas) pair (d_img, d_atlas: one device volume each,
+ * [nz][nx][ny]) at n voxels given by flat index, the 16 conv4 features (after ReLU, as the
+ * inference kernels keep them in BF16) into features [n][16], the proposal's 4 offsets per axis
+ * in rank order (dw, du, dv; values -5..5) into top [n][12], and its confidence into conf [n].
+ * Any output pointer may be NULL. Synchronous. */
+int pct_model_probe(pct_model *m, const float *d_img, const float *d_atlas, int nx, int ny, int nz,
+                    const int64_t *voxels, int n, float *features, int8_t *top, float *conf);
+
 /* In-place CT -> label scale L' = 255*((L+1024)/4095) on a device buffer of n floats
  * (PatchBasedPseudoCT.cu:2009-2020, NewPatchedBrainPureC.cpp:1583-1593). */
 int pct_normalize_labels_device(pct_handle *h, float *d_label, size_t n, void *stream);

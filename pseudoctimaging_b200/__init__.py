@@ -144,6 +144,9 @@ SIGNATURES = {
     "pct_train_set_destroy": (_I, [_P]),
     "pct_model_gradients": (_I, [_P, _P, _I, _I, _P, ctypes.POINTER(ctypes.c_float)]),
     "pct_model_train": (_I, [_P, _P, _I, _I, ctypes.c_float, ctypes.POINTER(ctypes.c_float)]),
+    "pct_attach_model": (_I, [_P, _P, ctypes.c_float]),
+    "pct_learned_stats": (_I, [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
+    "pct_model_probe": (_I, [_P, _P, _P, _I, _I, _I, _P, _I, _P, _P, _P]),
     "pct_synth_default_params": (_I, [ctypes.POINTER(SynthParams), _I, _I, _I, _I, _I,
                                       ctypes.c_uint64]),
     "pct_synth_generate": (_I, [ctypes.POINTER(SynthParams), _P, _P, _P]),
@@ -245,6 +248,22 @@ class Handle:
 
     def set_memory_limit(self, nbytes: int) -> None:
         self._check(lib.pct_set_memory_limit(self._h, nbytes), "pct_set_memory_limit")
+
+    def attach_model(self, model, conf_threshold: float = 0.0) -> None:
+        """Makes EXEC_LEARNED available (NH = 11) with a :class:`learned.LearnedModel` (None
+        detaches). Pairs whose 32 proposals hold less than ``conf_threshold`` of the proposal's
+        probability mass fall back to the full search. The model must outlive its use."""
+        self._model = model
+        self._check(lib.pct_attach_model(self._h, model.ptr if model is not None else None,
+                                         float(conf_threshold)), "pct_attach_model")
+
+    def learned_stats(self) -> dict:
+        """Counters of the last learned run: ``fallback_pairs`` ((voxel, atlas) pairs that took
+        the full search) and ``row_offsets`` (offsets evaluated, summed over 30-voxel rows)."""
+        f, r = ctypes.c_uint64(), ctypes.c_uint64()
+        self._check(lib.pct_learned_stats(self._h, ctypes.byref(f), ctypes.byref(r)),
+                    "pct_learned_stats")
+        return {"fallback_pairs": int(f.value), "row_offsets": int(r.value)}
 
     def synthesize(self, img, atlas, atlas_label, nh: int, div: float,
                    exec_choice: int = EXEC_B200_FP32) -> np.ndarray:

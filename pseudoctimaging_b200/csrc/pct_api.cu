@@ -35,6 +35,11 @@ struct pct_handle {
   unsigned long long wait_test_ns = 0;  // one-shot testing hook, see pct_test_wait_timeout
   int tile_set = 0;                     // register-tile set (pct_autotune / pct_set_tile_set)
   DevBuf batch_stage, batch_meta;       // pct_synthesize_batch: pitched stacks, subject table
+  pct_model *model = nullptr;           // learned form (EXEC_CHOICE 7), see pct_attach_model
+  float learned_conf = 0.f;             // its full-search fallback threshold
+  DevBuf learned;                       // its feature volumes and sums
+  long long learned_nvox = 0;           // volume size of the last learned run (0: none yet)
+  cudaStream_t learned_stream = nullptr;
   std::string last_error;
 };
 
@@ -92,9 +97,12 @@ int check_choice(pct_handle *h, int exec_choice) {
     case PCT_EXEC_BATCHED:
       return fail(h, PCT_ERR_UNSUPPORTED,
                   "exec_choice 8 (batched) runs through pct_synthesize_batch / pct_batch_create");
+    case PCT_EXEC_LEARNED:
+      if (h && h->model) return PCT_OK;
+      return fail(h, PCT_ERR_UNSUPPORTED,
+                  "exec_choice 7 (learned proposal) needs a model attached with pct_attach_model");
     case PCT_EXEC_TC_FP16:
     case PCT_EXEC_TC_BF16:
-    case PCT_EXEC_LEARNED:
       return fail(h, PCT_ERR_UNSUPPORTED,
                   "exec_choice " + std::to_string(exec_choice) + " is not available in this build");
     default:
@@ -142,6 +150,32 @@ int launch_fusion(pct_handle *h, const pct::Geometry &g, const pct::SlabInputs &
 }
 
 // Reads (and clears) the device status word after `s` has drained.
+// The learned form: conv features, proposal and exact rescoring over all atlases (NH = 11).
+int launch_learned_path(pct_handle *h, const pct::Geometry &g, const pct::SlabInputs &in,
+                        float *d_out, double div, cudaStream_t s) {
+  if (g.nh != 11)
+    return fail(h, PCT_ERR_UNSUPPORTED,
+                "exec_choice 7 (learned proposal) is trained for NH = 11 only, got NH = " +
+                    std::to_string(g.nh));
+  if (pct::learned::model_device(h->model) != h->device)
+    return fail(h, PCT_ERR_INVALID_ARG, "the attached model lives on another device");
+  int st = ensure(h, h->learned, pct::learned::infer_scratch_bytes(g.nvox()));
+  if (st || (st = ensure(h, h->err, 16))) return st;
+  int *err = static_cast<int *>(h->err.ptr);
+  PCT_CUDA(h, cudaMemsetAsync(err, 0, sizeof(int), s));
+  PCT_CUDA(h, pct::learned::launch_learned(g, pct::learned::model_weights(h->model), in, d_out, div,
+                                           h->learned_conf, h->learned.ptr, err, s));
+  h->learned_nvox = g.nvox();
+  h->learned_stream = s;
+  return PCT_OK;
+}
+
+int launch_path(pct_handle *h, const pct::Geometry &g, const pct::SlabInputs &in, float *d_out,
+                double div, int exec_choice, cudaStream_t s) {
+  if (exec_choice == PCT_EXEC_LEARNED) return launch_learned_path(h, g, in, d_out, div, s);
+  return launch_fusion(h, g, in, d_out, div, s);
+}
+
 int read_device_status(pct_handle *h, cudaStream_t s) {
   if (!h->err.ptr) return PCT_OK;
   int v = 0;
@@ -341,7 +375,7 @@ int pct_destroy(pct_handle *h) {
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   for (DevBuf *b : {&h->img, &h->atlas, &h->label, &h->out, &h->scratch, &h->err, &h->partial,
-                    &h->stage, &h->batch_stage, &h->batch_meta})
+                    &h->stage, &h->batch_stage, &h->batch_meta, &h->learned})
     if (b->ptr) cudaFree(b->ptr);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -357,6 +391,34 @@ int pct_set_stream(pct_handle *h, void *stream) {
 int pct_set_memory_limit(pct_handle *h, size_t bytes) {
   if (!h) return PCT_ERR_INVALID_ARG;
   h->mem_limit = bytes;
+  return PCT_OK;
+}
+
+int pct_attach_model(pct_handle *h, pct_model *m, float conf_threshold) {
+  if (!h) return PCT_ERR_INVALID_ARG;
+  h->last_error.clear();
+  if (!(conf_threshold >= 0.f) || !isfinite(conf_threshold))
+    return fail(h, PCT_ERR_INVALID_ARG, "conf_threshold must be finite and >= 0");
+  if (m && pct::learned::model_device(m) != h->device)
+    return fail(h, PCT_ERR_INVALID_ARG, "the model lives on another device than the handle");
+  h->model = m;
+  h->learned_conf = conf_threshold;
+  return PCT_OK;
+}
+
+int pct_learned_stats(pct_handle *h, uint64_t *fallback_pairs, uint64_t *row_offsets) {
+  if (!h) return PCT_ERR_INVALID_ARG;
+  if (fallback_pairs) *fallback_pairs = 0;
+  if (row_offsets) *row_offsets = 0;
+  if (!h->learned_nvox) return PCT_OK;
+  int st = select_device(h);
+  if (st) return st;
+  unsigned long long v[2] = {0, 0};
+  PCT_CUDA(h, cudaMemcpyAsync(v, pct::learned::infer_counters(h->learned.ptr, h->learned_nvox),
+                              sizeof(v), cudaMemcpyDeviceToHost, h->learned_stream));
+  PCT_CUDA(h, cudaStreamSynchronize(h->learned_stream));
+  if (fallback_pairs) *fallback_pairs = v[0];
+  if (row_offsets) *row_offsets = v[1];
   return PCT_OK;
 }
 
@@ -378,7 +440,7 @@ int pct_synthesize_device(pct_handle *h, const float *d_img, const float *d_atla
   pct::SlabInputs in{d_img, d_atlas, d_atlas_label, g.ny};
   const bool aligned = (g.ny % 4 == 0) && (reinterpret_cast<uintptr_t>(d_atlas) % 16 == 0) &&
                        (reinterpret_cast<uintptr_t>(d_atlas_label) % 16 == 0);
-  if (!aligned) {  // TMA needs 16-byte row strides: stage a pitched copy on the handle
+  if (!aligned && exec_choice != PCT_EXEC_LEARNED) {  // TMA needs 16-byte row strides: stage a pitched copy on the handle
     const int pitch = pct::slab_pitch(g.ny);
     const long long rows = (long long)g.num * g.nz * g.nx;
     const size_t bytes = (size_t)rows * pitch * sizeof(float);
@@ -390,7 +452,7 @@ int pct_synthesize_device(pct_handle *h, const float *d_img, const float *d_atla
     in = pct::SlabInputs{d_img, static_cast<const float *>(h->atlas.ptr),
                          static_cast<const float *>(h->label.ptr), pitch};
   }
-  return launch_fusion(h, g, in, d_out, div, s);
+  return launch_path(h, g, in, d_out, div, exec_choice, s);
 }
 
 int pct_synthesize(pct_handle *h, const float *img, const float *atlas, const float *atlas_label,
@@ -417,7 +479,8 @@ int pct_synthesize(pct_handle *h, const float *img, const float *atlas, const fl
   PCT_CUDA(h, cudaMemsetAsync(h->out.ptr, 0, vol, s));
   pct::SlabInputs in{static_cast<const float *>(h->img.ptr), static_cast<const float *>(h->atlas.ptr),
                      static_cast<const float *>(h->label.ptr), pct::slab_pitch(g.ny)};
-  if ((st = launch_fusion(h, g, in, static_cast<float *>(h->out.ptr), div, s))) return st;
+  if ((st = launch_path(h, g, in, static_cast<float *>(h->out.ptr), div, exec_choice, s)))
+    return st;
   PCT_CUDA(h, cudaMemcpyAsync(label_segmentation, h->out.ptr, vol, cudaMemcpyDeviceToHost, s));
   PCT_CUDA(h, cudaStreamSynchronize(s));
   return read_device_status(h, s);
@@ -537,7 +600,7 @@ int pct_run_pipeline(pct_handle *h, const float *img, const float *atlas_mri,
   PCT_CUDA(h, cudaMemsetAsync(d_out, 0, vol, s));
   pct::SlabInputs in{d_img, static_cast<const float *>(h->atlas.ptr),
                      static_cast<const float *>(h->label.ptr), pitch};
-  if ((st = launch_fusion(h, g, in, d_out, div, s))) return st;
+  if ((st = launch_path(h, g, in, d_out, div, exec_choice, s))) return st;
   if ((st = read_device_status(h, s))) return st;
   if (regularize) {
     long long f = 0;

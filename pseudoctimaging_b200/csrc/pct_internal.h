@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+struct pct_model;
+
 namespace pct {
 
 // Half window and interior of one subject, as in the reference (NewPatchedBrainPureC.cpp:1263-1265):
@@ -76,6 +78,10 @@ cudaError_t launch_pitch_copy(const float *src, float *dst, long long rows, int 
 
 inline int slab_pitch(int ny) { return (ny + 3) / 4 * 4; }
 
+// cuTensorMapEncodeTiled of the driver (a PFN_cuTensorMapEncodeTiled_v12000), found through the
+// runtime's entry-point query; NULL if the driver does not provide it.
+void *tensor_map_encoder();
+
 // NaN median fill (synchronous on `stream`: it reads back a counter after each round).
 // scratch must hold regularize_scratch_bytes(nx*ny*nz) bytes.
 size_t regularize_scratch_bytes(long long nvox);
@@ -84,5 +90,20 @@ cudaError_t launch_regularize(float *vol, int nx, int ny, int nz, int nh, void *
 
 cudaError_t launch_normalize_labels(float *label, size_t n, cudaStream_t stream);
 cudaError_t launch_finalize_hu(float *vol, size_t n, cudaStream_t stream);
+
+namespace learned {
+// Learned-proposal inference (NH = 11). `weights` are the model's BF16 parameters on the device.
+size_t infer_scratch_bytes(long long nvox);
+// Two device counters: (voxel, atlas) pairs that fell back, offsets evaluated by warp rows.
+unsigned long long *infer_counters(void *scratch, long long nvox);
+// *err (device) is set to a non-zero code if a bounded wait of the convolution pipeline gives up.
+cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInputs &in, float *out,
+                           double div, float conf_thr, void *scratch, int *err, cudaStream_t s);
+cudaError_t learned_probe(const Geometry &g, const void *weights, const float *img,
+                          const float *atlas_a, void *scratch, const int64_t *voxels, int n,
+                          float *features, signed char *top, float *conf, cudaStream_t s);
+const void *model_weights(const pct_model *m);
+int model_device(const pct_model *m);
+}  // namespace learned
 
 }  // namespace pct

@@ -48,6 +48,9 @@ struct pct_train_set {
   int pos = 0;               // next sample of the current epoch
 };
 
+const void *pct::learned::model_weights(const pct_model *m) { return m->wbf; }
+int pct::learned::model_device(const pct_model *m) { return m->device; }
+
 namespace {
 
 uint64_t mix64(uint64_t z) {
@@ -293,6 +296,28 @@ int pct_model_train(pct_model *m, pct_train_set *ts, int batch, int steps, float
   MCUDA(m, cudaMemcpyAsync(&l, m->loss, sizeof(float), cudaMemcpyDeviceToHost, m->stream));
   MCUDA(m, cudaStreamSynchronize(m->stream));
   if (mean_loss) *mean_loss = (float)(l / (double)seen);
+  return PCT_OK;
+}
+
+int pct_model_probe(pct_model *m, const float *d_img, const float *d_atlas, int nx, int ny, int nz,
+                    const int64_t *voxels, int n, float *features, int8_t *top, float *conf) {
+  if (!m || !d_img || !d_atlas || !voxels || n <= 0) return PCT_ERR_INVALID_ARG;
+  pct::Geometry g;
+  if (nx <= 0 || ny <= 0 || nz <= 0 || !pct::make_geometry(nx, ny, nz, 1, 11, &g))
+    return PCT_ERR_INVALID_ARG;
+  if ((long long)n * 24 + 16 > g.nvox() * 8) return PCT_ERR_INVALID_ARG;
+  for (int i = 0; i < n; ++i)
+    if (voxels[i] < 0 || voxels[i] >= g.nvox()) return PCT_ERR_INVALID_ARG;
+  MCUDA(m, cudaSetDevice(m->device));
+  void *scratch = nullptr;
+  if (cudaMalloc(&scratch, infer_scratch_bytes(g.nvox())) != cudaSuccess) {
+    cudaGetLastError();
+    return model_fail(m, PCT_ERR_OUT_OF_MEMORY, "feature scratch");
+  }
+  const cudaError_t e = learned_probe(g, m->wbf, d_img, d_atlas, scratch, voxels, n, features,
+                                      reinterpret_cast<signed char *>(top), conf, m->stream);
+  cudaFree(scratch);
+  if (e != cudaSuccess) return model_fail(m, PCT_ERR_CUDA, cudaGetErrorString(e));
   return PCT_OK;
 }
 

@@ -1,0 +1,764 @@
+// Inference side of the learned proposal (EXEC_CHOICE 7).
+//
+// Per atlas, over the whole volume:
+//   conv1 (2 -> 16 channels)            CUDA cores, FP32 math, BF16 channel-last output
+//   conv2..conv4 (16 -> 16 channels)    tensor cores: BF16 implicit GEMM with FP32 accumulation
+//                                       (mma m16n8k16; ldmatrix gathers 16 shifted voxel rows of a
+//                                       channel-last shared-memory slab per tap, 27 taps)
+//   heads, proposal and rescoring       one warp per row segment of 30 voxels along y: per voxel
+//                                       the 33 logits and a softmax per axis; the segment's summed
+//                                       probabilities pick 4 offsets per axis and the 32 rank
+//                                       triples with i + j + k <= 4; the exact FP32 SSD of those
+//                                       32 candidates -> weights exp(-SSD/div) -> product and
+//                                       weight sums. A voxel whose own probability mass on the 32
+//                                       is below the confidence threshold takes all 11^3.
+// The sums are kept per voxel across atlases and turned into the output with the reference's
+// NaN rule at the end. Out-of-volume inputs of the convolutions read as zero; interior voxels
+// (6 or more voxels from every face) only see in-volume values.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include "pct_internal.h"
+#include "pct_learned.h"
+#include "pct_ptx.cuh"
+
+namespace pct {
+namespace learned {
+namespace {
+
+constexpr float kDblEpsilonF = 2.220446049250313080847e-16f;
+
+
+// ---------------------------------------------------------------- conv1 (CUDA cores)
+
+constexpr int kC1Vox = 2;  // consecutive y voxels per thread
+
+// conv1 over the whole volume, FP32 math on BF16 weights: each thread owns 2 consecutive y
+// voxels of one (z, x) row, walks the 54 input taps once (4 y values per (channel, dz, dx)
+// cover the 2 voxels' 3 y taps) and keeps 2 x 16 accumulators.
+__global__ void __launch_bounds__(256, 2)
+    conv1_kernel(const float *__restrict__ img, const float *__restrict__ atl,
+                 const __nv_bfloat16 *__restrict__ wbf, __nv_bfloat16 *__restrict__ out, int nx,
+                 int ny, int nz, int apitch) {
+  __shared__ __align__(16) float w[kCin * 27][kC];  // [ci*27 + tap][co]
+  __shared__ float bias[kC];
+  for (int i = threadIdx.x; i < kC * kCin * 27; i += blockDim.x) {
+    const int co = i / (kCin * 27), r = i % (kCin * 27);
+    w[r][co] = __bfloat162float(wbf[kW1 + i]);
+  }
+  if (threadIdx.x < kC) bias[threadIdx.x] = __bfloat162float(wbf[kB1 + threadIdx.x]);
+  __syncthreads();
+  const int yq = (ny + kC1Vox - 1) / kC1Vox;
+  const long long items = (long long)nz * nx * yq;
+  const int nxy = nx * ny;
+  for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < items;
+       it += (long long)gridDim.x * blockDim.x) {
+    const int y0 = (int)(it % yq) * kC1Vox;
+    const long long r0 = it / yq;
+    const int x = (int)(r0 % nx), z = (int)(r0 / nx);
+    float acc[kC1Vox][kC];
+#pragma unroll
+    for (int v = 0; v < kC1Vox; ++v)
+#pragma unroll
+      for (int c = 0; c < kC; ++c) acc[v][c] = bias[c];
+#pragma unroll
+    for (int ci = 0; ci < kCin; ++ci) {
+#pragma unroll
+      for (int kzx = 0; kzx < 9; ++kzx) {
+        const int zz = z + kzx / 3 - 1, xx = x + kzx % 3 - 1;
+        const bool rok = zz >= 0 && zz < nz && xx >= 0 && xx < nx;
+        const float *src = ci == 0 ? img + (long long)zz * nxy + (long long)xx * ny
+                                   : atl + ((long long)zz * nx + xx) * apitch;
+        float in[kC1Vox + 2];
+#pragma unroll
+        for (int j = 0; j < kC1Vox + 2; ++j) {
+          const int yy = y0 + j - 1;
+          in[j] = (rok && yy >= 0 && yy < ny) ? __ldg(src + yy) * kInScale : 0.f;
+        }
+#pragma unroll
+        for (int ky = 0; ky < 3; ++ky) {
+          const float4 *wr = reinterpret_cast<const float4 *>(w[ci * 27 + kzx * 3 + ky]);
+#pragma unroll
+          for (int c4 = 0; c4 < kC / 4; ++c4) {
+            const float4 wv = wr[c4];
+#pragma unroll
+            for (int v = 0; v < kC1Vox; ++v) {
+              const float xv = in[v + ky];
+              acc[v][4 * c4 + 0] = fmaf(wv.x, xv, acc[v][4 * c4 + 0]);
+              acc[v][4 * c4 + 1] = fmaf(wv.y, xv, acc[v][4 * c4 + 1]);
+              acc[v][4 * c4 + 2] = fmaf(wv.z, xv, acc[v][4 * c4 + 2]);
+              acc[v][4 * c4 + 3] = fmaf(wv.w, xv, acc[v][4 * c4 + 3]);
+            }
+          }
+        }
+      }
+    }
+    __nv_bfloat16 *dst = out + ((long long)z * nxy + (long long)x * ny + y0) * kC;
+#pragma unroll
+    for (int v = 0; v < kC1Vox; ++v) {
+      if (y0 + v >= ny) break;
+      __align__(16) __nv_bfloat162 r[kC / 2];
+#pragma unroll
+      for (int c = 0; c < kC / 2; ++c)
+        r[c] = __floats2bfloat162_rn(fmaxf(acc[v][2 * c], 0.f), fmaxf(acc[v][2 * c + 1], 0.f));
+      uint4 *d4 = reinterpret_cast<uint4 *>(dst + v * kC);
+      d4[0] = reinterpret_cast<const uint4 *>(r)[0];
+      d4[1] = reinterpret_cast<const uint4 *>(r)[1];
+    }
+  }
+}
+
+// ---------------------------------------------------------------- conv 16 -> 16 (tensor cores)
+
+// A CTA tile is 1 z-plane x 4 x-rows x 64 y of outputs; its 4 warps each own a 16-voxel y
+// segment of all 4 x-rows. The input slab (3 z x 6 x x 66 y voxels, 16 BF16 channels = 32 bytes
+// each) arrives by TMA with 32-byte swizzling (the two 16-byte halves of a voxel swap places
+// where bit 2 of its slab index is set), which puts the 8 rows of every ldmatrix phase in
+// distinct banks; out-of-volume voxels arrive as zeros. CTAs are persistent and double-buffer the
+// slab. Each warp keeps the B fragments of all 27 taps in registers and walks the 3 x 6 x 3
+// (z, x, y-shift) input row segments once: one ldmatrix feeds the up to 3 output x-rows that use
+// that row (2 mma each, 16 output channels).
+constexpr int kCvWarps = 4;
+constexpr int kCvThreads = kCvWarps * 32;
+constexpr int kCvTX = 4, kCvTY = 16 * kCvWarps;
+constexpr int kCvSZ = 3, kCvSX = kCvTX + 2, kCvSY = kCvTY + 2;
+constexpr int kCvBoxBytes = kCvSZ * kCvSX * kCvSY * 32;    // 38,016
+constexpr int kCvBufBytes = (kCvBoxBytes + 1023) / 1024 * 1024;
+constexpr size_t kConvSmem = 2 * kCvBufBytes + 64 + 1024;  // two buffers, barriers, alignment
+constexpr int kFragWords = 27 * 2 * 2 * 32;  // per layer: tap x n-tile x register x lane
+constexpr unsigned long long kConvTimeoutNs = 2000000000ULL;
+
+// B fragments of one layer in mma register order: for tap t, n-tile j (8 output channels),
+// register r, lane l: {W[co][ci][t], W[co][ci+1][t]} with co = 8j + l/4, ci = 2(l%4) + 8r.
+__global__ void pack_frags_kernel(const __nv_bfloat16 *__restrict__ wbf, int woff,
+                                  uint32_t *__restrict__ frag) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= kFragWords) return;
+  const int lane = i % 32, r = (i / 32) % 2, j = (i / 64) % 2, t = i / 128;
+  const int co = 8 * j + lane / 4, ci = 2 * (lane % 4) + 8 * r;
+  const __nv_bfloat16 lo = wbf[woff + (co * kC + ci) * 27 + t];
+  const __nv_bfloat16 hi = wbf[woff + (co * kC + ci + 1) * 27 + t];
+  frag[i] = (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+}
+
+__device__ __forceinline__ void ldmatrix_x4(uint32_t addr, uint32_t &r0, uint32_t &r1,
+                                            uint32_t &r2, uint32_t &r3) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];"
+               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+               : "r"(addr));
+}
+
+__device__ __forceinline__ void mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2,
+                                         uint32_t a3, uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
+      "{%8, %9}, {%0, %1, %2, %3};"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+struct ConvGrid {
+  int nx, ny, nz, tiles_y, tiles_x, tiles;
+};
+
+__device__ __forceinline__ void conv_tile_origin(const ConvGrid &g, int tile, int &z, int &x0,
+                                                 int &y0) {
+  const int ty = tile % g.tiles_y;
+  const int r = tile / g.tiles_y;
+  x0 = (r % g.tiles_x) * kCvTX;
+  z = r / g.tiles_x;
+  y0 = ty * kCvTY;
+}
+
+__device__ __forceinline__ void conv_issue(const CUtensorMap *tm, uint32_t buf, uint32_t bar,
+                                           const ConvGrid &g, int tile) {
+  int z, x0, y0;
+  conv_tile_origin(g, tile, z, x0, y0);
+  ptx::fence_proxy_async_smem();
+  ptx::mbar_arrive_expect_tx(bar, kCvBoxBytes);
+  ptx::tma_load_4d(buf, tm, bar, 0, y0 - 1, x0 - 1, z - 1);
+}
+
+__global__ void __launch_bounds__(kCvThreads, 2)
+    conv16_kernel(const __grid_constant__ CUtensorMap tm, const uint32_t *__restrict__ frag,
+                  const __nv_bfloat16 *__restrict__ wbf, int boff, __nv_bfloat16 *__restrict__ out,
+                  ConvGrid g, int *__restrict__ err) {
+  extern __shared__ unsigned char smem_raw[];
+  const uint32_t base = (ptx::smem_u32(smem_raw) + 1023u) & ~1023u;
+  const uint32_t bar0 = base + 2 * kCvBufBytes;  // barrier of buffer b at bar0 + 8 * b
+  volatile int *abort_flag =
+      reinterpret_cast<volatile int *>(smem_raw + (base + 2 * kCvBufBytes + 16 - ptx::smem_u32(smem_raw)));
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t B[27][2][2];
+#pragma unroll
+  for (int t = 0; t < 27; ++t)
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int r = 0; r < 2; ++r) B[t][j][r] = __ldg(frag + ((t * 2 + j) * 2 + r) * 32 + lane);
+  const int c2 = 2 * (lane & 3), g8 = lane >> 2;
+  float bias[2][2];
+#pragma unroll
+  for (int j = 0; j < 2; ++j)
+#pragma unroll
+    for (int e = 0; e < 2; ++e) bias[j][e] = __bfloat162float(wbf[boff + 8 * j + c2 + e]);
+  if (threadIdx.x == 0) {
+    ptx::mbar_init(bar0, 1);
+    ptx::mbar_init(bar0 + 8, 1);
+    *abort_flag = 0;
+    ptx::fence_mbarrier_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if ((int)blockIdx.x < g.tiles) conv_issue(&tm, base, bar0, g, blockIdx.x);
+    if ((int)(blockIdx.x + gridDim.x) < g.tiles)
+      conv_issue(&tm, base + kCvBufBytes, bar0 + 8, g, blockIdx.x + gridDim.x);
+  }
+  const int m = lane >> 3, q = lane & 7;
+  const int arow = q + 8 * (m & 1), ahalf = m >> 1;  // ldmatrix: A row (voxel) and channel half
+  const int ys = warp * 16;
+  int k = 0;
+  for (int tile = blockIdx.x; tile < g.tiles; tile += gridDim.x, ++k) {
+    const int b = k & 1;
+    const uint32_t buf = base + b * kCvBufBytes, bar = bar0 + 8 * b;
+    if (!ptx::mbar_wait_bounded(bar, (k >> 1) & 1, kConvTimeoutNs)) *abort_flag = 1;
+    __syncthreads();
+    if (*abort_flag) {
+      if (threadIdx.x == 0) {
+        atomicExch(err, 3);
+        // let this CTA's own copies in flight land (bounded) before leaving
+        ptx::mbar_wait_bounded(bar, (k >> 1) & 1, kConvTimeoutNs);
+        if (tile + (int)gridDim.x < g.tiles)
+          ptx::mbar_wait_bounded(bar0 + 8 * (b ^ 1), ((k + 1) >> 1) & 1, kConvTimeoutNs);
+      }
+      return;
+    }
+    float acc[kCvTX][2][4];
+#pragma unroll
+    for (int o = 0; o < kCvTX; ++o)
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) acc[o][j][e] = 0.f;
+#pragma unroll
+    for (int iz = 0; iz < 3; ++iz) {
+#pragma unroll
+      for (int ix = 0; ix < kCvSX; ++ix) {
+#pragma unroll
+        for (int ky = 0; ky < 3; ++ky) {
+          const int sv = (iz * kCvSX + ix) * kCvSY + ys + arow + ky;
+          uint32_t a0, a1, a2, a3;
+          ldmatrix_x4(buf + (uint32_t)(sv * 32 + ((ahalf ^ ((sv >> 2) & 1)) << 4)), a0, a1, a2,
+                      a3);
+#pragma unroll
+          for (int o = 0; o < kCvTX; ++o) {
+            const int kx = ix - o;
+            if (kx < 0 || kx > 2) continue;
+            const int t = iz * 9 + kx * 3 + ky;
+            mma_bf16(acc[o][0], a0, a1, a2, a3, B[t][0][0], B[t][0][1]);
+            mma_bf16(acc[o][1], a0, a1, a2, a3, B[t][1][0], B[t][1][1]);
+          }
+        }
+      }
+    }
+    int z, x0, y0;
+    conv_tile_origin(g, tile, z, x0, y0);
+#pragma unroll
+    for (int o = 0; o < kCvTX; ++o) {
+      const int x = x0 + o;
+      if (x >= g.nx) break;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int y = y0 + ys + g8 + 8 * h;
+        if (y >= g.ny) continue;
+        __nv_bfloat16 *dst = out + (((long long)z * g.nx + x) * g.ny + y) * kC;
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          const float v0 = fmaxf(acc[o][j][2 * h] + bias[j][0], 0.f);
+          const float v1 = fmaxf(acc[o][j][2 * h + 1] + bias[j][1], 0.f);
+          *reinterpret_cast<__nv_bfloat162 *>(dst + 8 * j + c2) = __floats2bfloat162_rn(v0, v1);
+        }
+      }
+    }
+    __syncthreads();  // every warp is done with this buffer
+    if (threadIdx.x == 0 && tile + 2 * (int)gridDim.x < g.tiles)
+      conv_issue(&tm, buf, bar, g, tile + 2 * gridDim.x);
+  }
+}
+
+// ---------------------------------------------------------------- proposal + rescoring
+
+// Head weights [33][16] then biases [33], staged in shared memory by every kernel that proposes.
+constexpr int kHeadFloats = kHeads * kC + kHeads;
+
+// Per-axis offset probabilities of one (voxel, atlas) pair from its 16 conv4 features: the three
+// softmaxes over dw, du, dv of the heads' logits, p[a * 11 + j] for offset j - 5 on axis a.
+__device__ __forceinline__ void axis_probs(const __nv_bfloat16 *__restrict__ fv,
+                                           const float *__restrict__ hw, float (&p)[kHeads]) {
+  float f[kC];
+  {
+    __align__(16) __nv_bfloat16 fb[kC];
+    const uint4 *src = reinterpret_cast<const uint4 *>(fv);
+    reinterpret_cast<uint4 *>(fb)[0] = src[0];
+    reinterpret_cast<uint4 *>(fb)[1] = src[1];
+#pragma unroll
+    for (int c = 0; c < kC; ++c) f[c] = __bfloat162float(fb[c]);
+  }
+#pragma unroll
+  for (int o = 0; o < kHeads; ++o) {
+    float acc = hw[kHeads * kC + o];
+#pragma unroll
+    for (int c = 0; c < kC; ++c) acc = fmaf(hw[o * kC + c], f[c], acc);
+    p[o] = acc;
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    float m = p[a * kAxis];
+#pragma unroll
+    for (int j = 1; j < kAxis; ++j) m = fmaxf(m, p[a * kAxis + j]);
+    float sum = 0.f;
+#pragma unroll
+    for (int j = 0; j < kAxis; ++j) {
+      p[a * kAxis + j] = __expf(p[a * kAxis + j] - m);
+      sum += p[a * kAxis + j];
+    }
+    const float inv = 1.f / sum;
+#pragma unroll
+    for (int j = 0; j < kAxis; ++j) p[a * kAxis + j] *= inv;
+  }
+}
+
+// The 4 largest of p[a * 11 .. a * 11 + 10] in order, ties to the lower offset: indices 0..10.
+__device__ __forceinline__ void top4(const float (&p)[kHeads], int a, int (&idx)[4]) {
+  unsigned used = 0;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    int bi = 0;
+    float bp = -1.f;
+#pragma unroll
+    for (int j = 0; j < kAxis; ++j)
+      if (!((used >> j) & 1u) && p[a * kAxis + j] > bp) {
+        bp = p[a * kAxis + j];
+        bi = j;
+      }
+    used |= 1u << bi;
+    idx[r] = bi;
+  }
+}
+
+// p[a * 11 + idx] for a run-time idx, without local memory.
+__device__ __forceinline__ float pick(const float (&p)[kHeads], int a, int idx) {
+  float v = 0.f;
+#pragma unroll
+  for (int j = 0; j < kAxis; ++j) v = (j == idx) ? p[a * kAxis + j] : v;
+  return v;
+}
+
+// Probability mass p_w * p_u * p_v of the kept set: rank triples (i, j, k), i + j + k <= 4, of
+// the per-axis lists top[a][0..3].
+__device__ __forceinline__ float kept_mass(const float (&p)[kHeads], const int (&top)[3][4]) {
+  float tp[3][4];
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int r = 0; r < 4; ++r) tp[a][r] = pick(p, a, top[a][r]);
+  float t[5];
+#pragma unroll
+  for (int s2 = 1; s2 <= 4; ++s2) {
+    float acc = 0.f;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (j + k <= s2) acc = fmaf(tp[1][j], tp[2][k], acc);
+    t[s2] = acc;
+  }
+  return tp[0][0] * t[4] + tp[0][1] * t[3] + tp[0][2] * t[2] + tp[0][3] * t[1];
+}
+
+// The proposal of one voxel on its own (the testing hook reports it): its 4 most probable
+// offsets per axis (as -5..5) and the mass of its kept set.
+struct Proposal {
+  signed char top[3][4];
+  float conf;
+};
+
+__device__ __forceinline__ void propose(const __nv_bfloat16 *__restrict__ fv,
+                                        const float *__restrict__ hw, Proposal &pr) {
+  float p[kHeads];
+  axis_probs(fv, hw, p);
+  int top[3][4];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    top4(p, a, top[a]);
+#pragma unroll
+    for (int r = 0; r < 4; ++r) pr.top[a][r] = (signed char)(top[a][r] - 5);
+  }
+  pr.conf = kept_mass(p, top);
+}
+
+// Testing hook: the proposal of given voxels.
+__global__ void proposal_hook_kernel(const __nv_bfloat16 *__restrict__ f4,
+                                     const __nv_bfloat16 *__restrict__ wbf,
+                                     const int64_t *__restrict__ voxels, int n,
+                                     signed char *__restrict__ top, float *__restrict__ conf) {
+  __shared__ float hw[kHeadFloats];
+  for (int i = threadIdx.x; i < kHeadFloats; i += blockDim.x) hw[i] = __bfloat162float(wbf[kH + i]);
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Proposal pr;
+  propose(f4 + voxels[i] * kC, hw, pr);
+  for (int a = 0; a < 3; ++a)
+    for (int r = 0; r < 4; ++r) top[i * 12 + a * 4 + r] = pr.top[a][r];
+  conf[i] = pr.conf;
+}
+
+constexpr int kRowOut = 30;       // output voxels per warp row (lanes 1..30)
+constexpr int kRescoreWarps = 4;  // warps per CTA
+
+// Exact FP32 rescoring of one atlas. A warp owns a row segment (z, x, y0 .. y0+29) of interior
+// voxels; lane l sits at y = y0 - 1 + l (lanes 0 and 31 are the y halo). Every voxel of the
+// segment computes its per-axis probabilities; their sums over the segment give the row's
+// proposal: per axis the 4 most probable offsets, and the 32 rank triples with i + j + k <= 4.
+// A voxel whose own probability mass on those 32 is below conf_thr falls back to all 11^3
+// offsets. Each offset is evaluated once for all 32 lanes: D(y) = sum over the 3x3 (dz, dx) taps
+// of the squared differences at y, then SSD(y) = D(y-1) + D(y) + D(y+1) by warp shuffles; a lane
+// adds the weight exp(-SSD/div) and the weighted CT value for the offsets it keeps.
+__device__ __forceinline__ void eval_offset(const float *__restrict__ atl,
+                                            const float *__restrict__ lab, const float (&in)[9],
+                                            long long vz, long long axy, int apitch, int yc,
+                                            int dw, int du, int dv, bool take, float &P,
+                                            float &W, float neg_k) {
+  const float *a = atl + vz + (long long)(dw - 1) * axy + (long long)(du - 1) * apitch + yc + dv;
+  float d = 0.f;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    const float t = in[k] - __ldg(a + (long long)(k / 3) * axy + (long long)(k % 3) * apitch);
+    d = fmaf(t, t, d);
+  }
+  const float ssd =
+      __shfl_up_sync(0xffffffffu, d, 1) + d + __shfl_down_sync(0xffffffffu, d, 1);
+  if (take) {
+    const float w = ptx::ex2_approx(ssd * neg_k);
+    P = fmaf(w, __ldg(lab + vz + (long long)dw * axy + (long long)du * apitch + yc + dv), P);
+    W += w;
+  }
+}
+
+__global__ void __launch_bounds__(kRescoreWarps * 32, 3)
+    rescore_kernel(const __nv_bfloat16 *__restrict__ f4, const __nv_bfloat16 *__restrict__ wbf,
+                   const float *__restrict__ img, const float *__restrict__ atl,
+                   const float *__restrict__ lab, int nx, int ny, int nz, int apitch, float neg_k,
+                   float conf_thr, float *__restrict__ pacc, float *__restrict__ wacc,
+                   unsigned long long *__restrict__ fallbacks,
+                   unsigned long long *__restrict__ evaluated) {
+  __shared__ float hw[kHeadFloats];
+  for (int i = threadIdx.x; i < kHeadFloats; i += blockDim.x) hw[i] = __bfloat162float(wbf[kH + i]);
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int lo = 6;
+  const int ix = nx - 2 * lo, iz = nz - 2 * lo, iy = ny - 2 * lo;
+  if (ix <= 0 || iy <= 0 || iz <= 0) return;
+  const int segs = (iy + kRowOut - 1) / kRowOut;
+  const long long items = (long long)iz * ix * segs;
+  const int nxy = nx * ny;
+  const long long axy = (long long)nx * apitch;
+  unsigned long long my_fallbacks = 0, my_evals = 0;
+  for (long long it = (long long)blockIdx.x * kRescoreWarps + (threadIdx.x >> 5); it < items;
+       it += (long long)gridDim.x * kRescoreWarps) {
+    const int seg = (int)(it % segs);
+    const long long r0 = it / segs;
+    const int x = (int)(r0 % ix) + lo, z = (int)(r0 / ix) + lo;
+    const int y0 = lo + seg * kRowOut;
+    const int y = y0 - 1 + lane;
+    const bool out_lane = lane >= 1 && lane <= kRowOut && y < ny - lo;
+    const int yc = min(y, ny - lo);  // halo lanes past the interior load clamped (unused) values
+    // the voxel's probabilities, the row's sums, the row's proposal
+    float p[kHeads];
+    if (out_lane) {
+      axis_probs(f4 + ((long long)z * nxy + (long long)x * ny + y) * kC, hw, p);
+    } else {
+#pragma unroll
+      for (int o = 0; o < kHeads; ++o) p[o] = 0.f;
+    }
+    int top[3][4];
+    {
+      float rs[kHeads];
+#pragma unroll
+      for (int o = 0; o < kHeads; ++o) {
+        float v = p[o];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        rs[o] = v;
+      }
+#pragma unroll
+      for (int a = 0; a < 3; ++a) top4(rs, a, top[a]);
+    }
+    const bool full = out_lane && kept_mass(p, top) < conf_thr;
+    const unsigned any_full = __ballot_sync(0xffffffffu, full);
+    if (full) ++my_fallbacks;
+    // input taps of this lane: I(z+dz, x+dx, y), 3x3 (dz, dx)
+    float in[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k)
+      in[k] = __ldg(img + (long long)(z + k / 3 - 1) * nxy + (long long)(x + k % 3 - 1) * ny + yc);
+    const long long vz = (long long)(z - 1) * axy + (long long)(x - 1) * apitch;  // (dz,dx)=(-1,-1)
+    float P = 0.f, W = 0.f;
+    if (!any_full) {
+      // the 32 kept offsets, in rank-triple order
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j + i < 5 && j < 4; ++j)
+#pragma unroll
+          for (int k = 0; k + j + i < 5 && k < 4; ++k)
+            eval_offset(atl, lab, in, vz + axy + apitch, axy, apitch, yc, top[0][i] - 5,
+                        top[1][j] - 5, top[2][k] - 5, out_lane, P, W, neg_k);
+      my_evals += 32;
+    } else {
+      // the full window; lanes that did not fall back keep only their row's 32
+      unsigned long long rank[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        rank[a] = 0x77777777777ULL;  // nibble j: rank of offset j - 5 on axis a, 7 = not kept
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          rank[a] &= ~(0xFULL << (4 * top[a][r]));
+          rank[a] |= (unsigned long long)r << (4 * top[a][r]);
+        }
+      }
+      for (int jw = 0; jw < kAxis; ++jw) {
+        const int rw = (int)((rank[0] >> (4 * jw)) & 0xF);
+        for (int ju = 0; ju < kAxis; ++ju) {
+          const int ru = rw + (int)((rank[1] >> (4 * ju)) & 0xF);
+          for (int jv = 0; jv < kAxis; ++jv) {
+            const bool mine = full || (ru + (int)((rank[2] >> (4 * jv)) & 0xF) <= 4);
+            eval_offset(atl, lab, in, vz + axy + apitch, axy, apitch, yc, jw - 5, ju - 5, jv - 5,
+                        mine && out_lane, P, W, neg_k);
+          }
+        }
+      }
+      my_evals += kAxis * kAxis * kAxis;
+    }
+    if (out_lane) {
+      const long long v = (long long)z * nxy + (long long)x * ny + y;
+      pacc[v] += P;
+      wacc[v] += W;
+    }
+  }
+  if (my_fallbacks) atomicAdd(fallbacks, my_fallbacks);
+  if (lane == 0 && my_evals) atomicAdd(evaluated, my_evals);
+}
+
+__global__ void finalize_kernel(const float *__restrict__ pacc, const float *__restrict__ wacc,
+                                float *__restrict__ out, int nx, int ny, int nz) {
+  const int lo = 6;
+  const int ix = nx - 2 * lo, iy = ny - 2 * lo, iz = nz - 2 * lo;
+  const long long total = (ix > 0 && iy > 0 && iz > 0) ? (long long)ix * iy * iz : 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int y = (int)(i % iy) + lo;
+    const long long r0 = i / iy;
+    const int x = (int)(r0 % ix) + lo;
+    const int z = (int)(r0 / ix) + lo;
+    const long long v = (long long)z * nx * ny + (long long)x * ny + y;
+    const float pr = pacc[v], sw = wacc[v];
+    out[v] = (fabsf(pr) > kDblEpsilonF && fabsf(sw) > kDblEpsilonF) ? __fdiv_rn(pr, sw)
+                                                                    : __int_as_float(0x7fc00000);
+  }
+}
+
+int sms() {
+  int dev = 0, n = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  return n;
+}
+
+// Scratch layout: two BF16 channel-last feature volumes, the product and weight sums, the three
+// packed fragment tables and the fallback counter.
+struct InferScratch {
+  __nv_bfloat16 *fa, *fb;
+  float *pacc, *wacc;
+  uint32_t *frag;
+  unsigned long long *fallbacks;  // (voxel, atlas) pairs that took the full search
+  unsigned long long *evaluated;  // offsets evaluated by warp rows, summed over rows
+  int *err;                       // bounded-wait status of the probe hook
+};
+
+InferScratch carve(void *scratch, long long nvox) {
+  InferScratch r;
+  unsigned char *p = static_cast<unsigned char *>(scratch);
+  r.fa = reinterpret_cast<__nv_bfloat16 *>(p);
+  r.fb = r.fa + nvox * kC;
+  r.pacc = reinterpret_cast<float *>(r.fb + nvox * kC);
+  r.wacc = r.pacc + nvox;
+  r.frag = reinterpret_cast<uint32_t *>(r.wacc + nvox);
+  r.fallbacks = reinterpret_cast<unsigned long long *>(r.frag + 3 * kFragWords);
+  r.evaluated = r.fallbacks + 1;
+  r.err = reinterpret_cast<int *>(r.fallbacks + 2);
+  return r;
+}
+
+}  // namespace
+
+size_t infer_scratch_bytes(long long nvox) {
+  return (size_t)nvox * kC * 2 * 2 + (size_t)nvox * 4 * 2 + 3 * kFragWords * 4 + 256;
+}
+
+unsigned long long *infer_counters(void *scratch, long long nvox) {
+  return carve(scratch, nvox).fallbacks;
+}
+
+namespace {
+
+// TMA map over a channel-last BF16 feature volume [nz][nx][ny][16]: one box is a conv16 slab
+// (3 z x 6 x x 66 y voxels), 32-byte swizzled, out-of-volume voxels zero.
+cudaError_t make_feature_map(CUtensorMap *map, const __nv_bfloat16 *base, const Geometry &g) {
+  auto fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(tensor_map_encoder());
+  if (!fn) return cudaErrorNotSupported;
+  const cuuint64_t dims[4] = {(cuuint64_t)kC, (cuuint64_t)g.ny, (cuuint64_t)g.nx, (cuuint64_t)g.nz};
+  const cuuint64_t strides[3] = {(cuuint64_t)kC * 2, (cuuint64_t)kC * 2 * g.ny,
+                                 (cuuint64_t)kC * 2 * g.ny * g.nx};
+  const cuuint32_t box[4] = {(cuuint32_t)kC, (cuuint32_t)kCvSY, (cuuint32_t)kCvSX, (cuuint32_t)kCvSZ};
+  const cuuint32_t estr[4] = {1u, 1u, 1u, 1u};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16 *>(base), dims,
+                  strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+// conv1 .. conv4 of one (input, atlas) pair; returns the buffer holding the conv4 features.
+cudaError_t run_convs(const Geometry &g, const __nv_bfloat16 *wbf, const float *img,
+                      const float *atlas_a, int apitch, const InferScratch &sc, int *err,
+                      __nv_bfloat16 **features, cudaStream_t s) {
+  const int n_sm = sms();
+  {
+    const long long items = (long long)g.nz * g.nx * ((g.ny + kC1Vox - 1) / kC1Vox);
+    const long long want = (items + 255) / 256;
+    const int blocks = (int)(want < 8LL * n_sm ? want : 8LL * n_sm);
+    conv1_kernel<<<blocks, 256, 0, s>>>(img, atlas_a, wbf, sc.fa, g.nx, g.ny, g.nz, apitch);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  CUtensorMap maps[2];
+  if ((e = make_feature_map(&maps[0], sc.fa, g)) != cudaSuccess) return e;
+  if ((e = make_feature_map(&maps[1], sc.fb, g)) != cudaSuccess) return e;
+  ConvGrid cg;
+  cg.nx = g.nx;
+  cg.ny = g.ny;
+  cg.nz = g.nz;
+  cg.tiles_y = (g.ny + kCvTY - 1) / kCvTY;
+  cg.tiles_x = (g.nx + kCvTX - 1) / kCvTX;
+  cg.tiles = cg.tiles_y * cg.tiles_x * g.nz;
+  const int blocks = cg.tiles < 2 * n_sm ? cg.tiles : 2 * n_sm;
+  const int boffs[3] = {kB2, kB3, kB4};
+  __nv_bfloat16 *bufs[2] = {sc.fa, sc.fb};
+  for (int l = 0; l < 3; ++l) {
+    conv16_kernel<<<blocks, kCvThreads, kConvSmem, s>>>(maps[l & 1], sc.frag + l * kFragWords, wbf,
+                                                        boffs[l], bufs[(l + 1) & 1], cg, err);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  *features = bufs[1];  // conv2 -> fb, conv3 -> fa, conv4 -> fb
+  return cudaSuccess;
+}
+
+cudaError_t pack_all(const __nv_bfloat16 *wbf, uint32_t *frag, cudaStream_t s) {
+  cudaError_t e0 = cudaFuncSetAttribute(conv16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)kConvSmem);
+  if (e0 != cudaSuccess) return e0;
+  const int woffs[3] = {kW2, kW3, kW4};
+  for (int l = 0; l < 3; ++l) {
+    pack_frags_kernel<<<(kFragWords + 255) / 256, 256, 0, s>>>(wbf, woffs[l], frag + l * kFragWords);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+}  // namespace
+
+// The learned form over all atlases of `in` (atlas and label rows `in.pitch` floats apart, the
+// input MRI contiguous). Writes the interior of `out`; the border is left untouched.
+cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInputs &in, float *out,
+                           double div, float conf_thr, void *scratch, int *err, cudaStream_t s) {
+  const __nv_bfloat16 *wbf = static_cast<const __nv_bfloat16 *>(weights);
+  const long long nvox = g.nvox();
+  const long long astride = (long long)g.nz * g.nx * in.pitch;
+  const InferScratch sc = carve(scratch, nvox);
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(sc.pacc, 0, (size_t)nvox * 4 * 2, s)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(sc.fallbacks, 0, 2 * sizeof(unsigned long long), s)) != cudaSuccess)
+    return e;
+  if ((e = pack_all(wbf, sc.frag, s)) != cudaSuccess) return e;
+  const float neg_k = (float)(-1.4426950408889634 / div);
+  const int nblk = sms() * 8;
+  long long rows = 0;
+  if (g.nx > 12 && g.ny > 12 && g.nz > 12)
+    rows = (long long)(g.nz - 12) * (g.nx - 12) * ((g.ny - 12 + kRowOut - 1) / kRowOut);
+  const long long rblk = (rows + kRescoreWarps - 1) / kRescoreWarps;
+  const int rescore_blocks = (int)(rblk < 1 ? 1 : (rblk > 64LL * sms() ? 64LL * sms() : rblk));
+  for (int a = 0; a < g.num; ++a) {
+    const float *A = in.atlas + a * astride, *L = in.label + a * astride;
+    __nv_bfloat16 *f4 = nullptr;
+    if ((e = run_convs(g, wbf, in.img, A, in.pitch, sc, err, &f4, s)) != cudaSuccess) return e;
+    rescore_kernel<<<rescore_blocks, kRescoreWarps * 32, 0, s>>>(
+        f4, wbf, in.img, A, L, g.nx, g.ny, g.nz, in.pitch, neg_k, conf_thr, sc.pacc, sc.wacc,
+        sc.fallbacks, sc.evaluated);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  finalize_kernel<<<nblk, 256, 0, s>>>(sc.pacc, sc.wacc, out, g.nx, g.ny, g.nz);
+  return cudaGetLastError();
+}
+
+// Testing hook: conv4 features and proposals of one (input, atlas) pair at given voxels.
+cudaError_t learned_probe(const Geometry &g, const void *weights, const float *img,
+                          const float *atlas_a, void *scratch, const int64_t *voxels, int n,
+                          float *features, signed char *top, float *conf, cudaStream_t s) {
+  const __nv_bfloat16 *wbf = static_cast<const __nv_bfloat16 *>(weights);
+  const InferScratch sc = carve(scratch, g.nvox());
+  cudaError_t e;
+  if ((e = pack_all(wbf, sc.frag, s)) != cudaSuccess) return e;
+  __nv_bfloat16 *f4 = nullptr;
+  if ((e = cudaMemsetAsync(sc.err, 0, sizeof(int), s)) != cudaSuccess) return e;
+  if ((e = run_convs(g, wbf, img, atlas_a, g.ny, sc, sc.err, &f4, s)) != cudaSuccess) return e;
+  // the sums area is free here: voxel list, proposals and confidences go there
+  int64_t *d_vox = reinterpret_cast<int64_t *>(sc.pacc);
+  signed char *d_top = reinterpret_cast<signed char *>(d_vox + n);
+  float *d_conf = reinterpret_cast<float *>(d_top + ((12 * (size_t)n + 15) / 16) * 16);
+  if ((size_t)n * (8 + 12 + 4) + 16 > (size_t)g.nvox() * 8) return cudaErrorInvalidValue;
+  if ((e = cudaMemcpyAsync(d_vox, voxels, n * sizeof(int64_t), cudaMemcpyHostToDevice, s)) !=
+      cudaSuccess)
+    return e;
+  proposal_hook_kernel<<<(n + 127) / 128, 128, 0, s>>>(f4, wbf, d_vox, n, d_top, d_conf);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (top && (e = cudaMemcpyAsync(top, d_top, 12 * (size_t)n, cudaMemcpyDeviceToHost, s)) !=
+                 cudaSuccess)
+    return e;
+  if (conf && (e = cudaMemcpyAsync(conf, d_conf, 4 * (size_t)n, cudaMemcpyDeviceToHost, s)) !=
+                  cudaSuccess)
+    return e;
+  int status = 0;
+  if ((e = cudaMemcpyAsync(&status, sc.err, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+    return e;
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+  if (status != 0) return cudaErrorLaunchTimeout;
+  if (features) {
+    for (int i = 0; i < n; ++i) {
+      __nv_bfloat16 tmp[kC];
+      if ((e = cudaMemcpy(tmp, f4 + voxels[i] * kC, sizeof(tmp), cudaMemcpyDeviceToHost)) !=
+          cudaSuccess)
+        return e;
+      for (int c = 0; c < kC; ++c) features[i * kC + c] = __bfloat162float(tmp[c]);
+    }
+  }
+  return cudaSuccess;
+}
+
+}  // namespace learned
+}  // namespace pct

@@ -1,0 +1,278 @@
+"""Learned-proposal form, inference side, on the GPU (EXEC_CHOICE 7).
+
+* With every pair forced to the full search (threshold above 1) the form is the plain method and
+  must match the FP64 oracle within the plain gate (1e-4 relative).
+* With a fixed "prior" network (zero convolutions, head biases only) every voxel and every row
+  gets the same 32 offsets, so the output has an exact float64 restatement: the fusion over
+  those offsets.
+* The committed trained network beats the same-k baselines without it (the centre prior and an
+  untrained network) in recall of the plain method's top-32 and in error against the plain
+  method.
+* The tensor-core convolutions and the proposal step are checked voxel by voxel against a float64
+  restatement of the network on the BF16 weights.
+"""
+import numpy as np
+import pytest
+import torch
+import torch.nn.functional as F
+
+import learned_ref
+import oracle
+import pseudoctimaging_b200 as pct
+from conftest import DBL_EPS, compare_fused
+from pseudoctimaging_b200 import learned
+
+pytestmark = pytest.mark.gpu
+NH = 11
+LO = 6
+DIV = 337.5
+
+
+def subject(nx, ny, nz, num, seed):
+    s = pct.synth_subject(nx, ny, nz, num, n_blobs=12, seed=seed)
+    return s.img, s.atlas_mri, pct.normalize_labels(s.atlas_ct)
+
+
+prior_params = learned.prior_params
+
+
+def prior_proposal(scales=(0.7, 0.5, 0.3)):
+    """Offsets in rank order per axis and the confidence, in float64 (ties: lower offset first)."""
+    top, probs = [], []
+    for c in scales:
+        logits = np.array([-c * (j - 5) ** 2 for j in range(11)], np.float64)
+        p = np.exp(logits - logits.max())
+        p /= p.sum()
+        order = sorted(range(11), key=lambda j: (-p[j], j))[:4]
+        top.append([j - 5 for j in order])
+        probs.append([p[j] for j in order])
+    conf = sum(probs[0][i] * probs[1][j] * probs[2][k] for i in range(4) for j in range(4)
+               for k in range(4) if i + j + k <= 4)
+    return np.array(top), conf
+
+
+def fuse_offsets_f64(img, atlas, label, offsets, div):
+    """Float64 fusion over a fixed offset list at every interior voxel; (out, prod, sumw)."""
+    nz, nx, ny = img.shape
+    I = img.astype(np.float64)
+    shape = (nz - 2 * LO, nx - 2 * LO, ny - 2 * LO)
+    P, W = np.zeros(shape), np.zeros(shape)
+
+    def win(vol, dz, dx, dy):
+        return vol[LO + dz:nz - LO + dz, LO + dx:nx - LO + dx, LO + dy:ny - LO + dy]
+
+    for a in range(atlas.shape[0]):
+        A = atlas[a].astype(np.float64)
+        L = label[a].astype(np.float64)
+        for dw, du, dv in offsets:
+            ssd = np.zeros(shape)
+            for dz in (-1, 0, 1):
+                for dx in (-1, 0, 1):
+                    for dy in (-1, 0, 1):
+                        ssd += (win(I, dz, dx, dy) - win(A, dz + dw, dx + du, dy + dv)) ** 2
+            w = np.exp(-ssd / div)
+            P += w * win(L, dw, du, dv)
+            W += w
+    out = np.zeros_like(img)
+    prod, sumw = np.zeros(img.shape), np.zeros(img.shape)
+    core = (slice(LO, nz - LO), slice(LO, nx - LO), slice(LO, ny - LO))
+    ok = (np.abs(P) > DBL_EPS) & (np.abs(W) > DBL_EPS)
+    out[core] = np.where(ok, P / np.where(ok, W, 1.0), np.nan)
+    prod[core], sumw[core] = P, W
+    return out, prod, sumw
+
+
+def rows_of(nx, ny, nz):
+    return (nz - 2 * LO) * (nx - 2 * LO) * -(-(ny - 2 * LO) // 30)
+
+
+def interior(nx, ny, nz):
+    return (nz - 2 * LO) * (nx - 2 * LO) * (ny - 2 * LO)
+
+
+def test_attach_rules():
+    img, atl, lab = subject(30, 31, 28, 1, 5)
+    with pct.Handle(0) as h:
+        with pytest.raises(pct.PctError) as e:
+            h.synthesize(img, atl, lab, NH, DIV, pct.EXEC_LEARNED)
+        assert e.value.status == -4
+        with learned.LearnedModel(0, seed=1) as m:
+            with pytest.raises(pct.PctError) as e:
+                h.attach_model(m, -0.5)
+            assert e.value.status == -1
+            h.attach_model(m, 0.0)
+            with pytest.raises(pct.PctError) as e:
+                h.synthesize(img, atl, lab, 9, DIV, pct.EXEC_LEARNED)
+            assert e.value.status == -4
+            out = h.synthesize(img, atl, lab, NH, DIV, pct.EXEC_LEARNED)
+            assert np.all(out[:LO] == 0) and np.all(out[:, :, -LO:] == 0)
+            h.attach_model(None)
+            with pytest.raises(pct.PctError):
+                h.synthesize(img, atl, lab, NH, DIV, pct.EXEC_LEARNED)
+
+
+@pytest.mark.parametrize("shape", [(36, 41, 30, 2), (44, 70, 33, 3)])
+def test_full_fallback_is_the_plain_method(shape):
+    nx, ny, nz, num = shape
+    img, atl, lab = subject(nx, ny, nz, num, 11)
+    ref, prod, sumw = oracle.fuse_port(img, atl, lab, NH, DIV, with_sums=True)
+    with pct.Handle(0) as h, learned.LearnedModel(0, seed=2) as m:
+        h.attach_model(m, 2.0)
+        got = h.synthesize(img, atl, lab, NH, DIV, pct.EXEC_LEARNED)
+        st = h.learned_stats()
+    compare_fused(got, ref, NH, 1e-4, prod, sumw)
+    assert st["fallback_pairs"] == interior(nx, ny, nz) * num
+    assert st["row_offsets"] == rows_of(nx, ny, nz) * 1331 * num
+
+
+def test_prior_proposal_exact():
+    nx, ny, nz, num = 40, 47, 32, 2
+    img, atl, lab = subject(nx, ny, nz, num, 21)
+    top, conf = prior_proposal()
+    offsets = learned.rank_sum_set(top)
+    assert len({tuple(o) for o in offsets}) == 32
+    ref, prod, sumw = fuse_offsets_f64(img, atl, lab, offsets, DIV)
+    with pct.Handle(0) as h, learned.LearnedModel(0, params=prior_params()) as m:
+        h.attach_model(m, 0.0)
+        got = h.synthesize(img, atl, lab, NH, DIV, pct.EXEC_LEARNED)
+        st = h.learned_stats()
+    compare_fused(got, ref, NH, 1e-4, prod, sumw)
+    assert st["fallback_pairs"] == 0
+    assert st["row_offsets"] == rows_of(nx, ny, nz) * 32 * num
+
+
+def test_confidence_threshold():
+    nx, ny, nz, num = 34, 37, 29, 1
+    img, atl, lab = subject(nx, ny, nz, num, 31)
+    _, conf = prior_proposal()
+    ref = oracle.fuse_port(img, atl, lab, NH, DIV)
+    with pct.Handle(0) as h, learned.LearnedModel(0, params=prior_params()) as m:
+        h.attach_model(m, conf * (1 - 1e-3))
+        h.synthesize(img, atl, lab, NH, DIV, pct.EXEC_LEARNED)
+        assert h.learned_stats()["fallback_pairs"] == 0
+        h.attach_model(m, conf * (1 + 1e-3))
+        got = h.synthesize(img, atl, lab, NH, DIV, pct.EXEC_LEARNED)
+        assert h.learned_stats()["fallback_pairs"] == interior(nx, ny, nz) * num
+    compare_fused(got, ref, NH, 1e-4)
+
+
+def test_probe_matches_float64_network():
+    nx, ny, nz = 38, 45, 31
+    img, atl, _ = subject(nx, ny, nz, 1, 41)
+    rng = np.random.default_rng(0)
+    z = rng.integers(LO, nz - LO, 48)
+    x = rng.integers(LO, nx - LO, 48)
+    y = rng.integers(LO, ny - LO, 48)
+    vox = (z * nx + x) * ny + y
+    with learned.LearnedModel(0, seed=7) as m:
+        # larger head weights than the initialisation, so that the proposals are not ties
+        p = m.get_params()
+        p[-33 - 33 * 16:-33] *= 20.0
+        m.set_params(p)
+        wb = m.get_params(inference_precision=True)
+        d_img = torch.from_numpy(img).cuda()
+        d_atl = torch.from_numpy(atl[0]).cuda()
+        feats, top, conf = m.probe(d_img.data_ptr(), d_atl.data_ptr(), nx, ny, nz, vox)
+    ps = {k: torch.tensor(v, dtype=torch.float64) for k, v in learned_ref.unflatten(
+        wb.astype(np.float64)).items()}
+    x64 = torch.tensor(learned_ref.patches([img], [atl], [(0, 0, int(v)) for v in vox],
+                                           None))
+    h = x64
+    for i in range(1, 5):
+        h = F.relu(F.conv3d(h, ps[f"W{i}"], ps[f"B{i}"]))
+    ref = h.reshape(len(vox), 16).numpy()
+    scale = np.abs(ref).max()
+    err = np.abs(feats - ref)
+    assert err.max() <= 0.03 * scale + 1e-6, (err.max(), scale)
+    # proposals from the GPU's own features, in float64: same top-4 per axis, same confidence
+    logits = feats.astype(np.float64) @ ps["H"].numpy().T + ps["HB"].numpy()
+    for i in range(len(vox)):
+        probs = []
+        for a in range(3):
+            lg = logits[i, a * 11:(a + 1) * 11]
+            pr = np.exp(lg - lg.max())
+            pr /= pr.sum()
+            order = sorted(range(11), key=lambda j: (-pr[j], j))[:4]
+            got = [int(t) + 5 for t in top[i, a]]
+            # equal up to near-ties in FP32
+            for r in range(4):
+                assert got[r] == order[r] or abs(pr[got[r]] - pr[order[r]]) < 1e-5
+            probs.append([pr[j] for j in got])
+        c = sum(probs[0][a] * probs[1][b] * probs[2][k] for a in range(4) for b in range(4)
+                for k in range(4) if a + b + k <= 4)
+        assert abs(c - conf[i]) < 1e-4
+
+
+def test_host_device_and_pipeline_paths_agree():
+    nx, ny, nz, num = 33, 42, 30, 2
+    img, atl, lab = subject(nx, ny, nz, num, 51)
+    with pct.Handle(0) as h, learned.LearnedModel(0, seed=9) as m:
+        h.attach_model(m, 0.3)
+        host = h.synthesize(img, atl, lab, NH, DIV, pct.EXEC_LEARNED)
+        d = [torch.from_numpy(a).cuda() for a in (img, atl, lab)]
+        out = torch.zeros_like(d[0])
+        h.synthesize_device(d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), out.data_ptr(), nx,
+                            ny, nz, num, NH, DIV, pct.EXEC_LEARNED)
+        torch.cuda.synchronize()
+        dev = out.cpu().numpy()
+    np.testing.assert_array_equal(np.isnan(host), np.isnan(dev))
+    np.testing.assert_array_equal(np.nan_to_num(host), np.nan_to_num(dev))
+
+
+def test_checkpoint_round_trip(tmp_path):
+    with learned.LearnedModel(0, seed=4) as m:
+        p = m.get_params()
+        m.save(tmp_path / "m.pctl")
+    q = learned.load_params(tmp_path / "m.pctl")
+    np.testing.assert_array_equal(p, q)
+    with learned.LearnedModel.load(tmp_path / "m.pctl") as m2:
+        np.testing.assert_array_equal(m2.get_params(), p)
+
+
+def _structured_voxels(img, n, seed):
+    rng = np.random.default_rng(seed)
+    nz, nx, ny = img.shape
+    g = np.sqrt(sum(d.astype(np.float64) ** 2 for d in np.gradient(img)))
+    w = g[LO:nz - LO, LO:nx - LO, LO:ny - LO].ravel()
+    flat = rng.choice(w.size, n, replace=False, p=w / w.sum())
+    iz, ix, iy = np.unravel_index(flat, (nz - 2 * LO, nx - 2 * LO, ny - 2 * LO))
+    return ((iz + LO) * nx + ix + LO) * ny + iy + LO
+
+
+def test_trained_network_gain():
+    """The committed network against the same-k baselines without it, on a held-out subject:
+    the centre prior (no network) and an untrained network. Per-voxel recall of the plain
+    method's exact top-32 (float64) at structured voxels, and the fused result's error against
+    the plain FP32 method."""
+    nx, ny, nz, num = 128, 128, 80, 4
+    subj = pct.synth_subject(nx, ny, nz, num, n_blobs=14, seed=7001)
+    trained = learned.load_params(learned.CHECKPOINT)
+    with learned.LearnedModel(0, seed=7001) as m:
+        untrained = m.get_params()
+    models = {"trained": trained, "prior": learned.prior_params(), "untrained": untrained}
+    # recall of the exact top-32 by each voxel's own 32
+    vox = _structured_voxels(subj.img, 150, 3)
+    d_img = torch.from_numpy(subj.img).cuda()
+    d_atl = torch.from_numpy(subj.atlas_mri[0]).cuda()
+    truth = []
+    for v in vox:
+        ssd = learned_ref.top32_float64(subj.img, subj.atlas_mri[0], int(v))
+        truth.append(set(np.argsort(ssd, kind="stable")[:32].tolist()))
+    recall = {}
+    for name, p in models.items():
+        with learned.LearnedModel(0, params=p) as m:
+            _, top, _ = m.probe(d_img.data_ptr(), d_atl.data_ptr(), nx, ny, nz, vox)
+        hits = 0
+        for i in range(len(vox)):
+            kept = {(dw + 5) * 121 + (du + 5) * 11 + dv + 5
+                    for dw, du, dv in learned.rank_sum_set(top[i])}
+            hits += len(kept & truth[i])
+        recall[name] = hits / (32 * len(vox))
+    # fused error against the plain method, k = 32 (no fallback)
+    res = {name: learned.evaluate(p, [subj], thresholds=(0.0,), reps=1)[0]
+           for name, p in models.items()}
+    print("recall", recall, "mae", {k: v["mae_hu"] for k, v in res.items()})
+    assert recall["trained"] > recall["prior"] > recall["untrained"]
+    assert res["trained"]["mae_hu"] < res["prior"]["mae_hu"] < res["untrained"]["mae_hu"]
+    assert res["trained"]["mae_hu"] <= 5.0
+    assert res["trained"]["offsets_per_row"] == 32.0
