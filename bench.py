@@ -446,6 +446,191 @@ def run_batch_arm(args) -> None:
     print(json.dumps(line))
 
 
+def run_sharded_arm(args) -> None:
+    """One config-1 subject split into z slabs over the N ranks (one GPU each, strong scaling):
+    each rank holds its slab plus hw+1 halo planes of every input volume in its own HBM and runs
+    the plain kernel on that sub-volume; value = the whole subject's voxels / the slowest rank's
+    time. The outputs are disjoint; an untimed NCCL all-gather assembles them once at the end
+    and rank 0 checks the result against a whole-volume run on its GPU."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    import pseudoctimaging_b200 as pct
+    from pseudoctimaging_b200 import shard
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    s = pct.synth_subject(NX, NY, NZ, NUM, n_blobs=N_BLOBS, seed=1)
+    label = pct.normalize_labels(s.atlas_ct)
+    div = pct.div_from(SIGMA, BETA)
+    sl = shard.slab_plan(NZ, NH, world)[rank]
+    sub = shard.extract(s.img, s.atlas_mri, label, sl)
+    d = [torch.from_numpy(x).to(dev) for x in sub]
+    d_out = torch.zeros_like(d[0])
+    nzs = sl.src_planes
+    h = pct.Handle(local)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+
+    def step():
+        h.synthesize_device(d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), d_out.data_ptr(),
+                            NX, NY, nzs, NUM, NH, div, pct.EXEC_B200_FP32, stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    h.device_status(stream.cuda_stream)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t = torch.tensor([e0.elapsed_time(e1) / args.steps], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    # assemble once (untimed) and check on rank 0
+    mine = d_out[sl.z_begin - sl.src_begin:sl.z_end - sl.src_begin]
+    plan = shard.slab_plan(NZ, NH, world)
+    biggest = max(p.planes for p in plan)
+    buf = torch.zeros((biggest, NX, NY), device=dev)
+    buf[:mine.shape[0]] = mine
+    parts = [torch.empty_like(buf) for _ in range(world)]
+    if world > 1:
+        dist.all_gather(parts, buf)
+    else:
+        parts = [buf]
+    check = None
+    if rank == 0:
+        whole = np.zeros((NZ, NX, NY), np.float32)
+        for p, tt in zip(plan, parts):
+            whole[p.z_begin:p.z_end] = tt[:p.planes].cpu().numpy()
+        ref = h.synthesize(s.img, s.atlas_mri, label, NH, div, pct.EXEC_B200_FP32)
+        both = np.isfinite(ref) & np.isfinite(whole)
+        check = {"nan_mask_equal": bool(np.array_equal(np.isnan(ref), np.isnan(whole))),
+                 "max_rel_vs_whole_volume": float(np.max(np.abs(whole[both] - ref[both]) /
+                                                         np.maximum(np.abs(ref[both]), 1e-30)))}
+    clocks = clk.summary()
+    nvox = NX * NY * NZ
+    line = {
+        "metric": f"pseudo-CT voxels/s at {NX}x{NY}x{NZ}, 10 atlases, NH={NH}, one subject "
+                  "z-sharded over the GPUs",
+        "value": nvox / (ms / 1e3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator, config 1)",
+        "config": {"workload": "config 1 subject, z slabs + halo per GPU, plain FP32 kernel",
+                   "slabs": [[p.z_begin, p.z_end] for p in plan], "parallelism": f"z-slab x{world}"},
+        "check": check,
+        "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+    }
+    h.close()
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+def run_learned_arm(args) -> None:
+    """Config 4: the learned-proposal form (EXEC_CHOICE 7, the committed trained network) on a
+    held-out 222x222x112 subject with 10 atlases, NH = 11, against the plain FP32 kernel on the
+    same inputs in the same run: voxels/s of both, the speed-up, and the learned form's error
+    against the plain method in HU."""
+    import torch
+
+    import pseudoctimaging_b200 as pct
+    from pseudoctimaging_b200 import learned
+
+    dev = torch.device("cuda", 0)
+    s = pct.synth_subject(NX, NY, NZ, NUM, n_blobs=N_BLOBS, seed=5000)  # held out from training
+    label = pct.normalize_labels(s.atlas_ct)
+    div = pct.div_from(SIGMA, BETA)
+    d = [torch.from_numpy(x).to(dev) for x in (s.img, s.atlas_mri, label)]
+    o_plain, o_learn = torch.zeros_like(d[0]), torch.zeros_like(d[0])
+    h = pct.Handle(0)
+    model = learned.LearnedModel.load(learned.CHECKPOINT)
+    h.attach_model(model, args.conf)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+
+    def timed(choice, out, steps, warmup):
+        def step():
+            h.synthesize_device(d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), out.data_ptr(),
+                                NX, NY, NZ, NUM, 11, div, choice, stream.cuda_stream)
+        for _ in range(warmup):
+            step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        h.device_status(stream.cuda_stream)
+        return e0.elapsed_time(e1) / steps
+
+    ms_plain = timed(pct.EXEC_B200_FP32, o_plain, max(1, args.steps // 2), 1)
+    with ClockSampler(0) as clk:
+        ms = timed(pct.EXEC_LEARNED, o_learn, args.steps, args.warmup)
+    st = h.learned_stats()
+    core = (slice(6, -6),) * 3
+    a = o_learn.cpu().numpy()[core].astype(np.float64)
+    b = o_plain.cpu().numpy()[core].astype(np.float64)
+    both = np.isfinite(a) & np.isfinite(b)
+    err = np.abs(a[both] - b[both]) * (4095.0 / 255.0)
+    nvox = NX * NY * NZ
+    pairs = (NZ - 12) * (NX - 12) * (NY - 12) * NUM
+    rows = (NZ - 12) * (NX - 12) * -(-(NY - 12) // 30) * NUM
+    # tensor work of the convolutions: conv2..conv4 are 16x16x27 MACs per voxel per atlas
+    conv_flop = 3 * 2.0 * 16 * 16 * 27 * nvox * NUM
+    peaks = measured_peaks()
+    bf16 = peaks.get("bf16_tflops")
+    clocks = clk.summary()
+    line = {
+        "metric": f"pseudo-CT voxels/s at {NX}x{NY}x{NZ}, 10 atlases, NH=11, learned proposal "
+                  "(EXEC_CHOICE 7)",
+        "value": nvox / (ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "bf16 network, f32 rescoring",
+        "data": "synthetic (seeded generator, config 4 held-out subject, seed 5000)",
+        "config": {"workload": "config 4: learned proposal, k = 32 per row segment",
+                   "checkpoint": learned.CHECKPOINT.name, "conf_threshold": args.conf,
+                   "volume": [NX, NY, NZ], "atlases": NUM, "nh": 11},
+        "plain": {"ms_per_step": ms_plain, "value": nvox / (ms_plain / 1e3)},
+        "speedup_vs_plain": ms_plain / ms,
+        "quality_vs_plain": {"mae_hu": float(err.mean()), "max_abs_hu": float(err.max()),
+                             "nan_mismatch": int((np.isnan(a) != np.isnan(b)).sum())},
+        "fallback_share": st["fallback_pairs"] / pairs,
+        "offsets_per_row": st["row_offsets"] / rows,
+        "gpu_launches": args.steps * (3 + 5 * NUM + 1),
+        "roofline": {"bound": "tensor", "unit": "TFLOP/s",
+                     "achieved": conv_flop / (ms / 1e3) / 1e12, "peak": bf16,
+                     "frac": (conv_flop / (ms / 1e3) / 1e12 / bf16) if bf16 else None,
+                     "traffic": None,
+                     "note": "convolution FLOPs (conv2..conv4, 2*16*16*27 per voxel per atlas) "
+                             "over the whole step, which also holds conv1 and the rescoring"},
+        "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+    }
+    h.attach_model(None)
+    model.close()
+    h.close()
+    print(json.dumps(line))
+
+
 def main() -> None:
     global NZ, NH, METRIC
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
@@ -453,8 +638,13 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", choices=["single", "batch"], default="single",
-                    help="single: config 1 subject (the metric); batch: config 3 subjects")
+    ap.add_argument("--workload", choices=["single", "batch", "learned", "sharded"],
+                    default="single",
+                    help="single: config 1 subject (the metric); batch: config 3 subjects; "
+                         "learned: config 4, the learned proposal against the plain kernel; "
+                         "sharded: one config 1 subject split into z slabs over the GPUs")
+    ap.add_argument("--conf", type=float, default=0.0,
+                    help="learned workload: confidence threshold of the full-search fallback")
     ap.add_argument("--batch-subjects", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-pointer end-to-end leg")
@@ -474,6 +664,10 @@ def main() -> None:
         run_reference_arm(args)
     elif args.workload == "batch":
         run_batch_arm(args)
+    elif args.workload == "learned":
+        run_learned_arm(args)
+    elif args.workload == "sharded":
+        run_sharded_arm(args)
     else:
         run_b200_arm(args)
 

@@ -126,6 +126,20 @@ typedef struct pct_plan {
 int pct_query_plan(int device, int nx, int ny, int nz, int num_atlas, int nh, pct_plan *plan);
 
 /*
+ * Z-slab sharding of one subject over `parts` GPUs (or passes). No counterpart in the reference,
+ * which runs one subject on one device. The interior planes [hw+1, nz-hw-1) (hw = (nh-1)/2) are
+ * split into `parts` contiguous slabs of near-equal size; part `part` owns output planes
+ * [*z_begin, *z_end) and needs input planes [*src_begin, *src_end) = the slab plus hw+1 planes on
+ * each side, of the input MRI and of every atlas MRI and CT. Running pct_synthesize(_device) on
+ * that sub-volume (nz' = src_end - src_begin planes) gives the slab's output planes exactly
+ * where the sub-volume's interior lies, planes [z_begin - src_begin, z_end - src_begin) of the
+ * sub-volume; the slabs' outputs are disjoint and together cover the whole interior. A part with
+ * no planes gets z_begin == z_end and an empty source range. Pure host arithmetic.
+ */
+int pct_slab_plan(int nz, int nh, int parts, int part, int *z_begin, int *z_end, int *src_begin,
+                  int *src_end);
+
+/*
  * Batched form (EXEC_CHOICE 8): many subjects of uneven size, atlas count and NH in one
  * persistent kernel launch. Each subject's buffers are DEVICE buffers in the reference layout
  * (labels already normalised); only interior voxels of `out` are written. NH must be 7, 9 or 11.

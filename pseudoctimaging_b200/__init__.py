@@ -107,6 +107,7 @@ SIGNATURES = {
     "pct_synthesize_device": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _D, _I, _P]),
     "pct_device_status": (_I, [_P, _P]),
     "pct_query_plan": (_I, [_I, _I, _I, _I, _I, _I, ctypes.POINTER(Plan)]),
+    "pct_slab_plan": (_I, [_I, _I, _I, _I] + [ctypes.POINTER(_I)] * 4),
     "pct_synthesize_batch": (_I, [_P, ctypes.POINTER(SubjectDesc), _I, _P]),
     "pct_batch_create": (_I, [_P, ctypes.POINTER(SubjectDesc), _I, _P, ctypes.POINTER(_P)]),
     "pct_batch_launch": (_I, [_P, _P]),

@@ -486,6 +486,27 @@ int pct_synthesize(pct_handle *h, const float *img, const float *atlas, const fl
   return read_device_status(h, s);
 }
 
+int pct_slab_plan(int nz, int nh, int parts, int part, int *z_begin, int *z_end, int *src_begin,
+                  int *src_end) {
+  if (nz <= 0 || nh < 3 || (nh % 2) == 0 || parts <= 0 || part < 0 || part >= parts || !z_begin ||
+      !z_end || !src_begin || !src_end)
+    return PCT_ERR_INVALID_ARG;
+  const int lo = (nh - 1) / 2 + 1;  // first interior plane, hw + 1
+  const int planes = nz - 2 * lo > 0 ? nz - 2 * lo : 0;
+  // part p gets planes [lo + floor(p*planes/parts), lo + floor((p+1)*planes/parts))
+  const int b = lo + (int)((long long)part * planes / parts);
+  const int e = lo + (int)((long long)(part + 1) * planes / parts);
+  *z_begin = b;
+  *z_end = e;
+  if (b == e) {
+    *src_begin = *src_end = b;
+  } else {
+    *src_begin = b - lo;  // the patch and search window reach lo planes past the slab
+    *src_end = e + lo;
+  }
+  return PCT_OK;
+}
+
 int pct_query_plan(int device, int nx, int ny, int nz, int num_atlas, int nh, pct_plan *plan) {
   if (!plan) return PCT_ERR_INVALID_ARG;
   memset(plan, 0, sizeof(*plan));
