@@ -244,6 +244,22 @@ int pct_model_train(pct_model *m, pct_train_set *ts, int batch, int steps, float
  * method (voxels 6 or more from every face). No counterpart in the reference.
  */
 int pct_attach_model(pct_handle *h, pct_model *m, float conf_threshold);
+
+/*
+ * Tensor-core form (EXEC_CHOICE 5 = FP16, 6 = BF16; NH = 11) runs through pct_synthesize /
+ * pct_synthesize_device / pct_run_pipeline. Per (voxel, atlas) the SSD of all 11^3 positions is
+ * ranked by a tcgen05 correlation of 16-bit patches (the tile's mean removed, scaled by 1/64,
+ * FP32 accumulation, |b|^2/2 of the rounded patch folded in as 16-bit parts), the 16 best are
+ * rescored with the exact FP32 SSD and only they are weighted. Same interior, border and NaN rule
+ * as the plain method. No counterpart in the reference (its GPU kernels are FP64).
+ *
+ * Testing hook: one atlas (num_atlas = 1) through the tensor-core form, writing d_out as above and
+ * the 16 survivors of every interior voxel, best first, into d_top (device int16 [nz*nx*ny][16],
+ * offset index (dw+5)*121 + (du+5)*11 + (dv+5)). Synchronous on `stream`.
+ */
+int pct_tc_survivors(pct_handle *h, int exec_choice, const float *d_img, const float *d_atlas,
+                     const float *d_label, float *d_out, int nx, int ny, int nz, double div,
+                     int16_t *d_top, void *stream);
 /* Counters of the handle's last learned run (synchronises the stream that run used): the
  * (voxel, atlas) pairs that took the full search, and the offsets evaluated summed over warp
  * rows (one row = 30 output voxels of one atlas; the plain method evaluates 1331 per row).

@@ -146,6 +146,7 @@ SIGNATURES = {
     "pct_model_gradients": (_I, [_P, _P, _I, _I, _P, ctypes.POINTER(ctypes.c_float)]),
     "pct_model_train": (_I, [_P, _P, _I, _I, ctypes.c_float, ctypes.POINTER(ctypes.c_float)]),
     "pct_attach_model": (_I, [_P, _P, ctypes.c_float]),
+    "pct_tc_survivors": (_I, [_P, _I, _P, _P, _P, _P, _I, _I, _I, _D, _P, _P]),
     "pct_learned_stats": (_I, [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
     "pct_model_probe": (_I, [_P, _P, _P, _I, _I, _I, _P, _I, _P, _P, _P]),
     "pct_synth_default_params": (_I, [ctypes.POINTER(SynthParams), _I, _I, _I, _I, _I,

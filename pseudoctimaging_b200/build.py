@@ -33,7 +33,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", f"-ccbin={HOST_CXX}", "-Xcompiler", 
 # Sources that make up the shared library; the CLI main is linked separately against it.
 LIB_SOURCES = ["pct_api.cu", "pct_fuse_tma.cu", "pct_pointwise.cu", "pct_regularize.cu",
                "pct_noalloc.cu", "pct_synth.cpp", "pct_io.cpp", "pct_learned_train.cu",
-               "pct_learned_api.cu", "pct_learned_infer.cu"]
+               "pct_learned_api.cu", "pct_learned_infer.cu", "pct_tc_fuse.cu"]
 CLI_SOURCES = ["pct_cli.cpp"]
 
 

@@ -103,8 +103,7 @@ int check_choice(pct_handle *h, int exec_choice) {
                   "exec_choice 7 (learned proposal) needs a model attached with pct_attach_model");
     case PCT_EXEC_TC_FP16:
     case PCT_EXEC_TC_BF16:
-      return fail(h, PCT_ERR_UNSUPPORTED,
-                  "exec_choice " + std::to_string(exec_choice) + " is not available in this build");
+      return PCT_OK;
     default:
       return fail(h, PCT_ERR_INVALID_ARG, "unknown exec_choice " + std::to_string(exec_choice));
   }
@@ -170,9 +169,29 @@ int launch_learned_path(pct_handle *h, const pct::Geometry &g, const pct::SlabIn
   return PCT_OK;
 }
 
+// The tensor-core form (NH = 11).
+int launch_tc_path(pct_handle *h, const pct::Geometry &g, const pct::SlabInputs &in, float *d_out,
+                   double div, bool bf16, int16_t *dbg_top, cudaStream_t s) {
+  if (g.nh != 11)
+    return fail(h, PCT_ERR_UNSUPPORTED,
+                "exec_choice 5/6 (tensor-core form) is built for NH = 11 only, got NH = " +
+                    std::to_string(g.nh));
+  int st = ensure(h, h->err, 16);
+  if (st) return st;
+  int *err = static_cast<int *>(h->err.ptr);
+  PCT_CUDA(h, cudaMemsetAsync(err, 0, sizeof(int), s));
+  PCT_CUDA(h, pct::tc::launch_tc(g, in, d_out, div, bf16, err, dbg_top, s));
+  return PCT_OK;
+}
+
+// Whether a choice runs the TMA-staged plain kernel (which needs 16-byte row strides).
+bool uses_tma_rows(int exec_choice) { return exec_choice <= PCT_EXEC_B200_FP32; }
+
 int launch_path(pct_handle *h, const pct::Geometry &g, const pct::SlabInputs &in, float *d_out,
                 double div, int exec_choice, cudaStream_t s) {
   if (exec_choice == PCT_EXEC_LEARNED) return launch_learned_path(h, g, in, d_out, div, s);
+  if (exec_choice == PCT_EXEC_TC_FP16 || exec_choice == PCT_EXEC_TC_BF16)
+    return launch_tc_path(h, g, in, d_out, div, exec_choice == PCT_EXEC_TC_BF16, nullptr, s);
   return launch_fusion(h, g, in, d_out, div, s);
 }
 
@@ -394,6 +413,25 @@ int pct_set_memory_limit(pct_handle *h, size_t bytes) {
   return PCT_OK;
 }
 
+int pct_tc_survivors(pct_handle *h, int exec_choice, const float *d_img, const float *d_atlas,
+                     const float *d_label, float *d_out, int nx, int ny, int nz, double div,
+                     int16_t *d_top, void *stream) {
+  if (!h) return PCT_ERR_INVALID_ARG;
+  h->last_error.clear();
+  if (exec_choice != PCT_EXEC_TC_FP16 && exec_choice != PCT_EXEC_TC_BF16)
+    return fail(h, PCT_ERR_INVALID_ARG, "pct_tc_survivors takes exec_choice 5 or 6");
+  if (!d_img || !d_atlas || !d_label || !d_out || !d_top)
+    return fail(h, PCT_ERR_INVALID_ARG, "null device pointer");
+  pct::Geometry g;
+  int st = check_shape(h, nx, ny, nz, 1, 11, div, &g);
+  if (st || (st = select_device(h))) return st;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const pct::SlabInputs in{d_img, d_atlas, d_label, ny};
+  if ((st = launch_tc_path(h, g, in, d_out, div, exec_choice == PCT_EXEC_TC_BF16, d_top, s)))
+    return st;
+  return read_device_status(h, s);
+}
+
 int pct_attach_model(pct_handle *h, pct_model *m, float conf_threshold) {
   if (!h) return PCT_ERR_INVALID_ARG;
   h->last_error.clear();
@@ -440,7 +478,7 @@ int pct_synthesize_device(pct_handle *h, const float *d_img, const float *d_atla
   pct::SlabInputs in{d_img, d_atlas, d_atlas_label, g.ny};
   const bool aligned = (g.ny % 4 == 0) && (reinterpret_cast<uintptr_t>(d_atlas) % 16 == 0) &&
                        (reinterpret_cast<uintptr_t>(d_atlas_label) % 16 == 0);
-  if (!aligned && exec_choice != PCT_EXEC_LEARNED) {  // TMA needs 16-byte row strides: stage a pitched copy on the handle
+  if (!aligned && uses_tma_rows(exec_choice)) {  // TMA needs 16-byte row strides: stage a pitched copy on the handle
     const int pitch = pct::slab_pitch(g.ny);
     const long long rows = (long long)g.num * g.nz * g.nx;
     const size_t bytes = (size_t)rows * pitch * sizeof(float);

@@ -106,4 +106,12 @@ const void *model_weights(const pct_model *m);
 int model_device(const pct_model *m);
 }  // namespace learned
 
+namespace tc {
+// Tensor-core form (NH = 11): FP16 or BF16 correlation on tcgen05, top-16 per (voxel, atlas),
+// exact FP32 rescoring. Writes interior voxels of out. *err (device) is set if a bounded wait
+// gives up. dbg_top (optional, device [nvox][16]) receives atlas 0's survivors per voxel.
+cudaError_t launch_tc(const Geometry &g, const SlabInputs &in, float *out, double div, bool bf16,
+                      int *err, int16_t *dbg_top, cudaStream_t s);
+}  // namespace tc
+
 }  // namespace pct
