@@ -545,6 +545,90 @@ def run_sharded_arm(args) -> None:
         print(json.dumps(line))
 
 
+def run_tc_arm(args) -> None:
+    """Config 2: the tensor-core form (EXEC_CHOICE 5 FP16 and 6 BF16: tcgen05 correlation, top-16
+    per (voxel, atlas), exact FP32 rescoring) on a 222x222x112 subject with 20 atlases, NH = 11,
+    against the plain FP32 kernel on the same inputs: voxels/s of each and the error against the
+    plain method in HU (the error against the FP64 oracle is measured by the tests at small sizes;
+    a full-size FP64 run takes about half an hour of CPU)."""
+    import torch
+
+    import pseudoctimaging_b200 as pct
+
+    num = 20
+    dev = torch.device("cuda", 0)
+    s = pct.synth_subject(NX, NY, NZ, num, n_blobs=N_BLOBS, seed=2)
+    label = pct.normalize_labels(s.atlas_ct)
+    div = pct.div_from(SIGMA, BETA)
+    d = [torch.from_numpy(x).to(dev) for x in (s.img, s.atlas_mri, label)]
+    h = pct.Handle(0)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    outs, times = {}, {}
+    with ClockSampler(0) as clk:
+        for choice, steps in ((pct.EXEC_B200_FP32, max(1, args.steps // 2)),
+                              (pct.EXEC_TC_FP16, args.steps), (pct.EXEC_TC_BF16, args.steps)):
+            o = torch.zeros_like(d[0])
+
+            def step():
+                h.synthesize_device(d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), o.data_ptr(),
+                                    NX, NY, NZ, num, 11, div, choice, stream.cuda_stream)
+            for _ in range(args.warmup):
+                step()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                step()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            h.device_status(stream.cuda_stream)
+            times[choice] = e0.elapsed_time(e1) / steps
+            outs[choice] = o.cpu().numpy()
+    core = (slice(6, -6),) * 3
+    ref = outs[pct.EXEC_B200_FP32][core].astype(np.float64)
+    nvox = NX * NY * NZ
+    forms = {}
+    for choice, name in ((pct.EXEC_TC_FP16, "fp16"), (pct.EXEC_TC_BF16, "bf16")):
+        g = outs[choice][core].astype(np.float64)
+        both = np.isfinite(g) & np.isfinite(ref)
+        e = np.abs(g[both] - ref[both]) * (4095.0 / 255.0)
+        forms[name] = {"ms_per_step": times[choice], "value": nvox / (times[choice] / 1e3),
+                       "mae_hu_vs_plain": float(e.mean()), "max_abs_hu_vs_plain": float(e.max()),
+                       "nan_mismatch": int((np.isnan(g) != np.isnan(ref)).sum())}
+    # tensor work: 128 x 128 x 32 per chunk, 28 chunks per tile and atlas
+    tiles = -(-(NZ - 12) // 4) * -(-(NX - 12) // 4) * -(-(NY - 12) // 8)
+    flop = 2.0 * 128 * 128 * 32 * 28 * tiles * num
+    peaks = measured_peaks()
+    clocks = clk.summary()
+    ms = times[pct.EXEC_TC_FP16]
+    line = {
+        "metric": f"pseudo-CT voxels/s at {NX}x{NY}x{NZ}, 20 atlases, NH=11, tensor-core form "
+                  "(EXEC_CHOICE 5 FP16; BF16 beside it)",
+        "value": forms["fp16"]["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp16/bf16 correlation, f32 rescoring",
+        "data": "synthetic (seeded generator, config 2, seed 2)",
+        "config": {"workload": "config 2: tensor-core correlation, top-16 per (voxel, atlas)",
+                   "volume": [NX, NY, NZ], "atlases": num, "nh": 11},
+        "forms": forms,
+        "plain": {"ms_per_step": times[pct.EXEC_B200_FP32],
+                  "value": nvox / (times[pct.EXEC_B200_FP32] / 1e3)},
+        "gpu_launches": args.steps,
+        "roofline": {"bound": "tensor", "unit": "TFLOP/s", "achieved": flop / (ms / 1e3) / 1e12,
+                     "peak": peaks.get("bf16_tflops"),
+                     "frac": flop / (ms / 1e3) / 1e12 / peaks["bf16_tflops"]
+                     if peaks.get("bf16_tflops") else None,
+                     "traffic": None,
+                     "note": "dense correlation FLOPs (128 x 128 x 32 per chunk, 28 chunks per "
+                             "tile and atlas) over the FP16 step; the selection epilogue, not the "
+                             "tensor pipe, bounds this kernel"},
+        "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+    }
+    h.close()
+    print(json.dumps(line))
+
+
 def run_learned_arm(args) -> None:
     """Config 4: the learned-proposal form (EXEC_CHOICE 7, the committed trained network) on a
     held-out 222x222x112 subject with 10 atlases, NH = 11, against the plain FP32 kernel on the
@@ -638,11 +722,12 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", choices=["single", "batch", "learned", "sharded"],
+    ap.add_argument("--workload", choices=["single", "batch", "learned", "sharded", "tc"],
                     default="single",
                     help="single: config 1 subject (the metric); batch: config 3 subjects; "
                          "learned: config 4, the learned proposal against the plain kernel; "
-                         "sharded: one config 1 subject split into z slabs over the GPUs")
+                         "sharded: one config 1 subject split into z slabs over the GPUs; "
+                         "tc: config 2, the tensor-core form against the plain kernel")
     ap.add_argument("--conf", type=float, default=0.0,
                     help="learned workload: confidence threshold of the full-search fallback")
     ap.add_argument("--batch-subjects", type=int, default=16)
@@ -668,6 +753,8 @@ def main() -> None:
         run_learned_arm(args)
     elif args.workload == "sharded":
         run_sharded_arm(args)
+    elif args.workload == "tc":
+        run_tc_arm(args)
     else:
         run_b200_arm(args)
 

@@ -420,6 +420,8 @@ __global__ void proposal_hook_kernel(const __nv_bfloat16 *__restrict__ f4,
 
 constexpr int kRowOut = 30;       // output voxels per warp row (lanes 1..30)
 constexpr int kRescoreWarps = 4;  // warps per CTA
+constexpr int kProbStride = kHeads;  // 33 floats per lane row: column reads are conflict-free
+
 
 // Exact FP32 rescoring of one atlas. A warp owns a row segment (z, x, y0 .. y0+29) of interior
 // voxels; lane l sits at y = y0 - 1 + l (lanes 0 and 31 are the y halo). Every voxel of the
@@ -458,6 +460,9 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 3)
                    unsigned long long *__restrict__ fallbacks,
                    unsigned long long *__restrict__ evaluated) {
   __shared__ float hw[kHeadFloats];
+  __shared__ float s_prob[kRescoreWarps * 32 * kProbStride];
+  __shared__ float s_sum[kRescoreWarps * 36];
+  __shared__ int s_top[kRescoreWarps * 12];
   for (int i = threadIdx.x; i < kHeadFloats; i += blockDim.x) hw[i] = __bfloat162float(wbf[kH + i]);
   __syncthreads();
   const int lane = threadIdx.x & 31;
@@ -486,19 +491,50 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 3)
 #pragma unroll
       for (int o = 0; o < kHeads; ++o) p[o] = 0.f;
     }
-    int top[3][4];
+    // row sums through shared memory: lane l sums column l (and column 32) of the row's
+    // probabilities; lanes 0..2 pick the top 4 of axis 0..2
+    float *wp = s_prob + (threadIdx.x >> 5) * 32 * kProbStride;
+    float *wsum = s_sum + (threadIdx.x >> 5) * 36;
+    int *wtop = s_top + (threadIdx.x >> 5) * 12;
+#pragma unroll
+    for (int o = 0; o < kHeads; ++o) wp[lane * kProbStride + o] = p[o];
+    __syncwarp();
     {
-      float rs[kHeads];
-#pragma unroll
-      for (int o = 0; o < kHeads; ++o) {
-        float v = p[o];
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-        rs[o] = v;
+      float c0 = 0.f, c1 = 0.f;
+#pragma unroll 8
+      for (int r = 0; r < 32; ++r) {
+        c0 += wp[r * kProbStride + lane];
+        c1 += wp[r * kProbStride + 32];
       }
-#pragma unroll
-      for (int a = 0; a < 3; ++a) top4(rs, a, top[a]);
+      wsum[lane] = c0;
+      if (lane == 0) wsum[32] = c1;
     }
+    __syncwarp();
+    if (lane < 3) {
+      float q[kAxis];
+#pragma unroll
+      for (int j = 0; j < kAxis; ++j) q[j] = wsum[lane * kAxis + j];
+      unsigned used = 0;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        int bi = 0;
+        float bp = -1.f;
+#pragma unroll
+        for (int j = 0; j < kAxis; ++j)
+          if (!((used >> j) & 1u) && q[j] > bp) {
+            bp = q[j];
+            bi = j;
+          }
+        used |= 1u << bi;
+        wtop[lane * 4 + r] = bi;
+      }
+    }
+    __syncwarp();
+    int top[3][4];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) top[a][r] = wtop[a * 4 + r];
     const bool full = out_lane && kept_mass(p, top) < conf_thr;
     const unsigned any_full = __ballot_sync(0xffffffffu, full);
     if (full) ++my_fallbacks;
@@ -519,6 +555,7 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 3)
           for (int k = 0; k + j + i < 5 && k < 4; ++k)
             eval_offset(atl, lab, in, vz + axy + apitch, axy, apitch, yc, top[0][i] - 5,
                         top[1][j] - 5, top[2][k] - 5, out_lane, P, W, neg_k);
+      __syncwarp();  // wtop is rewritten by the warp's next row
       my_evals += 32;
     } else {
       // the full window; lanes that did not fall back keep only their row's 32
@@ -544,6 +581,7 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 3)
         }
       }
       my_evals += kAxis * kAxis * kAxis;
+      __syncwarp();
     }
     if (out_lane) {
       const long long v = (long long)z * nxy + (long long)x * ny + y;
