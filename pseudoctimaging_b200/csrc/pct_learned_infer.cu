@@ -1,7 +1,7 @@
 // Inference side of the learned proposal (EXEC_CHOICE 7).
 //
 // Per atlas, over the whole volume:
-//   conv1 (2 -> 16 channels)            CUDA cores, FP32 math, BF16 channel-last output
+//   conv1 (2 -> 16 channels)            tensor cores: FP16 im2col rows (K = 54 -> 64), FP32 accumulation
 //   conv2..conv4 (16 -> 16 channels)    tensor cores: BF16 implicit GEMM with FP32 accumulation
 //                                       (mma m16n8k16; ldmatrix gathers 16 shifted voxel rows of a
 //                                       channel-last shared-memory slab per tap, 27 taps)
@@ -16,6 +16,7 @@
 // NaN rule at the end. Out-of-volume inputs of the convolutions read as zero; interior voxels
 // (6 or more voxels from every face) only see in-volume values.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -33,81 +34,145 @@ namespace {
 constexpr float kDblEpsilonF = 2.220446049250313080847e-16f;
 
 
-// ---------------------------------------------------------------- conv1 (CUDA cores)
+// ---------------------------------------------------------------- conv1 (tensor cores)
 
-constexpr int kC1Vox = 2;  // consecutive y voxels per thread
+// conv1 as an FP16 implicit GEMM: a CTA item is 4 x-rows x 32 y of one z plane (warp w = x-row w,
+// lane = y). Each thread writes its voxel's im2col row, K = 2 channels x 27 taps = 54 (padded to
+// 64) scaled inputs in FP16 (out-of-volume taps 0), into shared memory: 128 bytes per row, the
+// 16-byte chunk c of row r stored at chunk c ^ (r & 7) so that ldmatrix phases hit distinct banks.
+// Its warp then runs 2 m-tiles x 4 k-steps x 2 n-tiles of mma m16n8k16 (FP16 in, FP32
+// accumulate) against the BF16 weights widened to FP16 (exact), adds the bias, applies ReLU and
+// stores BF16 channel-last. The only rounding beyond the FP32 reference is the FP16 input
+// (relative 2^-11 of the scaled intensity).
+constexpr int kC1Warps = 4;
+constexpr int kC1K = 64;
 
-// conv1 over the whole volume, FP32 math on BF16 weights: each thread owns 2 consecutive y
-// voxels of one (z, x) row, walks the 54 input taps once (4 y values per (channel, dz, dx)
-// cover the 2 voxels' 3 y taps) and keeps 2 x 16 accumulators.
-__global__ void __launch_bounds__(256, 2)
+__device__ __forceinline__ void mma_f16_sync(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2,
+                                             uint32_t a3, uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
+      "{%8, %9}, {%0, %1, %2, %3};"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ void ldmatrix_x4_c1(uint32_t addr, uint32_t &r0, uint32_t &r1,
+                                               uint32_t &r2, uint32_t &r3) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];"
+               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+               : "r"(addr));
+}
+
+__global__ void __launch_bounds__(kC1Warps * 32)
     conv1_kernel(const float *__restrict__ img, const float *__restrict__ atl,
                  const __nv_bfloat16 *__restrict__ wbf, __nv_bfloat16 *__restrict__ out, int nx,
                  int ny, int nz, int apitch) {
-  __shared__ __align__(16) float w[kCin * 27][kC];  // [ci*27 + tap][co]
-  __shared__ float bias[kC];
-  for (int i = threadIdx.x; i < kC * kCin * 27; i += blockDim.x) {
-    const int co = i / (kCin * 27), r = i % (kCin * 27);
-    w[r][co] = __bfloat162float(wbf[kW1 + i]);
-  }
-  if (threadIdx.x < kC) bias[threadIdx.x] = __bfloat162float(wbf[kB1 + threadIdx.x]);
-  __syncthreads();
-  const int yq = (ny + kC1Vox - 1) / kC1Vox;
-  const long long items = (long long)nz * nx * yq;
+  __shared__ __align__(128) unsigned char rows[kC1Warps * 32 * kC1K * 2];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  // B fragments (k-step ks, n-tile j, register r): {W[co][k0], W[co][k0 + 1]} as FP16,
+  // co = 8j + g, k0 = 16ks + 8r + 2t; K index = ci * 27 + tap, zero past 54
+  uint32_t B[4][2][2];
+#pragma unroll
+  for (int ks = 0; ks < 4; ++ks)
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        const int co = 8 * j + g, k0 = 16 * ks + 8 * r + 2 * t;
+        const float w0 = k0 < kCin * 27 ? __bfloat162float(wbf[kW1 + co * kCin * 27 + k0]) : 0.f;
+        const float w1 = k0 + 1 < kCin * 27 ? __bfloat162float(wbf[kW1 + co * kCin * 27 + k0 + 1]) : 0.f;
+        const __half2 h = __floats2half2_rn(w0, w1);
+        B[ks][j][r] = *reinterpret_cast<const uint32_t *>(&h);
+      }
+  float bias[2][2];
+#pragma unroll
+  for (int j = 0; j < 2; ++j)
+#pragma unroll
+    for (int e = 0; e < 2; ++e) bias[j][e] = __bfloat162float(wbf[kB1 + 8 * j + 2 * t + e]);
+  const uint32_t rows_u32 = static_cast<uint32_t>(__cvta_generic_to_shared(rows));
+  const int my_row = tid;
+  const int m = lane >> 3, q = lane & 7;
+  const int ytiles = (ny + 31) / 32, xtiles = (nx + kC1Warps - 1) / kC1Warps;
+  const long long items = (long long)nz * xtiles * ytiles;
   const int nxy = nx * ny;
-  for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < items;
-       it += (long long)gridDim.x * blockDim.x) {
-    const int y0 = (int)(it % yq) * kC1Vox;
-    const long long r0 = it / yq;
-    const int x = (int)(r0 % nx), z = (int)(r0 / nx);
-    float acc[kC1Vox][kC];
+  for (long long it = blockIdx.x; it < items; it += gridDim.x) {
+    const int y0 = (int)(it % ytiles) * 32;
+    const long long r0 = it / ytiles;
+    const int x = (int)(r0 % xtiles) * kC1Warps + warp, z = (int)(r0 / xtiles);
+    const int y = y0 + lane;
+    // this voxel's im2col row
+    {
+      float v[kC1K];
+      if (z >= 1 && z < nz - 1 && x >= 1 && x < nx - 1 && y >= 1 && y < ny - 1) {
+        // every tap inside the volume: one base pointer per channel, 32-bit tap offsets
+        const float *pi = img + (long long)z * nxy + (long long)x * ny + y;
+        const float *pa = atl + ((long long)z * nx + x) * apitch + y;
+        const int axy = nx * apitch;
 #pragma unroll
-    for (int v = 0; v < kC1Vox; ++v)
-#pragma unroll
-      for (int c = 0; c < kC; ++c) acc[v][c] = bias[c];
-#pragma unroll
-    for (int ci = 0; ci < kCin; ++ci) {
-#pragma unroll
-      for (int kzx = 0; kzx < 9; ++kzx) {
-        const int zz = z + kzx / 3 - 1, xx = x + kzx % 3 - 1;
-        const bool rok = zz >= 0 && zz < nz && xx >= 0 && xx < nx;
-        const float *src = ci == 0 ? img + (long long)zz * nxy + (long long)xx * ny
-                                   : atl + ((long long)zz * nx + xx) * apitch;
-        float in[kC1Vox + 2];
-#pragma unroll
-        for (int j = 0; j < kC1Vox + 2; ++j) {
-          const int yy = y0 + j - 1;
-          in[j] = (rok && yy >= 0 && yy < ny) ? __ldg(src + yy) * kInScale : 0.f;
+        for (int k = 0; k < 27; ++k) {
+          const int dz = k / 9 - 1, dx = (k / 3) % 3 - 1, dy = k % 3 - 1;
+          v[k] = __ldg(pi + (dz * nxy + dx * ny + dy)) * kInScale;
+          v[27 + k] = __ldg(pa + (dz * axy + dx * apitch + dy)) * kInScale;
         }
+      } else {
 #pragma unroll
-        for (int ky = 0; ky < 3; ++ky) {
-          const float4 *wr = reinterpret_cast<const float4 *>(w[ci * 27 + kzx * 3 + ky]);
-#pragma unroll
-          for (int c4 = 0; c4 < kC / 4; ++c4) {
-            const float4 wv = wr[c4];
-#pragma unroll
-            for (int v = 0; v < kC1Vox; ++v) {
-              const float xv = in[v + ky];
-              acc[v][4 * c4 + 0] = fmaf(wv.x, xv, acc[v][4 * c4 + 0]);
-              acc[v][4 * c4 + 1] = fmaf(wv.y, xv, acc[v][4 * c4 + 1]);
-              acc[v][4 * c4 + 2] = fmaf(wv.z, xv, acc[v][4 * c4 + 2]);
-              acc[v][4 * c4 + 3] = fmaf(wv.w, xv, acc[v][4 * c4 + 3]);
-            }
-          }
+        for (int k = 0; k < 27; ++k) {
+          const int zz = z + k / 9 - 1, xx = x + (k / 3) % 3 - 1, yy = y + k % 3 - 1;
+          const bool ok = zz >= 0 && zz < nz && xx >= 0 && xx < nx && yy >= 0 && yy < ny;
+          v[k] = ok ? __ldg(img + (long long)zz * nxy + (long long)xx * ny + yy) * kInScale : 0.f;
+          v[27 + k] = ok ? __ldg(atl + ((long long)zz * nx + xx) * apitch + yy) * kInScale : 0.f;
         }
       }
+#pragma unroll
+      for (int k = kCin * 27; k < kC1K; ++k) v[k] = 0.f;
+      unsigned char *row = rows + my_row * kC1K * 2;
+#pragma unroll
+      for (int c = 0; c < kC1K / 8; ++c) {
+        uint32_t w[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const __half2 h = __floats2half2_rn(v[8 * c + 2 * e], v[8 * c + 2 * e + 1]);
+          w[e] = *reinterpret_cast<const uint32_t *>(&h);
+        }
+        *reinterpret_cast<uint4 *>(row + ((c ^ (my_row & 7)) << 4)) = make_uint4(w[0], w[1], w[2], w[3]);
+      }
     }
-    __nv_bfloat16 *dst = out + ((long long)z * nxy + (long long)x * ny + y0) * kC;
+    __syncwarp();
+    float acc[2][2][4];
 #pragma unroll
-    for (int v = 0; v < kC1Vox; ++v) {
-      if (y0 + v >= ny) break;
-      __align__(16) __nv_bfloat162 r[kC / 2];
+    for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
-      for (int c = 0; c < kC / 2; ++c)
-        r[c] = __floats2bfloat162_rn(fmaxf(acc[v][2 * c], 0.f), fmaxf(acc[v][2 * c + 1], 0.f));
-      uint4 *d4 = reinterpret_cast<uint4 *>(dst + v * kC);
-      d4[0] = reinterpret_cast<const uint4 *>(r)[0];
-      d4[1] = reinterpret_cast<const uint4 *>(r)[1];
+      for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) acc[mt][j][e] = 0.f;
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+      for (int ks = 0; ks < 4; ++ks) {
+        const int r = warp * 32 + mt * 16 + q + 8 * (m & 1);
+        const int c = 2 * ks + (m >> 1);
+        uint32_t a0, a1, a2, a3;
+        ldmatrix_x4_c1(rows_u32 + (uint32_t)(r * kC1K * 2 + ((c ^ (r & 7)) << 4)), a0, a1, a2, a3);
+#pragma unroll
+        for (int j = 0; j < 2; ++j) mma_f16_sync(acc[mt][j], a0, a1, a2, a3, B[ks][j][0], B[ks][j][1]);
+      }
+    __syncwarp();  // the rows are rewritten by the next item
+    if (x < nx) {
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int yy = y0 + mt * 16 + g + 8 * h;
+          if (yy >= ny) continue;
+          __nv_bfloat16 *dst = out + ((long long)z * nxy + (long long)x * ny + yy) * kC;
+#pragma unroll
+          for (int j = 0; j < 2; ++j) {
+            const float v0 = fmaxf(acc[mt][j][2 * h] + bias[j][0], 0.f);
+            const float v1 = fmaxf(acc[mt][j][2 * h + 1] + bias[j][1], 0.f);
+            *reinterpret_cast<__nv_bfloat162 *>(dst + 8 * j + 2 * t) = __floats2bfloat162_rn(v0, v1);
+          }
+        }
     }
   }
 }
@@ -292,8 +357,23 @@ __global__ void __launch_bounds__(kCvThreads, 2)
 
 // ---------------------------------------------------------------- proposal + rescoring
 
-// Head weights [33][16] then biases [33], staged in shared memory by every kernel that proposes.
-constexpr int kHeadFloats = kHeads * kC + kHeads;
+// Head weights staged in shared memory by every kernel that proposes, transposed and padded for
+// packed FP32 FMAs: [16 channels][34 outputs] (output 33 is a zero pad), then 34 biases.
+constexpr int kHeadPad = kHeads + 1;
+constexpr int kHeadFloats = kC * kHeadPad + kHeadPad;
+
+__device__ __forceinline__ void stage_heads(const __nv_bfloat16 *__restrict__ wbf, float *hwt) {
+  for (int i = threadIdx.x; i < kHeadFloats; i += blockDim.x) {
+    float v = 0.f;
+    if (i < kC * kHeadPad) {
+      const int c = i / kHeadPad, o = i % kHeadPad;
+      if (o < kHeads) v = __bfloat162float(wbf[kH + o * kC + c]);
+    } else if (i - kC * kHeadPad < kHeads) {
+      v = __bfloat162float(wbf[kHB + i - kC * kHeadPad]);
+    }
+    hwt[i] = v;
+  }
+}
 
 // Per-axis offset probabilities of one (voxel, atlas) pair from its 16 conv4 features: the three
 // softmaxes over dw, du, dv of the heads' logits, p[a * 11 + j] for offset j - 5 on axis a.
@@ -308,13 +388,21 @@ __device__ __forceinline__ void axis_probs(const __nv_bfloat16 *__restrict__ fv,
 #pragma unroll
     for (int c = 0; c < kC; ++c) f[c] = __bfloat162float(fb[c]);
   }
+  // logits: for each pair of outputs one packed FMA per channel, in channel order
+  float2 acc[kHeadPad / 2];
 #pragma unroll
-  for (int o = 0; o < kHeads; ++o) {
-    float acc = hw[kHeads * kC + o];
+  for (int o2 = 0; o2 < kHeadPad / 2; ++o2)
+    acc[o2] = *reinterpret_cast<const float2 *>(hw + kC * kHeadPad + 2 * o2);
 #pragma unroll
-    for (int c = 0; c < kC; ++c) acc = fmaf(hw[o * kC + c], f[c], acc);
-    p[o] = acc;
+  for (int c = 0; c < kC; ++c) {
+    const float2 fc = make_float2(f[c], f[c]);
+#pragma unroll
+    for (int o2 = 0; o2 < kHeadPad / 2; ++o2)
+      acc[o2] = __ffma2_rn(*reinterpret_cast<const float2 *>(hw + c * kHeadPad + 2 * o2), fc,
+                           acc[o2]);
   }
+#pragma unroll
+  for (int o = 0; o < kHeads; ++o) p[o] = (o & 1) ? acc[o / 2].y : acc[o / 2].x;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     float m = p[a * kAxis];
@@ -358,14 +446,9 @@ __device__ __forceinline__ float pick(const float (&p)[kHeads], int a, int idx) 
   return v;
 }
 
-// Probability mass p_w * p_u * p_v of the kept set: rank triples (i, j, k), i + j + k <= 4, of
-// the per-axis lists top[a][0..3].
-__device__ __forceinline__ float kept_mass(const float (&p)[kHeads], const int (&top)[3][4]) {
-  float tp[3][4];
-#pragma unroll
-  for (int a = 0; a < 3; ++a)
-#pragma unroll
-    for (int r = 0; r < 4; ++r) tp[a][r] = pick(p, a, top[a][r]);
+// Probability mass p_w * p_u * p_v of the kept set, the rank triples (i, j, k) with
+// i + j + k <= 4, from the per-axis probabilities of ranks 0..3, tp[a][r].
+__device__ __forceinline__ float mass_of(const float (&tp)[3][4]) {
   float t[5];
 #pragma unroll
   for (int s2 = 1; s2 <= 4; ++s2) {
@@ -378,6 +461,16 @@ __device__ __forceinline__ float kept_mass(const float (&p)[kHeads], const int (
     t[s2] = acc;
   }
   return tp[0][0] * t[4] + tp[0][1] * t[3] + tp[0][2] * t[2] + tp[0][3] * t[1];
+}
+
+// The same mass from a voxel's own probabilities and per-axis lists top[a][0..3].
+__device__ __forceinline__ float kept_mass(const float (&p)[kHeads], const int (&top)[3][4]) {
+  float tp[3][4];
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int r = 0; r < 4; ++r) tp[a][r] = pick(p, a, top[a][r]);
+  return mass_of(tp);
 }
 
 // The proposal of one voxel on its own (the testing hook reports it): its 4 most probable
@@ -406,8 +499,8 @@ __global__ void proposal_hook_kernel(const __nv_bfloat16 *__restrict__ f4,
                                      const __nv_bfloat16 *__restrict__ wbf,
                                      const int64_t *__restrict__ voxels, int n,
                                      signed char *__restrict__ top, float *__restrict__ conf) {
-  __shared__ float hw[kHeadFloats];
-  for (int i = threadIdx.x; i < kHeadFloats; i += blockDim.x) hw[i] = __bfloat162float(wbf[kH + i]);
+  __shared__ __align__(16) float hw[kHeadFloats];
+  stage_heads(wbf, hw);
   __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -459,11 +552,11 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 3)
                    float conf_thr, float *__restrict__ pacc, float *__restrict__ wacc,
                    unsigned long long *__restrict__ fallbacks,
                    unsigned long long *__restrict__ evaluated) {
-  __shared__ float hw[kHeadFloats];
+  __shared__ __align__(16) float hw[kHeadFloats];
   __shared__ float s_prob[kRescoreWarps * 32 * kProbStride];
   __shared__ float s_sum[kRescoreWarps * 36];
   __shared__ int s_top[kRescoreWarps * 12];
-  for (int i = threadIdx.x; i < kHeadFloats; i += blockDim.x) hw[i] = __bfloat162float(wbf[kH + i]);
+  stage_heads(wbf, hw);
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const int lo = 6;
@@ -535,7 +628,16 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 3)
     for (int a = 0; a < 3; ++a)
 #pragma unroll
       for (int r = 0; r < 4; ++r) top[a][r] = wtop[a * 4 + r];
-    const bool full = out_lane && kept_mass(p, top) < conf_thr;
+    bool full = false;
+    if (out_lane) {
+      // this voxel's mass on the row's 32, its probabilities read back from its transpose row
+      float tp[3][4];
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) tp[a][r] = wp[lane * kProbStride + a * kAxis + top[a][r]];
+      full = mass_of(tp) < conf_thr;
+    }
     const unsigned any_full = __ballot_sync(0xffffffffu, full);
     if (full) ++my_fallbacks;
     // input taps of this lane: I(z+dz, x+dx, y), 3x3 (dz, dx)
@@ -677,10 +779,10 @@ cudaError_t run_convs(const Geometry &g, const __nv_bfloat16 *wbf, const float *
                       __nv_bfloat16 **features, cudaStream_t s) {
   const int n_sm = sms();
   {
-    const long long items = (long long)g.nz * g.nx * ((g.ny + kC1Vox - 1) / kC1Vox);
-    const long long want = (items + 255) / 256;
-    const int blocks = (int)(want < 8LL * n_sm ? want : 8LL * n_sm);
-    conv1_kernel<<<blocks, 256, 0, s>>>(img, atlas_a, wbf, sc.fa, g.nx, g.ny, g.nz, apitch);
+    const long long items = (long long)g.nz * ((g.nx + kC1Warps - 1) / kC1Warps) * ((g.ny + 31) / 32);
+    const int blocks = (int)(items < 16LL * n_sm ? items : 16LL * n_sm);
+    conv1_kernel<<<blocks, kC1Warps * 32, 0, s>>>(img, atlas_a, wbf, sc.fa, g.nx, g.ny, g.nz,
+                                                  apitch);
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
