@@ -91,7 +91,7 @@ struct SubjectView {
   const CUtensorMap *tmA, *tmL;  // atlas MRI / CT slab maps (param or global space)
   int nx, ny, nz, nxy;
   long long nvox;
-  float neg_k;        // -log2(e)/div
+  float scale;        // sqrt(log2(e)/div): taps are scaled so that the box sum is SSD*log2(e)/div
   int tiles_y, tiles_x, ntiles;
   int groups, atlases_per_group;  // items = groups * ntiles (group-major)
   int hw;             // half window of this subject (batched kernel dispatch)
@@ -109,7 +109,7 @@ struct TmaParams {
 template <int HW, int RX, int TZ>
 __device__ __forceinline__ void sweep_dw(const float2 (&In)[TZ + 2][RX + 2], float2 (&P)[TZ][RX],
                                          float2 (&W)[TZ][RX], const uint32_t (&rowA)[RX + 2],
-                                         const uint32_t (&rowL)[RX], const float2 negk2) {
+                                         const uint32_t (&rowL)[RX], const float2 scale2) {
   using C = Cfg<HW, RX, TZ>;
   constexpr int NQ = C::NQ, NR = C::NR;
   float2 Aw[NQ][NR];  // logical plane q at virtual step v lives in slot (q + v) % NQ
@@ -133,7 +133,7 @@ __device__ __forceinline__ void sweep_dw(const float2 (&In)[TZ + 2][RX + 2], flo
           Aw[sn][r] = make_float2(lds_f32(rowA[r] + so + qn * C::PLANE),
                                   lds_f32(rowA[r] + so + (TZ + qn) * C::PLANE));
       }
-      // x-box of D = (A - I)^2 per plane
+      // x-box of D = s^2 (A - I)^2 per plane
       float2 g[NQ][RX];
 #pragma unroll
       for (int q = 0; q < NQ; ++q) {
@@ -141,7 +141,7 @@ __device__ __forceinline__ void sweep_dw(const float2 (&In)[TZ + 2][RX + 2], flo
         float2 D[NR];
 #pragma unroll
         for (int r = 0; r < NR; ++r) {
-          const float2 d = add2(Aw[sq][r], In[q][r]);
+          const float2 d = fma2(Aw[sq][r], scale2, In[q][r]);  // s * (A - I)
           D[r] = mul2(d, d);
         }
 #pragma unroll
@@ -176,8 +176,8 @@ __device__ __forceinline__ void sweep_dw(const float2 (&In)[TZ + 2][RX + 2], flo
                                            __shfl_up_sync(0xffffffffu, cc.y, 1));
             const float2 rgt = make_float2(__shfl_down_sync(0xffffffffu, cc.x, 1),
                                            __shfl_down_sync(0xffffffffu, cc.y, 1));
-            const float2 e = mul2(add2(add2(cc, lft), rgt), negk2);
-            const float2 w = make_float2(ex2_approx(e.x), ex2_approx(e.y));
+            const float2 e = add2(add2(cc, lft), rgt);  // SSD * log2(e) / div
+            const float2 w = make_float2(ex2_approx(-e.x), ex2_approx(-e.y));
             const float2 lab = make_float2(lds_f32(rowL[x] + so + (q + k) * C::PLANE),
                                            lds_f32(rowL[x] + so + (TZ + q + k) * C::PLANE));
             P[q + k][x] = fma2(w, lab, P[q + k][x]);
@@ -209,7 +209,7 @@ __device__ __forceinline__ bool run_item(const SubjectView &sv, int item, Pipe &
   const uint32_t ringL = ringA + C::RA * C::SLOT_A;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int lo = HW + 1;
-  const float2 negk2 = make_float2(sv.neg_k, sv.neg_k);
+  const float2 scale2 = make_float2(sv.scale, sv.scale);
   const int T = sv.atlases_per_group * NS;  // du steps per item (atlas-major)
 
   const int grp = item / sv.ntiles;
@@ -229,7 +229,7 @@ __device__ __forceinline__ bool run_item(const SubjectView &sv, int item, Pipe &
   const int xL = X0 - HW, zL = z0 - HW;          // CT slab origin
   const uint32_t lane_off = (uint32_t)(lane + HW + e) * 4u;
 
-  // Input patch values (negated: D = (A + In)^2), zero outside the volume.
+  // Input patch values, negated and scaled (D = (s A + In)^2 = s^2 (A - I)^2), zero outside.
   float2 In[NQ][NR];
 #pragma unroll
   for (int q = 0; q < NQ; ++q)
@@ -240,7 +240,7 @@ __device__ __forceinline__ bool run_item(const SubjectView &sv, int item, Pipe &
       for (int h = 0; h < 2; ++h) {
         const int zz = z0 + h * TZ - 1 + q, xx = xw - 1 + r;
         v[h] = (zz < sv.nz && xx < sv.nx && y < sv.ny)
-                   ? -__ldg(sv.img + (long long)zz * sv.nxy + (long long)xx * sv.ny + y)
+                   ? -__ldg(sv.img + (long long)zz * sv.nxy + (long long)xx * sv.ny + y) * sv.scale
                    : 0.f;
       }
       In[q][r] = make_float2(v[0], v[1]);
@@ -305,7 +305,7 @@ __device__ __forceinline__ bool run_item(const SubjectView &sv, int item, Pipe &
       for (int r = 0; r < NR; ++r) ra[r] = rowA[r] + (uint32_t)(dv * 4);
 #pragma unroll
       for (int r = 0; r < RX; ++r) rl[r] = rowL[r] + (uint32_t)(dv * 4);
-      sweep_dw<HW, RX, TZ>(In, P, W, ra, rl, negk2);
+      sweep_dw<HW, RX, TZ>(In, P, W, ra, rl, scale2);
     }
   }
   __syncthreads();  // a timeout in the item's last step is seen here
@@ -574,7 +574,7 @@ SubjectView subject_view(const Geometry &g, const SlabInputs &in, float *out, do
   sv.nz = g.nz;
   sv.nxy = g.nx * g.ny;
   sv.nvox = g.nvox();
-  sv.neg_k = (float)(-1.4426950408889634 / div);
+  sv.scale = (float)sqrt(1.4426950408889634 / div);
   sv.tiles_y = pl.tiles_y;
   sv.tiles_x = pl.tiles_x;
   sv.ntiles = pl.ntiles;
