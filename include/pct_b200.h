@@ -213,6 +213,10 @@ const char *pct_model_last_error(const pct_model *m);
  * inference_precision != 0 the BF16 weights the kernels use are returned (as floats). */
 int pct_model_set_params(pct_model *m, const float *params);
 int pct_model_get_params(pct_model *m, float *params, int inference_precision);
+/* Checkpoint files: a 16-byte header ("PCTLRN01", uint32 parameter count, uint32 0) and the FP32
+ * master weights, little-endian, in the flat parameter order. Loading resets Adam. */
+int pct_model_load_file(pct_model *m, const char *path);
+int pct_model_save_file(pct_model *m, const char *path);
 
 /* samples: host array [n][3] of (subject index, atlas index, flat voxel index). */
 int pct_train_set_create(int device, const pct_train_subject *subjects, int nsub,

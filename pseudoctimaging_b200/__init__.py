@@ -139,6 +139,8 @@ SIGNATURES = {
     "pct_model_last_error": (ctypes.c_char_p, [_P]),
     "pct_model_set_params": (_I, [_P, _P]),
     "pct_model_get_params": (_I, [_P, _P, _I]),
+    "pct_model_load_file": (_I, [_P, ctypes.c_char_p]),
+    "pct_model_save_file": (_I, [_P, ctypes.c_char_p]),
     "pct_train_set_create": (_I, [_I, ctypes.POINTER(TrainSubject), _I, _P, _I,
                                   ctypes.POINTER(_P)]),
     "pct_train_set_targets": (_I, [_P, _P, _P]),

@@ -6,7 +6,9 @@
 // are read when at least 7 arguments are given, the device when 8 are (defaults sigma=1, beta=1,
 // device 0, as in the reference). EXEC_CHOICE 0/1/2/3 run the path (the reference's GM, GM2, SM
 // and this library's plain FP32 kernel, which compute the same function); 4 times it like the
-// reference's GpuTestTime (10 samples of 10 calls).
+// reference's GpuTestTime (10 samples of 10 calls); 5/6 run the tensor-core FP16/BF16 form and 7
+// the learned proposal (NH = 11; the network from $PCT_LEARNED_MODEL, else the checkpoint
+// shipped beside the program, with the fallback threshold $PCT_LEARNED_CONF, default 0).
 //
 // <data> is the reference's non-MATLAB configuration file (PatchBasedPseudoCT.cu:1376-1488):
 //   line 1: 0 -> lines 2-4: atlas MRI, atlas CT, input MRI as MatrixIO text files
@@ -151,8 +153,12 @@ void usage() {
   printf(
       "Usage: PatchBasedPseudoCT_b200 <data> <output name> <EXEC_CHOICE> <NH> [sigma beta] "
       "[device]\n"
-      "  EXEC_CHOICE {GM=0, GM2=1, SM=2, B200 FP32=3: the path; GpuTestTime=4: timing}\n"
-      "  NH {3,5,7,9,11}; sigma, beta default 1; device default 0\n");
+      "  EXEC_CHOICE {GM=0, GM2=1, SM=2, B200 FP32=3: the path; GpuTestTime=4: timing;\n"
+      "               5/6: tensor-core FP16/BF16 form; 7: learned proposal}\n"
+      "  NH {3,5,7,9,11} (11 for 5, 6, 7); sigma, beta default 1; device default 0\n"
+      "  EXEC_CHOICE 7 reads the network from $PCT_LEARNED_MODEL (default: the checkpoint\n"
+      "  shipped beside this program, ../checkpoints/learned_nh11.pctl) and the full-search\n"
+      "  confidence threshold from $PCT_LEARNED_CONF (default 0)\n");
 }
 
 }  // namespace
@@ -206,7 +212,30 @@ int main(int argc, char **argv) {
       printf("Iter %d Atlas %d Nh %d Elapsed Time %f ms %f voxels/s\n", i, s.num, nh, ms,
              n / (ms / 1e3));
     }
-  } else if (choice >= 0 && choice <= 3) {
+  } else if ((choice >= 0 && choice <= 3) || choice == 5 || choice == 6 || choice == 7) {
+    pct_model *model = nullptr;
+    if (choice == PCT_EXEC_LEARNED) {
+      std::string path;
+      if (const char *e = getenv("PCT_LEARNED_MODEL")) {
+        path = e;
+      } else {
+        std::string exe = argv[0];
+        const size_t slash = exe.rfind('/');
+        path = (slash == std::string::npos ? std::string(".") : exe.substr(0, slash)) +
+               "/../checkpoints/learned_nh11.pctl";
+      }
+      const char *c = getenv("PCT_LEARNED_CONF");
+      const float conf = c ? (float)atof(c) : 0.0f;
+      if ((st = pct_model_create(device, 0, &model)) != PCT_OK ||
+          (st = pct_model_load_file(model, path.c_str())) != PCT_OK ||
+          (st = pct_attach_model(h, model, conf)) != PCT_OK) {
+        fprintf(stderr, "learned model %s: %s %s\n", path.c_str(), pct_strerror(st),
+                model ? pct_model_last_error(model) : "");
+        if (model) pct_model_destroy(model);
+        pct_destroy(h);
+        return EXIT_FAILURE;
+      }
+    }
     const auto t0 = std::chrono::steady_clock::now();
     st = pct_run_pipeline(h, s.img.data(), s.atlas.data(), s.ct.data(), out.data(), s.nx, s.ny,
                           s.nz, s.num, nh, sigma, beta, choice, /*regularize=*/1);
@@ -224,6 +253,10 @@ int main(int argc, char **argv) {
       }
       printf("Elapsed Time %f ms (transfers, path, regularisation, HU map) %f voxels/s\n", ms,
              n / (ms / 1e3));
+    }
+    if (model) {
+      pct_attach_model(h, nullptr, 0.f);
+      pct_model_destroy(model);
     }
   } else {
     st = PCT_ERR_INVALID_ARG;

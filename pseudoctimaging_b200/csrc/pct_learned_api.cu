@@ -2,6 +2,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <math.h>
+#include <stdio.h>
 #include <string.h>
 
 #include <new>
@@ -173,6 +174,41 @@ int pct_model_get_params(pct_model *m, float *params, int inference_precision) {
   MCUDA(m, cudaMemcpyAsync(params, m->master, kParams * sizeof(float), cudaMemcpyDeviceToHost,
                            m->stream));
   MCUDA(m, cudaStreamSynchronize(m->stream));
+  return PCT_OK;
+}
+
+int pct_model_load_file(pct_model *m, const char *path) {
+  if (!m || !path) return PCT_ERR_INVALID_ARG;
+  FILE *f = fopen(path, "rb");
+  if (!f) return model_fail(m, PCT_ERR_INVALID_ARG, std::string("cannot open ") + path);
+  unsigned char hdr[16];
+  std::vector<float> p(kParams);
+  const bool ok = fread(hdr, 1, 16, f) == 16 && memcmp(hdr, "PCTLRN01", 8) == 0 &&
+                  (uint32_t)(hdr[8] | hdr[9] << 8 | hdr[10] << 16 | (uint32_t)hdr[11] << 24) ==
+                      (uint32_t)kParams &&
+                  fread(p.data(), sizeof(float), kParams, f) == (size_t)kParams &&
+                  fgetc(f) == EOF;
+  fclose(f);
+  if (!ok)
+    return model_fail(m, PCT_ERR_INVALID_ARG,
+                      std::string(path) + ": not a checkpoint of " + std::to_string(kParams) +
+                          " parameters");
+  return pct_model_set_params(m, p.data());
+}
+
+int pct_model_save_file(pct_model *m, const char *path) {
+  if (!m || !path) return PCT_ERR_INVALID_ARG;
+  std::vector<float> p(kParams);
+  int st = pct_model_get_params(m, p.data(), 0);
+  if (st) return st;
+  FILE *f = fopen(path, "wb");
+  if (!f) return model_fail(m, PCT_ERR_INVALID_ARG, std::string("cannot create ") + path);
+  unsigned char hdr[16] = {'P', 'C', 'T', 'L', 'R', 'N', '0', '1', 0, 0, 0, 0, 0, 0, 0, 0};
+  const uint32_t n = (uint32_t)kParams;
+  for (int i = 0; i < 4; ++i) hdr[8 + i] = (unsigned char)(n >> (8 * i));
+  const bool ok = fwrite(hdr, 1, 16, f) == 16 &&
+                  fwrite(p.data(), sizeof(float), kParams, f) == (size_t)kParams;
+  if (fclose(f) != 0 || !ok) return model_fail(m, PCT_ERR_INTERNAL, std::string("cannot write ") + path);
   return PCT_OK;
 }
 

@@ -122,11 +122,14 @@ class LearnedModel:
         return feats, top, conf
 
     def save(self, path) -> None:
-        save_params(path, self.get_params())
+        _check(lib.pct_model_save_file(self._m, str(path).encode()), "pct_model_save_file",
+               self._m)
 
     @classmethod
     def load(cls, path, device: int = 0) -> "LearnedModel":
-        return cls(device=device, params=load_params(path))
+        m = cls(device=device)
+        _check(lib.pct_model_load_file(m._m, str(path).encode()), "pct_model_load_file", m._m)
+        return m
 
 
 def save_params(path, params: np.ndarray) -> None:

@@ -64,3 +64,22 @@ def test_cli_timing_mode_and_usage(tmp_path):
     assert out.count("Elapsed Time") == 10
     res = subprocess.run([str(CLI)], capture_output=True, text=True, timeout=60)
     assert res.returncode == 0 and "Usage" in res.stdout
+
+
+def test_cli_tensor_core_and_learned_choices(tmp_path):
+    """EXEC_CHOICE 5, 6 and 7 through the drop-in command line (NH = 11), against choice 3 on the
+    same synthetic subject; 7 uses the checkpoint shipped beside the program by default."""
+    cfg = tmp_path / "synth.cfg"
+    cfg.write_text("3\n2\n34\n37\n30\n8\n17\n")
+    outs = {}
+    for choice in (3, 5, 6, 7):
+        run_cli(cfg, tmp_path / f"c{choice}", choice, 11, 2.5, 1.0)
+        outs[choice] = np.fromfile(str(tmp_path / f"c{choice}") + ".f32", np.float32)
+    for choice in (5, 6, 7):
+        d = np.abs(outs[choice] - outs[3])
+        assert np.isfinite(outs[choice]).all()
+        assert d.mean() < 5.0, (choice, d.mean())
+    res = subprocess.run([str(CLI), str(cfg), str(tmp_path / "bad"), "7", "11"],
+                         capture_output=True, text=True, timeout=300,
+                         env={"PCT_LEARNED_MODEL": str(tmp_path / "missing.pctl")})
+    assert res.returncode != 0 and "missing.pctl" in res.stderr
