@@ -325,6 +325,9 @@ def run_b200_arm(args) -> None:
 
     plan = pct.query_plan(NX, NY, NZ, NUM, NH, local)
     clocks = clk.summary()
+    forms = None
+    if world == 1 and NH == 11 and not args.no_forms:
+        forms = time_other_forms(pct, h, d_img, d_mri, d_lab, d_out, div, stream, args)
     peaks = measured_peaks()
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
     mhz = clocks["sm_mhz"] or peaks.get("sm_max_mhz", 1965.0)
@@ -363,6 +366,8 @@ def run_b200_arm(args) -> None:
         "e2e": e2e,
         "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
     }
+    if forms:
+        line["forms"] = forms
     h.close()
     if world > 1:
         dist.destroy_process_group()
@@ -374,6 +379,52 @@ def run_b200_arm(args) -> None:
                                 "seconds": r["seconds"], "cand_per_s": r["cand_per_s"]}
     if rank == 0:
         print(json.dumps(line))
+
+
+def time_other_forms(pct, h, d_img, d_mri, d_lab, d_plain, div, stream, args) -> dict:
+    """The learned proposal (EXEC_CHOICE 7, committed network) and the tensor-core forms
+    (5 FP16, 6 BF16) on the same resident subject as the plain kernel: CUDA-event time per step
+    and the error against the plain kernel's output (HU), so one bench line carries every form."""
+    import torch
+
+    from pseudoctimaging_b200 import learned
+
+    core = (slice(6, -6),) * 3
+    ref = d_plain.cpu().numpy()[core].astype(np.float64)
+    nvox = NX * NY * NZ
+    model = learned.LearnedModel.load(learned.CHECKPOINT, torch.cuda.current_device())
+    h.attach_model(model, 0.0)
+    out = {}
+    for name, choice, steps in (("learned", pct.EXEC_LEARNED, 5), ("tc_fp16", pct.EXEC_TC_FP16, 2),
+                                ("tc_bf16", pct.EXEC_TC_BF16, 2)):
+        o = torch.zeros_like(d_img)
+
+        def step():
+            h.synthesize_device(d_img.data_ptr(), d_mri.data_ptr(), d_lab.data_ptr(), o.data_ptr(),
+                                NX, NY, NZ, NUM, NH, div, choice, stream.cuda_stream)
+        step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        h.device_status(stream.cuda_stream)
+        ms = e0.elapsed_time(e1) / steps
+        g = o.cpu().numpy()[core].astype(np.float64)
+        both = np.isfinite(g) & np.isfinite(ref)
+        e = np.abs(g[both] - ref[both]) * (4095.0 / 255.0)
+        out[name] = {"ms_per_step": ms, "value": nvox / (ms / 1e3), "steps": steps,
+                     "mae_hu_vs_plain": float(e.mean()), "max_abs_hu_vs_plain": float(e.max()),
+                     "nan_mismatch": int((np.isnan(g) != np.isnan(ref)).sum())}
+    if "learned" in out:
+        st = h.learned_stats()
+        out["learned"]["offsets_per_row"] = st["row_offsets"] / (
+            (NZ - 12) * (NX - 12) * -(-(NY - 12) // 30) * NUM)
+    h.attach_model(None)
+    model.close()
+    return out
 
 
 def config3_specs(n: int = 16, seed: int = 3) -> list[tuple[int, int, int, int, int]]:
@@ -733,6 +784,8 @@ def main() -> None:
     ap.add_argument("--batch-subjects", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-pointer end-to-end leg")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip timing the learned and tensor-core forms beside the plain kernel")
     ap.add_argument("--nh", type=int, default=NH, choices=[3, 5, 7, 9, 11],
                     help="search window (default 11, the metric's; 7 and 9 are config-1 sweeps)")
     ap.add_argument("--nz", type=int, default=NZ,
