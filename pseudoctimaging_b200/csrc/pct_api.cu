@@ -40,6 +40,8 @@ struct pct_handle {
   DevBuf learned;                       // its feature volumes and sums
   long long learned_nvox = 0;           // volume size of the last learned run (0: none yet)
   cudaStream_t learned_stream = nullptr;
+  cudaStream_t copy_stream = nullptr;   // uploads of the pipelined host path
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};  // start, first group staged, rest staged
   std::string last_error;
 };
 
@@ -229,6 +231,86 @@ int stage_pitched_h2d(pct_handle *h, DevBuf &buf, const float *src, const pct::G
   return PCT_OK;
 }
 
+// Uploads atlases [a0, a1) of a host stack into the pitched device stack `buf`; `stage` (the
+// same [num][nz][nx][ny] shape as the host stack) holds the contiguous copy before the repack
+// when the pitch differs from ny.
+int stage_pitched_slice(pct_handle *h, DevBuf &buf, float *stage_base, const float *src,
+                        const pct::Geometry &g, int a0, int a1, bool normalize, cudaStream_t s) {
+  const int pitch = pct::slab_pitch(g.ny);
+  const size_t rows = (size_t)(a1 - a0) * g.nz * g.nx;
+  const size_t first_row = (size_t)a0 * g.nz * g.nx;
+  float *dst = static_cast<float *>(buf.ptr) + first_row * pitch;
+  const float *from = src + first_row * g.ny;
+  const size_t bytes = rows * g.ny * sizeof(float);
+  if (pitch == g.ny) {
+    PCT_CUDA(h, cudaMemcpyAsync(dst, from, bytes, cudaMemcpyHostToDevice, s));
+  } else {
+    float *stage = stage_base + first_row * g.ny;
+    PCT_CUDA(h, cudaMemcpyAsync(stage, from, bytes, cudaMemcpyHostToDevice, s));
+    PCT_CUDA(h, pct::launch_pitch_copy(stage, dst, (long long)rows, g.ny, pitch, s));
+  }
+  if (normalize) PCT_CUDA(h, pct::launch_normalize_labels(dst, rows * pitch, s));
+  return PCT_OK;
+}
+
+// The host-pointer path with uploads overlapped with the fusion: the input MRI and the first
+// atlas group are uploaded and repacked on the handle's copy stream, the fusion of that group
+// starts on `s`, the remaining groups upload meanwhile and run in a second launch, then the
+// group sums are combined into d_out. Used when the plan has two or more atlas groups; returns
+// PCT_ERR_UNSUPPORTED (nothing enqueued) otherwise. `normalize` applies the label normalisation
+// to the CT stack on the device (the pipeline entry point).
+int fuse_pipelined(pct_handle *h, const pct::Geometry &g, const float *img, const float *atlas,
+                   const float *atlas_ct, float *d_out, double div, bool normalize,
+                   cudaStream_t s) {
+  pct::FusePlanInfo pl;
+  PCT_CUDA(h, pct::fuse_tma_plan(g, h->tile_set, &pl));
+  if (pl.groups < 2 || h->wait_test_ns) return PCT_ERR_UNSUPPORTED;
+  const int pitch = pct::slab_pitch(g.ny);
+  const size_t rows = (size_t)g.num * g.nz * g.nx;
+  int st;
+  if ((st = ensure(h, h->atlas, rows * pitch * sizeof(float))) ||
+      (st = ensure(h, h->label, rows * pitch * sizeof(float))) ||
+      (st = ensure(h, h->partial, pl.partial_bytes)) || (st = ensure(h, h->err, 16)))
+    return st;
+  if (pitch != g.ny && ensure(h, h->stage, 2 * rows * g.ny * sizeof(float))) {
+    h->last_error.clear();  // over the handle's memory cap: the one-upload path needs half
+    return PCT_ERR_UNSUPPORTED;
+  }
+  if (!h->copy_stream)
+    PCT_CUDA(h, cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+  for (cudaEvent_t &e : h->ev)
+    if (!e) PCT_CUDA(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  const cudaStream_t cs = h->copy_stream;
+  const int per = g.num / pl.groups;
+  int *err = static_cast<int *>(h->err.ptr);
+  PCT_CUDA(h, cudaMemsetAsync(err, 0, sizeof(int), s));
+  PCT_CUDA(h, cudaEventRecord(h->ev[0], s));
+  PCT_CUDA(h, cudaStreamWaitEvent(cs, h->ev[0], 0));
+  PCT_CUDA(h, cudaMemcpyAsync(h->img.ptr, img, (size_t)g.nvox() * sizeof(float),
+                              cudaMemcpyHostToDevice, cs));
+  // staging: the MRI stack, then the CT stack (both in flight at once)
+  float *stage_mri = static_cast<float *>(h->stage.ptr);
+  float *stage_ct = stage_mri ? stage_mri + rows * g.ny : nullptr;
+  auto stage_group = [&](int a0, int a1) -> int {
+    const int r = stage_pitched_slice(h, h->atlas, stage_mri, atlas, g, a0, a1, false, cs);
+    return r ? r : stage_pitched_slice(h, h->label, stage_ct, atlas_ct, g, a0, a1, normalize, cs);
+  };
+  if ((st = stage_group(0, per))) return st;
+  PCT_CUDA(h, cudaEventRecord(h->ev[1], cs));
+  PCT_CUDA(h, cudaStreamWaitEvent(s, h->ev[1], 0));
+  const pct::SlabInputs in{static_cast<const float *>(h->img.ptr),
+                           static_cast<const float *>(h->atlas.ptr),
+                           static_cast<const float *>(h->label.ptr), pitch};
+  float *partial = static_cast<float *>(h->partial.ptr);
+  PCT_CUDA(h, pct::launch_fuse_tma_groups(g, in, div, partial, err, h->tile_set, 0, 1, s));
+  if ((st = stage_group(per, g.num))) return st;
+  PCT_CUDA(h, cudaEventRecord(h->ev[2], cs));
+  PCT_CUDA(h, cudaStreamWaitEvent(s, h->ev[2], 0));
+  PCT_CUDA(h, pct::launch_fuse_tma_groups(g, in, div, partial, err, h->tile_set, 1, pl.groups, s));
+  PCT_CUDA(h, pct::launch_fuse_tma_combine(g, partial, h->tile_set, d_out, s));
+  return PCT_OK;
+}
+
 // ---- FP64 error reduction -------------------------------------------------------------------
 
 struct ErrAccum {
@@ -396,6 +478,9 @@ int pct_destroy(pct_handle *h) {
   for (DevBuf *b : {&h->img, &h->atlas, &h->label, &h->out, &h->scratch, &h->err, &h->partial,
                     &h->stage, &h->batch_stage, &h->batch_meta, &h->learned})
     if (b->ptr) cudaFree(b->ptr);
+  if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
+  for (cudaEvent_t e : h->ev)
+    if (e) cudaEventDestroy(e);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return PCT_OK;
@@ -510,11 +595,23 @@ int pct_synthesize(pct_handle *h, const float *img, const float *atlas, const fl
   const size_t vol = (size_t)g.nvox() * sizeof(float);
   if ((st = ensure(h, h->img, vol)) || (st = ensure(h, h->out, vol))) return st;
   cudaStream_t s = h->user_stream ? h->user_stream : h->stream;
+  PCT_CUDA(h, cudaMemsetAsync(h->out.ptr, 0, vol, s));
+  if (uses_tma_rows(exec_choice)) {
+    // uploads overlapped with the fusion when the plan has two or more atlas groups
+    st = fuse_pipelined(h, g, img, atlas, atlas_label, static_cast<float *>(h->out.ptr), div,
+                        false, s);
+    if (st == PCT_OK) {
+      PCT_CUDA(h, cudaMemcpyAsync(label_segmentation, h->out.ptr, vol, cudaMemcpyDeviceToHost, s));
+      PCT_CUDA(h, cudaStreamSynchronize(s));
+      return read_device_status(h, s);
+    }
+    if (st != PCT_ERR_UNSUPPORTED) return st;
+    h->last_error.clear();
+  }
   PCT_CUDA(h, cudaMemcpyAsync(h->img.ptr, img, vol, cudaMemcpyHostToDevice, s));
   if ((st = stage_pitched_h2d(h, h->atlas, atlas, g, s)) ||
       (st = stage_pitched_h2d(h, h->label, atlas_label, g, s)))
     return st;
-  PCT_CUDA(h, cudaMemsetAsync(h->out.ptr, 0, vol, s));
   pct::SlabInputs in{static_cast<const float *>(h->img.ptr), static_cast<const float *>(h->atlas.ptr),
                      static_cast<const float *>(h->label.ptr), pct::slab_pitch(g.ny)};
   if ((st = launch_path(h, g, in, static_cast<float *>(h->out.ptr), div, exec_choice, s)))
@@ -648,18 +745,26 @@ int pct_run_pipeline(pct_handle *h, const float *img, const float *atlas_mri,
   if (regularize && (st = ensure(h, h->scratch, pct::regularize_scratch_bytes(g.nvox())))) return st;
   cudaStream_t s = h->user_stream ? h->user_stream : h->stream;
   float *d_img = static_cast<float *>(h->img.ptr), *d_out = static_cast<float *>(h->out.ptr);
-  PCT_CUDA(h, cudaMemcpyAsync(d_img, img, vol, cudaMemcpyHostToDevice, s));
-  if ((st = stage_pitched_h2d(h, h->atlas, atlas_mri, g, s)) ||
-      (st = stage_pitched_h2d(h, h->label, atlas_ct_hu, g, s)))
-    return st;
-  const int pitch = pct::slab_pitch(g.ny);
-  // Label normalisation over the whole pitched stack (padding columns are never read).
-  PCT_CUDA(h, pct::launch_normalize_labels(static_cast<float *>(h->label.ptr),
-                                           (size_t)g.num * g.nz * g.nx * pitch, s));
   PCT_CUDA(h, cudaMemsetAsync(d_out, 0, vol, s));
-  pct::SlabInputs in{d_img, static_cast<const float *>(h->atlas.ptr),
-                     static_cast<const float *>(h->label.ptr), pitch};
-  if ((st = launch_path(h, g, in, d_out, div, exec_choice, s))) return st;
+  st = uses_tma_rows(exec_choice)
+           ? fuse_pipelined(h, g, img, atlas_mri, atlas_ct_hu, d_out, div, true, s)
+           : PCT_ERR_UNSUPPORTED;
+  if (st == PCT_ERR_UNSUPPORTED) {  // one upload, then the path
+    h->last_error.clear();
+    PCT_CUDA(h, cudaMemcpyAsync(d_img, img, vol, cudaMemcpyHostToDevice, s));
+    if ((st = stage_pitched_h2d(h, h->atlas, atlas_mri, g, s)) ||
+        (st = stage_pitched_h2d(h, h->label, atlas_ct_hu, g, s)))
+      return st;
+    const int pitch = pct::slab_pitch(g.ny);
+    // Label normalisation over the whole pitched stack (padding columns are never read).
+    PCT_CUDA(h, pct::launch_normalize_labels(static_cast<float *>(h->label.ptr),
+                                             (size_t)g.num * g.nz * g.nx * pitch, s));
+    pct::SlabInputs in{d_img, static_cast<const float *>(h->atlas.ptr),
+                       static_cast<const float *>(h->label.ptr), pitch};
+    if ((st = launch_path(h, g, in, d_out, div, exec_choice, s))) return st;
+  } else if (st) {
+    return st;
+  }
   if ((st = read_device_status(h, s))) return st;
   if (regularize) {
     long long f = 0;

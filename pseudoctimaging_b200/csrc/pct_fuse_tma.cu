@@ -100,6 +100,7 @@ struct SubjectView {
 
 struct TmaParams {
   SubjectView sv;
+  int item_begin, item_end;  // the work items this launch covers (group-major numbering)
   int *err;           // device status word (0 = ok)
   unsigned long long timeout_ns;
   int withhold_cta;   // testing hook: this CTA withholds its first copies (-1 = none)
@@ -374,8 +375,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   Pipe pp = pipe_init(smem_raw);
   p.sv.tmA = &tmA;
   p.sv.tmL = &tmL;
-  const int nitems = p.sv.ntiles * p.sv.groups;
-  for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+  for (int item = p.item_begin + blockIdx.x; item < p.item_end; item += gridDim.x) {
     if (!run_item<HW, RX, TZ>(p.sv, item, pp, p.err, p.timeout_ns, p.withhold_cta)) {
       pipe_drain(pp, p.timeout_ns);
       return;
@@ -586,13 +586,21 @@ SubjectView subject_view(const Geometry &g, const SlabInputs &in, float *out, do
 
 template <int SET, int HW>
 cudaError_t launch_hw(const Geometry &g, const SlabInputs &in, float *out, double div,
-                      float *partial, int *err, const WaitTest &wt, cudaStream_t stream) {
+                      float *partial, int *err, const WaitTest &wt, int group_begin, int group_end,
+                      cudaStream_t stream) {
   constexpr int RX = TileOf<SET, HW>::RX, TZ = TileOf<SET, HW>::TZ;
   using C = Cfg<HW, RX, TZ>;
   Plan pl;
   cudaError_t e = plan_hw<SET, HW>(g, &pl);
   if (e != cudaSuccess) return e;
   if (pl.groups > 1 && !partial) return cudaErrorInvalidValue;
+  const bool whole = group_begin < 0;  // all groups, then the combine
+  if (whole) {
+    group_begin = 0;
+    group_end = pl.groups;
+  } else if (pl.groups < 2 || group_begin >= group_end || group_end > pl.groups) {
+    return cudaErrorInvalidValue;  // a group range needs partial sums and a later combine
+  }
   CUtensorMap tmA, tmL;
   if ((e = make_slab_map(&tmA, in.atlas, g.nx, g.ny, g.nz, g.num, in.pitch, C::YB, C::ZA)) !=
       cudaSuccess)
@@ -609,9 +617,12 @@ cudaError_t launch_hw(const Geometry &g, const SlabInputs &in, float *out, doubl
     p.timeout_ns = wt.timeout_ns;
     p.withhold_cta = 0;
   }
-  fuse_tma_kernel<HW, RX, TZ><<<pl.blocks, kThreads, C::SMEM, stream>>>(tmA, tmL, p);
+  p.item_begin = group_begin * pl.ntiles;
+  p.item_end = group_end * pl.ntiles;
+  const int blocks = std::min(pl.blocks, p.item_end - p.item_begin);
+  fuse_tma_kernel<HW, RX, TZ><<<blocks, kThreads, C::SMEM, stream>>>(tmA, tmL, p);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  if (pl.groups > 1) return launch_combine_groups(g, partial, pl.groups, out, stream);
+  if (whole && pl.groups > 1) return launch_combine_groups(g, partial, pl.groups, out, stream);
   return cudaSuccess;
 }
 
@@ -633,13 +644,14 @@ cudaError_t plan_any(const Geometry &g, int set, Plan *pl) {
 
 template <int SET>
 cudaError_t launch_set(const Geometry &g, const SlabInputs &in, float *out, double div,
-                       float *partial, int *err, const WaitTest &wt, cudaStream_t stream) {
+                       float *partial, int *err, const WaitTest &wt, int gb, int ge,
+                       cudaStream_t stream) {
   switch (g.hw) {
-    case 1: return launch_hw<SET, 1>(g, in, out, div, partial, err, wt, stream);
-    case 2: return launch_hw<SET, 2>(g, in, out, div, partial, err, wt, stream);
-    case 3: return launch_hw<SET, 3>(g, in, out, div, partial, err, wt, stream);
-    case 4: return launch_hw<SET, 4>(g, in, out, div, partial, err, wt, stream);
-    case 5: return launch_hw<SET, 5>(g, in, out, div, partial, err, wt, stream);
+    case 1: return launch_hw<SET, 1>(g, in, out, div, partial, err, wt, gb, ge, stream);
+    case 2: return launch_hw<SET, 2>(g, in, out, div, partial, err, wt, gb, ge, stream);
+    case 3: return launch_hw<SET, 3>(g, in, out, div, partial, err, wt, gb, ge, stream);
+    case 4: return launch_hw<SET, 4>(g, in, out, div, partial, err, wt, gb, ge, stream);
+    case 5: return launch_hw<SET, 5>(g, in, out, div, partial, err, wt, gb, ge, stream);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -787,8 +799,28 @@ cudaError_t launch_fuse_tma(const Geometry &g, const SlabInputs &in, float *out,
                             float *partial, int *err, const WaitTest &wt, int set,
                             cudaStream_t stream) {
   if (g.ix <= 0 || g.iy <= 0 || g.iz <= 0) return cudaSuccess;
-  return set == 1 ? launch_set<1>(g, in, out, div, partial, err, wt, stream)
-                  : launch_set<0>(g, in, out, div, partial, err, wt, stream);
+  return set == 1 ? launch_set<1>(g, in, out, div, partial, err, wt, -1, -1, stream)
+                  : launch_set<0>(g, in, out, div, partial, err, wt, -1, -1, stream);
+}
+
+cudaError_t launch_fuse_tma_groups(const Geometry &g, const SlabInputs &in, double div,
+                                   float *partial, int *err, int set, int group_begin,
+                                   int group_end, cudaStream_t stream) {
+  if (g.ix <= 0 || g.iy <= 0 || g.iz <= 0) return cudaSuccess;
+  const WaitTest wt{0};
+  return set == 1
+             ? launch_set<1>(g, in, nullptr, div, partial, err, wt, group_begin, group_end, stream)
+             : launch_set<0>(g, in, nullptr, div, partial, err, wt, group_begin, group_end, stream);
+}
+
+cudaError_t launch_fuse_tma_combine(const Geometry &g, const float *partial, int set, float *out,
+                                    cudaStream_t stream) {
+  if (g.ix <= 0 || g.iy <= 0 || g.iz <= 0) return cudaSuccess;
+  Plan pl;
+  cudaError_t e = plan_any(g, set, &pl);
+  if (e != cudaSuccess) return e;
+  if (pl.groups < 2) return cudaErrorInvalidValue;
+  return launch_combine_groups(g, partial, pl.groups, out, stream);
 }
 
 namespace {

@@ -50,6 +50,14 @@ cudaError_t fuse_tma_plan(const Geometry &g, int set, FusePlanInfo *info);
 cudaError_t launch_fuse_tma(const Geometry &g, const SlabInputs &in, float *out, double div,
                             float *partial, int *err, const WaitTest &wt, int set,
                             cudaStream_t stream);
+// Pipelined form of the same (plans with 2 or more atlas groups only): the work items of atlas
+// groups [group_begin, group_end) into the partial sums, and, once every group has run, the
+// combine into out. Lets the host start on the first groups while later groups are uploaded.
+cudaError_t launch_fuse_tma_groups(const Geometry &g, const SlabInputs &in, double div,
+                                   float *partial, int *err, int set, int group_begin,
+                                   int group_end, cudaStream_t stream);
+cudaError_t launch_fuse_tma_combine(const Geometry &g, const float *partial, int set, float *out,
+                                    cudaStream_t stream);
 
 // Batched form: many subjects (NH 7/9/11), one persistent launch.
 struct BatchSubjectIn {
