@@ -40,6 +40,9 @@ SIGMA, BETA = 2.5, 1.0
 N_BLOBS = 60
 METRIC = "pseudo-CT voxels/s at 222x222x112, 10 atlases, NH=11"
 UNIT = "voxels/s"
+# The reference's best published number for this metric: CUDA-SM on one V100 (DGX Station),
+# 10.30 s for the 222x222x112 subject with 10 atlases at NH=11, transfers included.
+PUBLISHED_NH11_VOXELS_PER_S = 535826.0
 # Algorithmic FP32 lane-operations per candidate (voxel, atlas, offset): 1 sub + 1 mul for the
 # squared difference, 6 adds for the separable 3x3x3 box sum, 1 scale, 1 FMA + 1 add for the two
 # accumulators; plus 1 MUFU ex2.
@@ -341,7 +344,11 @@ def run_b200_arm(args) -> None:
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32",
+        "vs_baseline": (value / PUBLISHED_NH11_VOXELS_PER_S
+                        if (NZ == 112 and NH == 11) else None),
+        "vs_baseline_ref": "reference's best published: CUDA-SM, 1x V100, 10.30 s incl. "
+                           "transfers = 535,826 voxels/s (NH=11)",
+        "dtype": "f32",
         "data": "synthetic (seeded blobs/displacement generator, config 1; one subject per GPU)",
         "config": {"workload": f"{NX}x{NY}x{NZ} subject, 10 atlases, NH={NH}, sigma 2.5, beta 1, "
                                "plain FP32 kernel (EXEC_CHOICE 3)",
