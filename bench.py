@@ -758,7 +758,7 @@ def run_learned_arm(args) -> None:
                              "nan_mismatch": int((np.isnan(a) != np.isnan(b)).sum())},
         "fallback_share": st["fallback_pairs"] / pairs,
         "offsets_per_row": st["row_offsets"] / rows,
-        "gpu_launches": args.steps * (3 + 5 * NUM + 1),
+        "gpu_launches": args.steps * (3 + 6 * NUM + 1),
         "roofline": {"bound": "tensor", "unit": "TFLOP/s",
                      "achieved": conv_flop / (ms / 1e3) / 1e12, "peak": bf16,
                      "frac": (conv_flop / (ms / 1e3) / 1e12 / bf16) if bf16 else None,

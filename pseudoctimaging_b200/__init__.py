@@ -148,6 +148,7 @@ SIGNATURES = {
     "pct_model_gradients": (_I, [_P, _P, _I, _I, _P, ctypes.POINTER(ctypes.c_float)]),
     "pct_model_train": (_I, [_P, _P, _I, _I, ctypes.c_float, ctypes.POINTER(ctypes.c_float)]),
     "pct_attach_model": (_I, [_P, _P, ctypes.c_float]),
+    "pct_set_learned_block": (_I, [_P, _I]),
     "pct_tc_survivors": (_I, [_P, _I, _P, _P, _P, _P, _I, _I, _I, _D, _P, _P]),
     "pct_learned_stats": (_I, [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
     "pct_model_probe": (_I, [_P, _P, _P, _I, _I, _I, _P, _I, _P, _P, _P]),
@@ -252,6 +253,11 @@ class Handle:
 
     def set_memory_limit(self, nbytes: int) -> None:
         self._check(lib.pct_set_memory_limit(self._h, nbytes), "pct_set_memory_limit")
+
+    def set_learned_block(self, block: int) -> None:
+        """Rows per proposal block along z and x for EXEC_LEARNED (default 4; 1 = per row
+        segment)."""
+        self._check(lib.pct_set_learned_block(self._h, int(block)), "pct_set_learned_block")
 
     def attach_model(self, model, conf_threshold: float = 0.0) -> None:
         """Makes EXEC_LEARNED available (NH = 11) with a :class:`learned.LearnedModel` (None

@@ -37,6 +37,7 @@ struct pct_handle {
   DevBuf batch_stage, batch_meta;       // pct_synthesize_batch: pitched stacks, subject table
   pct_model *model = nullptr;           // learned form (EXEC_CHOICE 7), see pct_attach_model
   float learned_conf = 0.f;             // its full-search fallback threshold
+  int learned_block = 4;                // rows per proposal block along z and x
   DevBuf learned;                       // its feature volumes and sums
   long long learned_nvox = 0;           // volume size of the last learned run (0: none yet)
   cudaStream_t learned_stream = nullptr;
@@ -160,12 +161,13 @@ int launch_learned_path(pct_handle *h, const pct::Geometry &g, const pct::SlabIn
                     std::to_string(g.nh));
   if (pct::learned::model_device(h->model) != h->device)
     return fail(h, PCT_ERR_INVALID_ARG, "the attached model lives on another device");
-  int st = ensure(h, h->learned, pct::learned::infer_scratch_bytes(g.nvox()));
+  int st = ensure(h, h->learned, pct::learned::infer_scratch_bytes(g));
   if (st || (st = ensure(h, h->err, 16))) return st;
   int *err = static_cast<int *>(h->err.ptr);
   PCT_CUDA(h, cudaMemsetAsync(err, 0, sizeof(int), s));
   PCT_CUDA(h, pct::learned::launch_learned(g, pct::learned::model_weights(h->model), in, d_out, div,
-                                           h->learned_conf, h->learned.ptr, err, s));
+                                           h->learned_conf, h->learned_block, h->learned.ptr, err,
+                                           s));
   h->learned_nvox = g.nvox();
   h->learned_stream = s;
   return PCT_OK;
@@ -526,6 +528,14 @@ int pct_attach_model(pct_handle *h, pct_model *m, float conf_threshold) {
     return fail(h, PCT_ERR_INVALID_ARG, "the model lives on another device than the handle");
   h->model = m;
   h->learned_conf = conf_threshold;
+  return PCT_OK;
+}
+
+int pct_set_learned_block(pct_handle *h, int block) {
+  if (!h) return PCT_ERR_INVALID_ARG;
+  if (block < 1 || block > 16)
+    return fail(h, PCT_ERR_INVALID_ARG, "learned proposal block must be 1..16 rows");
+  h->learned_block = block;
   return PCT_OK;
 }
 

@@ -101,12 +101,15 @@ cudaError_t launch_finalize_hu(float *vol, size_t n, cudaStream_t stream);
 
 namespace learned {
 // Learned-proposal inference (NH = 11). `weights` are the model's BF16 parameters on the device.
-size_t infer_scratch_bytes(long long nvox);
+size_t infer_scratch_bytes(const Geometry &g);
 // Two device counters: (voxel, atlas) pairs that fell back, offsets evaluated by warp rows.
 unsigned long long *infer_counters(void *scratch, long long nvox);
 // *err (device) is set to a non-zero code if a bounded wait of the convolution pipeline gives up.
+// Rows of voxels share the proposal of their block's anchor row: blocks of `block` x `block`
+// rows in (z, x) (1 = every row segment proposes for itself).
 cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInputs &in, float *out,
-                           double div, float conf_thr, void *scratch, int *err, cudaStream_t s);
+                           double div, float conf_thr, int block, void *scratch, int *err,
+                           cudaStream_t s);
 cudaError_t learned_probe(const Geometry &g, const void *weights, const float *img,
                           const float *atlas_a, void *scratch, const int64_t *voxels, int n,
                           float *features, signed char *top, float *conf, cudaStream_t s);

@@ -346,7 +346,7 @@ int pct_model_probe(pct_model *m, const float *d_img, const float *d_atlas, int 
     if (voxels[i] < 0 || voxels[i] >= g.nvox()) return PCT_ERR_INVALID_ARG;
   MCUDA(m, cudaSetDevice(m->device));
   void *scratch = nullptr;
-  if (cudaMalloc(&scratch, infer_scratch_bytes(g.nvox())) != cudaSuccess) {
+  if (cudaMalloc(&scratch, infer_scratch_bytes(g)) != cudaSuccess) {
     cudaGetLastError();
     return model_fail(m, PCT_ERR_OUT_OF_MEMORY, "feature scratch");
   }

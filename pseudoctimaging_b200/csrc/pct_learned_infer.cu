@@ -23,6 +23,8 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <vector>
+
 #include "pct_internal.h"
 #include "pct_learned.h"
 #include "pct_ptx.cuh"
@@ -228,6 +230,7 @@ __device__ __forceinline__ void mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1
 
 struct ConvGrid {
   int nx, ny, nz, tiles_y, tiles_x, tiles;
+  const int *zlist;  // the output z-planes to compute (NULL: every plane)
 };
 
 __device__ __forceinline__ void conv_tile_origin(const ConvGrid &g, int tile, int &z, int &x0,
@@ -235,7 +238,7 @@ __device__ __forceinline__ void conv_tile_origin(const ConvGrid &g, int tile, in
   const int ty = tile % g.tiles_y;
   const int r = tile / g.tiles_y;
   x0 = (r % g.tiles_x) * kCvTX;
-  z = r / g.tiles_x;
+  z = g.zlist ? g.zlist[r / g.tiles_x] : r / g.tiles_x;
   y0 = ty * kCvTY;
 }
 
@@ -516,42 +519,24 @@ constexpr int kRescoreWarps = 4;  // warps per CTA
 constexpr int kProbStride = kHeads;  // 33 floats per lane row: column reads are conflict-free
 
 
-// Exact FP32 rescoring of one atlas. A warp owns a row segment (z, x, y0 .. y0+29) of interior
-// voxels; lane l sits at y = y0 - 1 + l (lanes 0 and 31 are the y halo). Every voxel of the
-// segment computes its per-axis probabilities; their sums over the segment give the row's
-// proposal: per axis the 4 most probable offsets, and the 32 rank triples with i + j + k <= 4.
-// A voxel whose own probability mass on those 32 is below conf_thr falls back to all 11^3
-// offsets. Each offset is evaluated once for all 32 lanes: D(y) = sum over the 3x3 (dz, dx) taps
-// of the squared differences at y, then SSD(y) = D(y-1) + D(y) + D(y+1) by warp shuffles; a lane
-// adds the weight exp(-SSD/div) and the weighted CT value for the offsets it keeps.
-__device__ __forceinline__ void eval_offset(const float *__restrict__ atl,
-                                            const float *__restrict__ lab, const float (&in)[9],
-                                            long long vz, long long axy, int apitch, int yc,
-                                            int dw, int du, int dv, bool take, float &P,
-                                            float &W, float neg_k) {
-  const float *a = atl + vz + (long long)(dw - 1) * axy + (long long)(du - 1) * apitch + yc + dv;
-  float d = 0.f;
-#pragma unroll
-  for (int k = 0; k < 9; ++k) {
-    const float t = in[k] - __ldg(a + (long long)(k / 3) * axy + (long long)(k % 3) * apitch);
-    d = fmaf(t, t, d);
-  }
-  const float ssd =
-      __shfl_up_sync(0xffffffffu, d, 1) + d + __shfl_down_sync(0xffffffffu, d, 1);
-  if (take) {
-    const float w = ptx::ex2_approx(ssd * neg_k);
-    P = fmaf(w, __ldg(lab + vz + (long long)dw * axy + (long long)du * apitch + yc + dv), P);
-    W += w;
-  }
+// The proposal of one row segment (30 voxels along y) of a block anchor row: the segment's
+// per-axis probabilities summed over its voxels, the 4 most probable offsets per axis of the sums
+// (offset index 0..10, ties to the lower offset), and each voxel's own probability mass on the
+// resulting 32 rank triples. Rows share the proposal of their block's anchor row: blocks of
+// `block` x `block` rows in (z, x), anchored at their middle row (clamped to the interior).
+struct RowProp {
+  signed char top[12];  // [axis][rank]
+  float conf[kRowOut];  // per output voxel of the segment (lane - 1)
+};
+
+__device__ __forceinline__ int anchor_of(int b, int block, int extent) {
+  const int a = b * block + block / 2;
+  return a < extent ? a : extent - 1;
 }
 
-__global__ void __launch_bounds__(kRescoreWarps * 32, 3)
-    rescore_kernel(const __nv_bfloat16 *__restrict__ f4, const __nv_bfloat16 *__restrict__ wbf,
-                   const float *__restrict__ img, const float *__restrict__ atl,
-                   const float *__restrict__ lab, int nx, int ny, int nz, int apitch, float neg_k,
-                   float conf_thr, float *__restrict__ pacc, float *__restrict__ wacc,
-                   unsigned long long *__restrict__ fallbacks,
-                   unsigned long long *__restrict__ evaluated) {
+__global__ void __launch_bounds__(kRescoreWarps * 32)
+    propose_rows_kernel(const __nv_bfloat16 *__restrict__ f4, const __nv_bfloat16 *__restrict__ wbf,
+                        int nx, int ny, int nz, int block, RowProp *__restrict__ props) {
   __shared__ __align__(16) float hw[kHeadFloats];
   __shared__ float s_prob[kRescoreWarps * 32 * kProbStride];
   __shared__ float s_sum[kRescoreWarps * 36];
@@ -563,20 +548,17 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 3)
   const int ix = nx - 2 * lo, iz = nz - 2 * lo, iy = ny - 2 * lo;
   if (ix <= 0 || iy <= 0 || iz <= 0) return;
   const int segs = (iy + kRowOut - 1) / kRowOut;
-  const long long items = (long long)iz * ix * segs;
+  const int nbx = (ix + block - 1) / block, nbz = (iz + block - 1) / block;
+  const long long items = (long long)nbz * nbx * segs;
   const int nxy = nx * ny;
-  const long long axy = (long long)nx * apitch;
-  unsigned long long my_fallbacks = 0, my_evals = 0;
   for (long long it = (long long)blockIdx.x * kRescoreWarps + (threadIdx.x >> 5); it < items;
        it += (long long)gridDim.x * kRescoreWarps) {
     const int seg = (int)(it % segs);
     const long long r0 = it / segs;
-    const int x = (int)(r0 % ix) + lo, z = (int)(r0 / ix) + lo;
-    const int y0 = lo + seg * kRowOut;
-    const int y = y0 - 1 + lane;
+    const int bx = (int)(r0 % nbx), bz = (int)(r0 / nbx);
+    const int x = lo + anchor_of(bx, block, ix), z = lo + anchor_of(bz, block, iz);
+    const int y = lo + seg * kRowOut - 1 + lane;
     const bool out_lane = lane >= 1 && lane <= kRowOut && y < ny - lo;
-    const int yc = min(y, ny - lo);  // halo lanes past the interior load clamped (unused) values
-    // the voxel's probabilities, the row's sums, the row's proposal
     float p[kHeads];
     if (out_lane) {
       axis_probs(f4 + ((long long)z * nxy + (long long)x * ny + y) * kC, hw, p);
@@ -584,7 +566,7 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 3)
 #pragma unroll
       for (int o = 0; o < kHeads; ++o) p[o] = 0.f;
     }
-    // row sums through shared memory: lane l sums column l (and column 32) of the row's
+    // row sums through shared memory: lane l sums column l (and column 32) of the segment's
     // probabilities; lanes 0..2 pick the top 4 of axis 0..2
     float *wp = s_prob + (threadIdx.x >> 5) * 32 * kProbStride;
     float *wsum = s_sum + (threadIdx.x >> 5) * 36;
@@ -623,21 +605,85 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 3)
       }
     }
     __syncwarp();
-    int top[3][4];
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-      for (int r = 0; r < 4; ++r) top[a][r] = wtop[a * 4 + r];
-    bool full = false;
+    RowProp &rp = props[r0 * segs + seg];
+    if (lane < 12) rp.top[lane] = (signed char)wtop[lane];
     if (out_lane) {
-      // this voxel's mass on the row's 32, its probabilities read back from its transpose row
       float tp[3][4];
 #pragma unroll
       for (int a = 0; a < 3; ++a)
 #pragma unroll
-        for (int r = 0; r < 4; ++r) tp[a][r] = wp[lane * kProbStride + a * kAxis + top[a][r]];
-      full = mass_of(tp) < conf_thr;
+        for (int r = 0; r < 4; ++r) tp[a][r] = wp[lane * kProbStride + a * kAxis + wtop[a * 4 + r]];
+      rp.conf[lane - 1] = mass_of(tp);
+    } else if (lane >= 1 && lane <= kRowOut) {
+      rp.conf[lane - 1] = 0.f;
     }
+    __syncwarp();  // the warp's shared rows are rewritten by its next segment
+  }
+}
+
+// Exact FP32 rescoring of one atlas. A warp owns a row segment (z, x, y0 .. y0+29) of interior
+// voxels; lane l sits at y = y0 - 1 + l (lanes 0 and 31 are the y halo). Every voxel of the
+// segment computes its per-axis probabilities; their sums over the segment give the row's
+// proposal: per axis the 4 most probable offsets, and the 32 rank triples with i + j + k <= 4.
+// A voxel whose own probability mass on those 32 is below conf_thr falls back to all 11^3
+// offsets. Each offset is evaluated once for all 32 lanes: D(y) = sum over the 3x3 (dz, dx) taps
+// of the squared differences at y, then SSD(y) = D(y-1) + D(y) + D(y+1) by warp shuffles; a lane
+// adds the weight exp(-SSD/div) and the weighted CT value for the offsets it keeps.
+__device__ __forceinline__ void eval_offset(const float *__restrict__ atl,
+                                            const float *__restrict__ lab, const float (&in)[9],
+                                            long long vz, long long axy, int apitch, int yc,
+                                            int dw, int du, int dv, bool take, float &P,
+                                            float &W, float neg_k) {
+  const float *a = atl + vz + (long long)(dw - 1) * axy + (long long)(du - 1) * apitch + yc + dv;
+  float d = 0.f;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    const float t = in[k] - __ldg(a + (long long)(k / 3) * axy + (long long)(k % 3) * apitch);
+    d = fmaf(t, t, d);
+  }
+  const float ssd =
+      __shfl_up_sync(0xffffffffu, d, 1) + d + __shfl_down_sync(0xffffffffu, d, 1);
+  if (take) {
+    const float w = ptx::ex2_approx(ssd * neg_k);
+    P = fmaf(w, __ldg(lab + vz + (long long)dw * axy + (long long)du * apitch + yc + dv), P);
+    W += w;
+  }
+}
+
+__global__ void __launch_bounds__(kRescoreWarps * 32, 3)
+    rescore_kernel(const RowProp *__restrict__ props, int block, const float *__restrict__ img,
+                   const float *__restrict__ atl, const float *__restrict__ lab, int nx, int ny,
+                   int nz, int apitch, float neg_k, float conf_thr, float *__restrict__ pacc,
+                   float *__restrict__ wacc, unsigned long long *__restrict__ fallbacks,
+                   unsigned long long *__restrict__ evaluated) {
+  const int lane = threadIdx.x & 31;
+  const int lo = 6;
+  const int ix = nx - 2 * lo, iz = nz - 2 * lo, iy = ny - 2 * lo;
+  if (ix <= 0 || iy <= 0 || iz <= 0) return;
+  const int segs = (iy + kRowOut - 1) / kRowOut;
+  const int nbx = (ix + block - 1) / block;
+  const long long items = (long long)iz * ix * segs;
+  const int nxy = nx * ny;
+  const long long axy = (long long)nx * apitch;
+  unsigned long long my_fallbacks = 0, my_evals = 0;
+  for (long long it = (long long)blockIdx.x * kRescoreWarps + (threadIdx.x >> 5); it < items;
+       it += (long long)gridDim.x * kRescoreWarps) {
+    const int seg = (int)(it % segs);
+    const long long r0 = it / segs;
+    const int x = (int)(r0 % ix) + lo, z = (int)(r0 / ix) + lo;
+    const int y0 = lo + seg * kRowOut;
+    const int y = y0 - 1 + lane;
+    const bool out_lane = lane >= 1 && lane <= kRowOut && y < ny - lo;
+    const int yc = min(y, ny - lo);  // halo lanes past the interior load clamped (unused) values
+    // the proposal of this row's block (its anchor row's 4 offsets per axis) and this voxel's
+    // confidence, measured on the anchor row's voxel at the same y
+    const RowProp &rp = props[(((long long)((z - lo) / block) * nbx) + (x - lo) / block) * segs + seg];
+    int top[3][4];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) top[a][r] = rp.top[a * 4 + r];
+    const bool full = out_lane && conf_thr > 0.f && rp.conf[lane - 1] < conf_thr;
     const unsigned any_full = __ballot_sync(0xffffffffu, full);
     if (full) ++my_fallbacks;
     // input taps of this lane: I(z+dz, x+dx, y), 3x3 (dz, dx)
@@ -657,7 +703,6 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 3)
           for (int k = 0; k + j + i < 5 && k < 4; ++k)
             eval_offset(atl, lab, in, vz + axy + apitch, axy, apitch, yc, top[0][i] - 5,
                         top[1][j] - 5, top[2][k] - 5, out_lane, P, W, neg_k);
-      __syncwarp();  // wtop is rewritten by the warp's next row
       my_evals += 32;
     } else {
       // the full window; lanes that did not fall back keep only their row's 32
@@ -683,7 +728,6 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 3)
         }
       }
       my_evals += kAxis * kAxis * kAxis;
-      __syncwarp();
     }
     if (out_lane) {
       const long long v = (long long)z * nxy + (long long)x * ny + y;
@@ -720,6 +764,11 @@ int sms() {
   return n;
 }
 
+int anchor_of_host(int b, int block, int extent) {
+  const int a = b * block + block / 2;
+  return a < extent ? a : extent - 1;
+}
+
 // Scratch layout: two BF16 channel-last feature volumes, the product and weight sums, the three
 // packed fragment tables and the fallback counter.
 struct InferScratch {
@@ -729,7 +778,15 @@ struct InferScratch {
   unsigned long long *fallbacks;  // (voxel, atlas) pairs that took the full search
   unsigned long long *evaluated;  // offsets evaluated by warp rows, summed over rows
   int *err;                       // bounded-wait status of the probe hook
+  RowProp *props;                 // row-segment proposals of the block anchor rows
+  int *zlists;                    // conv2, conv3, conv4 output planes, nz entries each
 };
+
+// Bytes before the proposal table (features, sums, fragments, counters), 256-aligned.
+size_t infer_base_bytes(long long nvox) {
+  const size_t b = (size_t)nvox * kC * 2 * 2 + (size_t)nvox * 4 * 2 + 3 * kFragWords * 4 + 256;
+  return (b + 255) / 256 * 256;
+}
 
 InferScratch carve(void *scratch, long long nvox) {
   InferScratch r;
@@ -742,13 +799,21 @@ InferScratch carve(void *scratch, long long nvox) {
   r.fallbacks = reinterpret_cast<unsigned long long *>(r.frag + 3 * kFragWords);
   r.evaluated = r.fallbacks + 1;
   r.err = reinterpret_cast<int *>(r.fallbacks + 2);
+  r.props = reinterpret_cast<RowProp *>(static_cast<unsigned char *>(scratch) +
+                                        infer_base_bytes(nvox));
+  r.zlists = nullptr;  // placed by carve_tables, which knows the geometry
   return r;
 }
 
 }  // namespace
 
-size_t infer_scratch_bytes(long long nvox) {
-  return (size_t)nvox * kC * 2 * 2 + (size_t)nvox * 4 * 2 + 3 * kFragWords * 4 + 256;
+size_t prop_table_bytes(const Geometry &g) {
+  const size_t rows = (size_t)g.nz * g.nx * (size_t)((g.ny + kRowOut - 1) / kRowOut + 1);
+  return (rows * sizeof(RowProp) + 255) / 256 * 256;
+}
+
+size_t infer_scratch_bytes(const Geometry &g) {
+  return infer_base_bytes(g.nvox()) + prop_table_bytes(g) + 3 * (size_t)g.nz * sizeof(int) + 256;
 }
 
 unsigned long long *infer_counters(void *scratch, long long nvox) {
@@ -776,7 +841,7 @@ cudaError_t make_feature_map(CUtensorMap *map, const __nv_bfloat16 *base, const 
 // conv1 .. conv4 of one (input, atlas) pair; returns the buffer holding the conv4 features.
 cudaError_t run_convs(const Geometry &g, const __nv_bfloat16 *wbf, const float *img,
                       const float *atlas_a, int apitch, const InferScratch &sc, int *err,
-                      __nv_bfloat16 **features, cudaStream_t s) {
+                      const int (&planes)[3], __nv_bfloat16 **features, cudaStream_t s) {
   const int n_sm = sms();
   {
     const long long items = (long long)g.nz * ((g.nx + kC1Warps - 1) / kC1Warps) * ((g.ny + 31) / 32);
@@ -795,11 +860,15 @@ cudaError_t run_convs(const Geometry &g, const __nv_bfloat16 *wbf, const float *
   cg.nz = g.nz;
   cg.tiles_y = (g.ny + kCvTY - 1) / kCvTY;
   cg.tiles_x = (g.nx + kCvTX - 1) / kCvTX;
-  cg.tiles = cg.tiles_y * cg.tiles_x * g.nz;
-  const int blocks = cg.tiles < 2 * n_sm ? cg.tiles : 2 * n_sm;
   const int boffs[3] = {kB2, kB3, kB4};
   __nv_bfloat16 *bufs[2] = {sc.fa, sc.fb};
   for (int l = 0; l < 3; ++l) {
+    // planes[l] < nz: only the listed output planes of layer l are needed
+    const bool all = planes[l] >= g.nz;
+    cg.zlist = all ? nullptr : sc.zlists + l * g.nz;
+    cg.tiles = cg.tiles_y * cg.tiles_x * (all ? g.nz : planes[l]);
+    if (cg.tiles == 0) continue;
+    const int blocks = cg.tiles < 2 * n_sm ? cg.tiles : 2 * n_sm;
     conv16_kernel<<<blocks, kCvThreads, kConvSmem, s>>>(maps[l & 1], sc.frag + l * kFragWords, wbf,
                                                         boffs[l], bufs[(l + 1) & 1], cg, err);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -826,12 +895,39 @@ cudaError_t pack_all(const __nv_bfloat16 *wbf, uint32_t *frag, cudaStream_t s) {
 // The learned form over all atlases of `in` (atlas and label rows `in.pitch` floats apart, the
 // input MRI contiguous). Writes the interior of `out`; the border is left untouched.
 cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInputs &in, float *out,
-                           double div, float conf_thr, void *scratch, int *err, cudaStream_t s) {
+                           double div, float conf_thr, int block, void *scratch, int *err,
+                           cudaStream_t s) {
+  if (block < 1) return cudaErrorInvalidValue;
   const __nv_bfloat16 *wbf = static_cast<const __nv_bfloat16 *>(weights);
   const long long nvox = g.nvox();
   const long long astride = (long long)g.nz * g.nx * in.pitch;
-  const InferScratch sc = carve(scratch, nvox);
+  InferScratch sc = carve(scratch, nvox);
+  sc.zlists = reinterpret_cast<int *>(reinterpret_cast<unsigned char *>(sc.props) +
+                                      prop_table_bytes(g));
   cudaError_t e;
+  // output planes each convolution must produce: the proposals read conv4 features on the
+  // anchor planes only, conv3 is needed 1 plane around them, conv2 2 planes around them
+  int planes[3] = {g.nz, g.nz, g.nz};
+  if (block > 1 && g.nz > 12) {
+    std::vector<int> lists(3 * (size_t)g.nz);
+    const int iz = g.nz - 12;
+    for (int l = 0; l < 3; ++l) {
+      const int radius = 2 - l;
+      std::vector<char> need(g.nz, 0);
+      for (int bz = 0; bz * block < iz; ++bz) {
+        const int a = 6 + anchor_of_host(bz, block, iz);
+        for (int d = -radius; d <= radius; ++d)
+          if (a + d >= 0 && a + d < g.nz) need[a + d] = 1;
+      }
+      int n = 0;
+      for (int z = 0; z < g.nz; ++z)
+        if (need[z]) lists[(size_t)l * g.nz + n++] = z;
+      planes[l] = n;
+    }
+    if ((e = cudaMemcpyAsync(sc.zlists, lists.data(), lists.size() * sizeof(int),
+                             cudaMemcpyHostToDevice, s)) != cudaSuccess)
+      return e;
+  }
   if ((e = cudaMemsetAsync(sc.pacc, 0, (size_t)nvox * 4 * 2, s)) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(sc.fallbacks, 0, 2 * sizeof(unsigned long long), s)) != cudaSuccess)
     return e;
@@ -843,13 +939,23 @@ cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInp
     rows = (long long)(g.nz - 12) * (g.nx - 12) * ((g.ny - 12 + kRowOut - 1) / kRowOut);
   const long long rblk = (rows + kRescoreWarps - 1) / kRescoreWarps;
   const int rescore_blocks = (int)(rblk < 1 ? 1 : (rblk > 64LL * sms() ? 64LL * sms() : rblk));
+  long long prows = 0;
+  if (g.nx > 12 && g.ny > 12 && g.nz > 12)
+    prows = (long long)((g.nz - 12 + block - 1) / block) * ((g.nx - 12 + block - 1) / block) *
+            ((g.ny - 12 + kRowOut - 1) / kRowOut);
+  const long long pblk = (prows + kRescoreWarps - 1) / kRescoreWarps;
+  const int propose_blocks = (int)(pblk < 1 ? 1 : (pblk > 64LL * sms() ? 64LL * sms() : pblk));
   for (int a = 0; a < g.num; ++a) {
     const float *A = in.atlas + a * astride, *L = in.label + a * astride;
     __nv_bfloat16 *f4 = nullptr;
-    if ((e = run_convs(g, wbf, in.img, A, in.pitch, sc, err, &f4, s)) != cudaSuccess) return e;
+    if ((e = run_convs(g, wbf, in.img, A, in.pitch, sc, err, planes, &f4, s)) != cudaSuccess)
+      return e;
+    propose_rows_kernel<<<propose_blocks, kRescoreWarps * 32, 0, s>>>(f4, wbf, g.nx, g.ny, g.nz,
+                                                                      block, sc.props);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
     rescore_kernel<<<rescore_blocks, kRescoreWarps * 32, 0, s>>>(
-        f4, wbf, in.img, A, L, g.nx, g.ny, g.nz, in.pitch, neg_k, conf_thr, sc.pacc, sc.wacc,
-        sc.fallbacks, sc.evaluated);
+        sc.props, block, in.img, A, L, g.nx, g.ny, g.nz, in.pitch, neg_k, conf_thr, sc.pacc,
+        sc.wacc, sc.fallbacks, sc.evaluated);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   finalize_kernel<<<nblk, 256, 0, s>>>(sc.pacc, sc.wacc, out, g.nx, g.ny, g.nz);
@@ -866,7 +972,9 @@ cudaError_t learned_probe(const Geometry &g, const void *weights, const float *i
   if ((e = pack_all(wbf, sc.frag, s)) != cudaSuccess) return e;
   __nv_bfloat16 *f4 = nullptr;
   if ((e = cudaMemsetAsync(sc.err, 0, sizeof(int), s)) != cudaSuccess) return e;
-  if ((e = run_convs(g, wbf, img, atlas_a, g.ny, sc, sc.err, &f4, s)) != cudaSuccess) return e;
+  const int planes[3] = {g.nz, g.nz, g.nz};
+  if ((e = run_convs(g, wbf, img, atlas_a, g.ny, sc, sc.err, planes, &f4, s)) != cudaSuccess)
+    return e;
   // the sums area is free here: voxel list, proposals and confidences go there
   int64_t *d_vox = reinterpret_cast<int64_t *>(sc.pacc);
   signed char *d_top = reinterpret_cast<signed char *>(d_vox + n);

@@ -6,8 +6,10 @@ linear heads 16->11 that score the offsets dw, du and dv of the 11^3 search wind
 per axis). The inference kernels propose per row segment of 30 voxels along y and per atlas:
 the per-axis probabilities of the segment's voxels are summed, the 4 most probable offsets per
 axis kept and, of their 64 combinations, the 32 whose per-axis ranks sum to at most 4; only those
-32 offsets get the exact FP32 SSD and a weight. A voxel whose own probability mass on the 32 is
-below a confidence threshold takes the full 11^3 search instead.
+32 offsets get the exact FP32 SSD and a weight. Rows share the proposal of their block's anchor
+row (blocks of 4 x 4 rows in z and x by default, ``Handle.set_learned_block``). A voxel whose
+probability mass on the 32 (measured on the anchor row) is below a confidence threshold takes
+the full 11^3 search instead.
 
 Training targets come from the plain method itself: for a sampled (subject, atlas, voxel) the
 exact FP32 SSD of all 1331 offsets, the 32 smallest, as one distribution per axis. Forward,

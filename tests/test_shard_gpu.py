@@ -39,6 +39,7 @@ def test_sharded_learned_form_matches_whole_volume():
     div = pct.div_from(2.5, 1.0)
     with pct.Handle(0) as h, learned.LearnedModel.load(learned.CHECKPOINT) as m:
         h.attach_model(m, 0.0)
+        h.set_learned_block(1)  # per-row proposals: independent of where the slabs start
         whole = h.synthesize(s.img, s.atlas_mri, lab, 11, div, pct.EXEC_LEARNED)
         out = np.zeros_like(whole)
         for sl in shard.slab_plan(s.img.shape[0], 11, 3):
