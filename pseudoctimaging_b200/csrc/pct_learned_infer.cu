@@ -739,6 +739,163 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 3)
   if (lane == 0 && my_evals) atomicAdd(evaluated, my_evals);
 }
 
+// Blocks of 4 rows: the 4 x-rows of a block (one z plane) share their proposal, so one warp
+// rescores them together. Per offset it loads the 3 z x 6 x tap rows the 4 rows need once
+// (instead of 4 x 9), forms D = s^2 (A - I)^2 with the scale folded into the differences,
+// sums z in registers, x across the shared rows and y by warp shuffles.
+constexpr int kRows = 4;
+
+// The kept set's rank triples (i, j, k), i + j + k <= 4, packed as i | j << 2 | k << 4, in the
+// order the single-row kernel visits them.
+__constant__ unsigned char kRankTriples[kTopK] = {
+    0x00, 0x10, 0x20, 0x30, 0x04, 0x14, 0x24, 0x34, 0x08, 0x18, 0x28, 0x0c, 0x1c,
+    0x01, 0x11, 0x21, 0x31, 0x05, 0x15, 0x25, 0x09, 0x19, 0x0d,
+    0x02, 0x12, 0x22, 0x06, 0x16, 0x0a,
+    0x03, 0x13, 0x07};
+
+__device__ __forceinline__ int pick4(const int (&t)[4], int i) {
+  return i == 0 ? t[0] : i == 1 ? t[1] : i == 2 ? t[2] : t[3];
+}
+
+__device__ __forceinline__ void eval_offset4(const float *__restrict__ atl,
+                                             const float *__restrict__ lab,
+                                             const float (&in)[3][kRows + 2], long long zrow0,
+                                             long long axy, int apitch, int nx, int x0, int yc,
+                                             int dw, int du, int dv, const bool (&take)[kRows],
+                                             float s, float (&P)[kRows], float (&W)[kRows]) {
+  float Z[kRows + 2];
+  const long long zb = zrow0 + (long long)dw * axy;  // plane z + dw - 1
+#pragma unroll
+  for (int xr = 0; xr < kRows + 2; ++xr) {
+    const int xa = min(x0 - 1 + xr + du, nx - 1);  // rows past the volume feed no output
+    const float *a = atl + zb + (long long)xa * apitch + yc + dv;
+    float z = 0.f;
+#pragma unroll
+    for (int dz = 0; dz < 3; ++dz) {
+      const float t = fmaf(__ldg(a + dz * axy), s, in[dz][xr]);
+      z = fmaf(t, t, z);
+    }
+    Z[xr] = z;
+  }
+#pragma unroll
+  for (int r = 0; r < kRows; ++r) {
+    const float x = Z[r] + Z[r + 1] + Z[r + 2];
+    const float e =
+        __shfl_up_sync(0xffffffffu, x, 1) + x + __shfl_down_sync(0xffffffffu, x, 1);
+    if (take[r]) {
+      const float w = ptx::ex2_approx(-e);
+      const int xl = x0 + r + du;
+      P[r] = fmaf(w, __ldg(lab + zb + axy + (long long)xl * apitch + yc + dv), P[r]);
+      W[r] += w;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kRescoreWarps * 32, 3)
+    rescore4_kernel(const RowProp *__restrict__ props, const float *__restrict__ img,
+                    const float *__restrict__ atl, const float *__restrict__ lab, int nx, int ny,
+                    int nz, int apitch, float scale, float conf_thr, float *__restrict__ pacc,
+                    float *__restrict__ wacc, unsigned long long *__restrict__ fallbacks,
+                    unsigned long long *__restrict__ evaluated) {
+  const int lane = threadIdx.x & 31;
+  const int lo = 6;
+  const int ix = nx - 2 * lo, iz = nz - 2 * lo, iy = ny - 2 * lo;
+  if (ix <= 0 || iy <= 0 || iz <= 0) return;
+  const int segs = (iy + kRowOut - 1) / kRowOut;
+  const int nbx = (ix + kRows - 1) / kRows;
+  const long long items = (long long)iz * nbx * segs;
+  const int nxy = nx * ny;
+  const long long axy = (long long)nx * apitch;
+  unsigned long long my_fallbacks = 0, my_evals = 0;
+  for (long long it = (long long)blockIdx.x * kRescoreWarps + (threadIdx.x >> 5); it < items;
+       it += (long long)gridDim.x * kRescoreWarps) {
+    const int seg = (int)(it % segs);
+    const long long r0 = it / segs;
+    const int bx = (int)(r0 % nbx), z = (int)(r0 / nbx) + lo;
+    const int x0 = lo + bx * kRows;
+    const int y0 = lo + seg * kRowOut;
+    const int y = y0 - 1 + lane;
+    const bool out_lane = lane >= 1 && lane <= kRowOut && y < ny - lo;
+    const int yc = min(y, ny - lo);
+    const RowProp &rp = props[((long long)((z - lo) / kRows) * nbx + bx) * segs + seg];
+    int top[3][4];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) top[a][r] = rp.top[a * 4 + r];
+    bool valid[kRows];
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) valid[r] = out_lane && x0 + r < nx - lo;
+    const bool full = out_lane && conf_thr > 0.f && rp.conf[lane - 1] < conf_thr;
+    const unsigned any_full = __ballot_sync(0xffffffffu, full);
+    if (full) {
+#pragma unroll
+      for (int r = 0; r < kRows; ++r) my_fallbacks += valid[r] ? 1 : 0;
+    }
+    // input taps I(z+dz-1, x0-1+xr, y), negated and scaled
+    float in[3][kRows + 2];
+#pragma unroll
+    for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+      for (int xr = 0; xr < kRows + 2; ++xr) {
+        const int xx = min(x0 - 1 + xr, nx - 1);
+        in[dz][xr] = -__ldg(img + (long long)(z + dz - 1) * nxy + (long long)xx * ny + yc) * scale;
+      }
+    const long long zrow0 = (long long)(z - 1) * axy;
+    float P[kRows], W[kRows];
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) P[r] = W[r] = 0.f;
+    if (!any_full) {
+      bool take[kRows];
+#pragma unroll
+      for (int r = 0; r < kRows; ++r) take[r] = valid[r];
+#pragma unroll 1
+      for (int c = 0; c < kTopK; ++c) {
+        const int code = kRankTriples[c];
+        eval_offset4(atl, lab, in, zrow0, axy, apitch, nx, x0, yc, pick4(top[0], code & 3) - 5,
+                     pick4(top[1], (code >> 2) & 3) - 5, pick4(top[2], code >> 4) - 5, take,
+                     scale, P, W);
+      }
+      my_evals += 32 * (unsigned long long)min(kRows, nx - lo - x0);
+    } else {
+      unsigned long long rank[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        rank[a] = 0x77777777777ULL;  // nibble j: rank of offset j - 5 on axis a, 7 = not kept
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          rank[a] &= ~(0xFULL << (4 * top[a][r]));
+          rank[a] |= (unsigned long long)r << (4 * top[a][r]);
+        }
+      }
+      for (int jw = 0; jw < kAxis; ++jw) {
+        const int rw = (int)((rank[0] >> (4 * jw)) & 0xF);
+        for (int ju = 0; ju < kAxis; ++ju) {
+          const int ru = rw + (int)((rank[1] >> (4 * ju)) & 0xF);
+          for (int jv = 0; jv < kAxis; ++jv) {
+            const bool mine = full || (ru + (int)((rank[2] >> (4 * jv)) & 0xF) <= 4);
+            bool take[kRows];
+#pragma unroll
+            for (int r = 0; r < kRows; ++r) take[r] = valid[r] && mine;
+            eval_offset4(atl, lab, in, zrow0, axy, apitch, nx, x0, yc, jw - 5, ju - 5, jv - 5,
+                         take, scale, P, W);
+          }
+        }
+      }
+      my_evals += kAxis * kAxis * kAxis * (unsigned long long)min(kRows, nx - lo - x0);
+    }
+#pragma unroll
+    for (int r = 0; r < kRows; ++r)
+      if (valid[r]) {
+        const long long v = (long long)z * nxy + (long long)(x0 + r) * ny + y;
+        pacc[v] += P[r];
+        wacc[v] += W[r];
+      }
+  }
+  if (my_fallbacks) atomicAdd(fallbacks, my_fallbacks);
+  if (lane == 0 && my_evals) atomicAdd(evaluated, my_evals);
+}
+
 __global__ void finalize_kernel(const float *__restrict__ pacc, const float *__restrict__ wacc,
                                 float *__restrict__ out, int nx, int ny, int nz) {
   const int lo = 6;
@@ -933,6 +1090,7 @@ cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInp
     return e;
   if ((e = pack_all(wbf, sc.frag, s)) != cudaSuccess) return e;
   const float neg_k = (float)(-1.4426950408889634 / div);
+  const float scale = (float)sqrt(1.4426950408889634 / div);
   const int nblk = sms() * 8;
   long long rows = 0;
   if (g.nx > 12 && g.ny > 12 && g.nz > 12)
@@ -953,9 +1111,15 @@ cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInp
     propose_rows_kernel<<<propose_blocks, kRescoreWarps * 32, 0, s>>>(f4, wbf, g.nx, g.ny, g.nz,
                                                                       block, sc.props);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    rescore_kernel<<<rescore_blocks, kRescoreWarps * 32, 0, s>>>(
-        sc.props, block, in.img, A, L, g.nx, g.ny, g.nz, in.pitch, neg_k, conf_thr, sc.pacc,
-        sc.wacc, sc.fallbacks, sc.evaluated);
+    if (block == kRows) {
+      rescore4_kernel<<<rescore_blocks, kRescoreWarps * 32, 0, s>>>(
+          sc.props, in.img, A, L, g.nx, g.ny, g.nz, in.pitch, scale, conf_thr, sc.pacc, sc.wacc,
+          sc.fallbacks, sc.evaluated);
+    } else {
+      rescore_kernel<<<rescore_blocks, kRescoreWarps * 32, 0, s>>>(
+          sc.props, block, in.img, A, L, g.nx, g.ny, g.nz, in.pitch, neg_k, conf_thr, sc.pacc,
+          sc.wacc, sc.fallbacks, sc.evaluated);
+    }
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   finalize_kernel<<<nblk, 256, 0, s>>>(sc.pacc, sc.wacc, out, g.nx, g.ny, g.nz);
