@@ -791,7 +791,7 @@ __device__ __forceinline__ void eval_offset4(const float *__restrict__ atl,
   }
 }
 
-__global__ void __launch_bounds__(kRescoreWarps * 32, 3)
+__global__ void __launch_bounds__(kRescoreWarps * 32, 4)
     rescore4_kernel(const RowProp *__restrict__ props, const float *__restrict__ img,
                     const float *__restrict__ atl, const float *__restrict__ lab, int nx, int ny,
                     int nz, int apitch, float scale, float conf_thr, float *__restrict__ pacc,
@@ -849,7 +849,7 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 3)
       bool take[kRows];
 #pragma unroll
       for (int r = 0; r < kRows; ++r) take[r] = valid[r];
-#pragma unroll 1
+#pragma unroll 2
       for (int c = 0; c < kTopK; ++c) {
         const int code = kRankTriples[c];
         eval_offset4(atl, lab, in, zrow0, axy, apitch, nx, x0, yc, pick4(top[0], code & 3) - 5,
