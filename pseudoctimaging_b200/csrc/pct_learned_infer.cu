@@ -40,12 +40,13 @@ constexpr float kDblEpsilonF = 2.220446049250313080847e-16f;
 
 // conv1 as an FP16 implicit GEMM: a CTA item is 4 x-rows x 32 y of one z plane (warp w = x-row w,
 // lane = y). Each thread writes its voxel's im2col row, K = 2 channels x 27 taps = 54 (padded to
-// 64) scaled inputs in FP16 (out-of-volume taps 0), into shared memory: 128 bytes per row, the
+// 64) raw intensities in FP16 (out-of-volume taps 0), into shared memory: 128 bytes per row, the
 // 16-byte chunk c of row r stored at chunk c ^ (r & 7) so that ldmatrix phases hit distinct banks.
 // Its warp then runs 2 m-tiles x 4 k-steps x 2 n-tiles of mma m16n8k16 (FP16 in, FP32
-// accumulate) against the BF16 weights widened to FP16 (exact), adds the bias, applies ReLU and
-// stores BF16 channel-last. The only rounding beyond the FP32 reference is the FP16 input
-// (relative 2^-11 of the scaled intensity).
+// accumulate) against the BF16 weights widened to FP16 (exact), applies the network's input
+// scale 1/512 to the FP32 sums (the layer is linear before its bias, so the scale moves there
+// from the 54 taps), adds the bias, applies ReLU and stores BF16 channel-last. The only rounding
+// beyond the FP32 reference is the FP16 input (relative 2^-11 of the intensity).
 constexpr int kC1Warps = 4;
 constexpr int kC1K = 64;
 
@@ -114,16 +115,16 @@ __global__ void __launch_bounds__(kC1Warps * 32)
 #pragma unroll
         for (int k = 0; k < 27; ++k) {
           const int dz = k / 9 - 1, dx = (k / 3) % 3 - 1, dy = k % 3 - 1;
-          v[k] = __ldg(pi + (dz * nxy + dx * ny + dy)) * kInScale;
-          v[27 + k] = __ldg(pa + (dz * axy + dx * apitch + dy)) * kInScale;
+          v[k] = __ldg(pi + (dz * nxy + dx * ny + dy));
+          v[27 + k] = __ldg(pa + (dz * axy + dx * apitch + dy));
         }
       } else {
 #pragma unroll
         for (int k = 0; k < 27; ++k) {
           const int zz = z + k / 9 - 1, xx = x + (k / 3) % 3 - 1, yy = y + k % 3 - 1;
           const bool ok = zz >= 0 && zz < nz && xx >= 0 && xx < nx && yy >= 0 && yy < ny;
-          v[k] = ok ? __ldg(img + (long long)zz * nxy + (long long)xx * ny + yy) * kInScale : 0.f;
-          v[27 + k] = ok ? __ldg(atl + ((long long)zz * nx + xx) * apitch + yy) * kInScale : 0.f;
+          v[k] = ok ? __ldg(img + (long long)zz * nxy + (long long)xx * ny + yy) : 0.f;
+          v[27 + k] = ok ? __ldg(atl + ((long long)zz * nx + xx) * apitch + yy) : 0.f;
         }
       }
 #pragma unroll
@@ -170,8 +171,8 @@ __global__ void __launch_bounds__(kC1Warps * 32)
           __nv_bfloat16 *dst = out + ((long long)z * nxy + (long long)x * ny + yy) * kC;
 #pragma unroll
           for (int j = 0; j < 2; ++j) {
-            const float v0 = fmaxf(acc[mt][j][2 * h] + bias[j][0], 0.f);
-            const float v1 = fmaxf(acc[mt][j][2 * h + 1] + bias[j][1], 0.f);
+            const float v0 = fmaxf(fmaf(acc[mt][j][2 * h], kInScale, bias[j][0]), 0.f);
+            const float v1 = fmaxf(fmaf(acc[mt][j][2 * h + 1], kInScale, bias[j][1]), 0.f);
             *reinterpret_cast<__nv_bfloat162 *>(dst + 8 * j + 2 * t) = __floats2bfloat162_rn(v0, v1);
           }
         }
