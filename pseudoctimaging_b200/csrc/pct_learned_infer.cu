@@ -38,17 +38,19 @@ constexpr float kDblEpsilonF = 2.220446049250313080847e-16f;
 
 // ---------------------------------------------------------------- conv1 (tensor cores)
 
-// conv1 as an FP16 implicit GEMM: a CTA item is 4 x-rows x 32 y of one z plane (warp w = x-row w,
-// lane = y). Each thread writes its voxel's im2col row, K = 2 channels x 27 taps = 54 (padded to
-// 64) raw intensities in FP16 (out-of-volume taps 0), into shared memory: 128 bytes per row, the
-// 16-byte chunk c of row r stored at chunk c ^ (r & 7) so that ldmatrix phases hit distinct banks.
-// Its warp then runs 2 m-tiles x 4 k-steps x 2 n-tiles of mma m16n8k16 (FP16 in, FP32
-// accumulate) against the BF16 weights widened to FP16 (exact), applies the network's input
-// scale 1/512 to the FP32 sums (the layer is linear before its bias, so the scale moves there
-// from the 54 taps), adds the bias, applies ReLU and stores BF16 channel-last. The only rounding
+// conv1 as an FP16 implicit GEMM, one input channel per launch: the input-MRI half of the
+// convolution is the same for every atlas, so it runs once per subject (CH = 0) into FP32 partial
+// sums, and each atlas adds its own half (CH = 1). A CTA item is 4 x-rows x 32 y of one z plane
+// (warp w = x-row w, lane = y). Each thread writes its voxel's im2col row of the channel, 27 raw
+// intensities in FP16 (padded to K = 32, out-of-volume taps 0), into shared memory: 64 bytes per
+// row, the 16-byte chunk c of row r stored at chunk c ^ ((r >> 1) & 3) so that ldmatrix phases
+// hit distinct banks. Its warp then runs 2 m-tiles x 2 k-steps x 2 n-tiles of mma m16n8k16
+// (FP16 in, FP32 accumulate) against the channel's BF16 weights widened to FP16 (exact). CH = 0
+// stores the FP32 sums; CH = 1 adds them, applies the network's input scale 1/512 (the layer is
+// linear before its bias), the bias and ReLU, and stores BF16 channel-last. The only rounding
 // beyond the FP32 reference is the FP16 input (relative 2^-11 of the intensity).
 constexpr int kC1Warps = 4;
-constexpr int kC1K = 64;
+constexpr int kC1K = 32;
 
 __device__ __forceinline__ void mma_f16_sync(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2,
                                              uint32_t a3, uint32_t b0, uint32_t b1) {
@@ -66,25 +68,27 @@ __device__ __forceinline__ void ldmatrix_x4_c1(uint32_t addr, uint32_t &r0, uint
                : "r"(addr));
 }
 
+template <int CH>
 __global__ void __launch_bounds__(kC1Warps * 32)
-    conv1_kernel(const float *__restrict__ img, const float *__restrict__ atl,
-                 const __nv_bfloat16 *__restrict__ wbf, __nv_bfloat16 *__restrict__ out, int nx,
-                 int ny, int nz, int apitch) {
+    conv1_kernel(const float *__restrict__ src, int spitch, const __nv_bfloat16 *__restrict__ wbf,
+                 float *__restrict__ part, __nv_bfloat16 *__restrict__ out, int nx, int ny,
+                 int nz) {
   __shared__ __align__(128) unsigned char rows[kC1Warps * 32 * kC1K * 2];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
-  // B fragments (k-step ks, n-tile j, register r): {W[co][k0], W[co][k0 + 1]} as FP16,
-  // co = 8j + g, k0 = 16ks + 8r + 2t; K index = ci * 27 + tap, zero past 54
-  uint32_t B[4][2][2];
+  // B fragments (k-step ks, n-tile j, register r): {W[co][CH][k0], W[co][CH][k0 + 1]} as FP16,
+  // co = 8j + g, k0 = 16ks + 8r + 2t (the tap index), zero past 27
+  uint32_t B[2][2][2];
 #pragma unroll
-  for (int ks = 0; ks < 4; ++ks)
+  for (int ks = 0; ks < 2; ++ks)
 #pragma unroll
     for (int j = 0; j < 2; ++j)
 #pragma unroll
       for (int r = 0; r < 2; ++r) {
         const int co = 8 * j + g, k0 = 16 * ks + 8 * r + 2 * t;
-        const float w0 = k0 < kCin * 27 ? __bfloat162float(wbf[kW1 + co * kCin * 27 + k0]) : 0.f;
-        const float w1 = k0 + 1 < kCin * 27 ? __bfloat162float(wbf[kW1 + co * kCin * 27 + k0 + 1]) : 0.f;
+        const int wb = kW1 + (co * kCin + CH) * 27;
+        const float w0 = k0 < 27 ? __bfloat162float(wbf[wb + k0]) : 0.f;
+        const float w1 = k0 + 1 < 27 ? __bfloat162float(wbf[wb + k0 + 1]) : 0.f;
         const __half2 h = __floats2half2_rn(w0, w1);
         B[ks][j][r] = *reinterpret_cast<const uint32_t *>(&h);
       }
@@ -99,36 +103,31 @@ __global__ void __launch_bounds__(kC1Warps * 32)
   const int ytiles = (ny + 31) / 32, xtiles = (nx + kC1Warps - 1) / kC1Warps;
   const long long items = (long long)nz * xtiles * ytiles;
   const int nxy = nx * ny;
+  const int sxy = nx * spitch;
   for (long long it = blockIdx.x; it < items; it += gridDim.x) {
     const int y0 = (int)(it % ytiles) * 32;
     const long long r0 = it / ytiles;
     const int x = (int)(r0 % xtiles) * kC1Warps + warp, z = (int)(r0 / xtiles);
     const int y = y0 + lane;
-    // this voxel's im2col row
+    // this voxel's im2col row of channel CH
     {
       float v[kC1K];
       if (z >= 1 && z < nz - 1 && x >= 1 && x < nx - 1 && y >= 1 && y < ny - 1) {
-        // every tap inside the volume: one base pointer per channel, 32-bit tap offsets
-        const float *pi = img + (long long)z * nxy + (long long)x * ny + y;
-        const float *pa = atl + ((long long)z * nx + x) * apitch + y;
-        const int axy = nx * apitch;
+        // every tap inside the volume: one base pointer, 32-bit tap offsets
+        const float *ps = src + ((long long)z * nx + x) * spitch + y;
 #pragma unroll
-        for (int k = 0; k < 27; ++k) {
-          const int dz = k / 9 - 1, dx = (k / 3) % 3 - 1, dy = k % 3 - 1;
-          v[k] = __ldg(pi + (dz * nxy + dx * ny + dy));
-          v[27 + k] = __ldg(pa + (dz * axy + dx * apitch + dy));
-        }
+        for (int k = 0; k < 27; ++k)
+          v[k] = __ldg(ps + ((k / 9 - 1) * sxy + ((k / 3) % 3 - 1) * spitch + (k % 3 - 1)));
       } else {
 #pragma unroll
         for (int k = 0; k < 27; ++k) {
           const int zz = z + k / 9 - 1, xx = x + (k / 3) % 3 - 1, yy = y + k % 3 - 1;
           const bool ok = zz >= 0 && zz < nz && xx >= 0 && xx < nx && yy >= 0 && yy < ny;
-          v[k] = ok ? __ldg(img + (long long)zz * nxy + (long long)xx * ny + yy) : 0.f;
-          v[27 + k] = ok ? __ldg(atl + ((long long)zz * nx + xx) * apitch + yy) : 0.f;
+          v[k] = ok ? __ldg(src + ((long long)zz * nx + xx) * spitch + yy) : 0.f;
         }
       }
 #pragma unroll
-      for (int k = kCin * 27; k < kC1K; ++k) v[k] = 0.f;
+      for (int k = 27; k < kC1K; ++k) v[k] = 0.f;
       unsigned char *row = rows + my_row * kC1K * 2;
 #pragma unroll
       for (int c = 0; c < kC1K / 8; ++c) {
@@ -138,7 +137,8 @@ __global__ void __launch_bounds__(kC1Warps * 32)
           const __half2 h = __floats2half2_rn(v[8 * c + 2 * e], v[8 * c + 2 * e + 1]);
           w[e] = *reinterpret_cast<const uint32_t *>(&h);
         }
-        *reinterpret_cast<uint4 *>(row + ((c ^ (my_row & 7)) << 4)) = make_uint4(w[0], w[1], w[2], w[3]);
+        *reinterpret_cast<uint4 *>(row + ((c ^ ((my_row >> 1) & 3)) << 4)) =
+            make_uint4(w[0], w[1], w[2], w[3]);
       }
     }
     __syncwarp();
@@ -152,11 +152,12 @@ __global__ void __launch_bounds__(kC1Warps * 32)
 #pragma unroll
     for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
-      for (int ks = 0; ks < 4; ++ks) {
+      for (int ks = 0; ks < 2; ++ks) {
         const int r = warp * 32 + mt * 16 + q + 8 * (m & 1);
         const int c = 2 * ks + (m >> 1);
         uint32_t a0, a1, a2, a3;
-        ldmatrix_x4_c1(rows_u32 + (uint32_t)(r * kC1K * 2 + ((c ^ (r & 7)) << 4)), a0, a1, a2, a3);
+        ldmatrix_x4_c1(rows_u32 + (uint32_t)(r * kC1K * 2 + ((c ^ ((r >> 1) & 3)) << 4)), a0, a1,
+                       a2, a3);
 #pragma unroll
         for (int j = 0; j < 2; ++j) mma_f16_sync(acc[mt][j], a0, a1, a2, a3, B[ks][j][0], B[ks][j][1]);
       }
@@ -168,12 +169,20 @@ __global__ void __launch_bounds__(kC1Warps * 32)
         for (int h = 0; h < 2; ++h) {
           const int yy = y0 + mt * 16 + g + 8 * h;
           if (yy >= ny) continue;
-          __nv_bfloat16 *dst = out + ((long long)z * nxy + (long long)x * ny + yy) * kC;
+          const long long v = (long long)z * nxy + (long long)x * ny + yy;
 #pragma unroll
           for (int j = 0; j < 2; ++j) {
-            const float v0 = fmaxf(fmaf(acc[mt][j][2 * h], kInScale, bias[j][0]), 0.f);
-            const float v1 = fmaxf(fmaf(acc[mt][j][2 * h + 1], kInScale, bias[j][1]), 0.f);
-            *reinterpret_cast<__nv_bfloat162 *>(dst + 8 * j + 2 * t) = __floats2bfloat162_rn(v0, v1);
+            float2 *pp = reinterpret_cast<float2 *>(part + v * kC + 8 * j + 2 * t);
+            if (CH == 0) {
+              *pp = make_float2(acc[mt][j][2 * h], acc[mt][j][2 * h + 1]);
+            } else {
+              const float2 pi = *pp;
+              const float v0 = fmaxf(fmaf(acc[mt][j][2 * h] + pi.x, kInScale, bias[j][0]), 0.f);
+              const float v1 =
+                  fmaxf(fmaf(acc[mt][j][2 * h + 1] + pi.y, kInScale, bias[j][1]), 0.f);
+              *reinterpret_cast<__nv_bfloat162 *>(out + v * kC + 8 * j + 2 * t) =
+                  __floats2bfloat162_rn(v0, v1);
+            }
           }
         }
     }
@@ -936,13 +945,15 @@ struct InferScratch {
   unsigned long long *fallbacks;  // (voxel, atlas) pairs that took the full search
   unsigned long long *evaluated;  // offsets evaluated by warp rows, summed over rows
   int *err;                       // bounded-wait status of the probe hook
+  float *cimg;                    // conv1's input-MRI half, FP32 [nvox][16]
   RowProp *props;                 // row-segment proposals of the block anchor rows
   int *zlists;                    // conv2, conv3, conv4 output planes, nz entries each
 };
 
 // Bytes before the proposal table (features, sums, fragments, counters), 256-aligned.
 size_t infer_base_bytes(long long nvox) {
-  const size_t b = (size_t)nvox * kC * 2 * 2 + (size_t)nvox * 4 * 2 + 3 * kFragWords * 4 + 256;
+  const size_t b = (size_t)nvox * kC * 2 * 2 + (size_t)nvox * 4 * 2 + 3 * kFragWords * 4 + 256 +
+                   (size_t)nvox * kC * 4;
   return (b + 255) / 256 * 256;
 }
 
@@ -957,6 +968,7 @@ InferScratch carve(void *scratch, long long nvox) {
   r.fallbacks = reinterpret_cast<unsigned long long *>(r.frag + 3 * kFragWords);
   r.evaluated = r.fallbacks + 1;
   r.err = reinterpret_cast<int *>(r.fallbacks + 2);
+  r.cimg = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(r.fallbacks) + 256);
   r.props = reinterpret_cast<RowProp *>(static_cast<unsigned char *>(scratch) +
                                         infer_base_bytes(nvox));
   r.zlists = nullptr;  // placed by carve_tables, which knows the geometry
@@ -996,17 +1008,27 @@ cudaError_t make_feature_map(CUtensorMap *map, const __nv_bfloat16 *base, const 
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
-// conv1 .. conv4 of one (input, atlas) pair; returns the buffer holding the conv4 features.
-cudaError_t run_convs(const Geometry &g, const __nv_bfloat16 *wbf, const float *img,
-                      const float *atlas_a, int apitch, const InferScratch &sc, int *err,
-                      const int (&planes)[3], __nv_bfloat16 **features, cudaStream_t s) {
+int conv1_blocks(const Geometry &g) {
+  const long long items = (long long)g.nz * ((g.nx + kC1Warps - 1) / kC1Warps) * ((g.ny + 31) / 32);
+  return (int)(items < 16LL * sms() ? items : 16LL * sms());
+}
+
+// conv1's input-MRI half (FP32 sums, before scale and bias), shared by every atlas of the subject.
+cudaError_t run_conv1_img(const Geometry &g, const __nv_bfloat16 *wbf, const float *img,
+                          const InferScratch &sc, cudaStream_t s) {
+  conv1_kernel<0><<<conv1_blocks(g), kC1Warps * 32, 0, s>>>(img, g.ny, wbf, sc.cimg, nullptr,
+                                                             g.nx, g.ny, g.nz);
+  return cudaGetLastError();
+}
+
+// conv1 (atlas half + the shared input half) .. conv4 of one atlas; returns the buffer holding
+// the conv4 features.
+cudaError_t run_convs(const Geometry &g, const __nv_bfloat16 *wbf, const float *atlas_a,
+                      int apitch, const InferScratch &sc, int *err, const int (&planes)[3],
+                      __nv_bfloat16 **features, cudaStream_t s) {
   const int n_sm = sms();
-  {
-    const long long items = (long long)g.nz * ((g.nx + kC1Warps - 1) / kC1Warps) * ((g.ny + 31) / 32);
-    const int blocks = (int)(items < 16LL * n_sm ? items : 16LL * n_sm);
-    conv1_kernel<<<blocks, kC1Warps * 32, 0, s>>>(img, atlas_a, wbf, sc.fa, g.nx, g.ny, g.nz,
-                                                  apitch);
-  }
+  conv1_kernel<1><<<conv1_blocks(g), kC1Warps * 32, 0, s>>>(atlas_a, apitch, wbf, sc.cimg, sc.fa,
+                                                             g.nx, g.ny, g.nz);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   CUtensorMap maps[2];
@@ -1090,6 +1112,7 @@ cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInp
   if ((e = cudaMemsetAsync(sc.fallbacks, 0, 2 * sizeof(unsigned long long), s)) != cudaSuccess)
     return e;
   if ((e = pack_all(wbf, sc.frag, s)) != cudaSuccess) return e;
+  if ((e = run_conv1_img(g, wbf, in.img, sc, s)) != cudaSuccess) return e;
   const float neg_k = (float)(-1.4426950408889634 / div);
   const float scale = (float)sqrt(1.4426950408889634 / div);
   const int nblk = sms() * 8;
@@ -1107,7 +1130,7 @@ cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInp
   for (int a = 0; a < g.num; ++a) {
     const float *A = in.atlas + a * astride, *L = in.label + a * astride;
     __nv_bfloat16 *f4 = nullptr;
-    if ((e = run_convs(g, wbf, in.img, A, in.pitch, sc, err, planes, &f4, s)) != cudaSuccess)
+    if ((e = run_convs(g, wbf, A, in.pitch, sc, err, planes, &f4, s)) != cudaSuccess)
       return e;
     propose_rows_kernel<<<propose_blocks, kRescoreWarps * 32, 0, s>>>(f4, wbf, g.nx, g.ny, g.nz,
                                                                       block, sc.props);
@@ -1138,7 +1161,8 @@ cudaError_t learned_probe(const Geometry &g, const void *weights, const float *i
   __nv_bfloat16 *f4 = nullptr;
   if ((e = cudaMemsetAsync(sc.err, 0, sizeof(int), s)) != cudaSuccess) return e;
   const int planes[3] = {g.nz, g.nz, g.nz};
-  if ((e = run_convs(g, wbf, img, atlas_a, g.ny, sc, sc.err, planes, &f4, s)) != cudaSuccess)
+  if ((e = run_conv1_img(g, wbf, img, sc, s)) != cudaSuccess) return e;
+  if ((e = run_convs(g, wbf, atlas_a, g.ny, sc, sc.err, planes, &f4, s)) != cudaSuccess)
     return e;
   // the sums area is free here: voxel list, proposals and confidences go there
   int64_t *d_vox = reinterpret_cast<int64_t *>(sc.pacc);
