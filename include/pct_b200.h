@@ -250,12 +250,18 @@ int pct_model_train(pct_model *m, pct_train_set *ts, int batch, int steps, float
 int pct_attach_model(pct_handle *h, pct_model *m, float conf_threshold);
 /* Proposal sharing (default 4): row segments share the proposal of their block's anchor row,
  * blocks of `block` x `block` rows in (z, x) anchored at their middle row; the network's heads
- * and the proposal run only on anchor rows (its last two convolutions only on the z-planes
- * those need), and a voxel's confidence is that of the anchor-row voxel at the same y. 1 = every
+ * and the proposal run only on anchor rows (each convolution only on the rows, planes and y its
+ * successors need for them), and a voxel's confidence is that of the anchor-row voxel at the
+ * same y. 1 = every
  * row segment proposes for itself. Blocks start at the volume's first interior plane and row, so
  * z-slab shards reproduce the whole volume's result when their boundaries are multiples of
  * `block` interior planes apart. */
 int pct_set_learned_block(pct_handle *h, int block);
+/* Diagnostic (default 0): 1 = the learned form's convolutions compute every voxel of the volume
+ * instead of only the outputs the anchor rows need (conv4 on the anchor rows, conv(4 - r) within
+ * r rows and planes of them, interior y widened by r). The result is bit-identical; this is the
+ * check of the restricted plan. No counterpart in the reference. */
+int pct_set_learned_convs(pct_handle *h, int every_voxel);
 
 /*
  * Tensor-core form (EXEC_CHOICE 5 = FP16, 6 = BF16; NH = 11) runs through pct_synthesize /

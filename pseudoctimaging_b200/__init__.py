@@ -149,6 +149,7 @@ SIGNATURES = {
     "pct_model_train": (_I, [_P, _P, _I, _I, ctypes.c_float, ctypes.POINTER(ctypes.c_float)]),
     "pct_attach_model": (_I, [_P, _P, ctypes.c_float]),
     "pct_set_learned_block": (_I, [_P, _I]),
+    "pct_set_learned_convs": (_I, [_P, _I]),
     "pct_tc_survivors": (_I, [_P, _I, _P, _P, _P, _P, _I, _I, _I, _D, _P, _P]),
     "pct_learned_stats": (_I, [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
     "pct_model_probe": (_I, [_P, _P, _P, _I, _I, _I, _P, _I, _P, _P, _P]),
@@ -258,6 +259,12 @@ class Handle:
         """Rows per proposal block along z and x for EXEC_LEARNED (default 4; 1 = per row
         segment)."""
         self._check(lib.pct_set_learned_block(self._h, int(block)), "pct_set_learned_block")
+
+    def set_learned_convs(self, every_voxel: bool) -> None:
+        """Diagnostic: True = EXEC_LEARNED's convolutions over every voxel instead of only the
+        outputs the anchor rows need (bit-identical result)."""
+        self._check(lib.pct_set_learned_convs(self._h, int(bool(every_voxel))),
+                    "pct_set_learned_convs")
 
     def attach_model(self, model, conf_threshold: float = 0.0) -> None:
         """Makes EXEC_LEARNED available (NH = 11) with a :class:`learned.LearnedModel` (None

@@ -38,6 +38,7 @@ struct pct_handle {
   pct_model *model = nullptr;           // learned form (EXEC_CHOICE 7), see pct_attach_model
   float learned_conf = 0.f;             // its full-search fallback threshold
   int learned_block = 4;                // rows per proposal block along z and x
+  bool learned_every_voxel = false;     // convolutions over the whole volume (diagnostic)
   DevBuf learned;                       // its feature volumes and sums
   long long learned_nvox = 0;           // volume size of the last learned run (0: none yet)
   cudaStream_t learned_stream = nullptr;
@@ -166,8 +167,8 @@ int launch_learned_path(pct_handle *h, const pct::Geometry &g, const pct::SlabIn
   int *err = static_cast<int *>(h->err.ptr);
   PCT_CUDA(h, cudaMemsetAsync(err, 0, sizeof(int), s));
   PCT_CUDA(h, pct::learned::launch_learned(g, pct::learned::model_weights(h->model), in, d_out, div,
-                                           h->learned_conf, h->learned_block, h->learned.ptr, err,
-                                           s));
+                                           h->learned_conf, h->learned_block,
+                                           h->learned_every_voxel, h->learned.ptr, err, s));
   h->learned_nvox = g.nvox();
   h->learned_stream = s;
   return PCT_OK;
@@ -536,6 +537,14 @@ int pct_set_learned_block(pct_handle *h, int block) {
   if (block < 1 || block > 16)
     return fail(h, PCT_ERR_INVALID_ARG, "learned proposal block must be 1..16 rows");
   h->learned_block = block;
+  return PCT_OK;
+}
+
+int pct_set_learned_convs(pct_handle *h, int every_voxel) {
+  if (!h) return PCT_ERR_INVALID_ARG;
+  if (every_voxel != 0 && every_voxel != 1)
+    return fail(h, PCT_ERR_INVALID_ARG, "every_voxel must be 0 or 1");
+  h->learned_every_voxel = every_voxel == 1;
   return PCT_OK;
 }
 

@@ -48,7 +48,8 @@ constexpr float kDblEpsilonF = 2.220446049250313080847e-16f;
 // (FP16 in, FP32 accumulate) against the channel's BF16 weights widened to FP16 (exact). CH = 0
 // stores the FP32 sums; CH = 1 adds them, applies the network's input scale 1/512 (the layer is
 // linear before its bias), the bias and ReLU, and stores BF16 channel-last. The only rounding
-// beyond the FP32 reference is the FP16 input (relative 2^-11 of the intensity).
+// beyond the FP32 reference is the FP16 input (relative 2^-11 of the intensity). Only the output
+// box z in [z_lo, z_lo + z_n), x in [x_lo, x_lo + x_n) (every y) is computed.
 constexpr int kC1Warps = 4;
 constexpr int kC1K = 32;
 
@@ -72,7 +73,7 @@ template <int CH>
 __global__ void __launch_bounds__(kC1Warps * 32)
     conv1_kernel(const float *__restrict__ src, int spitch, const __nv_bfloat16 *__restrict__ wbf,
                  float *__restrict__ part, __nv_bfloat16 *__restrict__ out, int nx, int ny,
-                 int nz) {
+                 int nz, int z_lo, int z_n, int x_lo, int x_n) {
   __shared__ __align__(128) unsigned char rows[kC1Warps * 32 * kC1K * 2];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
@@ -100,14 +101,15 @@ __global__ void __launch_bounds__(kC1Warps * 32)
   const uint32_t rows_u32 = static_cast<uint32_t>(__cvta_generic_to_shared(rows));
   const int my_row = tid;
   const int m = lane >> 3, q = lane & 7;
-  const int ytiles = (ny + 31) / 32, xtiles = (nx + kC1Warps - 1) / kC1Warps;
-  const long long items = (long long)nz * xtiles * ytiles;
+  const int ytiles = (ny + 31) / 32, xtiles = (x_n + kC1Warps - 1) / kC1Warps;
+  const long long items = (long long)z_n * xtiles * ytiles;
   const int nxy = nx * ny;
   const int sxy = nx * spitch;
+  const int x_hi = x_lo + x_n;
   for (long long it = blockIdx.x; it < items; it += gridDim.x) {
     const int y0 = (int)(it % ytiles) * 32;
     const long long r0 = it / ytiles;
-    const int x = (int)(r0 % xtiles) * kC1Warps + warp, z = (int)(r0 / xtiles);
+    const int x = x_lo + (int)(r0 % xtiles) * kC1Warps + warp, z = z_lo + (int)(r0 / xtiles);
     const int y = y0 + lane;
     // this voxel's im2col row of channel CH
     {
@@ -162,7 +164,7 @@ __global__ void __launch_bounds__(kC1Warps * 32)
         for (int j = 0; j < 2; ++j) mma_f16_sync(acc[mt][j], a0, a1, a2, a3, B[ks][j][0], B[ks][j][1]);
       }
     __syncwarp();  // the rows are rewritten by the next item
-    if (x < nx) {
+    if (x < x_hi) {
 #pragma unroll
       for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
@@ -238,29 +240,45 @@ __device__ __forceinline__ void mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1
       : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
+// The output region of one layer: tiles_y tiles of 64 y from y_lo (warps whose 16-y segment
+// starts at or past y_hi skip their work), x tiles of 4 rows, z planes.
 struct ConvGrid {
   int nx, ny, nz, tiles_y, tiles_x, tiles;
+  int y_lo, y_hi;
   const int *zlist;  // the output z-planes to compute (NULL: every plane)
+  const int *xlist;  // x tiles: first row | (mask of the 4 rows to compute) << 16 (NULL: 4i, all)
 };
 
 __device__ __forceinline__ void conv_tile_origin(const ConvGrid &g, int tile, int &z, int &x0,
-                                                 int &y0) {
+                                                 int &y0, unsigned &mask) {
   const int ty = tile % g.tiles_y;
   const int r = tile / g.tiles_y;
-  x0 = (r % g.tiles_x) * kCvTX;
-  z = g.zlist ? g.zlist[r / g.tiles_x] : r / g.tiles_x;
-  y0 = ty * kCvTY;
+  const int xi = r % g.tiles_x, zi = r / g.tiles_x;
+  z = g.zlist ? g.zlist[zi] : zi;
+  if (g.xlist) {
+    const int e = g.xlist[xi];
+    x0 = e & 0xFFFF;
+    mask = (unsigned)e >> 16;
+  } else {
+    x0 = xi * kCvTX;
+    mask = 0xFu;
+  }
+  y0 = g.y_lo + ty * kCvTY;
 }
 
 __device__ __forceinline__ void conv_issue(const CUtensorMap *tm, uint32_t buf, uint32_t bar,
                                            const ConvGrid &g, int tile) {
   int z, x0, y0;
-  conv_tile_origin(g, tile, z, x0, y0);
+  unsigned mask;
+  conv_tile_origin(g, tile, z, x0, y0, mask);
   ptx::fence_proxy_async_smem();
   ptx::mbar_arrive_expect_tx(bar, kCvBoxBytes);
   ptx::tma_load_4d(buf, tm, bar, 0, y0 - 1, x0 - 1, z - 1);
 }
 
+// ROWMASK: tiles carry a mask of the x-rows to compute (rows outside it cost no mma; input rows
+// no masked-in output row uses are not loaded into registers).
+template <bool ROWMASK>
 __global__ void __launch_bounds__(kCvThreads, 2)
     conv16_kernel(const __grid_constant__ CUtensorMap tm, const uint32_t *__restrict__ frag,
                   const __nv_bfloat16 *__restrict__ wbf, int boff, __nv_bfloat16 *__restrict__ out,
@@ -315,50 +333,58 @@ __global__ void __launch_bounds__(kCvThreads, 2)
       }
       return;
     }
-    float acc[kCvTX][2][4];
+    int z, x0, y0;
+    unsigned mask;
+    conv_tile_origin(g, tile, z, x0, y0, mask);
+    if (y0 + ys < g.y_hi) {
+      float acc[kCvTX][2][4];
 #pragma unroll
-    for (int o = 0; o < kCvTX; ++o)
+      for (int o = 0; o < kCvTX; ++o)
 #pragma unroll
-      for (int j = 0; j < 2; ++j)
+        for (int j = 0; j < 2; ++j)
 #pragma unroll
-        for (int e = 0; e < 4; ++e) acc[o][j][e] = 0.f;
+          for (int e = 0; e < 4; ++e) acc[o][j][e] = 0.f;
 #pragma unroll
-    for (int iz = 0; iz < 3; ++iz) {
+      for (int iz = 0; iz < 3; ++iz) {
 #pragma unroll
-      for (int ix = 0; ix < kCvSX; ++ix) {
+        for (int ix = 0; ix < kCvSX; ++ix) {
+          // output rows o with ix - o in [0, 2]
+          const unsigned users = ix >= 2 ? (0x7u << (ix - 2)) & 0xFu : 0x7u >> (2 - ix);
+          if (ROWMASK && !(mask & users)) continue;
 #pragma unroll
-        for (int ky = 0; ky < 3; ++ky) {
-          const int sv = (iz * kCvSX + ix) * kCvSY + ys + arow + ky;
-          uint32_t a0, a1, a2, a3;
-          ldmatrix_x4(buf + (uint32_t)(sv * 32 + ((ahalf ^ ((sv >> 2) & 1)) << 4)), a0, a1, a2,
-                      a3);
+          for (int ky = 0; ky < 3; ++ky) {
+            const int sv = (iz * kCvSX + ix) * kCvSY + ys + arow + ky;
+            uint32_t a0, a1, a2, a3;
+            ldmatrix_x4(buf + (uint32_t)(sv * 32 + ((ahalf ^ ((sv >> 2) & 1)) << 4)), a0, a1, a2,
+                        a3);
 #pragma unroll
-          for (int o = 0; o < kCvTX; ++o) {
-            const int kx = ix - o;
-            if (kx < 0 || kx > 2) continue;
-            const int t = iz * 9 + kx * 3 + ky;
-            mma_bf16(acc[o][0], a0, a1, a2, a3, B[t][0][0], B[t][0][1]);
-            mma_bf16(acc[o][1], a0, a1, a2, a3, B[t][1][0], B[t][1][1]);
+            for (int o = 0; o < kCvTX; ++o) {
+              const int kx = ix - o;
+              if (kx < 0 || kx > 2) continue;
+              if (ROWMASK && !((mask >> o) & 1u)) continue;
+              const int t = iz * 9 + kx * 3 + ky;
+              mma_bf16(acc[o][0], a0, a1, a2, a3, B[t][0][0], B[t][0][1]);
+              mma_bf16(acc[o][1], a0, a1, a2, a3, B[t][1][0], B[t][1][1]);
+            }
           }
         }
       }
-    }
-    int z, x0, y0;
-    conv_tile_origin(g, tile, z, x0, y0);
 #pragma unroll
-    for (int o = 0; o < kCvTX; ++o) {
-      const int x = x0 + o;
-      if (x >= g.nx) break;
+      for (int o = 0; o < kCvTX; ++o) {
+        if (ROWMASK && !((mask >> o) & 1u)) continue;
+        const int x = x0 + o;
+        if (x >= g.nx) break;
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int y = y0 + ys + g8 + 8 * h;
-        if (y >= g.ny) continue;
-        __nv_bfloat16 *dst = out + (((long long)z * g.nx + x) * g.ny + y) * kC;
+        for (int h = 0; h < 2; ++h) {
+          const int y = y0 + ys + g8 + 8 * h;
+          if (y >= g.y_hi) continue;
+          __nv_bfloat16 *dst = out + (((long long)z * g.nx + x) * g.ny + y) * kC;
 #pragma unroll
-        for (int j = 0; j < 2; ++j) {
-          const float v0 = fmaxf(acc[o][j][2 * h] + bias[j][0], 0.f);
-          const float v1 = fmaxf(acc[o][j][2 * h + 1] + bias[j][1], 0.f);
-          *reinterpret_cast<__nv_bfloat162 *>(dst + 8 * j + c2) = __floats2bfloat162_rn(v0, v1);
+          for (int j = 0; j < 2; ++j) {
+            const float v0 = fmaxf(acc[o][j][2 * h] + bias[j][0], 0.f);
+            const float v1 = fmaxf(acc[o][j][2 * h + 1] + bias[j][1], 0.f);
+            *reinterpret_cast<__nv_bfloat162 *>(dst + 8 * j + c2) = __floats2bfloat162_rn(v0, v1);
+          }
         }
       }
     }
@@ -947,7 +973,8 @@ struct InferScratch {
   int *err;                       // bounded-wait status of the probe hook
   float *cimg;                    // conv1's input-MRI half, FP32 [nvox][16]
   RowProp *props;                 // row-segment proposals of the block anchor rows
-  int *zlists;                    // conv2, conv3, conv4 output planes, nz entries each
+  int *zlists;                    // conv2, conv3, conv4 output planes, nz entries each, then
+                                  // their x tiles, nx entries each
 };
 
 // Bytes before the proposal table (features, sums, fragments, counters), 256-aligned.
@@ -983,7 +1010,8 @@ size_t prop_table_bytes(const Geometry &g) {
 }
 
 size_t infer_scratch_bytes(const Geometry &g) {
-  return infer_base_bytes(g.nvox()) + prop_table_bytes(g) + 3 * (size_t)g.nz * sizeof(int) + 256;
+  return infer_base_bytes(g.nvox()) + prop_table_bytes(g) +
+         3 * ((size_t)g.nz + g.nx) * sizeof(int) + 256;
 }
 
 unsigned long long *infer_counters(void *scratch, long long nvox) {
@@ -1008,27 +1036,108 @@ cudaError_t make_feature_map(CUtensorMap *map, const __nv_bfloat16 *base, const 
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
-int conv1_blocks(const Geometry &g) {
-  const long long items = (long long)g.nz * ((g.nx + kC1Warps - 1) / kC1Warps) * ((g.ny + 31) / 32);
+// What each convolution must produce. The proposals read conv4 features on the anchor rows
+// (z, x) of the row blocks, at the interior y; layer conv(4 - r) is needed r voxels around them.
+// Every needed output's receptive field lies inside the volume (interior margin 6 > 4 layers), so
+// the zero padding of the volume edge never reaches a needed value and skipped outputs are never
+// read. Dense plans (no lists) compute every voxel.
+struct ConvPlan {
+  int c1_z, c1_nz, c1_x, c1_nx;  // conv1 box (z, x; every y)
+  int nzl[3], nxl[3];            // conv2..conv4: z planes and x tiles in the lists
+  int y_lo[3], y_hi[3];
+  bool rowmask[3];               // some x tile computes fewer than its 4 rows
+  bool dense;
+};
+
+ConvPlan dense_plan(const Geometry &g) {
+  ConvPlan p{};
+  p.c1_nz = g.nz;
+  p.c1_nx = g.nx;
+  for (int l = 0; l < 3; ++l) {
+    p.nzl[l] = g.nz;
+    p.nxl[l] = (g.nx + kCvTX - 1) / kCvTX;
+    p.y_hi[l] = g.ny;
+  }
+  p.dense = true;
+  return p;
+}
+
+// Anchor rows of blocks of `block` rows along an axis with `extent` interior rows from row 6.
+std::vector<int> anchors(int extent, int block) {
+  std::vector<int> a;
+  for (int b = 0; b * block < extent; ++b) a.push_back(6 + anchor_of_host(b, block, extent));
+  return a;
+}
+
+// The rows within `radius` of an anchor, in order.
+std::vector<int> rows_near(const std::vector<int> &anc, int radius, int n) {
+  std::vector<char> need(n, 0);
+  for (int a : anc)
+    for (int d = -radius; d <= radius; ++d)
+      if (a + d >= 0 && a + d < n) need[a + d] = 1;
+  std::vector<int> r;
+  for (int i = 0; i < n; ++i)
+    if (need[i]) r.push_back(i);
+  return r;
+}
+
+// Sparse plan for row blocks of `block`; `lists` receives 3 nz z-plane entries then 3 nx x-tile
+// entries (first row | row mask << 16), greedy 4-row tiles starting at the first uncovered row.
+ConvPlan sparse_plan(const Geometry &g, int block, std::vector<int> &lists) {
+  ConvPlan p{};
+  lists.assign(3 * ((size_t)g.nz + g.nx), 0);
+  const int iz = g.nz - 12, ix = g.nx - 12, iy = g.ny - 12;
+  if (iz <= 0 || ix <= 0 || iy <= 0) return p;  // no interior: nothing to compute
+  const std::vector<int> az = anchors(iz, block), ax = anchors(ix, block);
+  p.c1_z = az.front() - 3;
+  p.c1_nz = az.back() + 4 - p.c1_z;
+  p.c1_x = ax.front() - 3;
+  p.c1_nx = ax.back() + 4 - p.c1_x;
+  for (int l = 0; l < 3; ++l) {
+    const int radius = 2 - l;
+    const std::vector<int> zs = rows_near(az, radius, g.nz), xs = rows_near(ax, radius, g.nx);
+    p.nzl[l] = (int)zs.size();
+    for (size_t i = 0; i < zs.size(); ++i) lists[(size_t)l * g.nz + i] = zs[i];
+    int nt = 0;
+    for (size_t i = 0; i < xs.size();) {
+      const int x0 = xs[i];
+      unsigned mask = 0;
+      while (i < xs.size() && xs[i] < x0 + kCvTX) mask |= 1u << (xs[i++] - x0);
+      if (mask != 0xFu) p.rowmask[l] = true;
+      lists[3 * (size_t)g.nz + (size_t)l * g.nx + nt++] = x0 | (int)(mask << 16);
+    }
+    p.nxl[l] = nt;
+    p.y_lo[l] = 6 - radius;
+    p.y_hi[l] = g.ny - 6 + radius;
+  }
+  return p;
+}
+
+int conv1_blocks(const ConvPlan &p, int ny) {
+  const long long items =
+      (long long)p.c1_nz * ((p.c1_nx + kC1Warps - 1) / kC1Warps) * ((ny + 31) / 32);
   return (int)(items < 16LL * sms() ? items : 16LL * sms());
 }
 
 // conv1's input-MRI half (FP32 sums, before scale and bias), shared by every atlas of the subject.
 cudaError_t run_conv1_img(const Geometry &g, const __nv_bfloat16 *wbf, const float *img,
-                          const InferScratch &sc, cudaStream_t s) {
-  conv1_kernel<0><<<conv1_blocks(g), kC1Warps * 32, 0, s>>>(img, g.ny, wbf, sc.cimg, nullptr,
-                                                             g.nx, g.ny, g.nz);
+                          const ConvPlan &p, const InferScratch &sc, cudaStream_t s) {
+  if (p.c1_nz <= 0 || p.c1_nx <= 0) return cudaSuccess;
+  conv1_kernel<0><<<conv1_blocks(p, g.ny), kC1Warps * 32, 0, s>>>(
+      img, g.ny, wbf, sc.cimg, nullptr, g.nx, g.ny, g.nz, p.c1_z, p.c1_nz, p.c1_x, p.c1_nx);
   return cudaGetLastError();
 }
 
 // conv1 (atlas half + the shared input half) .. conv4 of one atlas; returns the buffer holding
 // the conv4 features.
 cudaError_t run_convs(const Geometry &g, const __nv_bfloat16 *wbf, const float *atlas_a,
-                      int apitch, const InferScratch &sc, int *err, const int (&planes)[3],
+                      int apitch, const InferScratch &sc, int *err, const ConvPlan &p,
                       __nv_bfloat16 **features, cudaStream_t s) {
   const int n_sm = sms();
-  conv1_kernel<1><<<conv1_blocks(g), kC1Warps * 32, 0, s>>>(atlas_a, apitch, wbf, sc.cimg, sc.fa,
-                                                             g.nx, g.ny, g.nz);
+  *features = sc.fb;  // conv2 -> fb, conv3 -> fa, conv4 -> fb
+  if (p.c1_nz <= 0 || p.c1_nx <= 0) return cudaSuccess;
+  conv1_kernel<1><<<conv1_blocks(p, g.ny), kC1Warps * 32, 0, s>>>(
+      atlas_a, apitch, wbf, sc.cimg, sc.fa, g.nx, g.ny, g.nz, p.c1_z, p.c1_nz, p.c1_x, p.c1_nx);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   CUtensorMap maps[2];
@@ -1038,28 +1147,35 @@ cudaError_t run_convs(const Geometry &g, const __nv_bfloat16 *wbf, const float *
   cg.nx = g.nx;
   cg.ny = g.ny;
   cg.nz = g.nz;
-  cg.tiles_y = (g.ny + kCvTY - 1) / kCvTY;
-  cg.tiles_x = (g.nx + kCvTX - 1) / kCvTX;
   const int boffs[3] = {kB2, kB3, kB4};
   __nv_bfloat16 *bufs[2] = {sc.fa, sc.fb};
   for (int l = 0; l < 3; ++l) {
-    // planes[l] < nz: only the listed output planes of layer l are needed
-    const bool all = planes[l] >= g.nz;
-    cg.zlist = all ? nullptr : sc.zlists + l * g.nz;
-    cg.tiles = cg.tiles_y * cg.tiles_x * (all ? g.nz : planes[l]);
-    if (cg.tiles == 0) continue;
+    cg.zlist = p.dense ? nullptr : sc.zlists + l * g.nz;
+    cg.xlist = p.dense ? nullptr : sc.zlists + 3 * g.nz + l * g.nx;
+    cg.y_lo = p.y_lo[l];
+    cg.y_hi = p.y_hi[l];
+    cg.tiles_y = (p.y_hi[l] - p.y_lo[l] + kCvTY - 1) / kCvTY;
+    cg.tiles_x = p.nxl[l];
+    cg.tiles = cg.tiles_y * cg.tiles_x * p.nzl[l];
+    if (cg.tiles <= 0) continue;
     const int blocks = cg.tiles < 2 * n_sm ? cg.tiles : 2 * n_sm;
-    conv16_kernel<<<blocks, kCvThreads, kConvSmem, s>>>(maps[l & 1], sc.frag + l * kFragWords, wbf,
-                                                        boffs[l], bufs[(l + 1) & 1], cg, err);
+    if (p.rowmask[l])
+      conv16_kernel<true><<<blocks, kCvThreads, kConvSmem, s>>>(
+          maps[l & 1], sc.frag + l * kFragWords, wbf, boffs[l], bufs[(l + 1) & 1], cg, err);
+    else
+      conv16_kernel<false><<<blocks, kCvThreads, kConvSmem, s>>>(
+          maps[l & 1], sc.frag + l * kFragWords, wbf, boffs[l], bufs[(l + 1) & 1], cg, err);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
-  *features = bufs[1];  // conv2 -> fb, conv3 -> fa, conv4 -> fb
   return cudaSuccess;
 }
 
 cudaError_t pack_all(const __nv_bfloat16 *wbf, uint32_t *frag, cudaStream_t s) {
-  cudaError_t e0 = cudaFuncSetAttribute(conv16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)kConvSmem);
+  cudaError_t e0 = cudaFuncSetAttribute(conv16_kernel<false>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kConvSmem);
+  if (e0 != cudaSuccess) return e0;
+  e0 = cudaFuncSetAttribute(conv16_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)kConvSmem);
   if (e0 != cudaSuccess) return e0;
   const int woffs[3] = {kW2, kW3, kW4};
   for (int l = 0; l < 3; ++l) {
@@ -1075,8 +1191,8 @@ cudaError_t pack_all(const __nv_bfloat16 *wbf, uint32_t *frag, cudaStream_t s) {
 // The learned form over all atlases of `in` (atlas and label rows `in.pitch` floats apart, the
 // input MRI contiguous). Writes the interior of `out`; the border is left untouched.
 cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInputs &in, float *out,
-                           double div, float conf_thr, int block, void *scratch, int *err,
-                           cudaStream_t s) {
+                           double div, float conf_thr, int block, bool every_voxel, void *scratch,
+                           int *err, cudaStream_t s) {
   if (block < 1) return cudaErrorInvalidValue;
   const __nv_bfloat16 *wbf = static_cast<const __nv_bfloat16 *>(weights);
   const long long nvox = g.nvox();
@@ -1085,34 +1201,16 @@ cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInp
   sc.zlists = reinterpret_cast<int *>(reinterpret_cast<unsigned char *>(sc.props) +
                                       prop_table_bytes(g));
   cudaError_t e;
-  // output planes each convolution must produce: the proposals read conv4 features on the
-  // anchor planes only, conv3 is needed 1 plane around them, conv2 2 planes around them
-  int planes[3] = {g.nz, g.nz, g.nz};
-  if (block > 1 && g.nz > 12) {
-    std::vector<int> lists(3 * (size_t)g.nz);
-    const int iz = g.nz - 12;
-    for (int l = 0; l < 3; ++l) {
-      const int radius = 2 - l;
-      std::vector<char> need(g.nz, 0);
-      for (int bz = 0; bz * block < iz; ++bz) {
-        const int a = 6 + anchor_of_host(bz, block, iz);
-        for (int d = -radius; d <= radius; ++d)
-          if (a + d >= 0 && a + d < g.nz) need[a + d] = 1;
-      }
-      int n = 0;
-      for (int z = 0; z < g.nz; ++z)
-        if (need[z]) lists[(size_t)l * g.nz + n++] = z;
-      planes[l] = n;
-    }
-    if ((e = cudaMemcpyAsync(sc.zlists, lists.data(), lists.size() * sizeof(int),
-                             cudaMemcpyHostToDevice, s)) != cudaSuccess)
-      return e;
-  }
+  std::vector<int> lists;
+  const ConvPlan plan = every_voxel ? dense_plan(g) : sparse_plan(g, block, lists);
+  if (!lists.empty() && (e = cudaMemcpyAsync(sc.zlists, lists.data(), lists.size() * sizeof(int),
+                                             cudaMemcpyHostToDevice, s)) != cudaSuccess)
+    return e;
   if ((e = cudaMemsetAsync(sc.pacc, 0, (size_t)nvox * 4 * 2, s)) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(sc.fallbacks, 0, 2 * sizeof(unsigned long long), s)) != cudaSuccess)
     return e;
   if ((e = pack_all(wbf, sc.frag, s)) != cudaSuccess) return e;
-  if ((e = run_conv1_img(g, wbf, in.img, sc, s)) != cudaSuccess) return e;
+  if ((e = run_conv1_img(g, wbf, in.img, plan, sc, s)) != cudaSuccess) return e;
   const float neg_k = (float)(-1.4426950408889634 / div);
   const float scale = (float)sqrt(1.4426950408889634 / div);
   const int nblk = sms() * 8;
@@ -1130,7 +1228,7 @@ cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInp
   for (int a = 0; a < g.num; ++a) {
     const float *A = in.atlas + a * astride, *L = in.label + a * astride;
     __nv_bfloat16 *f4 = nullptr;
-    if ((e = run_convs(g, wbf, A, in.pitch, sc, err, planes, &f4, s)) != cudaSuccess)
+    if ((e = run_convs(g, wbf, A, in.pitch, sc, err, plan, &f4, s)) != cudaSuccess)
       return e;
     propose_rows_kernel<<<propose_blocks, kRescoreWarps * 32, 0, s>>>(f4, wbf, g.nx, g.ny, g.nz,
                                                                       block, sc.props);
@@ -1160,9 +1258,9 @@ cudaError_t learned_probe(const Geometry &g, const void *weights, const float *i
   if ((e = pack_all(wbf, sc.frag, s)) != cudaSuccess) return e;
   __nv_bfloat16 *f4 = nullptr;
   if ((e = cudaMemsetAsync(sc.err, 0, sizeof(int), s)) != cudaSuccess) return e;
-  const int planes[3] = {g.nz, g.nz, g.nz};
-  if ((e = run_conv1_img(g, wbf, img, sc, s)) != cudaSuccess) return e;
-  if ((e = run_convs(g, wbf, atlas_a, g.ny, sc, sc.err, planes, &f4, s)) != cudaSuccess)
+  const ConvPlan plan = dense_plan(g);
+  if ((e = run_conv1_img(g, wbf, img, plan, sc, s)) != cudaSuccess) return e;
+  if ((e = run_convs(g, wbf, atlas_a, g.ny, sc, sc.err, plan, &f4, s)) != cudaSuccess)
     return e;
   // the sums area is free here: voxel list, proposals and confidences go there
   int64_t *d_vox = reinterpret_cast<int64_t *>(sc.pacc);
