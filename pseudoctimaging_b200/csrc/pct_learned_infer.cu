@@ -104,6 +104,7 @@ __global__ void __launch_bounds__(kC1Warps * 32)
   const int ytiles = (ny + 31) / 32, xtiles = (x_n + kC1Warps - 1) / kC1Warps;
   const long long items = (long long)z_n * xtiles * ytiles;
   const int nxy = nx * ny;
+  const long long nvox = (long long)nz * nxy;
   const int sxy = nx * spitch;
   const int x_hi = x_lo + x_n;
   for (long long it = blockIdx.x; it < items; it += gridDim.x) {
@@ -182,7 +183,7 @@ __global__ void __launch_bounds__(kC1Warps * 32)
               const float v0 = fmaxf(fmaf(acc[mt][j][2 * h] + pi.x, kInScale, bias[j][0]), 0.f);
               const float v1 =
                   fmaxf(fmaf(acc[mt][j][2 * h + 1] + pi.y, kInScale, bias[j][1]), 0.f);
-              *reinterpret_cast<__nv_bfloat162 *>(out + v * kC + 8 * j + 2 * t) =
+              *reinterpret_cast<__nv_bfloat162 *>(out + ((long long)j * nvox + v) * 8 + 2 * t) =
                   __floats2bfloat162_rn(v0, v1);
             }
           }
@@ -191,60 +192,59 @@ __global__ void __launch_bounds__(kC1Warps * 32)
   }
 }
 
-// ---------------------------------------------------------------- conv 16 -> 16 (tensor cores)
+// ---------------------------------------------------------------- conv 16 -> 16 (tcgen05)
 
-// A CTA tile is 1 z-plane x 4 x-rows x 64 y of outputs; its 4 warps each own a 16-voxel y
-// segment of all 4 x-rows. The input slab (3 z x 6 x x 66 y voxels, 16 BF16 channels = 32 bytes
-// each) arrives by TMA with 32-byte swizzling (the two 16-byte halves of a voxel swap places
-// where bit 2 of its slab index is set), which puts the 8 rows of every ldmatrix phase in
-// distinct banks; out-of-volume voxels arrive as zeros. CTAs are persistent and double-buffer the
-// slab. Each warp keeps the B fragments of all 27 taps in registers and walks the 3 x 6 x 3
-// (z, x, y-shift) input row segments once: one ldmatrix feeds the up to 3 output x-rows that use
-// that row (2 mma each, 16 output channels).
-constexpr int kCvWarps = 4;
-constexpr int kCvThreads = kCvWarps * 32;
-constexpr int kCvTX = 4, kCvTY = 16 * kCvWarps;
-constexpr int kCvSZ = 3, kCvSX = kCvTX + 2, kCvSY = kCvTY + 2;
-constexpr int kCvBoxBytes = kCvSZ * kCvSX * kCvSY * 32;    // 38,016
-constexpr int kCvBufBytes = (kCvBoxBytes + 1023) / 1024 * 1024;
-constexpr size_t kConvSmem = 2 * kCvBufBytes + 64 + 1024;  // two buffers, barriers, alignment
-constexpr int kFragWords = 27 * 2 * 2 * 32;  // per layer: tap x n-tile x register x lane
+// Feature volumes are BF16 with the 16 channels split in two halves of 8: half h of voxel v at
+// element (h * nvox + v) * 8, so that a run of voxels of one half is a run of 16-byte rows.
+//
+// conv 16 -> 16 is an implicit GEMM on tcgen05: M = 128 consecutive output y of one x-row,
+// K = 16 input channels per tap, N = 16 output channels per output row. A CTA tile is 1 z-plane
+// x 4 x-rows x 126 y; its input slab (3 z x 6 x x 128 y voxels from y0 - 1) arrives by one TMA
+// box as [half][z][x][y][8 channels] (each (half, z, x) row of 128 voxels is one 2 KB line, read
+// as 256 8-byte elements), which is the canonical K-major no-swizzle operand layout (8-row core
+// matrices of 16-byte rows, the two halves LBO apart). The A operand of tap (kz, kx, ky) for
+// output row o is the slab row (kz, o + kx) from y offset ky: a descriptor start address, no
+// copies; its rows 126 and 127 run into the next slab row and only feed the MMA rows 126 and 127,
+// which are not stored. An input row (kz, ix) at y shift ky feeds output rows o = ix - kx for kx = 0..2, whose
+// accumulators are adjacent TMEM column blocks; the weights of one (kz, ky) are stored as the
+// sequence W(kx = 2) | W(kx = 1) | W(kx = 0) (16 rows each), so a single MMA with N = 16 x (rows
+// fed) covers all of them: 54 MMAs per tile. Warp roles: warps 0-3 epilogue (TMEM lane quarter =
+// warp, one voxel per thread: bias, ReLU, BF16, then the accumulator is zeroed for reuse), warp 4
+// the TMA producer, warp 5 the MMA issuer. Slabs and accumulators are double-buffered; every wait
+// is bounded.
+constexpr int kCvTX = 4, kCvTY = 126;  // output x-rows and y per tile (M = 128)
+constexpr int kCvSZ = 3, kCvSX = kCvTX + 2, kCvSY = 128;
+constexpr int kCvHalf = kCvSZ * kCvSX * kCvSY * 16;                 // 36,864 B
+constexpr int kCvSlab = 2 * kCvHalf;                                // 73,728 B
+constexpr int kCvSlabPad = (kCvSlab + 1023) / 1024 * 1024;          // 75,776 B
+constexpr int kCvSeq = 2 * 48 * 16;                                  // one (kz, ky) weight sequence
+constexpr int kCvWBytes = 9 * kCvSeq;                                // 13,824 B
+constexpr int kCvCols = 2 * kCvTX * 16;                              // two accumulators
+constexpr int kCvThreads = 192;
+constexpr size_t kConvSmem = 1024 + 2 * kCvSlabPad + kCvWBytes + 128;
+constexpr int kFragWords = kCvWBytes / 4;  // per layer: the weight sequences as stored in smem
 constexpr unsigned long long kConvTimeoutNs = 2000000000ULL;
 
-// B fragments of one layer in mma register order: for tap t, n-tile j (8 output channels),
-// register r, lane l: {W[co][ci][t], W[co][ci+1][t]} with co = 8j + l/4, ci = 2(l%4) + 8r.
+// Weight sequences of one layer, byte offset ((kz * 3 + ky) * 2 + h) * 768 + n * 16 + 2 c8 holds
+// W[co][8h + c8][kz * 9 + kx * 3 + ky] for n = 16 (2 - kx) + co.
 __global__ void pack_frags_kernel(const __nv_bfloat16 *__restrict__ wbf, int woff,
                                   uint32_t *__restrict__ frag) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= kFragWords) return;
-  const int lane = i % 32, r = (i / 32) % 2, j = (i / 64) % 2, t = i / 128;
-  const int co = 8 * j + lane / 4, ci = 2 * (lane % 4) + 8 * r;
+  const int off = 4 * i;
+  const int sq = off / kCvSeq, h = (off % kCvSeq) / 768, n = (off % 768) / 16, c8 = (off % 16) / 2;
+  const int kz = sq / 3, ky = sq % 3, kx = 2 - n / 16, co = n % 16, ci = 8 * h + c8;
+  const int t = kz * 9 + kx * 3 + ky;
   const __nv_bfloat16 lo = wbf[woff + (co * kC + ci) * 27 + t];
   const __nv_bfloat16 hi = wbf[woff + (co * kC + ci + 1) * 27 + t];
   frag[i] = (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
 }
 
-__device__ __forceinline__ void ldmatrix_x4(uint32_t addr, uint32_t &r0, uint32_t &r1,
-                                            uint32_t &r2, uint32_t &r3) {
-  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];"
-               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
-               : "r"(addr));
-}
-
-__device__ __forceinline__ void mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2,
-                                         uint32_t a3, uint32_t b0, uint32_t b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
-      "{%8, %9}, {%0, %1, %2, %3};"
-      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
-}
-
-// The output region of one layer: tiles_y tiles of 64 y from y_lo (warps whose 16-y segment
-// starts at or past y_hi skip their work), x tiles of 4 rows, z planes.
+// The output region of one layer: tiles_y tiles of 126 y from y_lo, x tiles of 4 rows, z planes.
 struct ConvGrid {
   int nx, ny, nz, tiles_y, tiles_x, tiles;
   int y_lo, y_hi;
+  long long nvox;
   const int *zlist;  // the output z-planes to compute (NULL: every plane)
   const int *xlist;  // x tiles: first row | (mask of the 4 rows to compute) << 16 (NULL: 4i, all)
 };
@@ -266,131 +266,240 @@ __device__ __forceinline__ void conv_tile_origin(const ConvGrid &g, int tile, in
   y0 = g.y_lo + ty * kCvTY;
 }
 
-__device__ __forceinline__ void conv_issue(const CUtensorMap *tm, uint32_t buf, uint32_t bar,
-                                           const ConvGrid &g, int tile) {
-  int z, x0, y0;
-  unsigned mask;
-  conv_tile_origin(g, tile, z, x0, y0, mask);
-  ptx::fence_proxy_async_smem();
-  ptx::mbar_arrive_expect_tx(bar, kCvBoxBytes);
-  ptx::tma_load_4d(buf, tm, bar, 0, y0 - 1, x0 - 1, z - 1);
+namespace tc5 {
+
+__device__ __forceinline__ uint64_t desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  // K-major, no swizzle: start >> 4 | LBO >> 4 | SBO >> 4 | descriptor version 1
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
-// ROWMASK: tiles carry a mask of the x-rows to compute (rows outside it cost no mma; input rows
-// no masked-in output row uses are not loaded into registers).
-template <bool ROWMASK>
-__global__ void __launch_bounds__(kCvThreads, 2)
+__device__ __forceinline__ uint32_t idesc_bf16(int n) {
+  // D FP32, A and B BF16 (K-major), N, M = 128
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((128u >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, 1, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(idesc)
+      : "memory");
+}
+
+__device__ __forceinline__ void commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   bar)
+               : "memory");
+}
+
+__device__ __forceinline__ void fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ void ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+      "%12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+
+__device__ __forceinline__ void st16_zero(uint32_t taddr) {
+  const uint32_t z = 0u;
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, "
+      "%1, %1, %1, %1, %1};" ::"r"(taddr),
+      "r"(z)
+      : "memory");
+}
+
+__device__ __forceinline__ void wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+}  // namespace tc5
+
+__global__ void __launch_bounds__(kCvThreads, 1)
     conv16_kernel(const __grid_constant__ CUtensorMap tm, const uint32_t *__restrict__ frag,
                   const __nv_bfloat16 *__restrict__ wbf, int boff, __nv_bfloat16 *__restrict__ out,
                   ConvGrid g, int *__restrict__ err) {
   extern __shared__ unsigned char smem_raw[];
-  const uint32_t base = (ptx::smem_u32(smem_raw) + 1023u) & ~1023u;
-  const uint32_t bar0 = base + 2 * kCvBufBytes;  // barrier of buffer b at bar0 + 8 * b
-  volatile int *abort_flag =
-      reinterpret_cast<volatile int *>(smem_raw + (base + 2 * kCvBufBytes + 16 - ptx::smem_u32(smem_raw)));
+  const uint32_t raw = ptx::smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  const uint32_t wtab = base + 2 * kCvSlabPad;
+  const uint32_t bars = wtab + kCvWBytes;  // full[2], empty[2], dfull[2], dempty[2]
+  const uint32_t full0 = bars, empty0 = bars + 16, dfull0 = bars + 32, dempty0 = bars + 48;
+  unsigned char *gen = smem_raw + (bars - raw);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(gen + 64);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(gen + 68);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  uint32_t B[27][2][2];
-#pragma unroll
-  for (int t = 0; t < 27; ++t)
-#pragma unroll
-    for (int j = 0; j < 2; ++j)
-#pragma unroll
-      for (int r = 0; r < 2; ++r) B[t][j][r] = __ldg(frag + ((t * 2 + j) * 2 + r) * 32 + lane);
-  const int c2 = 2 * (lane & 3), g8 = lane >> 2;
-  float bias[2][2];
-#pragma unroll
-  for (int j = 0; j < 2; ++j)
-#pragma unroll
-    for (int e = 0; e < 2; ++e) bias[j][e] = __bfloat162float(wbf[boff + 8 * j + c2 + e]);
+
+  // weight sequences into shared memory (visible to the tensor core through the async proxy)
+  {
+    uint32_t *w = reinterpret_cast<uint32_t *>(smem_raw + (wtab - raw));
+    for (int i = threadIdx.x; i < kFragWords; i += kCvThreads) w[i] = __ldg(frag + i);
+    ptx::fence_proxy_async_smem();
+  }
   if (threadIdx.x == 0) {
-    ptx::mbar_init(bar0, 1);
-    ptx::mbar_init(bar0 + 8, 1);
+    for (int i = 0; i < 2; ++i) {
+      ptx::mbar_init(full0 + 8 * i, 1);
+      ptx::mbar_init(empty0 + 8 * i, 1);
+      ptx::mbar_init(dfull0 + 8 * i, 1);
+      ptx::mbar_init(dempty0 + 8 * i, 4);
+    }
     *abort_flag = 0;
     ptx::fence_mbarrier_init();
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    if ((int)blockIdx.x < g.tiles) conv_issue(&tm, base, bar0, g, blockIdx.x);
-    if ((int)(blockIdx.x + gridDim.x) < g.tiles)
-      conv_issue(&tm, base + kCvBufBytes, bar0 + 8, g, blockIdx.x + gridDim.x);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     ptx::smem_u32(tmem_slot)),
+                 "r"(kCvCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
-  const int m = lane >> 3, q = lane & 7;
-  const int arow = q + 8 * (m & 1), ahalf = m >> 1;  // ldmatrix: A row (voxel) and channel half
-  const int ys = warp * 16;
-  int k = 0;
-  for (int tile = blockIdx.x; tile < g.tiles; tile += gridDim.x, ++k) {
-    const int b = k & 1;
-    const uint32_t buf = base + b * kCvBufBytes, bar = bar0 + 8 * b;
-    if (!ptx::mbar_wait_bounded(bar, (k >> 1) & 1, kConvTimeoutNs)) *abort_flag = 1;
-    __syncthreads();
-    if (*abort_flag) {
-      if (threadIdx.x == 0) {
-        atomicExch(err, 3);
-        // let this CTA's own copies in flight land (bounded) before leaving
-        ptx::mbar_wait_bounded(bar, (k >> 1) & 1, kConvTimeoutNs);
-        if (tile + (int)gridDim.x < g.tiles)
-          ptx::mbar_wait_bounded(bar0 + 8 * (b ^ 1), ((k + 1) >> 1) & 1, kConvTimeoutNs);
+  tc5::fence_before();
+  __syncthreads();
+  tc5::fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 4) {
+    // TMA producer
+    if (lane == 0) {
+      int k = 0;
+      for (int tile = blockIdx.x; tile < g.tiles; tile += gridDim.x, ++k) {
+        const int b = k & 1;
+        if (k >= 2 && !ptx::mbar_wait_bounded(empty0 + 8 * b, ((k >> 1) - 1) & 1, kConvTimeoutNs)) {
+          *abort_flag = 1;
+          break;
+        }
+        if (*abort_flag) break;
+        int z, x0, y0;
+        unsigned mask;
+        conv_tile_origin(g, tile, z, x0, y0, mask);
+        ptx::mbar_arrive_expect_tx(full0 + 8 * b, kCvSlab);
+        ptx::tma_load_4d(base + b * kCvSlabPad, &tm, full0 + 8 * b, 2 * (y0 - 1), x0 - 1, z - 1, 0);
       }
-      return;
+      // the slabs of the last two tiles may still be landing: wait for them (bounded)
+      const int issued = k;
+      for (int j = issued - 2 < 0 ? 0 : issued - 2; j < issued; ++j)
+        ptx::mbar_wait_bounded(full0 + 8 * (j & 1), (j >> 1) & 1, kConvTimeoutNs);
     }
-    int z, x0, y0;
-    unsigned mask;
-    conv_tile_origin(g, tile, z, x0, y0, mask);
-    if (y0 + ys < g.y_hi) {
-      float acc[kCvTX][2][4];
-#pragma unroll
-      for (int o = 0; o < kCvTX; ++o)
-#pragma unroll
-        for (int j = 0; j < 2; ++j)
-#pragma unroll
-          for (int e = 0; e < 4; ++e) acc[o][j][e] = 0.f;
-#pragma unroll
-      for (int iz = 0; iz < 3; ++iz) {
-#pragma unroll
+  } else if (warp == 5) {
+    // MMA issuer
+    if (lane == 0) {
+      int k = 0;
+      for (int tile = blockIdx.x; tile < g.tiles; tile += gridDim.x, ++k) {
+        const int b = k & 1;
+        const uint32_t par = (k >> 1) & 1;
+        if (!ptx::mbar_wait_bounded(full0 + 8 * b, par, kConvTimeoutNs) ||
+            !ptx::mbar_wait_bounded(dempty0 + 8 * b, par, kConvTimeoutNs)) {
+          *abort_flag = 1;
+          break;
+        }
+        if (*abort_flag) break;
+        tc5::fence_after();
+        int z, x0, y0;
+        unsigned mask;
+        conv_tile_origin(g, tile, z, x0, y0, mask);
+        const uint32_t dcol = tmem + b * (kCvTX * 16);
+        const uint64_t da0 = tc5::desc(base + b * kCvSlabPad, kCvHalf, 128);
+        const uint64_t db0 = tc5::desc(wtab, 768, 128);
+#pragma unroll 1
         for (int ix = 0; ix < kCvSX; ++ix) {
-          // output rows o with ix - o in [0, 2]
-          const unsigned users = ix >= 2 ? (0x7u << (ix - 2)) & 0xFu : 0x7u >> (2 - ix);
-          if (ROWMASK && !(mask & users)) continue;
+          // output rows fed by input row ix: o = ix - kx, kx = 2..0, within the tile's mask
+          int o_lo = ix - 2 < 0 ? 0 : ix - 2, o_hi = ix < kCvTX - 1 ? ix : kCvTX - 1;
+          while (o_lo <= o_hi && !((mask >> o_lo) & 1u)) ++o_lo;
+          while (o_hi >= o_lo && !((mask >> o_hi) & 1u)) --o_hi;
+          if (o_lo > o_hi) continue;
+          const uint32_t id = tc5::idesc_bf16(16 * (o_hi - o_lo + 1));
+          const uint32_t d = dcol + 16 * o_lo;
+          // descriptor start fields count 16-byte units
+          const uint64_t da = da0 + (uint64_t)(ix * kCvSY);
+          const uint64_t db = db0 + (uint64_t)((o_lo - ix + 2) * 16);
 #pragma unroll
-          for (int ky = 0; ky < 3; ++ky) {
-            const int sv = (iz * kCvSX + ix) * kCvSY + ys + arow + ky;
-            uint32_t a0, a1, a2, a3;
-            ldmatrix_x4(buf + (uint32_t)(sv * 32 + ((ahalf ^ ((sv >> 2) & 1)) << 4)), a0, a1, a2,
-                        a3);
-#pragma unroll
-            for (int o = 0; o < kCvTX; ++o) {
-              const int kx = ix - o;
-              if (kx < 0 || kx > 2) continue;
-              if (ROWMASK && !((mask >> o) & 1u)) continue;
-              const int t = iz * 9 + kx * 3 + ky;
-              mma_bf16(acc[o][0], a0, a1, a2, a3, B[t][0][0], B[t][0][1]);
-              mma_bf16(acc[o][1], a0, a1, a2, a3, B[t][1][0], B[t][1][1]);
-            }
+          for (int sq = 0; sq < 9; ++sq) {
+            const int kz = sq / 3, ky = sq % 3;
+            tc5::mma(d, da + (uint64_t)(kz * kCvSX * kCvSY + ky), db + (uint64_t)(sq * kCvSeq / 16),
+                     id);
           }
         }
+        tc5::commit(empty0 + 8 * b);
+        tc5::commit(dfull0 + 8 * b);
       }
+      // let every issued MMA finish before the accumulators are released (bounded)
+      if (k > 0) ptx::mbar_wait_bounded(dfull0 + 8 * ((k - 1) & 1), ((k - 1) >> 1) & 1, kConvTimeoutNs);
+    }
+  } else {
+    // epilogue: warp w reads TMEM lanes 32w..32w+31 = output y0 + 32w + lane
+    const uint32_t lane_addr = tmem + ((uint32_t)(32 * warp) << 16);
+    float bias[kC];
+#pragma unroll
+    for (int c = 0; c < kC; ++c) bias[c] = __bfloat162float(wbf[boff + c]);
+    // both accumulators start at zero
+#pragma unroll
+    for (int q = 0; q < kCvCols / 16; ++q) tc5::st16_zero(lane_addr + 16 * q);
+    tc5::wait_st();
+    tc5::fence_before();
+    __syncwarp();
+    if (lane == 0) {
+      ptx::mbar_arrive(dempty0);
+      ptx::mbar_arrive(dempty0 + 8);
+    }
+    int k = 0;
+    for (int tile = blockIdx.x; tile < g.tiles; tile += gridDim.x, ++k) {
+      const int b = k & 1;
+      if (!ptx::mbar_wait_bounded(dfull0 + 8 * b, (k >> 1) & 1, kConvTimeoutNs)) {
+        *abort_flag = 1;
+        break;
+      }
+      tc5::fence_after();
+      int z, x0, y0;
+      unsigned mask;
+      conv_tile_origin(g, tile, z, x0, y0, mask);
+      const int y = y0 + 32 * warp + lane;
+      const uint32_t acc = lane_addr + b * (kCvTX * 16);
 #pragma unroll
       for (int o = 0; o < kCvTX; ++o) {
-        if (ROWMASK && !((mask >> o) & 1u)) continue;
+        uint32_t r[16];
+        tc5::ld16(acc + 16 * o, r);
+        tc5::wait_ld();
         const int x = x0 + o;
-        if (x >= g.nx) break;
+        if (((mask >> o) & 1u) && x < g.nx && y < g.y_hi && 32 * warp + lane < kCvTY) {
+          uint32_t h[8];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int y = y0 + ys + g8 + 8 * h;
-          if (y >= g.y_hi) continue;
-          __nv_bfloat16 *dst = out + (((long long)z * g.nx + x) * g.ny + y) * kC;
-#pragma unroll
-          for (int j = 0; j < 2; ++j) {
-            const float v0 = fmaxf(acc[o][j][2 * h] + bias[j][0], 0.f);
-            const float v1 = fmaxf(acc[o][j][2 * h + 1] + bias[j][1], 0.f);
-            *reinterpret_cast<__nv_bfloat162 *>(dst + 8 * j + c2) = __floats2bfloat162_rn(v0, v1);
+          for (int c = 0; c < 8; ++c) {
+            const float v0 = fmaxf(__uint_as_float(r[2 * c]) + bias[2 * c], 0.f);
+            const float v1 = fmaxf(__uint_as_float(r[2 * c + 1]) + bias[2 * c + 1], 0.f);
+            const __nv_bfloat162 pr = __floats2bfloat162_rn(v0, v1);
+            h[c] = *reinterpret_cast<const uint32_t *>(&pr);
           }
+          const long long v = ((long long)z * g.nx + x) * g.ny + y;
+          *reinterpret_cast<uint4 *>(out + v * 8) = make_uint4(h[0], h[1], h[2], h[3]);
+          *reinterpret_cast<uint4 *>(out + (g.nvox + v) * 8) = make_uint4(h[4], h[5], h[6], h[7]);
         }
       }
+#pragma unroll
+      for (int o = 0; o < kCvTX; ++o) tc5::st16_zero(acc + 16 * o);
+      tc5::wait_st();
+      tc5::fence_before();
+      __syncwarp();
+      if (lane == 0) ptx::mbar_arrive(dempty0 + 8 * b);
     }
-    __syncthreads();  // every warp is done with this buffer
-    if (threadIdx.x == 0 && tile + 2 * (int)gridDim.x < g.tiles)
-      conv_issue(&tm, buf, bar, g, tile + 2 * gridDim.x);
+  }
+  tc5::fence_before();
+  __syncthreads();
+  if (*abort_flag && threadIdx.x == 0) atomicExch(err, 3);
+  if (warp == 0) {
+    tc5::fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCvCols)
+                 : "memory");
   }
 }
 
@@ -416,14 +525,14 @@ __device__ __forceinline__ void stage_heads(const __nv_bfloat16 *__restrict__ wb
 
 // Per-axis offset probabilities of one (voxel, atlas) pair from its 16 conv4 features: the three
 // softmaxes over dw, du, dv of the heads' logits, p[a * 11 + j] for offset j - 5 on axis a.
-__device__ __forceinline__ void axis_probs(const __nv_bfloat16 *__restrict__ fv,
-                                           const float *__restrict__ hw, float (&p)[kHeads]) {
+__device__ __forceinline__ void axis_probs(const __nv_bfloat16 *__restrict__ f4, long long v,
+                                           long long nvox, const float *__restrict__ hw,
+                                           float (&p)[kHeads]) {
   float f[kC];
   {
     __align__(16) __nv_bfloat16 fb[kC];
-    const uint4 *src = reinterpret_cast<const uint4 *>(fv);
-    reinterpret_cast<uint4 *>(fb)[0] = src[0];
-    reinterpret_cast<uint4 *>(fb)[1] = src[1];
+    reinterpret_cast<uint4 *>(fb)[0] = *reinterpret_cast<const uint4 *>(f4 + v * 8);
+    reinterpret_cast<uint4 *>(fb)[1] = *reinterpret_cast<const uint4 *>(f4 + (nvox + v) * 8);
 #pragma unroll
     for (int c = 0; c < kC; ++c) f[c] = __bfloat162float(fb[c]);
   }
@@ -519,10 +628,11 @@ struct Proposal {
   float conf;
 };
 
-__device__ __forceinline__ void propose(const __nv_bfloat16 *__restrict__ fv,
-                                        const float *__restrict__ hw, Proposal &pr) {
+__device__ __forceinline__ void propose(const __nv_bfloat16 *__restrict__ f4, long long v,
+                                        long long nvox, const float *__restrict__ hw,
+                                        Proposal &pr) {
   float p[kHeads];
-  axis_probs(fv, hw, p);
+  axis_probs(f4, v, nvox, hw, p);
   int top[3][4];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
@@ -536,7 +646,7 @@ __device__ __forceinline__ void propose(const __nv_bfloat16 *__restrict__ fv,
 // Testing hook: the proposal of given voxels.
 __global__ void proposal_hook_kernel(const __nv_bfloat16 *__restrict__ f4,
                                      const __nv_bfloat16 *__restrict__ wbf,
-                                     const int64_t *__restrict__ voxels, int n,
+                                     const int64_t *__restrict__ voxels, int n, long long nvox,
                                      signed char *__restrict__ top, float *__restrict__ conf) {
   __shared__ __align__(16) float hw[kHeadFloats];
   stage_heads(wbf, hw);
@@ -544,7 +654,7 @@ __global__ void proposal_hook_kernel(const __nv_bfloat16 *__restrict__ f4,
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   Proposal pr;
-  propose(f4 + voxels[i] * kC, hw, pr);
+  propose(f4, voxels[i], nvox, hw, pr);
   for (int a = 0; a < 3; ++a)
     for (int r = 0; r < 4; ++r) top[i * 12 + a * 4 + r] = pr.top[a][r];
   conf[i] = pr.conf;
@@ -597,7 +707,7 @@ __global__ void __launch_bounds__(kRescoreWarps * 32)
     const bool out_lane = lane >= 1 && lane <= kRowOut && y < ny - lo;
     float p[kHeads];
     if (out_lane) {
-      axis_probs(f4 + ((long long)z * nxy + (long long)x * ny + y) * kC, hw, p);
+      axis_probs(f4, (long long)z * nxy + (long long)x * ny + y, (long long)nz * nxy, hw, p);
     } else {
 #pragma unroll
       for (int o = 0; o < kHeads; ++o) p[o] = 0.f;
@@ -1025,13 +1135,15 @@ namespace {
 cudaError_t make_feature_map(CUtensorMap *map, const __nv_bfloat16 *base, const Geometry &g) {
   auto fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(tensor_map_encoder());
   if (!fn) return cudaErrorNotSupported;
-  const cuuint64_t dims[4] = {(cuuint64_t)kC, (cuuint64_t)g.ny, (cuuint64_t)g.nx, (cuuint64_t)g.nz};
-  const cuuint64_t strides[3] = {(cuuint64_t)kC * 2, (cuuint64_t)kC * 2 * g.ny,
-                                 (cuuint64_t)kC * 2 * g.ny * g.nx};
-  const cuuint32_t box[4] = {(cuuint32_t)kC, (cuuint32_t)kCvSY, (cuuint32_t)kCvSX, (cuuint32_t)kCvSZ};
+  // [half][z][x][y, 8 channels] with each (half, z, x) row as 2 ny 8-byte elements; one box = a
+  // conv16 slab (128 y), out-of-volume voxels zero
+  const cuuint64_t dims[4] = {2 * (cuuint64_t)g.ny, (cuuint64_t)g.nx, (cuuint64_t)g.nz, 2};
+  const cuuint64_t strides[3] = {16 * (cuuint64_t)g.ny, 16 * (cuuint64_t)g.ny * g.nx,
+                                 16 * (cuuint64_t)g.nvox()};
+  const cuuint32_t box[4] = {2 * kCvSY, (cuuint32_t)kCvSX, (cuuint32_t)kCvSZ, 2};
   const cuuint32_t estr[4] = {1u, 1u, 1u, 1u};
-  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16 *>(base), dims,
-                  strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B,
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<__nv_bfloat16 *>(base), dims,
+                  strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
@@ -1045,7 +1157,6 @@ struct ConvPlan {
   int c1_z, c1_nz, c1_x, c1_nx;  // conv1 box (z, x; every y)
   int nzl[3], nxl[3];            // conv2..conv4: z planes and x tiles in the lists
   int y_lo[3], y_hi[3];
-  bool rowmask[3];               // some x tile computes fewer than its 4 rows
   bool dense;
 };
 
@@ -1103,7 +1214,6 @@ ConvPlan sparse_plan(const Geometry &g, int block, std::vector<int> &lists) {
       const int x0 = xs[i];
       unsigned mask = 0;
       while (i < xs.size() && xs[i] < x0 + kCvTX) mask |= 1u << (xs[i++] - x0);
-      if (mask != 0xFu) p.rowmask[l] = true;
       lists[3 * (size_t)g.nz + (size_t)l * g.nx + nt++] = x0 | (int)(mask << 16);
     }
     p.nxl[l] = nt;
@@ -1147,6 +1257,7 @@ cudaError_t run_convs(const Geometry &g, const __nv_bfloat16 *wbf, const float *
   cg.nx = g.nx;
   cg.ny = g.ny;
   cg.nz = g.nz;
+  cg.nvox = g.nvox();
   const int boffs[3] = {kB2, kB3, kB4};
   __nv_bfloat16 *bufs[2] = {sc.fa, sc.fb};
   for (int l = 0; l < 3; ++l) {
@@ -1158,24 +1269,17 @@ cudaError_t run_convs(const Geometry &g, const __nv_bfloat16 *wbf, const float *
     cg.tiles_x = p.nxl[l];
     cg.tiles = cg.tiles_y * cg.tiles_x * p.nzl[l];
     if (cg.tiles <= 0) continue;
-    const int blocks = cg.tiles < 2 * n_sm ? cg.tiles : 2 * n_sm;
-    if (p.rowmask[l])
-      conv16_kernel<true><<<blocks, kCvThreads, kConvSmem, s>>>(
-          maps[l & 1], sc.frag + l * kFragWords, wbf, boffs[l], bufs[(l + 1) & 1], cg, err);
-    else
-      conv16_kernel<false><<<blocks, kCvThreads, kConvSmem, s>>>(
-          maps[l & 1], sc.frag + l * kFragWords, wbf, boffs[l], bufs[(l + 1) & 1], cg, err);
+    const int blocks = cg.tiles < n_sm ? cg.tiles : n_sm;
+    conv16_kernel<<<blocks, kCvThreads, kConvSmem, s>>>(maps[l & 1], sc.frag + l * kFragWords, wbf,
+                                                        boffs[l], bufs[(l + 1) & 1], cg, err);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   return cudaSuccess;
 }
 
 cudaError_t pack_all(const __nv_bfloat16 *wbf, uint32_t *frag, cudaStream_t s) {
-  cudaError_t e0 = cudaFuncSetAttribute(conv16_kernel<false>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kConvSmem);
-  if (e0 != cudaSuccess) return e0;
-  e0 = cudaFuncSetAttribute(conv16_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)kConvSmem);
+  cudaError_t e0 = cudaFuncSetAttribute(conv16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)kConvSmem);
   if (e0 != cudaSuccess) return e0;
   const int woffs[3] = {kW2, kW3, kW4};
   for (int l = 0; l < 3; ++l) {
@@ -1270,7 +1374,7 @@ cudaError_t learned_probe(const Geometry &g, const void *weights, const float *i
   if ((e = cudaMemcpyAsync(d_vox, voxels, n * sizeof(int64_t), cudaMemcpyHostToDevice, s)) !=
       cudaSuccess)
     return e;
-  proposal_hook_kernel<<<(n + 127) / 128, 128, 0, s>>>(f4, wbf, d_vox, n, d_top, d_conf);
+  proposal_hook_kernel<<<(n + 127) / 128, 128, 0, s>>>(f4, wbf, d_vox, n, g.nvox(), d_top, d_conf);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (top && (e = cudaMemcpyAsync(top, d_top, 12 * (size_t)n, cudaMemcpyDeviceToHost, s)) !=
                  cudaSuccess)
@@ -1286,9 +1390,10 @@ cudaError_t learned_probe(const Geometry &g, const void *weights, const float *i
   if (features) {
     for (int i = 0; i < n; ++i) {
       __nv_bfloat16 tmp[kC];
-      if ((e = cudaMemcpy(tmp, f4 + voxels[i] * kC, sizeof(tmp), cudaMemcpyDeviceToHost)) !=
-          cudaSuccess)
-        return e;
+      for (int h = 0; h < 2; ++h)
+        if ((e = cudaMemcpy(tmp + 8 * h, f4 + ((long long)h * g.nvox() + voxels[i]) * 8,
+                            8 * sizeof(__nv_bfloat16), cudaMemcpyDeviceToHost)) != cudaSuccess)
+          return e;
       for (int c = 0; c < kC; ++c) features[i * kC + c] = __bfloat162float(tmp[c]);
     }
   }
