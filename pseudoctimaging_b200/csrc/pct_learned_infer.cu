@@ -197,33 +197,45 @@ __global__ void __launch_bounds__(kC1Warps * 32)
 // Feature volumes are BF16 with the 16 channels split in two halves of 8: half h of voxel v at
 // element (h * nvox + v) * 8, so that a run of voxels of one half is a run of 16-byte rows.
 //
-// conv 16 -> 16 is an implicit GEMM on tcgen05: M = 128 consecutive output y of one x-row,
-// K = 16 input channels per tap, N = 16 output channels per output row. A CTA tile is 1 z-plane
-// x 4 x-rows x 126 y; its input slab (3 z x 6 x x 128 y voxels from y0 - 1) arrives by one TMA
-// box as [half][z][x][y][8 channels] (each (half, z, x) row of 128 voxels is one 2 KB line, read
-// as 256 8-byte elements), which is the canonical K-major no-swizzle operand layout (8-row core
-// matrices of 16-byte rows, the two halves LBO apart). The A operand of tap (kz, kx, ky) for
-// output row o is the slab row (kz, o + kx) from y offset ky: a descriptor start address, no
-// copies; its rows 126 and 127 run into the next slab row and only feed the MMA rows 126 and 127,
-// which are not stored. An input row (kz, ix) at y shift ky feeds output rows o = ix - kx for kx = 0..2, whose
-// accumulators are adjacent TMEM column blocks; the weights of one (kz, ky) are stored as the
-// sequence W(kx = 2) | W(kx = 1) | W(kx = 0) (16 rows each), so a single MMA with N = 16 x (rows
-// fed) covers all of them: 54 MMAs per tile. Warp roles: warps 0-3 epilogue (TMEM lane quarter =
-// warp, one voxel per thread: bias, ReLU, BF16, then the accumulator is zeroed for reuse), warp 4
-// the TMA producer, warp 5 the MMA issuer. Slabs and accumulators are double-buffered; every wait
-// is bounded.
-constexpr int kCvTX = 4, kCvTY = 126;  // output x-rows and y per tile (M = 128)
-constexpr int kCvSZ = 3, kCvSX = kCvTX + 2, kCvSY = 128;
-constexpr int kCvHalf = kCvSZ * kCvSX * kCvSY * 16;                 // 36,864 B
-constexpr int kCvSlab = 2 * kCvHalf;                                // 73,728 B
-constexpr int kCvSlabPad = (kCvSlab + 1023) / 1024 * 1024;          // 75,776 B
+// conv 16 -> 16 is an implicit GEMM on tcgen05: M = 128 consecutive y of one output x-row (126
+// stored), K = 16 input channels per tap, N = 16 output channels per output row. A CTA work item
+// is a column of 4 x-rows x 126 y over a run of consecutive output z-planes; the input planes
+// stream through a ring of shared-memory slots, one TMA box per plane ([half][x][y][8 channels],
+// 6 x-rows of 128 y from y0 - 1; each (half, x) row is one 2 KB line, read as 256 8-byte
+// elements), so an input plane is loaded once for the up to 3 output planes that use it. The slot
+// layout is the canonical K-major no-swizzle operand layout (8-row core matrices of 16-byte rows,
+// the two halves LBO apart): the A operand of tap (kz, kx, ky) for output row o is row o + kx of
+// the plane z + kz - 1 from y offset ky, a descriptor start address (its rows 126 and 127 run into
+// the next row and feed only the MMA rows 126 and 127, which are not stored). An input row ix at
+// y shift ky feeds output rows o = ix - kx for kx = 0..2, whose accumulators are adjacent TMEM
+// column blocks; the weights of one (kz, ky) are stored as the sequence W(kx = 2) | W(kx = 1) |
+// W(kx = 0) (16 rows each), so one MMA with N = 16 x (rows fed) covers them: 54 MMAs per output
+// plane. Warp roles: warps 0-3 epilogue (TMEM lane quarter = warp, one voxel per thread: bias,
+// ReLU, BF16, then the accumulator is zeroed for reuse), warp 4 the TMA producer, warp 5 the MMA
+// issuer. Accumulators are double-buffered; every wait is bounded. Small-N MMAs are bound by the
+// issue rate of one CTA, so two CTAs share each SM (a 4-plane ring each).
+constexpr int kCvTX = 4, kCvTY = 126;  // output x-rows and stored y per tile (M = 128)
+constexpr int kCvSX = kCvTX + 2, kCvSY = 128;
+constexpr int kCvHalf = kCvSX * kCvSY * 16;                          // 12,288 B
+constexpr int kCvPlane = 2 * kCvHalf;                                // 24,576 B per ring slot
+constexpr int kCvRing = 4;                                           // input-plane slots
+constexpr int kCvChunk = 8;                                          // output planes per item
 constexpr int kCvSeq = 2 * 48 * 16;                                  // one (kz, ky) weight sequence
 constexpr int kCvWBytes = 9 * kCvSeq;                                // 13,824 B
 constexpr int kCvCols = 2 * kCvTX * 16;                              // two accumulators
 constexpr int kCvThreads = 192;
-constexpr size_t kConvSmem = 1024 + 2 * kCvSlabPad + kCvWBytes + 128;
+constexpr size_t kConvSmem = 1024 + kCvRing * kCvPlane + kCvWBytes + 128;  // 2 CTAs per SM
 constexpr int kFragWords = kCvWBytes / 4;  // per layer: the weight sequences as stored in smem
 constexpr unsigned long long kConvTimeoutNs = 2000000000ULL;
+
+// Upper bound of one layer's work items: x tiles x y tiles x planes.
+long long conv_items_bound(const Geometry &g) {
+  return (long long)g.nx * ((g.ny + kCvTY - 1) / kCvTY) * g.nz;
+}
+
+size_t conv_list_bytes(const Geometry &g) {
+  return (3 * (size_t)g.nx + 2 * 3 * (size_t)conv_items_bound(g) + 8) * sizeof(int);
+}
 
 // Weight sequences of one layer, byte offset ((kz * 3 + ky) * 2 + h) * 768 + n * 16 + 2 c8 holds
 // W[co][8h + c8][kz * 9 + kx * 3 + ky] for n = 16 (2 - kx) + co.
@@ -240,30 +252,39 @@ __global__ void pack_frags_kernel(const __nv_bfloat16 *__restrict__ wbf, int wof
   frag[i] = (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
 }
 
-// The output region of one layer: tiles_y tiles of 126 y from y_lo, x tiles of 4 rows, z planes.
+// The output region of one layer: work items {x tile | y tile << 16, first plane | planes << 16}
+// over x tiles of 4 rows (first row | mask of the rows to compute << 16; NULL: 4i, all rows) and
+// y tiles of 126 from y_lo.
 struct ConvGrid {
-  int nx, ny, nz, tiles_y, tiles_x, tiles;
+  int nx, ny, nz;
   int y_lo, y_hi;
+  int n_items;
   long long nvox;
-  const int *zlist;  // the output z-planes to compute (NULL: every plane)
-  const int *xlist;  // x tiles: first row | (mask of the 4 rows to compute) << 16 (NULL: 4i, all)
+  const int2 *items;
+  const int *xlist;
 };
 
-__device__ __forceinline__ void conv_tile_origin(const ConvGrid &g, int tile, int &z, int &x0,
-                                                 int &y0, unsigned &mask) {
-  const int ty = tile % g.tiles_y;
-  const int r = tile / g.tiles_y;
-  const int xi = r % g.tiles_x, zi = r / g.tiles_x;
-  z = g.zlist ? g.zlist[zi] : zi;
+struct ConvItem {
+  int x0, y0, z0, planes;
+  unsigned mask;
+};
+
+__device__ __forceinline__ ConvItem conv_item(const ConvGrid &g, int i) {
+  const int2 e = g.items[i];
+  ConvItem r;
+  const int xi = e.x & 0xFFFF, ty = (int)((unsigned)e.x >> 16);
   if (g.xlist) {
-    const int e = g.xlist[xi];
-    x0 = e & 0xFFFF;
-    mask = (unsigned)e >> 16;
+    const int xe = g.xlist[xi];
+    r.x0 = xe & 0xFFFF;
+    r.mask = (unsigned)xe >> 16;
   } else {
-    x0 = xi * kCvTX;
-    mask = 0xFu;
+    r.x0 = xi * kCvTX;
+    r.mask = 0xFu;
   }
-  y0 = g.y_lo + ty * kCvTY;
+  r.y0 = g.y_lo + ty * kCvTY;
+  r.z0 = e.y & 0xFFFF;
+  r.planes = (int)((unsigned)e.y >> 16);
+  return r;
 }
 
 namespace tc5 {
@@ -279,19 +300,22 @@ __device__ __forceinline__ uint32_t idesc_bf16(int n) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((128u >> 4) << 24);
 }
 
+// MMA (accumulating) and commit, issued by one elected lane of a converged warp: the warp
+// computes the operands together, which keeps them warp-uniform.
 __device__ __forceinline__ void mma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc) {
   asm volatile(
-      "{\n\t.reg .pred p;\n\t"
+      "{\n\t.reg .pred e, p;\n\telect.sync _|e, 0xffffffff;\n\t"
       "setp.ne.b32 p, 1, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "@e tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
       "l"(a), "l"(b), "r"(idesc)
       : "memory");
 }
 
 __device__ __forceinline__ void commit(uint32_t bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                   bar)
-               : "memory");
+  asm volatile(
+      "{\n\t.reg .pred e;\n\telect.sync _|e, 0xffffffff;\n\t"
+      "@e tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n\t}" ::"r"(bar)
+      : "memory");
 }
 
 __device__ __forceinline__ void fence_before() {
@@ -326,19 +350,20 @@ __device__ __forceinline__ void wait_st() { asm volatile("tcgen05.wait::st.sync.
 
 }  // namespace tc5
 
-__global__ void __launch_bounds__(kCvThreads, 1)
+__global__ void __launch_bounds__(kCvThreads, 2)
     conv16_kernel(const __grid_constant__ CUtensorMap tm, const uint32_t *__restrict__ frag,
                   const __nv_bfloat16 *__restrict__ wbf, int boff, __nv_bfloat16 *__restrict__ out,
                   ConvGrid g, int *__restrict__ err) {
   extern __shared__ unsigned char smem_raw[];
   const uint32_t raw = ptx::smem_u32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
-  const uint32_t wtab = base + 2 * kCvSlabPad;
-  const uint32_t bars = wtab + kCvWBytes;  // full[2], empty[2], dfull[2], dempty[2]
-  const uint32_t full0 = bars, empty0 = bars + 16, dfull0 = bars + 32, dempty0 = bars + 48;
-  unsigned char *gen = smem_raw + (bars - raw);
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(gen + 64);
-  volatile int *abort_flag = reinterpret_cast<volatile int *>(gen + 68);
+  const uint32_t wtab = base + kCvRing * kCvPlane;
+  // barriers: full[kCvRing], empty[kCvRing], dfull[2], dempty[2]
+  const uint32_t full0 = wtab + kCvWBytes, empty0 = full0 + 8 * kCvRing;
+  const uint32_t dfull0 = empty0 + 8 * kCvRing, dempty0 = dfull0 + 16;
+  unsigned char *gen = smem_raw + (dempty0 + 16 - raw);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(gen);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(gen + 4);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
   // weight sequences into shared memory (visible to the tensor core through the async proxy)
@@ -348,9 +373,11 @@ __global__ void __launch_bounds__(kCvThreads, 1)
     ptx::fence_proxy_async_smem();
   }
   if (threadIdx.x == 0) {
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < kCvRing; ++i) {
       ptx::mbar_init(full0 + 8 * i, 1);
       ptx::mbar_init(empty0 + 8 * i, 1);
+    }
+    for (int i = 0; i < 2; ++i) {
       ptx::mbar_init(dfull0 + 8 * i, 1);
       ptx::mbar_init(dempty0 + 8 * i, 4);
     }
@@ -370,71 +397,81 @@ __global__ void __launch_bounds__(kCvThreads, 1)
   const uint32_t tmem = *tmem_slot;
 
   if (warp == 4) {
-    // TMA producer
+    // TMA producer: the input planes z0 - 1 .. z0 + planes of every item, in order, into the ring
     if (lane == 0) {
-      int k = 0;
-      for (int tile = blockIdx.x; tile < g.tiles; tile += gridDim.x, ++k) {
-        const int b = k & 1;
-        if (k >= 2 && !ptx::mbar_wait_bounded(empty0 + 8 * b, ((k >> 1) - 1) & 1, kConvTimeoutNs)) {
-          *abort_flag = 1;
-          break;
+      uint32_t j = 0;  // planes issued
+      for (int it = blockIdx.x; it < g.n_items && !*abort_flag; it += gridDim.x) {
+        const ConvItem c = conv_item(g, it);
+        for (int p = 0; p < c.planes + 2; ++p, ++j) {
+          const uint32_t slot = j % kCvRing;
+          if (j >= kCvRing &&
+              !ptx::mbar_wait_bounded(empty0 + 8 * slot, ((j / kCvRing) - 1) & 1, kConvTimeoutNs)) {
+            *abort_flag = 1;
+            break;
+          }
+          ptx::mbar_arrive_expect_tx(full0 + 8 * slot, kCvPlane);
+          ptx::tma_load_4d(base + slot * kCvPlane, &tm, full0 + 8 * slot, 2 * (c.y0 - 1), c.x0 - 1,
+                           c.z0 - 1 + p, 0);
         }
-        if (*abort_flag) break;
-        int z, x0, y0;
-        unsigned mask;
-        conv_tile_origin(g, tile, z, x0, y0, mask);
-        ptx::mbar_arrive_expect_tx(full0 + 8 * b, kCvSlab);
-        ptx::tma_load_4d(base + b * kCvSlabPad, &tm, full0 + 8 * b, 2 * (y0 - 1), x0 - 1, z - 1, 0);
       }
-      // the slabs of the last two tiles may still be landing: wait for them (bounded)
-      const int issued = k;
-      for (int j = issued - 2 < 0 ? 0 : issued - 2; j < issued; ++j)
-        ptx::mbar_wait_bounded(full0 + 8 * (j & 1), (j >> 1) & 1, kConvTimeoutNs);
+      // planes still landing: wait for the last ring's worth (bounded)
+      for (uint32_t q = j > kCvRing ? j - kCvRing : 0; q < j; ++q)
+        ptx::mbar_wait_bounded(full0 + 8 * (q % kCvRing), (q / kCvRing) & 1, kConvTimeoutNs);
     }
   } else if (warp == 5) {
-    // MMA issuer
-    if (lane == 0) {
-      int k = 0;
-      for (int tile = blockIdx.x; tile < g.tiles; tile += gridDim.x, ++k) {
-        const int b = k & 1;
-        const uint32_t par = (k >> 1) & 1;
-        if (!ptx::mbar_wait_bounded(full0 + 8 * b, par, kConvTimeoutNs) ||
-            !ptx::mbar_wait_bounded(dempty0 + 8 * b, par, kConvTimeoutNs)) {
-          *abort_flag = 1;
-          break;
-        }
-        if (*abort_flag) break;
-        tc5::fence_after();
-        int z, x0, y0;
-        unsigned mask;
-        conv_tile_origin(g, tile, z, x0, y0, mask);
-        const uint32_t dcol = tmem + b * (kCvTX * 16);
-        const uint64_t da0 = tc5::desc(base + b * kCvSlabPad, kCvHalf, 128);
-        const uint64_t db0 = tc5::desc(wtab, 768, 128);
-#pragma unroll 1
-        for (int ix = 0; ix < kCvSX; ++ix) {
-          // output rows fed by input row ix: o = ix - kx, kx = 2..0, within the tile's mask
-          int o_lo = ix - 2 < 0 ? 0 : ix - 2, o_hi = ix < kCvTX - 1 ? ix : kCvTX - 1;
-          while (o_lo <= o_hi && !((mask >> o_lo) & 1u)) ++o_lo;
-          while (o_hi >= o_lo && !((mask >> o_hi) & 1u)) --o_hi;
-          if (o_lo > o_hi) continue;
-          const uint32_t id = tc5::idesc_bf16(16 * (o_hi - o_lo + 1));
-          const uint32_t d = dcol + 16 * o_lo;
-          // descriptor start fields count 16-byte units
-          const uint64_t da = da0 + (uint64_t)(ix * kCvSY);
-          const uint64_t db = db0 + (uint64_t)((o_lo - ix + 2) * 16);
+    // MMA issuer: the whole warp runs the loop, one elected lane issues
+    {
+      uint32_t j0 = 0, t = 0;  // first ring load of the item, output planes issued
+      const uint64_t db0 = tc5::desc(wtab, 768, 128);
+      for (int it = blockIdx.x; it < g.n_items && !*abort_flag; it += gridDim.x) {
+        const ConvItem c = conv_item(g, it);
+        for (int i = 0; i < c.planes; ++i, ++t) {
+          const int b = t & 1;
+          bool ok = ptx::mbar_wait_bounded(dempty0 + 8 * b, (t >> 1) & 1, kConvTimeoutNs);
+          uint64_t da[3];
 #pragma unroll
-          for (int sq = 0; sq < 9; ++sq) {
-            const int kz = sq / 3, ky = sq % 3;
-            tc5::mma(d, da + (uint64_t)(kz * kCvSX * kCvSY + ky), db + (uint64_t)(sq * kCvSeq / 16),
-                     id);
+          for (int kz = 0; kz < 3; ++kz) {
+            const uint32_t q = j0 + i + kz;
+            ok = ok && ptx::mbar_wait_bounded(full0 + 8 * (q % kCvRing), (q / kCvRing) & 1,
+                                               kConvTimeoutNs);
+            da[kz] = tc5::desc(base + (q % kCvRing) * kCvPlane, kCvHalf, 128);
+          }
+          if (!ok) {
+            *abort_flag = 1;
+            break;
+          }
+          tc5::fence_after();
+          const uint32_t dcol = tmem + b * (kCvTX * 16);
+#pragma unroll 1
+          for (int ix = 0; ix < kCvSX; ++ix) {
+            // output rows fed by input row ix: o = ix - kx, kx = 2..0, within the item's mask
+            int o_lo = ix - 2 < 0 ? 0 : ix - 2, o_hi = ix < kCvTX - 1 ? ix : kCvTX - 1;
+            while (o_lo <= o_hi && !((c.mask >> o_lo) & 1u)) ++o_lo;
+            while (o_hi >= o_lo && !((c.mask >> o_hi) & 1u)) --o_hi;
+            if (o_lo > o_hi) continue;
+            const uint32_t id = tc5::idesc_bf16(16 * (o_hi - o_lo + 1));
+            const uint32_t d = dcol + 16 * o_lo;
+            // descriptor start fields count 16-byte units
+            const uint64_t db = db0 + (uint64_t)((o_lo - ix + 2) * 16);
+#pragma unroll
+            for (int sq = 0; sq < 9; ++sq) {
+              const int kz = sq / 3, ky = sq % 3;
+              tc5::mma(d, da[kz] + (uint64_t)(ix * kCvSY + ky), db + (uint64_t)(sq * kCvSeq / 16),
+                       id);
+            }
+          }
+          tc5::commit(dfull0 + 8 * b);
+          // plane j0 + i feeds no later output of the item; the last output frees all three
+          tc5::commit(empty0 + 8 * ((j0 + i) % kCvRing));
+          if (i == c.planes - 1) {
+            tc5::commit(empty0 + 8 * ((j0 + i + 1) % kCvRing));
+            tc5::commit(empty0 + 8 * ((j0 + i + 2) % kCvRing));
           }
         }
-        tc5::commit(empty0 + 8 * b);
-        tc5::commit(dfull0 + 8 * b);
+        j0 += c.planes + 2;
       }
       // let every issued MMA finish before the accumulators are released (bounded)
-      if (k > 0) ptx::mbar_wait_bounded(dfull0 + 8 * ((k - 1) & 1), ((k - 1) >> 1) & 1, kConvTimeoutNs);
+      if (t > 0) ptx::mbar_wait_bounded(dfull0 + 8 * ((t - 1) & 1), ((t - 1) >> 1) & 1, kConvTimeoutNs);
     }
   } else {
     // epilogue: warp w reads TMEM lanes 32w..32w+31 = output y0 + 32w + lane
@@ -452,45 +489,51 @@ __global__ void __launch_bounds__(kCvThreads, 1)
       ptx::mbar_arrive(dempty0);
       ptx::mbar_arrive(dempty0 + 8);
     }
-    int k = 0;
-    for (int tile = blockIdx.x; tile < g.tiles; tile += gridDim.x, ++k) {
-      const int b = k & 1;
-      if (!ptx::mbar_wait_bounded(dfull0 + 8 * b, (k >> 1) & 1, kConvTimeoutNs)) {
-        *abort_flag = 1;
-        break;
-      }
-      tc5::fence_after();
-      int z, x0, y0;
-      unsigned mask;
-      conv_tile_origin(g, tile, z, x0, y0, mask);
-      const int y = y0 + 32 * warp + lane;
-      const uint32_t acc = lane_addr + b * (kCvTX * 16);
-#pragma unroll
-      for (int o = 0; o < kCvTX; ++o) {
-        uint32_t r[16];
-        tc5::ld16(acc + 16 * o, r);
-        tc5::wait_ld();
-        const int x = x0 + o;
-        if (((mask >> o) & 1u) && x < g.nx && y < g.y_hi && 32 * warp + lane < kCvTY) {
-          uint32_t h[8];
-#pragma unroll
-          for (int c = 0; c < 8; ++c) {
-            const float v0 = fmaxf(__uint_as_float(r[2 * c]) + bias[2 * c], 0.f);
-            const float v1 = fmaxf(__uint_as_float(r[2 * c + 1]) + bias[2 * c + 1], 0.f);
-            const __nv_bfloat162 pr = __floats2bfloat162_rn(v0, v1);
-            h[c] = *reinterpret_cast<const uint32_t *>(&pr);
-          }
-          const long long v = ((long long)z * g.nx + x) * g.ny + y;
-          *reinterpret_cast<uint4 *>(out + v * 8) = make_uint4(h[0], h[1], h[2], h[3]);
-          *reinterpret_cast<uint4 *>(out + (g.nvox + v) * 8) = make_uint4(h[4], h[5], h[6], h[7]);
+    uint32_t t = 0;
+    bool stop = false;
+    for (int it = blockIdx.x; it < g.n_items && !stop; it += gridDim.x) {
+      const ConvItem c = conv_item(g, it);
+      const int y = c.y0 + 32 * warp + lane;
+      const bool y_ok = y < g.y_hi && 32 * warp + lane < kCvTY;
+      for (int i = 0; i < c.planes; ++i, ++t) {
+        const int b = t & 1;
+        if (!ptx::mbar_wait_bounded(dfull0 + 8 * b, (t >> 1) & 1, kConvTimeoutNs)) {
+          *abort_flag = 1;
+          stop = true;
+          break;
         }
-      }
+        tc5::fence_after();
+        const int z = c.z0 + i;
+        const uint32_t acc = lane_addr + b * (kCvTX * 16);
+        uint32_t r[kCvTX][16];
 #pragma unroll
-      for (int o = 0; o < kCvTX; ++o) tc5::st16_zero(acc + 16 * o);
-      tc5::wait_st();
-      tc5::fence_before();
-      __syncwarp();
-      if (lane == 0) ptx::mbar_arrive(dempty0 + 8 * b);
+        for (int o = 0; o < kCvTX; ++o) tc5::ld16(acc + 16 * o, r[o]);
+        tc5::wait_ld();
+#pragma unroll
+        for (int o = 0; o < kCvTX; ++o) {
+          const int x = c.x0 + o;
+          if (((c.mask >> o) & 1u) && x < g.nx && y_ok) {
+            uint32_t h[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+              const float v0 = fmaxf(__uint_as_float(r[o][2 * q]) + bias[2 * q], 0.f);
+              const float v1 = fmaxf(__uint_as_float(r[o][2 * q + 1]) + bias[2 * q + 1], 0.f);
+              const __nv_bfloat162 pr = __floats2bfloat162_rn(v0, v1);
+              h[q] = *reinterpret_cast<const uint32_t *>(&pr);
+            }
+            const long long v = ((long long)z * g.nx + x) * g.ny + y;
+            *reinterpret_cast<uint4 *>(out + v * 8) = make_uint4(h[0], h[1], h[2], h[3]);
+            *reinterpret_cast<uint4 *>(out + (g.nvox + v) * 8) =
+                make_uint4(h[4], h[5], h[6], h[7]);
+          }
+        }
+#pragma unroll
+        for (int o = 0; o < kCvTX; ++o) tc5::st16_zero(acc + 16 * o);
+        tc5::wait_st();
+        tc5::fence_before();
+        __syncwarp();
+        if (lane == 0) ptx::mbar_arrive(dempty0 + 8 * b);
+      }
     }
   }
   tc5::fence_before();
@@ -1083,8 +1126,7 @@ struct InferScratch {
   int *err;                       // bounded-wait status of the probe hook
   float *cimg;                    // conv1's input-MRI half, FP32 [nvox][16]
   RowProp *props;                 // row-segment proposals of the block anchor rows
-  int *zlists;                    // conv2, conv3, conv4 output planes, nz entries each, then
-                                  // their x tiles, nx entries each
+  int *lists;                     // the convolutions' x tiles and work items
 };
 
 // Bytes before the proposal table (features, sums, fragments, counters), 256-aligned.
@@ -1108,7 +1150,7 @@ InferScratch carve(void *scratch, long long nvox) {
   r.cimg = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(r.fallbacks) + 256);
   r.props = reinterpret_cast<RowProp *>(static_cast<unsigned char *>(scratch) +
                                         infer_base_bytes(nvox));
-  r.zlists = nullptr;  // placed by carve_tables, which knows the geometry
+  r.lists = nullptr;  // placed by the launch, which knows the geometry
   return r;
 }
 
@@ -1120,8 +1162,7 @@ size_t prop_table_bytes(const Geometry &g) {
 }
 
 size_t infer_scratch_bytes(const Geometry &g) {
-  return infer_base_bytes(g.nvox()) + prop_table_bytes(g) +
-         3 * ((size_t)g.nz + g.nx) * sizeof(int) + 256;
+  return infer_base_bytes(g.nvox()) + prop_table_bytes(g) + conv_list_bytes(g) + 256;
 }
 
 unsigned long long *infer_counters(void *scratch, long long nvox) {
@@ -1136,11 +1177,11 @@ cudaError_t make_feature_map(CUtensorMap *map, const __nv_bfloat16 *base, const 
   auto fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(tensor_map_encoder());
   if (!fn) return cudaErrorNotSupported;
   // [half][z][x][y, 8 channels] with each (half, z, x) row as 2 ny 8-byte elements; one box = a
-  // conv16 slab (128 y), out-of-volume voxels zero
+  // conv16 ring slot (one plane, 6 x-rows of 128 y), out-of-volume voxels zero
   const cuuint64_t dims[4] = {2 * (cuuint64_t)g.ny, (cuuint64_t)g.nx, (cuuint64_t)g.nz, 2};
   const cuuint64_t strides[3] = {16 * (cuuint64_t)g.ny, 16 * (cuuint64_t)g.ny * g.nx,
                                  16 * (cuuint64_t)g.nvox()};
-  const cuuint32_t box[4] = {2 * kCvSY, (cuuint32_t)kCvSX, (cuuint32_t)kCvSZ, 2};
+  const cuuint32_t box[4] = {2 * kCvSY, (cuuint32_t)kCvSX, 1, 2};
   const cuuint32_t estr[4] = {1u, 1u, 1u, 1u};
   CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<__nv_bfloat16 *>(base), dims,
                   strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -1152,22 +1193,43 @@ cudaError_t make_feature_map(CUtensorMap *map, const __nv_bfloat16 *base, const 
 // (z, x) of the row blocks, at the interior y; layer conv(4 - r) is needed r voxels around them.
 // Every needed output's receptive field lies inside the volume (interior margin 6 > 4 layers), so
 // the zero padding of the volume edge never reaches a needed value and skipped outputs are never
-// read. Dense plans (no lists) compute every voxel.
+// read. Dense plans compute every voxel. `lists` (uploaded to the device) holds the 3 nx x-tile
+// entries of the sparse plans (first row | row mask << 16), then each layer's work items.
 struct ConvPlan {
   int c1_z, c1_nz, c1_x, c1_nx;  // conv1 box (z, x; every y)
-  int nzl[3], nxl[3];            // conv2..conv4: z planes and x tiles in the lists
   int y_lo[3], y_hi[3];
+  int n_items[3], item_off[3];   // work items of conv2..conv4 (offset in ints into the lists)
   bool dense;
 };
 
-ConvPlan dense_plan(const Geometry &g) {
+// Work items of a layer: every (x tile, y tile) column over each run of consecutive planes of
+// `zs`, cut into pieces of at most kCvChunk planes.
+void add_items(ConvPlan &p, int l, const std::vector<int> &zs, int x_tiles, std::vector<int> &lists) {
+  const int tiles_y = (p.y_hi[l] - p.y_lo[l] + kCvTY - 1) / kCvTY;
+  if (lists.size() & 1) lists.push_back(0);  // items are read as 8-byte int2
+  p.item_off[l] = (int)lists.size();
+  for (int xi = 0; xi < x_tiles; ++xi)
+    for (int ty = 0; ty < tiles_y; ++ty)
+      for (size_t i = 0; i < zs.size();) {
+        size_t e = i + 1;
+        while (e < zs.size() && zs[e] == zs[e - 1] + 1 && (int)(e - i) < kCvChunk) ++e;
+        lists.push_back(xi | (ty << 16));
+        lists.push_back(zs[i] | ((int)(e - i) << 16));
+        i = e;
+      }
+  p.n_items[l] = (int)((lists.size() - p.item_off[l]) / 2);
+}
+
+ConvPlan dense_plan(const Geometry &g, std::vector<int> &lists) {
   ConvPlan p{};
+  lists.assign(3 * (size_t)g.nx, 0);
   p.c1_nz = g.nz;
   p.c1_nx = g.nx;
+  std::vector<int> zs(g.nz);
+  for (int z = 0; z < g.nz; ++z) zs[z] = z;
   for (int l = 0; l < 3; ++l) {
-    p.nzl[l] = g.nz;
-    p.nxl[l] = (g.nx + kCvTX - 1) / kCvTX;
     p.y_hi[l] = g.ny;
+    add_items(p, l, zs, (g.nx + kCvTX - 1) / kCvTX, lists);
   }
   p.dense = true;
   return p;
@@ -1192,11 +1254,11 @@ std::vector<int> rows_near(const std::vector<int> &anc, int radius, int n) {
   return r;
 }
 
-// Sparse plan for row blocks of `block`; `lists` receives 3 nz z-plane entries then 3 nx x-tile
-// entries (first row | row mask << 16), greedy 4-row tiles starting at the first uncovered row.
+// Sparse plan for row blocks of `block`: greedy 4-row x tiles starting at the first uncovered
+// needed row, items over the needed planes.
 ConvPlan sparse_plan(const Geometry &g, int block, std::vector<int> &lists) {
   ConvPlan p{};
-  lists.assign(3 * ((size_t)g.nz + g.nx), 0);
+  lists.assign(3 * (size_t)g.nx, 0);
   const int iz = g.nz - 12, ix = g.nx - 12, iy = g.ny - 12;
   if (iz <= 0 || ix <= 0 || iy <= 0) return p;  // no interior: nothing to compute
   const std::vector<int> az = anchors(iz, block), ax = anchors(ix, block);
@@ -1207,18 +1269,16 @@ ConvPlan sparse_plan(const Geometry &g, int block, std::vector<int> &lists) {
   for (int l = 0; l < 3; ++l) {
     const int radius = 2 - l;
     const std::vector<int> zs = rows_near(az, radius, g.nz), xs = rows_near(ax, radius, g.nx);
-    p.nzl[l] = (int)zs.size();
-    for (size_t i = 0; i < zs.size(); ++i) lists[(size_t)l * g.nz + i] = zs[i];
     int nt = 0;
     for (size_t i = 0; i < xs.size();) {
       const int x0 = xs[i];
       unsigned mask = 0;
       while (i < xs.size() && xs[i] < x0 + kCvTX) mask |= 1u << (xs[i++] - x0);
-      lists[3 * (size_t)g.nz + (size_t)l * g.nx + nt++] = x0 | (int)(mask << 16);
+      lists[(size_t)l * g.nx + nt++] = x0 | (int)(mask << 16);
     }
-    p.nxl[l] = nt;
     p.y_lo[l] = 6 - radius;
     p.y_hi[l] = g.ny - 6 + radius;
+    add_items(p, l, zs, nt, lists);
   }
   return p;
 }
@@ -1261,15 +1321,13 @@ cudaError_t run_convs(const Geometry &g, const __nv_bfloat16 *wbf, const float *
   const int boffs[3] = {kB2, kB3, kB4};
   __nv_bfloat16 *bufs[2] = {sc.fa, sc.fb};
   for (int l = 0; l < 3; ++l) {
-    cg.zlist = p.dense ? nullptr : sc.zlists + l * g.nz;
-    cg.xlist = p.dense ? nullptr : sc.zlists + 3 * g.nz + l * g.nx;
+    cg.xlist = p.dense ? nullptr : sc.lists + l * g.nx;
+    cg.items = reinterpret_cast<const int2 *>(sc.lists + p.item_off[l]);
+    cg.n_items = p.n_items[l];
     cg.y_lo = p.y_lo[l];
     cg.y_hi = p.y_hi[l];
-    cg.tiles_y = (p.y_hi[l] - p.y_lo[l] + kCvTY - 1) / kCvTY;
-    cg.tiles_x = p.nxl[l];
-    cg.tiles = cg.tiles_y * cg.tiles_x * p.nzl[l];
-    if (cg.tiles <= 0) continue;
-    const int blocks = cg.tiles < n_sm ? cg.tiles : n_sm;
+    if (cg.n_items <= 0) continue;
+    const int blocks = cg.n_items < 2 * n_sm ? cg.n_items : 2 * n_sm;
     conv16_kernel<<<blocks, kCvThreads, kConvSmem, s>>>(maps[l & 1], sc.frag + l * kFragWords, wbf,
                                                         boffs[l], bufs[(l + 1) & 1], cg, err);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -1302,13 +1360,14 @@ cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInp
   const long long nvox = g.nvox();
   const long long astride = (long long)g.nz * g.nx * in.pitch;
   InferScratch sc = carve(scratch, nvox);
-  sc.zlists = reinterpret_cast<int *>(reinterpret_cast<unsigned char *>(sc.props) +
-                                      prop_table_bytes(g));
+  sc.lists = reinterpret_cast<int *>(reinterpret_cast<unsigned char *>(sc.props) +
+                                     prop_table_bytes(g));
   cudaError_t e;
   std::vector<int> lists;
-  const ConvPlan plan = every_voxel ? dense_plan(g) : sparse_plan(g, block, lists);
-  if (!lists.empty() && (e = cudaMemcpyAsync(sc.zlists, lists.data(), lists.size() * sizeof(int),
-                                             cudaMemcpyHostToDevice, s)) != cudaSuccess)
+  const ConvPlan plan = every_voxel ? dense_plan(g, lists) : sparse_plan(g, block, lists);
+  if (lists.size() * sizeof(int) > conv_list_bytes(g)) return cudaErrorInvalidValue;
+  if ((e = cudaMemcpyAsync(sc.lists, lists.data(), lists.size() * sizeof(int),
+                           cudaMemcpyHostToDevice, s)) != cudaSuccess)
     return e;
   if ((e = cudaMemsetAsync(sc.pacc, 0, (size_t)nvox * 4 * 2, s)) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(sc.fallbacks, 0, 2 * sizeof(unsigned long long), s)) != cudaSuccess)
@@ -1357,12 +1416,19 @@ cudaError_t learned_probe(const Geometry &g, const void *weights, const float *i
                           const float *atlas_a, void *scratch, const int64_t *voxels, int n,
                           float *features, signed char *top, float *conf, cudaStream_t s) {
   const __nv_bfloat16 *wbf = static_cast<const __nv_bfloat16 *>(weights);
-  const InferScratch sc = carve(scratch, g.nvox());
+  InferScratch sc = carve(scratch, g.nvox());
+  sc.lists = reinterpret_cast<int *>(reinterpret_cast<unsigned char *>(sc.props) +
+                                     prop_table_bytes(g));
   cudaError_t e;
   if ((e = pack_all(wbf, sc.frag, s)) != cudaSuccess) return e;
   __nv_bfloat16 *f4 = nullptr;
   if ((e = cudaMemsetAsync(sc.err, 0, sizeof(int), s)) != cudaSuccess) return e;
-  const ConvPlan plan = dense_plan(g);
+  std::vector<int> lists;
+  const ConvPlan plan = dense_plan(g, lists);
+  if (lists.size() * sizeof(int) > conv_list_bytes(g)) return cudaErrorInvalidValue;
+  if ((e = cudaMemcpyAsync(sc.lists, lists.data(), lists.size() * sizeof(int),
+                           cudaMemcpyHostToDevice, s)) != cudaSuccess)
+    return e;
   if ((e = run_conv1_img(g, wbf, img, plan, sc, s)) != cudaSuccess) return e;
   if ((e = run_convs(g, wbf, atlas_a, g.ny, sc, sc.err, plan, &f4, s)) != cudaSuccess)
     return e;
