@@ -946,22 +946,21 @@ __device__ __forceinline__ int pick4(const int (&t)[4], int i) {
   return i == 0 ? t[0] : i == 1 ? t[1] : i == 2 ? t[2] : t[3];
 }
 
-__device__ __forceinline__ void eval_offset4(const float *__restrict__ atl,
-                                             const float *__restrict__ lab,
-                                             const float (&in)[3][kRows + 2], long long zrow0,
-                                             long long axy, int apitch, int nx, int x0, int yc,
-                                             int dw, int du, int dv, const bool (&take)[kRows],
-                                             float s, float (&P)[kRows], float (&W)[kRows]) {
+// One offset for the 4 rows of a warp item. `a` points at the atlas voxel (z - 1 + dw, x0 - 1 +
+// du, yc + dv), `l` at the label voxel (z + dw, x0 + du, yc + dv); row strides are 32-bit.
+__device__ __forceinline__ void eval_offset4(const float *__restrict__ a,
+                                             const float *__restrict__ l,
+                                             const float (&in)[3][kRows + 2], int axy, int apitch,
+                                             unsigned take, float s, float (&P)[kRows],
+                                             float (&W)[kRows]) {
   float Z[kRows + 2];
-  const long long zb = zrow0 + (long long)dw * axy;  // plane z + dw - 1
 #pragma unroll
   for (int xr = 0; xr < kRows + 2; ++xr) {
-    const int xa = min(x0 - 1 + xr + du, nx - 1);  // rows past the volume feed no output
-    const float *a = atl + zb + (long long)xa * apitch + yc + dv;
+    const int ro = xr * apitch;
     float z = 0.f;
 #pragma unroll
     for (int dz = 0; dz < 3; ++dz) {
-      const float t = fmaf(__ldg(a + dz * axy), s, in[dz][xr]);
+      const float t = fmaf(__ldg(a + (ro + dz * axy)), s, in[dz][xr]);
       z = fmaf(t, t, z);
     }
     Z[xr] = z;
@@ -971,37 +970,42 @@ __device__ __forceinline__ void eval_offset4(const float *__restrict__ atl,
     const float x = Z[r] + Z[r + 1] + Z[r + 2];
     const float e =
         __shfl_up_sync(0xffffffffu, x, 1) + x + __shfl_down_sync(0xffffffffu, x, 1);
-    if (take[r]) {
+    if ((take >> r) & 1u) {
       const float w = ptx::ex2_approx(-e);
-      const int xl = x0 + r + du;
-      P[r] = fmaf(w, __ldg(lab + zb + axy + (long long)xl * apitch + yc + dv), P[r]);
+      P[r] = fmaf(w, __ldg(l + r * apitch), P[r]);
       W[r] += w;
     }
   }
 }
 
+// Items are 4 x-rows of one z plane; the last item of an x-row band is shifted back to end at
+// the last interior row, the rows the previous item owns left out, so no load needs a clamp.
+// Needs at least 4 interior x-rows and an atlas volume below 2^31 voxels (32-bit offsets).
 __global__ void __launch_bounds__(kRescoreWarps * 32, 4)
     rescore4_kernel(const RowProp *__restrict__ props, const float *__restrict__ img,
                     const float *__restrict__ atl, const float *__restrict__ lab, int nx, int ny,
                     int nz, int apitch, float scale, float conf_thr, float *__restrict__ pacc,
                     float *__restrict__ wacc, unsigned long long *__restrict__ fallbacks,
                     unsigned long long *__restrict__ evaluated) {
+  __shared__ int s_off[kRescoreWarps][kTopK];  // per warp: the item's 32 offsets, 32-bit
   const int lane = threadIdx.x & 31;
+  int *w_off = s_off[threadIdx.x >> 5];
   const int lo = 6;
   const int ix = nx - 2 * lo, iz = nz - 2 * lo, iy = ny - 2 * lo;
-  if (ix <= 0 || iy <= 0 || iz <= 0) return;
+  if (ix < kRows || iy <= 0 || iz <= 0) return;
   const int segs = (iy + kRowOut - 1) / kRowOut;
   const int nbx = (ix + kRows - 1) / kRows;
   const long long items = (long long)iz * nbx * segs;
   const int nxy = nx * ny;
-  const long long axy = (long long)nx * apitch;
+  const int axy = nx * apitch;
   unsigned long long my_fallbacks = 0, my_evals = 0;
   for (long long it = (long long)blockIdx.x * kRescoreWarps + (threadIdx.x >> 5); it < items;
        it += (long long)gridDim.x * kRescoreWarps) {
     const int seg = (int)(it % segs);
     const long long r0 = it / segs;
     const int bx = (int)(r0 % nbx), z = (int)(r0 / nbx) + lo;
-    const int x0 = lo + bx * kRows;
+    const int xb = lo + bx * kRows;
+    const int x0 = min(xb, nx - lo - kRows);
     const int y0 = lo + seg * kRowOut;
     const int y = y0 - 1 + lane;
     const bool out_lane = lane >= 1 && lane <= kRowOut && y < ny - lo;
@@ -1012,40 +1016,43 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 4)
     for (int a = 0; a < 3; ++a)
 #pragma unroll
       for (int r = 0; r < 4; ++r) top[a][r] = rp.top[a * 4 + r];
-    bool valid[kRows];
+    // lane c: the offset of kept triple c
+    {
+      const int code = kRankTriples[lane];
+      const int dw = pick4(top[0], code & 3) - 5, du = pick4(top[1], (code >> 2) & 3) - 5,
+                dv = pick4(top[2], code >> 4) - 5;
+      __syncwarp();
+      w_off[lane] = dw * axy + du * apitch + dv;
+      __syncwarp();
+    }
+    unsigned owned = 0;
 #pragma unroll
-    for (int r = 0; r < kRows; ++r) valid[r] = out_lane && x0 + r < nx - lo;
+    for (int r = 0; r < kRows; ++r)
+      if (x0 + r >= xb) owned |= 1u << r;
+    const unsigned take = out_lane ? owned : 0u;
     const bool full = out_lane && conf_thr > 0.f && rp.conf[lane - 1] < conf_thr;
     const unsigned any_full = __ballot_sync(0xffffffffu, full);
-    if (full) {
-#pragma unroll
-      for (int r = 0; r < kRows; ++r) my_fallbacks += valid[r] ? 1 : 0;
-    }
-    // input taps I(z+dz-1, x0-1+xr, y), negated and scaled
+    if (full) my_fallbacks += __popc(take);
+    // input taps I(z+dz-1, x0-1+xr, yc), negated and scaled
     float in[3][kRows + 2];
 #pragma unroll
     for (int dz = 0; dz < 3; ++dz)
 #pragma unroll
-      for (int xr = 0; xr < kRows + 2; ++xr) {
-        const int xx = min(x0 - 1 + xr, nx - 1);
-        in[dz][xr] = -__ldg(img + (long long)(z + dz - 1) * nxy + (long long)xx * ny + yc) * scale;
-      }
-    const long long zrow0 = (long long)(z - 1) * axy;
+      for (int xr = 0; xr < kRows + 2; ++xr)
+        in[dz][xr] =
+            -__ldg(img + (long long)(z + dz - 1) * nxy + (long long)(x0 - 1 + xr) * ny + yc) * scale;
+    const float *ab = atl + ((long long)(z - 1) * axy + (long long)(x0 - 1) * apitch + yc);
+    const float *lb = lab + ((long long)z * axy + (long long)x0 * apitch + yc);
     float P[kRows], W[kRows];
 #pragma unroll
     for (int r = 0; r < kRows; ++r) P[r] = W[r] = 0.f;
     if (!any_full) {
-      bool take[kRows];
-#pragma unroll
-      for (int r = 0; r < kRows; ++r) take[r] = valid[r];
 #pragma unroll 2
       for (int c = 0; c < kTopK; ++c) {
-        const int code = kRankTriples[c];
-        eval_offset4(atl, lab, in, zrow0, axy, apitch, nx, x0, yc, pick4(top[0], code & 3) - 5,
-                     pick4(top[1], (code >> 2) & 3) - 5, pick4(top[2], code >> 4) - 5, take,
-                     scale, P, W);
+        const int off = w_off[c];
+        eval_offset4(ab + off, lb + off, in, axy, apitch, take, scale, P, W);
       }
-      my_evals += 32 * (unsigned long long)min(kRows, nx - lo - x0);
+      my_evals += (unsigned long long)kTopK * __popc(owned);
     } else {
       unsigned long long rank[3];
 #pragma unroll
@@ -1063,19 +1070,16 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 4)
           const int ru = rw + (int)((rank[1] >> (4 * ju)) & 0xF);
           for (int jv = 0; jv < kAxis; ++jv) {
             const bool mine = full || (ru + (int)((rank[2] >> (4 * jv)) & 0xF) <= 4);
-            bool take[kRows];
-#pragma unroll
-            for (int r = 0; r < kRows; ++r) take[r] = valid[r] && mine;
-            eval_offset4(atl, lab, in, zrow0, axy, apitch, nx, x0, yc, jw - 5, ju - 5, jv - 5,
-                         take, scale, P, W);
+            const int off = (jw - 5) * axy + (ju - 5) * apitch + (jv - 5);
+            eval_offset4(ab + off, lb + off, in, axy, apitch, mine ? take : 0u, scale, P, W);
           }
         }
       }
-      my_evals += kAxis * kAxis * kAxis * (unsigned long long)min(kRows, nx - lo - x0);
+      my_evals += (unsigned long long)kAxis * kAxis * kAxis * __popc(owned);
     }
 #pragma unroll
     for (int r = 0; r < kRows; ++r)
-      if (valid[r]) {
+      if ((take >> r) & 1u) {
         const long long v = (long long)z * nxy + (long long)(x0 + r) * ny + y;
         pacc[v] += P[r];
         wacc[v] += W[r];
@@ -1396,7 +1400,8 @@ cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInp
     propose_rows_kernel<<<propose_blocks, kRescoreWarps * 32, 0, s>>>(f4, wbf, g.nx, g.ny, g.nz,
                                                                       block, sc.props);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if (block == kRows) {
+    if (block == kRows && g.nx - 12 >= kRows &&
+        (long long)g.nz * g.nx * in.pitch < (1LL << 31) - 1) {
       rescore4_kernel<<<rescore_blocks, kRescoreWarps * 32, 0, s>>>(
           sc.props, in.img, A, L, g.nx, g.ny, g.nz, in.pitch, scale, conf_thr, sc.pacc, sc.wacc,
           sc.fallbacks, sc.evaluated);
