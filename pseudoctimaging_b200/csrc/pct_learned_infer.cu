@@ -198,33 +198,42 @@ __global__ void __launch_bounds__(kC1Warps * 32)
 // element (h * nvox + v) * 8, so that a run of voxels of one half is a run of 16-byte rows.
 //
 // conv 16 -> 16 is an implicit GEMM on tcgen05: M = 128 consecutive y of one output x-row (126
-// stored), K = 16 input channels per tap, N = 16 output channels per output row. A CTA work item
-// is a column of 4 x-rows x 126 y over a run of consecutive output z-planes; the input planes
-// stream through a ring of shared-memory slots, one TMA box per plane ([half][x][y][8 channels],
-// 6 x-rows of 128 y from y0 - 1; each (half, x) row is one 2 KB line, read as 256 8-byte
-// elements), so an input plane is loaded once for the up to 3 output planes that use it. The slot
-// layout is the canonical K-major no-swizzle operand layout (8-row core matrices of 16-byte rows,
-// the two halves LBO apart): the A operand of tap (kz, kx, ky) for output row o is row o + kx of
-// the plane z + kz - 1 from y offset ky, a descriptor start address (its rows 126 and 127 run into
-// the next row and feed only the MMA rows 126 and 127, which are not stored). An input row ix at
-// y shift ky feeds output rows o = ix - kx for kx = 0..2, whose accumulators are adjacent TMEM
-// column blocks; the weights of one (kz, ky) are stored as the sequence W(kx = 2) | W(kx = 1) |
-// W(kx = 0) (16 rows each), so one MMA with N = 16 x (rows fed) covers them: 54 MMAs per output
-// plane. Warp roles: warps 0-3 epilogue (TMEM lane quarter = warp, one voxel per thread: bias,
-// ReLU, BF16, then the accumulator is zeroed for reuse), warp 4 the TMA producer, warp 5 the MMA
-// issuer. Accumulators are double-buffered; every wait is bounded. Small-N MMAs are bound by the
-// issue rate of one CTA, so two CTAs share each SM (a 4-plane ring each).
-constexpr int kCvTX = 4, kCvTY = 126;  // output x-rows and stored y per tile (M = 128)
+// stored), K = 16 input channels per tap. A CTA work item is a column of 4 x-rows x 126 y over a
+// run of consecutive output z-planes; its input planes z0 - 1 .. z0 + planes stream through a
+// 2-slot ring of shared memory, one TMA box per plane ([half][x][y][8 channels], 6 x-rows of 128
+// y from y0 - 1; each (half, x) row is one 2 KB line read as 256 8-byte elements), which is the
+// canonical K-major no-swizzle operand layout (8-row core matrices of 16-byte rows, the two
+// halves LBO apart). The A operand for input row ix at y shift ky is a descriptor start address
+// in the plane's slot (its rows 126 and 127 run into the next row and feed only the MMA rows 126
+// and 127, which are not stored).
+//
+// An input row (plane p, row ix, shift ky) feeds the output rows o = ix - kx (kx = 0..2) of the
+// three output planes p + 1 - kz (kz = 0..2). The accumulators of three consecutive output planes
+// live in TMEM as a ring of plane slots r = z mod 3, column 16 (3 o + r) + channel, so the nine
+// (kz, kx) blocks an input row feeds are adjacent columns: one MMA with N = 48 x (rows fed) <= 144
+// covers them. Its B operand is a weight sequence ordered the same way, W(kz = (rho - r) mod 3,
+// kx, ky) for kx = 2, 1, 0 and r = 0, 1, 2, stored for each ky and rotation rho = (p + 1) mod 3.
+// 18 MMAs per input plane; after the MMAs of plane p the output plane p - 1 is complete, and the
+// epilogue reads it, zeroes its slot for plane p + 2 and then stores it. The first two and last
+// two outputs of an item are the run's halo and are only zeroed; an item of one plane reuses no
+// slot, so its three input planes run back to back and it is finalised once.
+//
+// Warp roles: warps 0-3 epilogue (TMEM lane quarter = warp, one voxel per thread: bias, ReLU,
+// BF16 store, zeroing), warp 4 the TMA producer, warp 5 the MMA issuer (the whole warp computes
+// the operands, one elected lane issues). Two CTAs share each SM, so one CTA's MMAs overlap the
+// other's epilogue; every wait is bounded.
+constexpr int kCvTX = 4, kCvTY = 126;  // output x-rows and stored y per item column (M = 128)
 constexpr int kCvSX = kCvTX + 2, kCvSY = 128;
 constexpr int kCvHalf = kCvSX * kCvSY * 16;                          // 12,288 B
 constexpr int kCvPlane = 2 * kCvHalf;                                // 24,576 B per ring slot
-constexpr int kCvRing = 4;                                           // input-plane slots
+constexpr int kCvRing = 2;                                           // input-plane slots
 constexpr int kCvChunk = 8;                                          // output planes per item
-constexpr int kCvSeq = 2 * 48 * 16;                                  // one (kz, ky) weight sequence
-constexpr int kCvWBytes = 9 * kCvSeq;                                // 13,824 B
-constexpr int kCvCols = 2 * kCvTX * 16;                              // two accumulators
+constexpr int kCvSeqRows = 144;                                      // 9 blocks of 16 channels
+constexpr int kCvSeq = 2 * kCvSeqRows * 16;                          // 4,608 B per (ky, rho)
+constexpr int kCvWBytes = 9 * kCvSeq;                                // 41,472 B
+constexpr int kCvCols = 256;                                         // 3 plane slots x 64 used
 constexpr int kCvThreads = 192;
-constexpr size_t kConvSmem = 1024 + kCvRing * kCvPlane + kCvWBytes + 128;  // 2 CTAs per SM
+constexpr size_t kConvSmem = 128 + kCvRing * kCvPlane + kCvWBytes + 128;  // 2 CTAs per SM
 constexpr int kFragWords = kCvWBytes / 4;  // per layer: the weight sequences as stored in smem
 constexpr unsigned long long kConvTimeoutNs = 2000000000ULL;
 
@@ -237,15 +246,18 @@ size_t conv_list_bytes(const Geometry &g) {
   return (3 * (size_t)g.nx + 2 * 3 * (size_t)conv_items_bound(g) + 8) * sizeof(int);
 }
 
-// Weight sequences of one layer, byte offset ((kz * 3 + ky) * 2 + h) * 768 + n * 16 + 2 c8 holds
-// W[co][8h + c8][kz * 9 + kx * 3 + ky] for n = 16 (2 - kx) + co.
+// Weight sequences of one layer: sequence q = 3 ky + rho, byte offset q * 4608 + h * 2304 +
+// n * 16 + 2 c8 holds W[co][8h + c8][kz * 9 + kx * 3 + ky] for row n = 16 (3 kxi + r) + co,
+// kx = 2 - kxi, kz = (rho - r) mod 3.
 __global__ void pack_frags_kernel(const __nv_bfloat16 *__restrict__ wbf, int woff,
                                   uint32_t *__restrict__ frag) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= kFragWords) return;
   const int off = 4 * i;
-  const int sq = off / kCvSeq, h = (off % kCvSeq) / 768, n = (off % 768) / 16, c8 = (off % 16) / 2;
-  const int kz = sq / 3, ky = sq % 3, kx = 2 - n / 16, co = n % 16, ci = 8 * h + c8;
+  const int q = off / kCvSeq, h = (off % kCvSeq) / (kCvSeqRows * 16);
+  const int n = (off % (kCvSeqRows * 16)) / 16, c8 = (off % 16) / 2;
+  const int ky = q / 3, rho = q % 3, blk = n / 16, co = n % 16, ci = 8 * h + c8;
+  const int kx = 2 - blk / 3, r = blk % 3, kz = (rho - r + 3) % 3;
   const int t = kz * 9 + kx * 3 + ky;
   const __nv_bfloat16 lo = wbf[woff + (co * kC + ci) * 27 + t];
   const __nv_bfloat16 hi = wbf[woff + (co * kC + ci + 1) * 27 + t];
@@ -356,12 +368,12 @@ __global__ void __launch_bounds__(kCvThreads, 2)
                   ConvGrid g, int *__restrict__ err) {
   extern __shared__ unsigned char smem_raw[];
   const uint32_t raw = ptx::smem_u32(smem_raw);
-  const uint32_t base = (raw + 1023u) & ~1023u;
+  const uint32_t base = (raw + 127u) & ~127u;
   const uint32_t wtab = base + kCvRing * kCvPlane;
-  // barriers: full[kCvRing], empty[kCvRing], dfull[2], dempty[2]
+  // barriers: full[ring], empty[ring], mdone (MMAs of an input plane complete), zeroed[3]
   const uint32_t full0 = wtab + kCvWBytes, empty0 = full0 + 8 * kCvRing;
-  const uint32_t dfull0 = empty0 + 8 * kCvRing, dempty0 = dfull0 + 16;
-  unsigned char *gen = smem_raw + (dempty0 + 16 - raw);
+  const uint32_t mdone = empty0 + 8 * kCvRing, zeroed0 = mdone + 8;
+  unsigned char *gen = smem_raw + (zeroed0 + 24 - raw);
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(gen);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(gen + 4);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -377,10 +389,8 @@ __global__ void __launch_bounds__(kCvThreads, 2)
       ptx::mbar_init(full0 + 8 * i, 1);
       ptx::mbar_init(empty0 + 8 * i, 1);
     }
-    for (int i = 0; i < 2; ++i) {
-      ptx::mbar_init(dfull0 + 8 * i, 1);
-      ptx::mbar_init(dempty0 + 8 * i, 4);
-    }
+    ptx::mbar_init(mdone, 1);
+    for (int i = 0; i < 3; ++i) ptx::mbar_init(zeroed0 + 8 * i, 4);
     *abort_flag = 0;
     ptx::fence_mbarrier_init();
   }
@@ -420,119 +430,138 @@ __global__ void __launch_bounds__(kCvThreads, 2)
     }
   } else if (warp == 5) {
     // MMA issuer: the whole warp runs the loop, one elected lane issues
-    {
-      uint32_t j0 = 0, t = 0;  // first ring load of the item, output planes issued
-      const uint64_t db0 = tc5::desc(wtab, 768, 128);
-      for (int it = blockIdx.x; it < g.n_items && !*abort_flag; it += gridDim.x) {
-        const ConvItem c = conv_item(g, it);
-        for (int i = 0; i < c.planes; ++i, ++t) {
-          const int b = t & 1;
-          bool ok = ptx::mbar_wait_bounded(dempty0 + 8 * b, (t >> 1) & 1, kConvTimeoutNs);
-          uint64_t da[3];
-#pragma unroll
-          for (int kz = 0; kz < 3; ++kz) {
-            const uint32_t q = j0 + i + kz;
-            ok = ok && ptx::mbar_wait_bounded(full0 + 8 * (q % kCvRing), (q / kCvRing) & 1,
-                                               kConvTimeoutNs);
-            da[kz] = tc5::desc(base + (q % kCvRing) * kCvPlane, kCvHalf, 128);
-          }
-          if (!ok) {
-            *abort_flag = 1;
-            break;
-          }
-          tc5::fence_after();
-          const uint32_t dcol = tmem + b * (kCvTX * 16);
-#pragma unroll 1
-          for (int ix = 0; ix < kCvSX; ++ix) {
-            // output rows fed by input row ix: o = ix - kx, kx = 2..0, within the item's mask
-            int o_lo = ix - 2 < 0 ? 0 : ix - 2, o_hi = ix < kCvTX - 1 ? ix : kCvTX - 1;
-            while (o_lo <= o_hi && !((c.mask >> o_lo) & 1u)) ++o_lo;
-            while (o_hi >= o_lo && !((c.mask >> o_hi) & 1u)) --o_hi;
-            if (o_lo > o_hi) continue;
-            const uint32_t id = tc5::idesc_bf16(16 * (o_hi - o_lo + 1));
-            const uint32_t d = dcol + 16 * o_lo;
-            // descriptor start fields count 16-byte units
-            const uint64_t db = db0 + (uint64_t)((o_lo - ix + 2) * 16);
-#pragma unroll
-            for (int sq = 0; sq < 9; ++sq) {
-              const int kz = sq / 3, ky = sq % 3;
-              tc5::mma(d, da[kz] + (uint64_t)(ix * kCvSY + ky), db + (uint64_t)(sq * kCvSeq / 16),
-                       id);
-            }
-          }
-          tc5::commit(dfull0 + 8 * b);
-          // plane j0 + i feeds no later output of the item; the last output frees all three
-          tc5::commit(empty0 + 8 * ((j0 + i) % kCvRing));
-          if (i == c.planes - 1) {
-            tc5::commit(empty0 + 8 * ((j0 + i + 1) % kCvRing));
-            tc5::commit(empty0 + 8 * ((j0 + i + 2) % kCvRing));
-          }
+    uint32_t j = 0;              // input planes consumed
+    uint32_t nz[3] = {1, 1, 1};  // completed zeroings each plane slot must reach (initial one)
+    const uint64_t db0 = tc5::desc(wtab, kCvSeqRows * 16, 128);
+    for (int it = blockIdx.x; it < g.n_items && !*abort_flag; it += gridDim.x) {
+      const ConvItem c = conv_item(g, it);
+      bool ok = true;
+      for (int p = 0; p < c.planes + 2 && ok; ++p, ++j) {
+        const int zin = c.z0 - 1 + p;  // input plane; feeds output planes zin - 1 .. zin + 1
+        // the slots of the outputs this plane feeds must be zeroed: all three at the first plane
+        // of an item, else the one that output zin + 1 takes over (an item of one plane reuses
+        // no slot and waits only at its start)
+        for (int r = 0; r < 3 && ok; ++r)
+          if (p == 0 || (c.planes > 1 && r == (zin + 1 + 3) % 3))
+            ok = ptx::mbar_wait_bounded(zeroed0 + 8 * r, (nz[r] - 1) & 1, kConvTimeoutNs);
+        ok = ok && ptx::mbar_wait_bounded(full0 + 8 * (j % kCvRing), (j / kCvRing) & 1,
+                                          kConvTimeoutNs);
+        if (!ok) {
+          *abort_flag = 1;
+          break;
         }
-        j0 += c.planes + 2;
+        tc5::fence_after();
+        const uint64_t da = tc5::desc(base + (j % kCvRing) * kCvPlane, kCvHalf, 128);
+        const int rho = (zin + 1 + 3) % 3;
+#pragma unroll 1
+        for (int ix = 0; ix < kCvSX; ++ix) {
+          int o_lo = ix - 2 < 0 ? 0 : ix - 2, o_hi = ix < kCvTX - 1 ? ix : kCvTX - 1;
+          while (o_lo <= o_hi && !((c.mask >> o_lo) & 1u)) ++o_lo;
+          while (o_hi >= o_lo && !((c.mask >> o_hi) & 1u)) --o_hi;
+          if (o_lo > o_hi) continue;
+          const uint32_t id = tc5::idesc_bf16(48 * (o_hi - o_lo + 1));
+          const uint32_t d = tmem + 48 * o_lo;
+          // descriptor start fields count 16-byte units: sequence (ky, rho), block 3 (2 - ix + o_lo)
+          const uint64_t db = db0 + (uint64_t)(rho * (kCvSeq / 16) + 3 * (2 - ix + o_lo) * 16);
+#pragma unroll
+          for (int ky = 0; ky < 3; ++ky)
+            tc5::mma(d, da + (uint64_t)(ix * kCvSY + ky), db + (uint64_t)(ky * 3 * (kCvSeq / 16)),
+                     id);
+        }
+        tc5::commit(empty0 + 8 * (j % kCvRing));
+        tc5::commit(mdone);
+        // output zin - 1 completes with this plane; its slot is zeroed next (and, at the end of
+        // the item, the two halo outputs after it); a one-plane item zeroes all three at its end
+        if (c.planes > 1 || p == c.planes + 1) nz[(zin - 1 + 3) % 3] += 1;
+        if (p == c.planes + 1) {
+          nz[(zin + 3) % 3] += 1;
+          nz[(zin + 1 + 3) % 3] += 1;
+        }
       }
-      // let every issued MMA finish before the accumulators are released (bounded)
-      if (t > 0) ptx::mbar_wait_bounded(dfull0 + 8 * ((t - 1) & 1), ((t - 1) >> 1) & 1, kConvTimeoutNs);
     }
+    // let every issued MMA finish before the accumulators are released (bounded)
+    if (j > 0) ptx::mbar_wait_bounded(mdone, (j - 1) & 1, kConvTimeoutNs);
   } else {
     // epilogue: warp w reads TMEM lanes 32w..32w+31 = output y0 + 32w + lane
     const uint32_t lane_addr = tmem + ((uint32_t)(32 * warp) << 16);
     float bias[kC];
 #pragma unroll
     for (int c = 0; c < kC; ++c) bias[c] = __bfloat162float(wbf[boff + c]);
-    // both accumulators start at zero
+    // every plane slot starts at zero
 #pragma unroll
-    for (int q = 0; q < kCvCols / 16; ++q) tc5::st16_zero(lane_addr + 16 * q);
+    for (int q = 0; q < 12; ++q) tc5::st16_zero(lane_addr + 16 * q);
     tc5::wait_st();
     tc5::fence_before();
     __syncwarp();
-    if (lane == 0) {
-      ptx::mbar_arrive(dempty0);
-      ptx::mbar_arrive(dempty0 + 8);
-    }
-    uint32_t t = 0;
+    if (lane == 0)
+      for (int r = 0; r < 3; ++r) ptx::mbar_arrive(zeroed0 + 8 * r);
+    uint32_t j = 0;  // input planes whose MMAs were waited for
     bool stop = false;
     for (int it = blockIdx.x; it < g.n_items && !stop; it += gridDim.x) {
       const ConvItem c = conv_item(g, it);
       const int y = c.y0 + 32 * warp + lane;
       const bool y_ok = y < g.y_hi && 32 * warp + lane < kCvTY;
-      for (int i = 0; i < c.planes; ++i, ++t) {
-        const int b = t & 1;
-        if (!ptx::mbar_wait_bounded(dfull0 + 8 * b, (t >> 1) & 1, kConvTimeoutNs)) {
-          *abort_flag = 1;
-          stop = true;
-          break;
-        }
-        tc5::fence_after();
-        const int z = c.z0 + i;
-        const uint32_t acc = lane_addr + b * (kCvTX * 16);
-        uint32_t r[kCvTX][16];
-#pragma unroll
-        for (int o = 0; o < kCvTX; ++o) tc5::ld16(acc + 16 * o, r[o]);
-        tc5::wait_ld();
-#pragma unroll
-        for (int o = 0; o < kCvTX; ++o) {
-          const int x = c.x0 + o;
-          if (((c.mask >> o) & 1u) && x < g.nx && y_ok) {
-            uint32_t h[8];
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-              const float v0 = fmaxf(__uint_as_float(r[o][2 * q]) + bias[2 * q], 0.f);
-              const float v1 = fmaxf(__uint_as_float(r[o][2 * q + 1]) + bias[2 * q + 1], 0.f);
-              const __nv_bfloat162 pr = __floats2bfloat162_rn(v0, v1);
-              h[q] = *reinterpret_cast<const uint32_t *>(&pr);
-            }
-            const long long v = ((long long)z * g.nx + x) * g.ny + y;
-            *reinterpret_cast<uint4 *>(out + v * 8) = make_uint4(h[0], h[1], h[2], h[3]);
-            *reinterpret_cast<uint4 *>(out + (g.nvox + v) * 8) =
-                make_uint4(h[4], h[5], h[6], h[7]);
+      // outputs z0 - 2 .. z0 + planes + 1: after input plane z0 - 1 + i for i <= planes + 1
+      for (int i = 0; i < c.planes + 4; ++i) {
+        if (i < c.planes + 2) {
+          if (!ptx::mbar_wait_bounded(mdone, j & 1, kConvTimeoutNs)) {
+            *abort_flag = 1;
+            stop = true;
+            break;
           }
+          ++j;
+          tc5::fence_after();
         }
+        const bool single = c.planes == 1;
+        if (single && i != 2) continue;  // one-plane item: finalised once, after its last plane
+        const int z = c.z0 - 2 + i;
+        const int r = (z + 3) % 3;
+        const uint32_t acc = lane_addr + 16 * r;
+        const bool real = i >= 2 && i < c.planes + 2;
+        // read the plane slot, zero it (all three for a one-plane item) and release it to the MMA
+        // warp, then store
+        uint32_t v[kCvTX][16];
+        if (real) {
 #pragma unroll
-        for (int o = 0; o < kCvTX; ++o) tc5::st16_zero(acc + 16 * o);
+          for (int o = 0; o < kCvTX; ++o) tc5::ld16(acc + 48 * o, v[o]);
+          tc5::wait_ld();
+        }
+        if (single) {
+#pragma unroll
+          for (int q = 0; q < 12; ++q) tc5::st16_zero(lane_addr + 16 * q);
+        } else {
+#pragma unroll
+          for (int o = 0; o < kCvTX; ++o) tc5::st16_zero(acc + 48 * o);
+        }
         tc5::wait_st();
         tc5::fence_before();
         __syncwarp();
-        if (lane == 0) ptx::mbar_arrive(dempty0 + 8 * b);
+        if (lane == 0) {
+          if (single)
+            for (int q = 0; q < 3; ++q) ptx::mbar_arrive(zeroed0 + 8 * q);
+          else
+            ptx::mbar_arrive(zeroed0 + 8 * r);
+        }
+        if (real) {
+#pragma unroll
+          for (int o = 0; o < kCvTX; ++o) {
+            const int x = c.x0 + o;
+            if (((c.mask >> o) & 1u) && x < g.nx && y_ok) {
+              uint32_t h[8];
+#pragma unroll
+              for (int q = 0; q < 8; ++q) {
+                const float v0 = fmaxf(__uint_as_float(v[o][2 * q]) + bias[2 * q], 0.f);
+                const float v1 = fmaxf(__uint_as_float(v[o][2 * q + 1]) + bias[2 * q + 1], 0.f);
+                const __nv_bfloat162 pr = __floats2bfloat162_rn(v0, v1);
+                h[q] = *reinterpret_cast<const uint32_t *>(&pr);
+              }
+              const long long vx = ((long long)z * g.nx + x) * g.ny + y;
+              *reinterpret_cast<uint4 *>(out + vx * 8) = make_uint4(h[0], h[1], h[2], h[3]);
+              *reinterpret_cast<uint4 *>(out + (g.nvox + vx) * 8) =
+                  make_uint4(h[4], h[5], h[6], h[7]);
+            }
+          }
+        }
       }
     }
   }
