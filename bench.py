@@ -402,9 +402,13 @@ def time_other_forms(pct, h, d_img, d_mri, d_lab, d_plain, div, stream, args) ->
     model = learned.LearnedModel.load(learned.CHECKPOINT, torch.cuda.current_device())
     h.attach_model(model, 0.0)
     out = {}
-    for name, choice, steps in (("learned", pct.EXEC_LEARNED, 5), ("tc_fp16", pct.EXEC_TC_FP16, 2),
-                                ("tc_bf16", pct.EXEC_TC_BF16, 2)):
+    for name, choice, steps, k in (("learned", pct.EXEC_LEARNED, 5, 32),
+                                   ("learned_k10", pct.EXEC_LEARNED, 5, 10),
+                                   ("tc_fp16", pct.EXEC_TC_FP16, 2, 0),
+                                   ("tc_bf16", pct.EXEC_TC_BF16, 2, 0)):
         o = torch.zeros_like(d_img)
+        if k:
+            h.set_learned_k(k)
 
         def step():
             h.synthesize_device(d_img.data_ptr(), d_mri.data_ptr(), d_lab.data_ptr(), o.data_ptr(),
@@ -425,10 +429,10 @@ def time_other_forms(pct, h, d_img, d_mri, d_lab, d_plain, div, stream, args) ->
         out[name] = {"ms_per_step": ms, "value": nvox / (ms / 1e3), "steps": steps,
                      "mae_hu_vs_plain": float(e.mean()), "max_abs_hu_vs_plain": float(e.max()),
                      "nan_mismatch": int((np.isnan(g) != np.isnan(ref)).sum())}
-    if "learned" in out:
-        st = h.learned_stats()
-        out["learned"]["offsets_per_row"] = st["row_offsets"] / (
-            (NZ - 12) * (NX - 12) * -(-(NY - 12) // 30) * NUM)
+        if k:
+            out[name]["offsets_per_row"] = h.learned_stats()["row_offsets"] / (
+                (NZ - 12) * (NX - 12) * -(-(NY - 12) // 30) * NUM)
+    h.set_learned_k(32)
     h.attach_model(None)
     model.close()
     return out
@@ -706,6 +710,7 @@ def run_learned_arm(args) -> None:
     h = pct.Handle(0)
     model = learned.LearnedModel.load(learned.CHECKPOINT)
     h.attach_model(model, args.conf)
+    h.set_learned_k(args.k)
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
 
@@ -749,7 +754,7 @@ def run_learned_arm(args) -> None:
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "bf16 network, f32 rescoring",
         "data": "synthetic (seeded generator, config 4 held-out subject, seed 5000)",
-        "config": {"workload": "config 4: learned proposal, k = 32 per row segment",
+        "config": {"workload": f"config 4: learned proposal, k = {args.k} per row segment",
                    "checkpoint": learned.CHECKPOINT.name, "conf_threshold": args.conf,
                    "volume": [NX, NY, NZ], "atlases": NUM, "nh": 11},
         "plain": {"ms_per_step": ms_plain, "value": nvox / (ms_plain / 1e3)},
@@ -788,6 +793,8 @@ def main() -> None:
                          "tc: config 2, the tensor-core form against the plain kernel")
     ap.add_argument("--conf", type=float, default=0.0,
                     help="learned workload: confidence threshold of the full-search fallback")
+    ap.add_argument("--k", type=int, default=32, choices=[10, 20, 32],
+                    help="learned workload: offsets rescored per proposal")
     ap.add_argument("--batch-subjects", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-pointer end-to-end leg")

@@ -262,6 +262,11 @@ int pct_set_learned_block(pct_handle *h, int block);
  * r rows and planes of them, interior y widened by r). The result is bit-identical; this is the
  * check of the restricted plan. No counterpart in the reference. */
 int pct_set_learned_convs(pct_handle *h, int every_voxel);
+/* Size of the kept set (default 32): from the 4 most probable offsets per axis, the rank triples
+ * (i, j, k) with i + j + k <= 4 (k = 32), <= 3 (k = 20) or <= 2 (k = 10) are rescored exactly;
+ * the confidence test uses the probability mass of the same set. Fewer offsets trade accuracy
+ * for speed. No counterpart in the reference. */
+int pct_set_learned_k(pct_handle *h, int k);
 
 /*
  * Tensor-core form (EXEC_CHOICE 5 = FP16, 6 = BF16; NH = 11) runs through pct_synthesize /

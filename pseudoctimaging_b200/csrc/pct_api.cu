@@ -39,6 +39,7 @@ struct pct_handle {
   float learned_conf = 0.f;             // its full-search fallback threshold
   int learned_block = 4;                // rows per proposal block along z and x
   bool learned_every_voxel = false;     // convolutions over the whole volume (diagnostic)
+  int learned_level = 4;                // kept rank triples i + j + k <= level (32 offsets)
   DevBuf learned;                       // its feature volumes and sums
   long long learned_nvox = 0;           // volume size of the last learned run (0: none yet)
   cudaStream_t learned_stream = nullptr;
@@ -167,7 +168,7 @@ int launch_learned_path(pct_handle *h, const pct::Geometry &g, const pct::SlabIn
   int *err = static_cast<int *>(h->err.ptr);
   PCT_CUDA(h, cudaMemsetAsync(err, 0, sizeof(int), s));
   PCT_CUDA(h, pct::learned::launch_learned(g, pct::learned::model_weights(h->model), in, d_out, div,
-                                           h->learned_conf, h->learned_block,
+                                           h->learned_conf, h->learned_block, h->learned_level,
                                            h->learned_every_voxel, h->learned.ptr, err, s));
   h->learned_nvox = g.nvox();
   h->learned_stream = s;
@@ -537,6 +538,14 @@ int pct_set_learned_block(pct_handle *h, int block) {
   if (block < 1 || block > 16)
     return fail(h, PCT_ERR_INVALID_ARG, "learned proposal block must be 1..16 rows");
   h->learned_block = block;
+  return PCT_OK;
+}
+
+int pct_set_learned_k(pct_handle *h, int k) {
+  if (!h) return PCT_ERR_INVALID_ARG;
+  if (k != 10 && k != 20 && k != 32)
+    return fail(h, PCT_ERR_INVALID_ARG, "learned proposal k must be 10, 20 or 32");
+  h->learned_level = k == 10 ? 2 : k == 20 ? 3 : 4;
   return PCT_OK;
 }
 

@@ -106,11 +106,12 @@ size_t infer_scratch_bytes(const Geometry &g);
 unsigned long long *infer_counters(void *scratch, long long nvox);
 // *err (device) is set to a non-zero code if a bounded wait of the convolution pipeline gives up.
 // Rows of voxels share the proposal of their block's anchor row: blocks of `block` x `block`
-// rows in (z, x) (1 = every row segment proposes for itself). The convolutions compute only the
-// outputs the anchor rows need unless `every_voxel` (same result).
+// rows in (z, x) (1 = every row segment proposes for itself); the kept set of a proposal is the
+// rank triples with i + j + k <= level (2, 3, 4: 10, 20, 32 offsets). The convolutions compute
+// only the outputs the anchor rows need unless `every_voxel` (same result).
 cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInputs &in, float *out,
-                           double div, float conf_thr, int block, bool every_voxel, void *scratch,
-                           int *err, cudaStream_t s);
+                           double div, float conf_thr, int block, int level, bool every_voxel,
+                           void *scratch, int *err, cudaStream_t s);
 cudaError_t learned_probe(const Geometry &g, const void *weights, const float *img,
                           const float *atlas_a, void *scratch, const int64_t *voxels, int n,
                           float *features, signed char *top, float *conf, cudaStream_t s);

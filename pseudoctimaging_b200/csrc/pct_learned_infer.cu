@@ -1,17 +1,17 @@
 // Inference side of the learned proposal (EXEC_CHOICE 7).
 //
 // Per atlas, over the whole volume:
-//   conv1 (2 -> 16 channels)            tensor cores: FP16 im2col rows (K = 54 -> 64), FP32 accumulation
-//   conv2..conv4 (16 -> 16 channels)    tensor cores: BF16 implicit GEMM with FP32 accumulation
-//                                       (mma m16n8k16; ldmatrix gathers 16 shifted voxel rows of a
-//                                       channel-last shared-memory slab per tap, 27 taps)
-//   heads, proposal and rescoring       one warp per row segment of 30 voxels along y: per voxel
-//                                       the 33 logits and a softmax per axis; the segment's summed
-//                                       probabilities pick 4 offsets per axis and the 32 rank
-//                                       triples with i + j + k <= 4; the exact FP32 SSD of those
-//                                       32 candidates -> weights exp(-SSD/div) -> product and
-//                                       weight sums. A voxel whose own probability mass on the 32
-//                                       is below the confidence threshold takes all 11^3.
+//   conv1 (2 -> 16 channels)            tensor cores: FP16 im2col rows per input channel, FP32
+//                                       accumulation (mma.sync)
+//   conv2..conv4 (16 -> 16 channels)    tensor cores: BF16 implicit GEMM on tcgen05, FP32 in TMEM
+//   heads, proposal and rescoring       row segments of 30 voxels along y: per voxel the 33
+//                                       logits and a softmax per axis; the summed probabilities of
+//                                       a block's anchor segment pick 4 offsets per axis and the
+//                                       rank triples with i + j + k <= L (L = 4, 3, 2: 32, 20 or
+//                                       10 offsets); the exact FP32 SSD of those candidates ->
+//                                       weights exp(-SSD/div) -> product and weight sums. A voxel
+//                                       whose own probability mass on the kept set is below the
+//                                       confidence threshold takes all 11^3.
 // The sums are kept per voxel across atlases and turned into the output with the reference's
 // NaN rule at the end. Out-of-volume inputs of the convolutions read as zero; interior voxels
 // (6 or more voxels from every face) only see in-volume values.
@@ -667,11 +667,11 @@ __device__ __forceinline__ float pick(const float (&p)[kHeads], int a, int idx) 
 }
 
 // Probability mass p_w * p_u * p_v of the kept set, the rank triples (i, j, k) with
-// i + j + k <= 4, from the per-axis probabilities of ranks 0..3, tp[a][r].
-__device__ __forceinline__ float mass_of(const float (&tp)[3][4]) {
+// i + j + k <= level (2, 3 or 4), from the per-axis probabilities of ranks 0..3, tp[a][r].
+__device__ __forceinline__ float mass_of(const float (&tp)[3][4], int level) {
   float t[5];
 #pragma unroll
-  for (int s2 = 1; s2 <= 4; ++s2) {
+  for (int s2 = 0; s2 <= 4; ++s2) {
     float acc = 0.f;
 #pragma unroll
     for (int j = 0; j < 4; ++j)
@@ -680,7 +680,12 @@ __device__ __forceinline__ float mass_of(const float (&tp)[3][4]) {
         if (j + k <= s2) acc = fmaf(tp[1][j], tp[2][k], acc);
     t[s2] = acc;
   }
-  return tp[0][0] * t[4] + tp[0][1] * t[3] + tp[0][2] * t[2] + tp[0][3] * t[1];
+  float m = 0.f;
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+    if (i <= level) m += tp[0][i] * (level - i == 4 ? t[4] : level - i == 3 ? t[3]
+                                     : level - i == 2 ? t[2] : level - i == 1 ? t[1] : t[0]);
+  return m;
 }
 
 // The same mass from a voxel's own probabilities and per-axis lists top[a][0..3].
@@ -690,7 +695,7 @@ __device__ __forceinline__ float kept_mass(const float (&p)[kHeads], const int (
   for (int a = 0; a < 3; ++a)
 #pragma unroll
     for (int r = 0; r < 4; ++r) tp[a][r] = pick(p, a, top[a][r]);
-  return mass_of(tp);
+  return mass_of(tp, 4);
 }
 
 // The proposal of one voxel on its own (the testing hook reports it): its 4 most probable
@@ -740,7 +745,7 @@ constexpr int kProbStride = kHeads;  // 33 floats per lane row: column reads are
 // The proposal of one row segment (30 voxels along y) of a block anchor row: the segment's
 // per-axis probabilities summed over its voxels, the 4 most probable offsets per axis of the sums
 // (offset index 0..10, ties to the lower offset), and each voxel's own probability mass on the
-// resulting 32 rank triples. Rows share the proposal of their block's anchor row: blocks of
+// resulting rank triples (i + j + k <= level). Rows share the proposal of their block's anchor row: blocks of
 // `block` x `block` rows in (z, x), anchored at their middle row (clamped to the interior).
 struct RowProp {
   signed char top[12];  // [axis][rank]
@@ -754,7 +759,8 @@ __device__ __forceinline__ int anchor_of(int b, int block, int extent) {
 
 __global__ void __launch_bounds__(kRescoreWarps * 32)
     propose_rows_kernel(const __nv_bfloat16 *__restrict__ f4, const __nv_bfloat16 *__restrict__ wbf,
-                        int nx, int ny, int nz, int block, RowProp *__restrict__ props) {
+                        int nx, int ny, int nz, int block, int level,
+                        RowProp *__restrict__ props) {
   __shared__ __align__(16) float hw[kHeadFloats];
   __shared__ float s_prob[kRescoreWarps * 32 * kProbStride];
   __shared__ float s_sum[kRescoreWarps * 36];
@@ -831,7 +837,7 @@ __global__ void __launch_bounds__(kRescoreWarps * 32)
       for (int a = 0; a < 3; ++a)
 #pragma unroll
         for (int r = 0; r < 4; ++r) tp[a][r] = wp[lane * kProbStride + a * kAxis + wtop[a * 4 + r]];
-      rp.conf[lane - 1] = mass_of(tp);
+      rp.conf[lane - 1] = mass_of(tp, level);
     } else if (lane >= 1 && lane <= kRowOut) {
       rp.conf[lane - 1] = 0.f;
     }
@@ -842,8 +848,8 @@ __global__ void __launch_bounds__(kRescoreWarps * 32)
 // Exact FP32 rescoring of one atlas. A warp owns a row segment (z, x, y0 .. y0+29) of interior
 // voxels; lane l sits at y = y0 - 1 + l (lanes 0 and 31 are the y halo). Every voxel of the
 // segment computes its per-axis probabilities; their sums over the segment give the row's
-// proposal: per axis the 4 most probable offsets, and the 32 rank triples with i + j + k <= 4.
-// A voxel whose own probability mass on those 32 is below conf_thr falls back to all 11^3
+// proposal: per axis the 4 most probable offsets, and the rank triples with i + j + k <= level.
+// A voxel whose own probability mass on those is below conf_thr falls back to all 11^3
 // offsets. Each offset is evaluated once for all 32 lanes: D(y) = sum over the 3x3 (dz, dx) taps
 // of the squared differences at y, then SSD(y) = D(y-1) + D(y) + D(y+1) by warp shuffles; a lane
 // adds the weight exp(-SSD/div) and the weighted CT value for the offsets it keeps.
@@ -869,7 +875,8 @@ __device__ __forceinline__ void eval_offset(const float *__restrict__ atl,
 }
 
 __global__ void __launch_bounds__(kRescoreWarps * 32, 3)
-    rescore_kernel(const RowProp *__restrict__ props, int block, const float *__restrict__ img,
+    rescore_kernel(const RowProp *__restrict__ props, int block, int level,
+                   const float *__restrict__ img,
                    const float *__restrict__ atl, const float *__restrict__ lab, int nx, int ny,
                    int nz, int apitch, float neg_k, float conf_thr, float *__restrict__ pacc,
                    float *__restrict__ wacc, unsigned long long *__restrict__ fallbacks,
@@ -912,18 +919,22 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 3)
     const long long vz = (long long)(z - 1) * axy + (long long)(x - 1) * apitch;  // (dz,dx)=(-1,-1)
     float P = 0.f, W = 0.f;
     if (!any_full) {
-      // the 32 kept offsets, in rank-triple order
+      // the kept offsets, in rank-triple order
+      int kept = 0;
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j + i < 5 && j < 4; ++j)
 #pragma unroll
           for (int k = 0; k + j + i < 5 && k < 4; ++k)
-            eval_offset(atl, lab, in, vz + axy + apitch, axy, apitch, yc, top[0][i] - 5,
-                        top[1][j] - 5, top[2][k] - 5, out_lane, P, W, neg_k);
-      my_evals += 32;
+            if (i + j + k <= level) {
+              eval_offset(atl, lab, in, vz + axy + apitch, axy, apitch, yc, top[0][i] - 5,
+                          top[1][j] - 5, top[2][k] - 5, out_lane, P, W, neg_k);
+              ++kept;
+            }
+      my_evals += kept;
     } else {
-      // the full window; lanes that did not fall back keep only their row's 32
+      // the full window; lanes that did not fall back keep only their row's kept set
       unsigned long long rank[3];
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
@@ -939,7 +950,7 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 3)
         for (int ju = 0; ju < kAxis; ++ju) {
           const int ru = rw + (int)((rank[1] >> (4 * ju)) & 0xF);
           for (int jv = 0; jv < kAxis; ++jv) {
-            const bool mine = full || (ru + (int)((rank[2] >> (4 * jv)) & 0xF) <= 4);
+            const bool mine = full || (ru + (int)((rank[2] >> (4 * jv)) & 0xF) <= level);
             eval_offset(atl, lab, in, vz + axy + apitch, axy, apitch, yc, jw - 5, ju - 5, jv - 5,
                         mine && out_lane, P, W, neg_k);
           }
@@ -963,13 +974,16 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 3)
 // sums z in registers, x across the shared rows and y by warp shuffles.
 constexpr int kRows = 4;
 
-// The kept set's rank triples (i, j, k), i + j + k <= 4, packed as i | j << 2 | k << 4, in the
-// order the single-row kernel visits them.
+// The kept set's rank triples (i, j, k), i + j + k <= 4, packed as i | j << 2 | k << 4, in
+// order of rank sum: the first 10, 20 or 32 are the kept sets of levels 2, 3 and 4.
 __constant__ unsigned char kRankTriples[kTopK] = {
-    0x00, 0x10, 0x20, 0x30, 0x04, 0x14, 0x24, 0x34, 0x08, 0x18, 0x28, 0x0c, 0x1c,
-    0x01, 0x11, 0x21, 0x31, 0x05, 0x15, 0x25, 0x09, 0x19, 0x0d,
-    0x02, 0x12, 0x22, 0x06, 0x16, 0x0a,
-    0x03, 0x13, 0x07};
+    0x00, 0x01, 0x04, 0x10, 0x02, 0x05, 0x08, 0x11, 0x14, 0x20, 0x03, 0x06, 0x09, 0x0c, 0x12, 0x15,
+    0x18, 0x21, 0x24, 0x30, 0x07, 0x0a, 0x0d, 0x13, 0x16, 0x19, 0x1c, 0x22, 0x25, 0x28, 0x31, 0x34};
+
+// Offsets kept at a level (i + j + k <= level): 10, 20 or 32.
+__host__ __device__ __forceinline__ int kept_count(int level) {
+  return level <= 2 ? 10 : level == 3 ? 20 : 32;
+}
 
 __device__ __forceinline__ int pick4(const int (&t)[4], int i) {
   return i == 0 ? t[0] : i == 1 ? t[1] : i == 2 ? t[2] : t[3];
@@ -1011,12 +1025,12 @@ __device__ __forceinline__ void eval_offset4(const float *__restrict__ a,
 // the last interior row, the rows the previous item owns left out, so no load needs a clamp.
 // Needs at least 4 interior x-rows and an atlas volume below 2^31 voxels (32-bit offsets).
 __global__ void __launch_bounds__(kRescoreWarps * 32, 4)
-    rescore4_kernel(const RowProp *__restrict__ props, const float *__restrict__ img,
+    rescore4_kernel(const RowProp *__restrict__ props, int level, const float *__restrict__ img,
                     const float *__restrict__ atl, const float *__restrict__ lab, int nx, int ny,
                     int nz, int apitch, float scale, float conf_thr, float *__restrict__ pacc,
                     float *__restrict__ wacc, unsigned long long *__restrict__ fallbacks,
                     unsigned long long *__restrict__ evaluated) {
-  __shared__ int s_off[kRescoreWarps][kTopK];  // per warp: the item's 32 offsets, 32-bit
+  __shared__ int s_off[kRescoreWarps][kTopK];  // per warp: the item's kept offsets, 32-bit
   const int lane = threadIdx.x & 31;
   int *w_off = s_off[threadIdx.x >> 5];
   const int lo = 6;
@@ -1077,11 +1091,12 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 4)
     for (int r = 0; r < kRows; ++r) P[r] = W[r] = 0.f;
     if (!any_full) {
 #pragma unroll 2
-      for (int c = 0; c < kTopK; ++c) {
+      const int kept = kept_count(level);
+      for (int c = 0; c < kept; ++c) {
         const int off = w_off[c];
         eval_offset4(ab + off, lb + off, in, axy, apitch, take, scale, P, W);
       }
-      my_evals += (unsigned long long)kTopK * __popc(owned);
+      my_evals += (unsigned long long)kept * __popc(owned);
     } else {
       unsigned long long rank[3];
 #pragma unroll
@@ -1098,7 +1113,7 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 4)
         for (int ju = 0; ju < kAxis; ++ju) {
           const int ru = rw + (int)((rank[1] >> (4 * ju)) & 0xF);
           for (int jv = 0; jv < kAxis; ++jv) {
-            const bool mine = full || (ru + (int)((rank[2] >> (4 * jv)) & 0xF) <= 4);
+            const bool mine = full || (ru + (int)((rank[2] >> (4 * jv)) & 0xF) <= level);
             const int off = (jw - 5) * axy + (ju - 5) * apitch + (jv - 5);
             eval_offset4(ab + off, lb + off, in, axy, apitch, mine ? take : 0u, scale, P, W);
           }
@@ -1386,9 +1401,9 @@ cudaError_t pack_all(const __nv_bfloat16 *wbf, uint32_t *frag, cudaStream_t s) {
 // The learned form over all atlases of `in` (atlas and label rows `in.pitch` floats apart, the
 // input MRI contiguous). Writes the interior of `out`; the border is left untouched.
 cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInputs &in, float *out,
-                           double div, float conf_thr, int block, bool every_voxel, void *scratch,
-                           int *err, cudaStream_t s) {
-  if (block < 1) return cudaErrorInvalidValue;
+                           double div, float conf_thr, int block, int level, bool every_voxel,
+                           void *scratch, int *err, cudaStream_t s) {
+  if (block < 1 || level < 2 || level > 4) return cudaErrorInvalidValue;
   const __nv_bfloat16 *wbf = static_cast<const __nv_bfloat16 *>(weights);
   const long long nvox = g.nvox();
   const long long astride = (long long)g.nz * g.nx * in.pitch;
@@ -1427,16 +1442,16 @@ cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInp
     if ((e = run_convs(g, wbf, A, in.pitch, sc, err, plan, &f4, s)) != cudaSuccess)
       return e;
     propose_rows_kernel<<<propose_blocks, kRescoreWarps * 32, 0, s>>>(f4, wbf, g.nx, g.ny, g.nz,
-                                                                      block, sc.props);
+                                                                      block, level, sc.props);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (block == kRows && g.nx - 12 >= kRows &&
         (long long)g.nz * g.nx * in.pitch < (1LL << 31) - 1) {
       rescore4_kernel<<<rescore_blocks, kRescoreWarps * 32, 0, s>>>(
-          sc.props, in.img, A, L, g.nx, g.ny, g.nz, in.pitch, scale, conf_thr, sc.pacc, sc.wacc,
+          sc.props, level, in.img, A, L, g.nx, g.ny, g.nz, in.pitch, scale, conf_thr, sc.pacc, sc.wacc,
           sc.fallbacks, sc.evaluated);
     } else {
       rescore_kernel<<<rescore_blocks, kRescoreWarps * 32, 0, s>>>(
-          sc.props, block, in.img, A, L, g.nx, g.ny, g.nz, in.pitch, neg_k, conf_thr, sc.pacc,
+          sc.props, block, level, in.img, A, L, g.nx, g.ny, g.nz, in.pitch, neg_k, conf_thr, sc.pacc,
           sc.wacc, sc.fallbacks, sc.evaluated);
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return e;

@@ -221,11 +221,16 @@ def structured_samples(images, num_atlas: int, n: int, seed: int) -> np.ndarray:
     return smp[rng.permutation(len(smp))].astype(np.int32)
 
 
-def rank_sum_set(top: np.ndarray) -> np.ndarray:
-    """The 32 kept offsets of one proposal, top [3][4] (dw, du, dv in rank order): rank triples
-    (i, j, k) with i + j + k <= 4. Returns [32][3] offsets in -5..5."""
-    out = [(top[0][i], top[1][j], top[2][k]) for i in range(4) for j in range(4) for k in range(4)
-           if i + j + k <= 4]
+KEPT_LEVEL = {10: 2, 20: 3, 32: 4}
+
+
+def rank_sum_set(top: np.ndarray, k: int = 32) -> np.ndarray:
+    """The kept offsets of one proposal, top [3][4] (dw, du, dv in rank order): rank triples
+    (i, j, l) with i + j + l <= 4 for k = 32 (3 for k = 20, 2 for k = 10). Returns [k][3]
+    offsets in -5..5."""
+    level = KEPT_LEVEL[k]
+    out = [(top[0][i], top[1][j], top[2][l]) for i in range(4) for j in range(4) for l in range(4)
+           if i + j + l <= level]
     return np.array(out, np.int64)
 
 

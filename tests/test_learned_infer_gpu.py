@@ -3,8 +3,8 @@
 * With every pair forced to the full search (threshold above 1) the form is the plain method and
   must match the FP64 oracle within the plain gate (1e-4 relative).
 * With a fixed "prior" network (zero convolutions, head biases only) every voxel and every row
-  gets the same 32 offsets, so the output has an exact float64 restatement: the fusion over
-  those offsets.
+  gets the same k offsets (32, 20 or 10), so the output has an exact float64 restatement: the
+  fusion over those offsets.
 * The committed trained network beats the same-k baselines without it (the centre prior and an
   untrained network) in recall of the plain method's top-32 and in error against the plain
   method.
@@ -36,8 +36,9 @@ def subject(nx, ny, nz, num, seed):
 prior_params = learned.prior_params
 
 
-def prior_proposal(scales=(0.7, 0.5, 0.3)):
-    """Offsets in rank order per axis and the confidence, in float64 (ties: lower offset first)."""
+def prior_proposal(scales=(0.7, 0.5, 0.3), k=32):
+    """Offsets in rank order per axis and the confidence of the k kept offsets, in float64 (ties:
+    lower offset first)."""
     top, probs = [], []
     for c in scales:
         logits = np.array([-c * (j - 5) ** 2 for j in range(11)], np.float64)
@@ -46,8 +47,9 @@ def prior_proposal(scales=(0.7, 0.5, 0.3)):
         order = sorted(range(11), key=lambda j: (-p[j], j))[:4]
         top.append([j - 5 for j in order])
         probs.append([p[j] for j in order])
-    conf = sum(probs[0][i] * probs[1][j] * probs[2][k] for i in range(4) for j in range(4)
-               for k in range(4) if i + j + k <= 4)
+    level = learned.KEPT_LEVEL[k]
+    conf = sum(probs[0][i] * probs[1][j] * probs[2][l] for i in range(4) for j in range(4)
+               for l in range(4) if i + j + l <= level)
     return np.array(top), conf
 
 
@@ -109,6 +111,10 @@ def test_attach_rules():
             h.attach_model(None)
             with pytest.raises(pct.PctError):
                 h.synthesize(img, atl, lab, NH, DIV, pct.EXEC_LEARNED)
+        for bad in (0, 16, 33):
+            with pytest.raises(pct.PctError) as e:
+                h.set_learned_k(bad)
+            assert e.value.status == -1
 
 
 @pytest.mark.parametrize("shape", [(36, 41, 30, 2), (44, 70, 33, 3)])
@@ -125,28 +131,33 @@ def test_full_fallback_is_the_plain_method(shape):
     assert st["row_offsets"] == rows_of(nx, ny, nz) * 1331 * num
 
 
-def test_prior_proposal_exact():
+@pytest.mark.parametrize("k,block", [(32, 4), (20, 4), (10, 4), (20, 1)])
+def test_prior_proposal_exact(k, block):
     nx, ny, nz, num = 40, 47, 32, 2
     img, atl, lab = subject(nx, ny, nz, num, 21)
-    top, conf = prior_proposal()
-    offsets = learned.rank_sum_set(top)
-    assert len({tuple(o) for o in offsets}) == 32
+    top, conf = prior_proposal(k=k)
+    offsets = learned.rank_sum_set(top, k)
+    assert len({tuple(o) for o in offsets}) == k
     ref, prod, sumw = fuse_offsets_f64(img, atl, lab, offsets, DIV)
     with pct.Handle(0) as h, learned.LearnedModel(0, params=prior_params()) as m:
         h.attach_model(m, 0.0)
+        h.set_learned_k(k)
+        h.set_learned_block(block)
         got = h.synthesize(img, atl, lab, NH, DIV, pct.EXEC_LEARNED)
         st = h.learned_stats()
     compare_fused(got, ref, NH, 1e-4, prod, sumw)
     assert st["fallback_pairs"] == 0
-    assert st["row_offsets"] == rows_of(nx, ny, nz) * 32 * num
+    assert st["row_offsets"] == rows_of(nx, ny, nz) * k * num
 
 
-def test_confidence_threshold():
+@pytest.mark.parametrize("k", [32, 20])
+def test_confidence_threshold(k):
     nx, ny, nz, num = 34, 37, 29, 1
     img, atl, lab = subject(nx, ny, nz, num, 31)
-    _, conf = prior_proposal()
+    _, conf = prior_proposal(k=k)
     ref = oracle.fuse_port(img, atl, lab, NH, DIV)
     with pct.Handle(0) as h, learned.LearnedModel(0, params=prior_params()) as m:
+        h.set_learned_k(k)
         h.attach_model(m, conf * (1 - 1e-3))
         h.synthesize(img, atl, lab, NH, DIV, pct.EXEC_LEARNED)
         assert h.learned_stats()["fallback_pairs"] == 0
