@@ -1024,8 +1024,9 @@ __device__ __forceinline__ void eval_offset4(const float *__restrict__ a,
 // Items are 4 x-rows of one z plane; the last item of an x-row band is shifted back to end at
 // the last interior row, the rows the previous item owns left out, so no load needs a clamp.
 // Needs at least 4 interior x-rows and an atlas volume below 2^31 voxels (32-bit offsets).
+template <int LEVEL>
 __global__ void __launch_bounds__(kRescoreWarps * 32, 4)
-    rescore4_kernel(const RowProp *__restrict__ props, int level, const float *__restrict__ img,
+    rescore4_kernel(const RowProp *__restrict__ props, const float *__restrict__ img,
                     const float *__restrict__ atl, const float *__restrict__ lab, int nx, int ny,
                     int nz, int apitch, float scale, float conf_thr, float *__restrict__ pacc,
                     float *__restrict__ wacc, unsigned long long *__restrict__ fallbacks,
@@ -1090,8 +1091,8 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 4)
 #pragma unroll
     for (int r = 0; r < kRows; ++r) P[r] = W[r] = 0.f;
     if (!any_full) {
+      constexpr int kept = LEVEL <= 2 ? 10 : LEVEL == 3 ? 20 : 32;
 #pragma unroll 2
-      const int kept = kept_count(level);
       for (int c = 0; c < kept; ++c) {
         const int off = w_off[c];
         eval_offset4(ab + off, lb + off, in, axy, apitch, take, scale, P, W);
@@ -1113,7 +1114,7 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 4)
         for (int ju = 0; ju < kAxis; ++ju) {
           const int ru = rw + (int)((rank[1] >> (4 * ju)) & 0xF);
           for (int jv = 0; jv < kAxis; ++jv) {
-            const bool mine = full || (ru + (int)((rank[2] >> (4 * jv)) & 0xF) <= level);
+            const bool mine = full || (ru + (int)((rank[2] >> (4 * jv)) & 0xF) <= LEVEL);
             const int off = (jw - 5) * axy + (ju - 5) * apitch + (jv - 5);
             eval_offset4(ab + off, lb + off, in, axy, apitch, mine ? take : 0u, scale, P, W);
           }
@@ -1446,8 +1447,9 @@ cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInp
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (block == kRows && g.nx - 12 >= kRows &&
         (long long)g.nz * g.nx * in.pitch < (1LL << 31) - 1) {
-      rescore4_kernel<<<rescore_blocks, kRescoreWarps * 32, 0, s>>>(
-          sc.props, level, in.img, A, L, g.nx, g.ny, g.nz, in.pitch, scale, conf_thr, sc.pacc, sc.wacc,
+      auto k4 = level == 2 ? rescore4_kernel<2> : level == 3 ? rescore4_kernel<3> : rescore4_kernel<4>;
+      k4<<<rescore_blocks, kRescoreWarps * 32, 0, s>>>(
+          sc.props, in.img, A, L, g.nx, g.ny, g.nz, in.pitch, scale, conf_thr, sc.pacc, sc.wacc,
           sc.fallbacks, sc.evaluated);
     } else {
       rescore_kernel<<<rescore_blocks, kRescoreWarps * 32, 0, s>>>(
