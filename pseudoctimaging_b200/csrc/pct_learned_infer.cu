@@ -575,6 +575,232 @@ __global__ void __launch_bounds__(kCvThreads, 2)
   }
 }
 
+// Variant for layers whose planes are needed in short runs (isolated anchor planes, or 3 around
+// them): the accumulators of two consecutive output planes are double-buffered (64 columns
+// each) instead of forming the three-plane ring, so an output plane costs 54 MMAs of N <= 48 (an
+// input row at one y shift feeds up to 3 output rows of one plane through one MMA, weights stored
+// per (kz, ky) as W(kx = 2) | W(kx = 1) | W(kx = 0)) but no output waits for another's epilogue;
+// input planes stream through a 4-slot ring, so an item's three planes are all in flight.
+constexpr int kRwRing = 4;
+constexpr int kRwSeq = 2 * 48 * 16;                     // one (kz, ky) weight sequence
+constexpr int kRwWBytes = 9 * kRwSeq;                   // 13,824 B
+constexpr int kRwCols = 2 * kCvTX * 16;                 // two accumulators
+constexpr size_t kRwSmem = 128 + kRwRing * kCvPlane + kRwWBytes + 128;  // 2 CTAs per SM
+constexpr int kRwFragWords = kRwWBytes / 4;
+
+// conv16_rows_kernel weight sequences of one layer, byte offset ((kz * 3 + ky) * 2 + h) * 768 + n * 16 + 2 c8 holds
+// W[co][8h + c8][kz * 9 + kx * 3 + ky] for n = 16 (2 - kx) + co.
+__global__ void pack_rows_kernel(const __nv_bfloat16 *__restrict__ wbf, int woff,
+                                  uint32_t *__restrict__ frag) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= kRwFragWords) return;
+  const int off = 4 * i;
+  const int sq = off / kRwSeq, h = (off % kRwSeq) / 768, n = (off % 768) / 16, c8 = (off % 16) / 2;
+  const int kz = sq / 3, ky = sq % 3, kx = 2 - n / 16, co = n % 16, ci = 8 * h + c8;
+  const int t = kz * 9 + kx * 3 + ky;
+  const __nv_bfloat16 lo = wbf[woff + (co * kC + ci) * 27 + t];
+  const __nv_bfloat16 hi = wbf[woff + (co * kC + ci + 1) * 27 + t];
+  frag[i] = (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+}
+
+// The output region of one layer: work items {x tile | y tile << 16, first plane | planes << 16}
+
+__global__ void __launch_bounds__(kCvThreads, 2)
+    conv16_rows_kernel(const __grid_constant__ CUtensorMap tm, const uint32_t *__restrict__ frag,
+                  const __nv_bfloat16 *__restrict__ wbf, int boff, __nv_bfloat16 *__restrict__ out,
+                  ConvGrid g, int *__restrict__ err) {
+  extern __shared__ unsigned char smem_raw[];
+  const uint32_t raw = ptx::smem_u32(smem_raw);
+  const uint32_t base = (raw + 127u) & ~127u;
+  const uint32_t wtab = base + kRwRing * kCvPlane;
+  // barriers: full[kRwRing], empty[kRwRing], dfull[2], dempty[2]
+  const uint32_t full0 = wtab + kRwWBytes, empty0 = full0 + 8 * kRwRing;
+  const uint32_t dfull0 = empty0 + 8 * kRwRing, dempty0 = dfull0 + 16;
+  unsigned char *gen = smem_raw + (dempty0 + 16 - raw);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(gen);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(gen + 4);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+
+  // weight sequences into shared memory (visible to the tensor core through the async proxy)
+  {
+    uint32_t *w = reinterpret_cast<uint32_t *>(smem_raw + (wtab - raw));
+    for (int i = threadIdx.x; i < kRwFragWords; i += kCvThreads) w[i] = __ldg(frag + i);
+    ptx::fence_proxy_async_smem();
+  }
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kRwRing; ++i) {
+      ptx::mbar_init(full0 + 8 * i, 1);
+      ptx::mbar_init(empty0 + 8 * i, 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      ptx::mbar_init(dfull0 + 8 * i, 1);
+      ptx::mbar_init(dempty0 + 8 * i, 4);
+    }
+    *abort_flag = 0;
+    ptx::fence_mbarrier_init();
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     ptx::smem_u32(tmem_slot)),
+                 "r"(kRwCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc5::fence_before();
+  __syncthreads();
+  tc5::fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 4) {
+    // TMA producer: the input planes z0 - 1 .. z0 + planes of every item, in order, into the ring
+    if (lane == 0) {
+      uint32_t j = 0;  // planes issued
+      for (int it = blockIdx.x; it < g.n_items && !*abort_flag; it += gridDim.x) {
+        const ConvItem c = conv_item(g, it);
+        for (int p = 0; p < c.planes + 2; ++p, ++j) {
+          const uint32_t slot = j % kRwRing;
+          if (j >= kRwRing &&
+              !ptx::mbar_wait_bounded(empty0 + 8 * slot, ((j / kRwRing) - 1) & 1, kConvTimeoutNs)) {
+            *abort_flag = 1;
+            break;
+          }
+          ptx::mbar_arrive_expect_tx(full0 + 8 * slot, kCvPlane);
+          ptx::tma_load_4d(base + slot * kCvPlane, &tm, full0 + 8 * slot, 2 * (c.y0 - 1), c.x0 - 1,
+                           c.z0 - 1 + p, 0);
+        }
+      }
+      // planes still landing: wait for the last ring's worth (bounded)
+      for (uint32_t q = j > kRwRing ? j - kRwRing : 0; q < j; ++q)
+        ptx::mbar_wait_bounded(full0 + 8 * (q % kRwRing), (q / kRwRing) & 1, kConvTimeoutNs);
+    }
+  } else if (warp == 5) {
+    // MMA issuer: the whole warp runs the loop, one elected lane issues
+    {
+      uint32_t j0 = 0, t = 0;  // first ring load of the item, output planes issued
+      const uint64_t db0 = tc5::desc(wtab, 768, 128);
+      for (int it = blockIdx.x; it < g.n_items && !*abort_flag; it += gridDim.x) {
+        const ConvItem c = conv_item(g, it);
+        for (int i = 0; i < c.planes; ++i, ++t) {
+          const int b = t & 1;
+          bool ok = ptx::mbar_wait_bounded(dempty0 + 8 * b, (t >> 1) & 1, kConvTimeoutNs);
+          uint64_t da[3];
+#pragma unroll
+          for (int kz = 0; kz < 3; ++kz) {
+            const uint32_t q = j0 + i + kz;
+            ok = ok && ptx::mbar_wait_bounded(full0 + 8 * (q % kRwRing), (q / kRwRing) & 1,
+                                               kConvTimeoutNs);
+            da[kz] = tc5::desc(base + (q % kRwRing) * kCvPlane, kCvHalf, 128);
+          }
+          if (!ok) {
+            *abort_flag = 1;
+            break;
+          }
+          tc5::fence_after();
+          const uint32_t dcol = tmem + b * (kCvTX * 16);
+#pragma unroll 1
+          for (int ix = 0; ix < kCvSX; ++ix) {
+            // output rows fed by input row ix: o = ix - kx, kx = 2..0, within the item's mask
+            int o_lo = ix - 2 < 0 ? 0 : ix - 2, o_hi = ix < kCvTX - 1 ? ix : kCvTX - 1;
+            while (o_lo <= o_hi && !((c.mask >> o_lo) & 1u)) ++o_lo;
+            while (o_hi >= o_lo && !((c.mask >> o_hi) & 1u)) --o_hi;
+            if (o_lo > o_hi) continue;
+            const uint32_t id = tc5::idesc_bf16(16 * (o_hi - o_lo + 1));
+            const uint32_t d = dcol + 16 * o_lo;
+            // descriptor start fields count 16-byte units
+            const uint64_t db = db0 + (uint64_t)((o_lo - ix + 2) * 16);
+#pragma unroll
+            for (int sq = 0; sq < 9; ++sq) {
+              const int kz = sq / 3, ky = sq % 3;
+              tc5::mma(d, da[kz] + (uint64_t)(ix * kCvSY + ky), db + (uint64_t)(sq * kRwSeq / 16),
+                       id);
+            }
+          }
+          tc5::commit(dfull0 + 8 * b);
+          // plane j0 + i feeds no later output of the item; the last output frees all three
+          tc5::commit(empty0 + 8 * ((j0 + i) % kRwRing));
+          if (i == c.planes - 1) {
+            tc5::commit(empty0 + 8 * ((j0 + i + 1) % kRwRing));
+            tc5::commit(empty0 + 8 * ((j0 + i + 2) % kRwRing));
+          }
+        }
+        j0 += c.planes + 2;
+      }
+      // let every issued MMA finish before the accumulators are released (bounded)
+      if (t > 0) ptx::mbar_wait_bounded(dfull0 + 8 * ((t - 1) & 1), ((t - 1) >> 1) & 1, kConvTimeoutNs);
+    }
+  } else {
+    // epilogue: warp w reads TMEM lanes 32w..32w+31 = output y0 + 32w + lane
+    const uint32_t lane_addr = tmem + ((uint32_t)(32 * warp) << 16);
+    float bias[kC];
+#pragma unroll
+    for (int c = 0; c < kC; ++c) bias[c] = __bfloat162float(wbf[boff + c]);
+    // both accumulators start at zero
+#pragma unroll
+    for (int q = 0; q < kRwCols / 16; ++q) tc5::st16_zero(lane_addr + 16 * q);
+    tc5::wait_st();
+    tc5::fence_before();
+    __syncwarp();
+    if (lane == 0) {
+      ptx::mbar_arrive(dempty0);
+      ptx::mbar_arrive(dempty0 + 8);
+    }
+    uint32_t t = 0;
+    bool stop = false;
+    for (int it = blockIdx.x; it < g.n_items && !stop; it += gridDim.x) {
+      const ConvItem c = conv_item(g, it);
+      const int y = c.y0 + 32 * warp + lane;
+      const bool y_ok = y < g.y_hi && 32 * warp + lane < kCvTY;
+      for (int i = 0; i < c.planes; ++i, ++t) {
+        const int b = t & 1;
+        if (!ptx::mbar_wait_bounded(dfull0 + 8 * b, (t >> 1) & 1, kConvTimeoutNs)) {
+          *abort_flag = 1;
+          stop = true;
+          break;
+        }
+        tc5::fence_after();
+        const int z = c.z0 + i;
+        const uint32_t acc = lane_addr + b * (kCvTX * 16);
+        uint32_t r[kCvTX][16];
+#pragma unroll
+        for (int o = 0; o < kCvTX; ++o) tc5::ld16(acc + 16 * o, r[o]);
+        tc5::wait_ld();
+#pragma unroll
+        for (int o = 0; o < kCvTX; ++o) {
+          const int x = c.x0 + o;
+          if (((c.mask >> o) & 1u) && x < g.nx && y_ok) {
+            uint32_t h[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+              const float v0 = fmaxf(__uint_as_float(r[o][2 * q]) + bias[2 * q], 0.f);
+              const float v1 = fmaxf(__uint_as_float(r[o][2 * q + 1]) + bias[2 * q + 1], 0.f);
+              const __nv_bfloat162 pr = __floats2bfloat162_rn(v0, v1);
+              h[q] = *reinterpret_cast<const uint32_t *>(&pr);
+            }
+            const long long v = ((long long)z * g.nx + x) * g.ny + y;
+            *reinterpret_cast<uint4 *>(out + v * 8) = make_uint4(h[0], h[1], h[2], h[3]);
+            *reinterpret_cast<uint4 *>(out + (g.nvox + v) * 8) =
+                make_uint4(h[4], h[5], h[6], h[7]);
+          }
+        }
+#pragma unroll
+        for (int o = 0; o < kCvTX; ++o) tc5::st16_zero(acc + 16 * o);
+        tc5::wait_st();
+        tc5::fence_before();
+        __syncwarp();
+        if (lane == 0) ptx::mbar_arrive(dempty0 + 8 * b);
+      }
+    }
+  }
+  tc5::fence_before();
+  __syncthreads();
+  if (*abort_flag && threadIdx.x == 0) atomicExch(err, 3);
+  if (warp == 0) {
+    tc5::fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kRwCols)
+                 : "memory");
+  }
+}
+
 // ---------------------------------------------------------------- proposal + rescoring
 
 // Head weights staged in shared memory by every kernel that proposes, transposed and padded for
@@ -1180,7 +1406,8 @@ struct InferScratch {
 
 // Bytes before the proposal table (features, sums, fragments, counters), 256-aligned.
 size_t infer_base_bytes(long long nvox) {
-  const size_t b = (size_t)nvox * kC * 2 * 2 + (size_t)nvox * 4 * 2 + 3 * kFragWords * 4 + 256 +
+  const size_t b = (size_t)nvox * kC * 2 * 2 + (size_t)nvox * 4 * 2 +
+                   3 * (size_t)(kFragWords + kRwFragWords) * 4 + 256 +
                    (size_t)nvox * kC * 4;
   return (b + 255) / 256 * 256;
 }
@@ -1193,7 +1420,7 @@ InferScratch carve(void *scratch, long long nvox) {
   r.pacc = reinterpret_cast<float *>(r.fb + nvox * kC);
   r.wacc = r.pacc + nvox;
   r.frag = reinterpret_cast<uint32_t *>(r.wacc + nvox);
-  r.fallbacks = reinterpret_cast<unsigned long long *>(r.frag + 3 * kFragWords);
+  r.fallbacks = reinterpret_cast<unsigned long long *>(r.frag + 3 * (kFragWords + kRwFragWords));
   r.evaluated = r.fallbacks + 1;
   r.err = reinterpret_cast<int *>(r.fallbacks + 2);
   r.cimg = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(r.fallbacks) + 256);
@@ -1248,6 +1475,7 @@ struct ConvPlan {
   int c1_z, c1_nz, c1_x, c1_nx;  // conv1 box (z, x; every y)
   int y_lo[3], y_hi[3];
   int n_items[3], item_off[3];   // work items of conv2..conv4 (offset in ints into the lists)
+  bool ring[3];                  // conv16_kernel (plane-slot ring) or conv16_rows_kernel
   bool dense;
 };
 
@@ -1267,6 +1495,11 @@ void add_items(ConvPlan &p, int l, const std::vector<int> &zs, int x_tiles, std:
         i = e;
       }
   p.n_items[l] = (int)((lists.size() - p.item_off[l]) / 2);
+  // the plane-slot ring pays off when items hold runs of planes; short runs (isolated anchor
+  // planes, or 3 around them) take the double-buffered variant
+  long long planes = 0;
+  for (size_t i = p.item_off[l] + 1; i < lists.size(); i += 2) planes += (unsigned)lists[i] >> 16;
+  p.ring[l] = planes >= 4LL * p.n_items[l];
 }
 
 ConvPlan dense_plan(const Geometry &g, std::vector<int> &lists) {
@@ -1377,6 +1610,13 @@ cudaError_t run_convs(const Geometry &g, const __nv_bfloat16 *wbf, const float *
     cg.y_hi = p.y_hi[l];
     if (cg.n_items <= 0) continue;
     const int blocks = cg.n_items < 2 * n_sm ? cg.n_items : 2 * n_sm;
+    if (!p.ring[l]) {
+      conv16_rows_kernel<<<blocks, kCvThreads, kRwSmem, s>>>(
+          maps[l & 1], sc.frag + 3 * kFragWords + l * kRwFragWords, wbf, boffs[l],
+          bufs[(l + 1) & 1], cg, err);
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+      continue;
+    }
     conv16_kernel<<<blocks, kCvThreads, kConvSmem, s>>>(maps[l & 1], sc.frag + l * kFragWords, wbf,
                                                         boffs[l], bufs[(l + 1) & 1], cg, err);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -1388,11 +1628,17 @@ cudaError_t pack_all(const __nv_bfloat16 *wbf, uint32_t *frag, cudaStream_t s) {
   cudaError_t e0 = cudaFuncSetAttribute(conv16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)kConvSmem);
   if (e0 != cudaSuccess) return e0;
+  e0 = cudaFuncSetAttribute(conv16_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)kRwSmem);
+  if (e0 != cudaSuccess) return e0;
   const int woffs[3] = {kW2, kW3, kW4};
   for (int l = 0; l < 3; ++l) {
     pack_frags_kernel<<<(kFragWords + 255) / 256, 256, 0, s>>>(wbf, woffs[l], frag + l * kFragWords);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    pack_rows_kernel<<<(kRwFragWords + 255) / 256, 256, 0, s>>>(
+        wbf, woffs[l], frag + 3 * kFragWords + l * kRwFragWords);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   return cudaSuccess;
 }
@@ -1413,7 +1659,14 @@ cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInp
                                      prop_table_bytes(g));
   cudaError_t e;
   std::vector<int> lists;
-  const ConvPlan plan = every_voxel ? dense_plan(g, lists) : sparse_plan(g, block, lists);
+  ConvPlan plan = sparse_plan(g, block, lists);
+  if (every_voxel) {
+    // whole-volume convolutions with the same kernel per layer as the restricted plan, so that
+    // both give the same values
+    const ConvPlan restricted = plan;
+    plan = dense_plan(g, lists);
+    for (int l = 0; l < 3; ++l) plan.ring[l] = restricted.ring[l];
+  }
   if (lists.size() * sizeof(int) > conv_list_bytes(g)) return cudaErrorInvalidValue;
   if ((e = cudaMemcpyAsync(sc.lists, lists.data(), lists.size() * sizeof(int),
                            cudaMemcpyHostToDevice, s)) != cudaSuccess)
