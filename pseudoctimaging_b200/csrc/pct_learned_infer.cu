@@ -38,160 +38,6 @@ constexpr float kDblEpsilonF = 2.220446049250313080847e-16f;
 
 // ---------------------------------------------------------------- conv1 (tensor cores)
 
-// conv1 as an FP16 implicit GEMM, one input channel per launch: the input-MRI half of the
-// convolution is the same for every atlas, so it runs once per subject (CH = 0) into FP32 partial
-// sums, and each atlas adds its own half (CH = 1). A CTA item is 4 x-rows x 32 y of one z plane
-// (warp w = x-row w, lane = y). Each thread writes its voxel's im2col row of the channel, 27 raw
-// intensities in FP16 (padded to K = 32, out-of-volume taps 0), into shared memory: 64 bytes per
-// row, the 16-byte chunk c of row r stored at chunk c ^ ((r >> 1) & 3) so that ldmatrix phases
-// hit distinct banks. Its warp then runs 2 m-tiles x 2 k-steps x 2 n-tiles of mma m16n8k16
-// (FP16 in, FP32 accumulate) against the channel's BF16 weights widened to FP16 (exact). CH = 0
-// stores the FP32 sums; CH = 1 adds them, applies the network's input scale 1/512 (the layer is
-// linear before its bias), the bias and ReLU, and stores BF16 channel-last. The only rounding
-// beyond the FP32 reference is the FP16 input (relative 2^-11 of the intensity). Only the output
-// box z in [z_lo, z_lo + z_n), x in [x_lo, x_lo + x_n) (every y) is computed.
-constexpr int kC1Warps = 4;
-constexpr int kC1K = 32;
-
-__device__ __forceinline__ void mma_f16_sync(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2,
-                                             uint32_t a3, uint32_t b0, uint32_t b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
-      "{%8, %9}, {%0, %1, %2, %3};"
-      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
-}
-
-__device__ __forceinline__ void ldmatrix_x4_c1(uint32_t addr, uint32_t &r0, uint32_t &r1,
-                                               uint32_t &r2, uint32_t &r3) {
-  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];"
-               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
-               : "r"(addr));
-}
-
-template <int CH>
-__global__ void __launch_bounds__(kC1Warps * 32)
-    conv1_kernel(const float *__restrict__ src, int spitch, const __nv_bfloat16 *__restrict__ wbf,
-                 float *__restrict__ part, __nv_bfloat16 *__restrict__ out, int nx, int ny,
-                 int nz, int z_lo, int z_n, int x_lo, int x_n) {
-  __shared__ __align__(128) unsigned char rows[kC1Warps * 32 * kC1K * 2];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int g = lane >> 2, t = lane & 3;
-  // B fragments (k-step ks, n-tile j, register r): {W[co][CH][k0], W[co][CH][k0 + 1]} as FP16,
-  // co = 8j + g, k0 = 16ks + 8r + 2t (the tap index), zero past 27
-  uint32_t B[2][2][2];
-#pragma unroll
-  for (int ks = 0; ks < 2; ++ks)
-#pragma unroll
-    for (int j = 0; j < 2; ++j)
-#pragma unroll
-      for (int r = 0; r < 2; ++r) {
-        const int co = 8 * j + g, k0 = 16 * ks + 8 * r + 2 * t;
-        const int wb = kW1 + (co * kCin + CH) * 27;
-        const float w0 = k0 < 27 ? __bfloat162float(wbf[wb + k0]) : 0.f;
-        const float w1 = k0 + 1 < 27 ? __bfloat162float(wbf[wb + k0 + 1]) : 0.f;
-        const __half2 h = __floats2half2_rn(w0, w1);
-        B[ks][j][r] = *reinterpret_cast<const uint32_t *>(&h);
-      }
-  float bias[2][2];
-#pragma unroll
-  for (int j = 0; j < 2; ++j)
-#pragma unroll
-    for (int e = 0; e < 2; ++e) bias[j][e] = __bfloat162float(wbf[kB1 + 8 * j + 2 * t + e]);
-  const uint32_t rows_u32 = static_cast<uint32_t>(__cvta_generic_to_shared(rows));
-  const int my_row = tid;
-  const int m = lane >> 3, q = lane & 7;
-  const int ytiles = (ny + 31) / 32, xtiles = (x_n + kC1Warps - 1) / kC1Warps;
-  const long long items = (long long)z_n * xtiles * ytiles;
-  const int nxy = nx * ny;
-  const long long nvox = (long long)nz * nxy;
-  const int sxy = nx * spitch;
-  const int x_hi = x_lo + x_n;
-  for (long long it = blockIdx.x; it < items; it += gridDim.x) {
-    const int y0 = (int)(it % ytiles) * 32;
-    const long long r0 = it / ytiles;
-    const int x = x_lo + (int)(r0 % xtiles) * kC1Warps + warp, z = z_lo + (int)(r0 / xtiles);
-    const int y = y0 + lane;
-    // this voxel's im2col row of channel CH
-    {
-      float v[kC1K];
-      if (z >= 1 && z < nz - 1 && x >= 1 && x < nx - 1 && y >= 1 && y < ny - 1) {
-        // every tap inside the volume: one base pointer, 32-bit tap offsets
-        const float *ps = src + ((long long)z * nx + x) * spitch + y;
-#pragma unroll
-        for (int k = 0; k < 27; ++k)
-          v[k] = __ldg(ps + ((k / 9 - 1) * sxy + ((k / 3) % 3 - 1) * spitch + (k % 3 - 1)));
-      } else {
-#pragma unroll
-        for (int k = 0; k < 27; ++k) {
-          const int zz = z + k / 9 - 1, xx = x + (k / 3) % 3 - 1, yy = y + k % 3 - 1;
-          const bool ok = zz >= 0 && zz < nz && xx >= 0 && xx < nx && yy >= 0 && yy < ny;
-          v[k] = ok ? __ldg(src + ((long long)zz * nx + xx) * spitch + yy) : 0.f;
-        }
-      }
-#pragma unroll
-      for (int k = 27; k < kC1K; ++k) v[k] = 0.f;
-      unsigned char *row = rows + my_row * kC1K * 2;
-#pragma unroll
-      for (int c = 0; c < kC1K / 8; ++c) {
-        uint32_t w[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const __half2 h = __floats2half2_rn(v[8 * c + 2 * e], v[8 * c + 2 * e + 1]);
-          w[e] = *reinterpret_cast<const uint32_t *>(&h);
-        }
-        *reinterpret_cast<uint4 *>(row + ((c ^ ((my_row >> 1) & 3)) << 4)) =
-            make_uint4(w[0], w[1], w[2], w[3]);
-      }
-    }
-    __syncwarp();
-    float acc[2][2][4];
-#pragma unroll
-    for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-      for (int j = 0; j < 2; ++j)
-#pragma unroll
-        for (int e = 0; e < 4; ++e) acc[mt][j][e] = 0.f;
-#pragma unroll
-    for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-      for (int ks = 0; ks < 2; ++ks) {
-        const int r = warp * 32 + mt * 16 + q + 8 * (m & 1);
-        const int c = 2 * ks + (m >> 1);
-        uint32_t a0, a1, a2, a3;
-        ldmatrix_x4_c1(rows_u32 + (uint32_t)(r * kC1K * 2 + ((c ^ ((r >> 1) & 3)) << 4)), a0, a1,
-                       a2, a3);
-#pragma unroll
-        for (int j = 0; j < 2; ++j) mma_f16_sync(acc[mt][j], a0, a1, a2, a3, B[ks][j][0], B[ks][j][1]);
-      }
-    __syncwarp();  // the rows are rewritten by the next item
-    if (x < x_hi) {
-#pragma unroll
-      for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int yy = y0 + mt * 16 + g + 8 * h;
-          if (yy >= ny) continue;
-          const long long v = (long long)z * nxy + (long long)x * ny + yy;
-#pragma unroll
-          for (int j = 0; j < 2; ++j) {
-            float2 *pp = reinterpret_cast<float2 *>(part + v * kC + 8 * j + 2 * t);
-            if (CH == 0) {
-              *pp = make_float2(acc[mt][j][2 * h], acc[mt][j][2 * h + 1]);
-            } else {
-              const float2 pi = *pp;
-              const float v0 = fmaxf(fmaf(acc[mt][j][2 * h] + pi.x, kInScale, bias[j][0]), 0.f);
-              const float v1 =
-                  fmaxf(fmaf(acc[mt][j][2 * h + 1] + pi.y, kInScale, bias[j][1]), 0.f);
-              *reinterpret_cast<__nv_bfloat162 *>(out + ((long long)j * nvox + v) * 8 + 2 * t) =
-                  __floats2bfloat162_rn(v0, v1);
-            }
-          }
-        }
-    }
-  }
-}
-
 // ---------------------------------------------------------------- conv 16 -> 16 (tcgen05)
 
 // Feature volumes are BF16 with the 16 channels split in two halves of 8: half h of voxel v at
@@ -243,7 +89,7 @@ long long conv_items_bound(const Geometry &g) {
 }
 
 size_t conv_list_bytes(const Geometry &g) {
-  return (3 * (size_t)g.nx + 2 * 3 * (size_t)conv_items_bound(g) + 8) * sizeof(int);
+  return (4 * (size_t)g.nx + 2 * 4 * (size_t)conv_items_bound(g) + 8) * sizeof(int);
 }
 
 // Weight sequences of one layer: sequence q = 3 ky + rho, byte offset q * 4608 + h * 2304 +
@@ -269,7 +115,7 @@ __global__ void pack_frags_kernel(const __nv_bfloat16 *__restrict__ wbf, int wof
 // y tiles of 126 from y_lo.
 struct ConvGrid {
   int nx, ny, nz;
-  int y_lo, y_hi;
+  int y_lo, y_hi, tile_y;
   int n_items;
   long long nvox;
   const int2 *items;
@@ -293,7 +139,7 @@ __device__ __forceinline__ ConvItem conv_item(const ConvGrid &g, int i) {
     r.x0 = xi * kCvTX;
     r.mask = 0xFu;
   }
-  r.y0 = g.y_lo + ty * kCvTY;
+  r.y0 = g.y_lo + ty * g.tile_y;
   r.z0 = e.y & 0xFFFF;
   r.planes = (int)((unsigned)e.y >> 16);
   return r;
@@ -801,6 +647,288 @@ __global__ void __launch_bounds__(kCvThreads, 2)
   }
 }
 
+// ---------------------------------------------------------------- conv 2 -> 16 (tcgen05)
+
+// conv1 on tcgen05, as a 3 x 3 (z, x) convolution over 16 "channels" per voxel: for input MRI
+// and atlas MRI c, the raw intensities at y - 1, y, y + 1 (FP16) and five zeros, so the y taps
+// are folded into K and both input channels fill one K = 16 MMA. Items, the TMEM ring of three
+// output-plane accumulators, the weight-sequence rotations and the warp roles follow
+// conv16_kernel, except that the producer warps build each input plane's operand slot in shared
+// memory from the FP32 volumes (the y expansion has no TMA form) and that an item column covers
+// 128 y: 6 MMAs (N = 48 x rows fed) per input plane. The epilogue applies the network's input
+// scale 1/512 to the FP32 sums (the layer is linear before its bias), the bias and ReLU.
+constexpr int kC1Y = 128;                    // output y per item column (M = 128, all stored)
+constexpr int kC1Seq = 2 * kCvSeqRows * 16;  // one rotation: 144 rows x 16 FP16 channels
+constexpr int kC1WBytes = 3 * kC1Seq;        // 13,824 B
+constexpr int kC1Ring = 3;
+constexpr int kC1Threads = 288;  // warps 0-3 epilogue, 4 MMA, 5-8 producers
+constexpr size_t kC1Smem = 128 + kC1Ring * kCvPlane + kC1WBytes + 128;  // 2 CTAs per SM
+constexpr int kC1FragWords = kC1WBytes / 4;
+
+// conv1 weight sequences: rotation rho, byte offset rho * 4608 + h * 2304 + n * 16 + 2 c holds
+// (c < 3) W1[co][h][kz * 9 + kx * 3 + c] as FP16 (c = y tap, h = input channel) for row
+// n = 16 (3 kxi + r) + co, kx = 2 - kxi, kz = (rho - r) mod 3.
+__global__ void pack_c1_kernel(const __nv_bfloat16 *__restrict__ wbf, uint32_t *__restrict__ frag) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= kC1FragWords) return;
+  const int off = 4 * i;
+  const int rho = off / kC1Seq, h = (off % kC1Seq) / (kCvSeqRows * 16);
+  const int n = (off % (kCvSeqRows * 16)) / 16, c = (off % 16) / 2;
+  const int blk = n / 16, co = n % 16;
+  const int kx = 2 - blk / 3, r = blk % 3, kz = (rho - r + 3) % 3;
+  const int wb = kW1 + (co * kCin + h) * 27 + kz * 9 + kx * 3;
+  const float w0 = c < 3 ? __bfloat162float(wbf[wb + c]) : 0.f;
+  const float w1 = c + 1 < 3 ? __bfloat162float(wbf[wb + c + 1]) : 0.f;
+  const __half2 hw = __floats2half2_rn(w0, w1);
+  frag[i] = *reinterpret_cast<const uint32_t *>(&hw);
+}
+
+__device__ __forceinline__ uint32_t idesc_f16(int n) {
+  // D FP32, A and B FP16 (K-major), N, M = 128
+  return (1u << 4) | ((uint32_t)(n >> 3) << 17) | ((128u >> 4) << 24);
+}
+
+__global__ void __launch_bounds__(kC1Threads, 2)
+    conv1_tc_kernel(const float *__restrict__ img, const float *__restrict__ atl, int apitch,
+                    const uint32_t *__restrict__ frag, const __nv_bfloat16 *__restrict__ wbf,
+                    __nv_bfloat16 *__restrict__ out, ConvGrid g, int *__restrict__ err) {
+  extern __shared__ unsigned char smem_raw[];
+  const uint32_t raw = ptx::smem_u32(smem_raw);
+  const uint32_t base = (raw + 127u) & ~127u;
+  const uint32_t wtab = base + kC1Ring * kCvPlane;
+  // barriers: full[ring] (4 producer warps), empty[ring], mdone, zeroed[3]
+  const uint32_t full0 = wtab + kC1WBytes, empty0 = full0 + 8 * kC1Ring;
+  const uint32_t mdone = empty0 + 8 * kC1Ring, zeroed0 = mdone + 8;
+  unsigned char *gen = smem_raw + (zeroed0 + 24 - raw);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(gen);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(gen + 4);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+
+  {
+    uint32_t *w = reinterpret_cast<uint32_t *>(smem_raw + (wtab - raw));
+    for (int i = threadIdx.x; i < kC1FragWords; i += kC1Threads) w[i] = __ldg(frag + i);
+    ptx::fence_proxy_async_smem();
+  }
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kC1Ring; ++i) {
+      ptx::mbar_init(full0 + 8 * i, 4);
+      ptx::mbar_init(empty0 + 8 * i, 1);
+    }
+    ptx::mbar_init(mdone, 1);
+    for (int i = 0; i < 3; ++i) ptx::mbar_init(zeroed0 + 8 * i, 4);
+    *abort_flag = 0;
+    ptx::fence_mbarrier_init();
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     ptx::smem_u32(tmem_slot)),
+                 "r"(kCvCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc5::fence_before();
+  __syncthreads();
+  tc5::fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp >= 5) {
+    // producers: thread tp builds the operand rows of y = y0 + tp for the 6 x-rows of a plane
+    const int tp = threadIdx.x - 160;
+    unsigned char *slots = smem_raw + (base - raw);
+    uint32_t j = 0;
+    bool stop = false;
+    for (int it = blockIdx.x; it < g.n_items && !stop && !*abort_flag; it += gridDim.x) {
+      const ConvItem c = conv_item(g, it);
+      const int y = c.y0 + tp;
+      for (int p = 0; p < c.planes + 2; ++p, ++j) {
+        const uint32_t slot = j % kC1Ring;
+        if (j >= kC1Ring &&
+            !ptx::mbar_wait_bounded(empty0 + 8 * slot, ((j / kC1Ring) - 1) & 1, kConvTimeoutNs)) {
+          *abort_flag = 1;
+          stop = true;
+          break;
+        }
+        const int z = c.z0 - 1 + p;
+        unsigned char *dst = slots + slot * kCvPlane + tp * 16;
+        // each lane loads its own y of the 6 rows of both volumes (all loads in flight at once);
+        // y - 1 and y + 1 come from the neighbouring lanes, the warp's edge lanes load theirs
+        const bool zin_ok = z >= 0 && z < g.nz;
+        const int ye = lane == 0 ? y - 1 : y + 1;  // the edge neighbour this lane may need
+        float ci[kCvSX], ca[kCvSX], ei[kCvSX], ea[kCvSX];
+#pragma unroll
+        for (int xr = 0; xr < kCvSX; ++xr) {
+          const int x = c.x0 - 1 + xr;
+          const bool row_ok = zin_ok && x >= 0 && x < g.nx;
+          const long long ro = (long long)z * g.nx + x;
+          ci[xr] = ca[xr] = ei[xr] = ea[xr] = 0.f;
+          if (row_ok && y < g.ny) {
+            ci[xr] = __ldg(img + ro * g.ny + y);
+            ca[xr] = __ldg(atl + ro * apitch + y);
+          }
+          if (row_ok && (lane == 0 || lane == 31) && ye >= 0 && ye < g.ny) {
+            ei[xr] = __ldg(img + ro * g.ny + ye);
+            ea[xr] = __ldg(atl + ro * apitch + ye);
+          }
+        }
+#pragma unroll
+        for (int xr = 0; xr < kCvSX; ++xr) {
+          float im = __shfl_up_sync(0xffffffffu, ci[xr], 1), ip = __shfl_down_sync(0xffffffffu, ci[xr], 1);
+          float am = __shfl_up_sync(0xffffffffu, ca[xr], 1), ap = __shfl_down_sync(0xffffffffu, ca[xr], 1);
+          if (lane == 0) {
+            im = ei[xr];
+            am = ea[xr];
+          }
+          if (lane == 31) {
+            ip = ei[xr];
+            ap = ea[xr];
+          }
+          const __half2 i01 = __floats2half2_rn(im, ci[xr]), a01 = __floats2half2_rn(am, ca[xr]);
+          const __half2 i2 = __floats2half2_rn(ip, 0.f), a2 = __floats2half2_rn(ap, 0.f);
+          *reinterpret_cast<uint4 *>(dst + xr * kCvSY * 16) =
+              make_uint4(*reinterpret_cast<const uint32_t *>(&i01),
+                         *reinterpret_cast<const uint32_t *>(&i2), 0u, 0u);
+          *reinterpret_cast<uint4 *>(dst + kCvHalf + xr * kCvSY * 16) =
+              make_uint4(*reinterpret_cast<const uint32_t *>(&a01),
+                         *reinterpret_cast<const uint32_t *>(&a2), 0u, 0u);
+        }
+        ptx::fence_proxy_async_smem();  // the tensor core reads the slot through the async proxy
+        __syncwarp();
+        if (lane == 0) ptx::mbar_arrive(full0 + 8 * slot);
+      }
+    }
+  } else if (warp == 4) {
+    // MMA issuer: the whole warp runs the loop, one elected lane issues
+    uint32_t j = 0;
+    uint32_t nz[3] = {1, 1, 1};
+    const uint64_t db0 = tc5::desc(wtab, kCvSeqRows * 16, 128);
+    for (int it = blockIdx.x; it < g.n_items && !*abort_flag; it += gridDim.x) {
+      const ConvItem c = conv_item(g, it);
+      bool ok = true;
+      for (int p = 0; p < c.planes + 2 && ok; ++p, ++j) {
+        const int zin = c.z0 - 1 + p;
+        for (int r = 0; r < 3 && ok; ++r)
+          if (p == 0 || (c.planes > 1 && r == (zin + 1 + 3) % 3))
+            ok = ptx::mbar_wait_bounded(zeroed0 + 8 * r, (nz[r] - 1) & 1, kConvTimeoutNs);
+        ok = ok && ptx::mbar_wait_bounded(full0 + 8 * (j % kC1Ring), (j / kC1Ring) & 1,
+                                          kConvTimeoutNs);
+        if (!ok) {
+          *abort_flag = 1;
+          break;
+        }
+        tc5::fence_after();
+        const uint64_t da = tc5::desc(base + (j % kC1Ring) * kCvPlane, kCvHalf, 128);
+        const int rho = (zin + 1 + 3) % 3;
+#pragma unroll 1
+        for (int ix = 0; ix < kCvSX; ++ix) {
+          int o_lo = ix - 2 < 0 ? 0 : ix - 2, o_hi = ix < kCvTX - 1 ? ix : kCvTX - 1;
+          while (o_lo <= o_hi && !((c.mask >> o_lo) & 1u)) ++o_lo;
+          while (o_hi >= o_lo && !((c.mask >> o_hi) & 1u)) --o_hi;
+          if (o_lo > o_hi) continue;
+          tc5::mma(tmem + 48 * o_lo, da + (uint64_t)(ix * kCvSY),
+                   db0 + (uint64_t)(rho * (kC1Seq / 16) + 3 * (2 - ix + o_lo) * 16),
+                   idesc_f16(48 * (o_hi - o_lo + 1)));
+        }
+        tc5::commit(empty0 + 8 * (j % kC1Ring));
+        tc5::commit(mdone);
+        if (c.planes > 1 || p == c.planes + 1) nz[(zin - 1 + 3) % 3] += 1;
+        if (p == c.planes + 1) {
+          nz[(zin + 3) % 3] += 1;
+          nz[(zin + 1 + 3) % 3] += 1;
+        }
+      }
+    }
+    if (j > 0) ptx::mbar_wait_bounded(mdone, (j - 1) & 1, kConvTimeoutNs);
+  } else {
+    // epilogue: warp w reads TMEM lanes 32w..32w+31 = output y0 + 32w + lane
+    const uint32_t lane_addr = tmem + ((uint32_t)(32 * warp) << 16);
+    float bias[kC];
+#pragma unroll
+    for (int q = 0; q < kC; ++q) bias[q] = __bfloat162float(wbf[kB1 + q]);
+#pragma unroll
+    for (int q = 0; q < 12; ++q) tc5::st16_zero(lane_addr + 16 * q);
+    tc5::wait_st();
+    tc5::fence_before();
+    __syncwarp();
+    if (lane == 0)
+      for (int r = 0; r < 3; ++r) ptx::mbar_arrive(zeroed0 + 8 * r);
+    uint32_t j = 0;
+    bool stop = false;
+    for (int it = blockIdx.x; it < g.n_items && !stop; it += gridDim.x) {
+      const ConvItem c = conv_item(g, it);
+      const int y = c.y0 + 32 * warp + lane;
+      const bool y_ok = y < g.y_hi;
+      for (int i = 0; i < c.planes + 4; ++i) {
+        if (i < c.planes + 2) {
+          if (!ptx::mbar_wait_bounded(mdone, j & 1, kConvTimeoutNs)) {
+            *abort_flag = 1;
+            stop = true;
+            break;
+          }
+          ++j;
+          tc5::fence_after();
+        }
+        const bool single = c.planes == 1;
+        if (single && i != 2) continue;
+        const int z = c.z0 - 2 + i;
+        const int r = (z + 3) % 3;
+        const uint32_t acc = lane_addr + 16 * r;
+        const bool real = i >= 2 && i < c.planes + 2;
+        uint32_t v[kCvTX][16];
+        if (real) {
+#pragma unroll
+          for (int o = 0; o < kCvTX; ++o) tc5::ld16(acc + 48 * o, v[o]);
+          tc5::wait_ld();
+        }
+        if (single) {
+#pragma unroll
+          for (int q = 0; q < 12; ++q) tc5::st16_zero(lane_addr + 16 * q);
+        } else {
+#pragma unroll
+          for (int o = 0; o < kCvTX; ++o) tc5::st16_zero(acc + 48 * o);
+        }
+        tc5::wait_st();
+        tc5::fence_before();
+        __syncwarp();
+        if (lane == 0) {
+          if (single)
+            for (int q = 0; q < 3; ++q) ptx::mbar_arrive(zeroed0 + 8 * q);
+          else
+            ptx::mbar_arrive(zeroed0 + 8 * r);
+        }
+        if (real) {
+#pragma unroll
+          for (int o = 0; o < kCvTX; ++o) {
+            const int x = c.x0 + o;
+            if (((c.mask >> o) & 1u) && x < g.nx && y_ok) {
+              uint32_t h[8];
+#pragma unroll
+              for (int q = 0; q < 8; ++q) {
+                const float v0 = fmaxf(fmaf(__uint_as_float(v[o][2 * q]), kInScale, bias[2 * q]), 0.f);
+                const float v1 =
+                    fmaxf(fmaf(__uint_as_float(v[o][2 * q + 1]), kInScale, bias[2 * q + 1]), 0.f);
+                const __nv_bfloat162 pr = __floats2bfloat162_rn(v0, v1);
+                h[q] = *reinterpret_cast<const uint32_t *>(&pr);
+              }
+              const long long vx = ((long long)z * g.nx + x) * g.ny + y;
+              *reinterpret_cast<uint4 *>(out + vx * 8) = make_uint4(h[0], h[1], h[2], h[3]);
+              *reinterpret_cast<uint4 *>(out + (g.nvox + vx) * 8) =
+                  make_uint4(h[4], h[5], h[6], h[7]);
+            }
+          }
+        }
+      }
+    }
+  }
+  tc5::fence_before();
+  __syncthreads();
+  if (*abort_flag && threadIdx.x == 0) atomicExch(err, 3);
+  if (warp == 0) {
+    tc5::fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCvCols)
+                 : "memory");
+  }
+}
+
 // ---------------------------------------------------------------- proposal + rescoring
 
 // Head weights staged in shared memory by every kernel that proposes, transposed and padded for
@@ -1206,11 +1334,6 @@ __constant__ unsigned char kRankTriples[kTopK] = {
     0x00, 0x01, 0x04, 0x10, 0x02, 0x05, 0x08, 0x11, 0x14, 0x20, 0x03, 0x06, 0x09, 0x0c, 0x12, 0x15,
     0x18, 0x21, 0x24, 0x30, 0x07, 0x0a, 0x0d, 0x13, 0x16, 0x19, 0x1c, 0x22, 0x25, 0x28, 0x31, 0x34};
 
-// Offsets kept at a level (i + j + k <= level): 10, 20 or 32.
-__host__ __device__ __forceinline__ int kept_count(int level) {
-  return level <= 2 ? 10 : level == 3 ? 20 : 32;
-}
-
 __device__ __forceinline__ int pick4(const int (&t)[4], int i) {
   return i == 0 ? t[0] : i == 1 ? t[1] : i == 2 ? t[2] : t[3];
 }
@@ -1399,7 +1522,6 @@ struct InferScratch {
   unsigned long long *fallbacks;  // (voxel, atlas) pairs that took the full search
   unsigned long long *evaluated;  // offsets evaluated by warp rows, summed over rows
   int *err;                       // bounded-wait status of the probe hook
-  float *cimg;                    // conv1's input-MRI half, FP32 [nvox][16]
   RowProp *props;                 // row-segment proposals of the block anchor rows
   int *lists;                     // the convolutions' x tiles and work items
 };
@@ -1407,8 +1529,7 @@ struct InferScratch {
 // Bytes before the proposal table (features, sums, fragments, counters), 256-aligned.
 size_t infer_base_bytes(long long nvox) {
   const size_t b = (size_t)nvox * kC * 2 * 2 + (size_t)nvox * 4 * 2 +
-                   3 * (size_t)(kFragWords + kRwFragWords) * 4 + 256 +
-                   (size_t)nvox * kC * 4;
+                   (3 * (size_t)(kFragWords + kRwFragWords) + kC1FragWords) * 4 + 256;
   return (b + 255) / 256 * 256;
 }
 
@@ -1420,10 +1541,10 @@ InferScratch carve(void *scratch, long long nvox) {
   r.pacc = reinterpret_cast<float *>(r.fb + nvox * kC);
   r.wacc = r.pacc + nvox;
   r.frag = reinterpret_cast<uint32_t *>(r.wacc + nvox);
-  r.fallbacks = reinterpret_cast<unsigned long long *>(r.frag + 3 * (kFragWords + kRwFragWords));
+  r.fallbacks = reinterpret_cast<unsigned long long *>(
+      r.frag + 3 * (kFragWords + kRwFragWords) + kC1FragWords);
   r.evaluated = r.fallbacks + 1;
   r.err = reinterpret_cast<int *>(r.fallbacks + 2);
-  r.cimg = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(r.fallbacks) + 256);
   r.props = reinterpret_cast<RowProp *>(static_cast<unsigned char *>(scratch) +
                                         infer_base_bytes(nvox));
   r.lists = nullptr;  // placed by the launch, which knows the geometry
@@ -1473,16 +1594,17 @@ cudaError_t make_feature_map(CUtensorMap *map, const __nv_bfloat16 *base, const 
 // entries of the sparse plans (first row | row mask << 16), then each layer's work items.
 struct ConvPlan {
   int c1_z, c1_nz, c1_x, c1_nx;  // conv1 box (z, x; every y)
-  int y_lo[3], y_hi[3];
-  int n_items[3], item_off[3];   // work items of conv2..conv4 (offset in ints into the lists)
-  bool ring[3];                  // conv16_kernel (plane-slot ring) or conv16_rows_kernel
+  int y_lo[4], y_hi[4];          // [0..2]: conv2..conv4, [3]: conv1
+  int n_items[4], item_off[4];   // work items (offset in ints into the lists)
+  bool ring[4];                  // conv16_kernel (plane-slot ring) or conv16_rows_kernel
   bool dense;
 };
 
 // Work items of a layer: every (x tile, y tile) column over each run of consecutive planes of
 // `zs`, cut into pieces of at most kCvChunk planes.
-void add_items(ConvPlan &p, int l, const std::vector<int> &zs, int x_tiles, std::vector<int> &lists) {
-  const int tiles_y = (p.y_hi[l] - p.y_lo[l] + kCvTY - 1) / kCvTY;
+void add_items(ConvPlan &p, int l, const std::vector<int> &zs, int x_tiles, std::vector<int> &lists,
+               int tile_y = kCvTY) {
+  const int tiles_y = (p.y_hi[l] - p.y_lo[l] + tile_y - 1) / tile_y;
   if (lists.size() & 1) lists.push_back(0);  // items are read as 8-byte int2
   p.item_off[l] = (int)lists.size();
   for (int xi = 0; xi < x_tiles; ++xi)
@@ -1504,14 +1626,14 @@ void add_items(ConvPlan &p, int l, const std::vector<int> &zs, int x_tiles, std:
 
 ConvPlan dense_plan(const Geometry &g, std::vector<int> &lists) {
   ConvPlan p{};
-  lists.assign(3 * (size_t)g.nx, 0);
+  lists.assign(4 * (size_t)g.nx, 0);
   p.c1_nz = g.nz;
   p.c1_nx = g.nx;
   std::vector<int> zs(g.nz);
   for (int z = 0; z < g.nz; ++z) zs[z] = z;
-  for (int l = 0; l < 3; ++l) {
+  for (int l = 0; l < 4; ++l) {
     p.y_hi[l] = g.ny;
-    add_items(p, l, zs, (g.nx + kCvTX - 1) / kCvTX, lists);
+    add_items(p, l, zs, (g.nx + kCvTX - 1) / kCvTX, lists, l == 3 ? kC1Y : kCvTY);
   }
   p.dense = true;
   return p;
@@ -1540,7 +1662,7 @@ std::vector<int> rows_near(const std::vector<int> &anc, int radius, int n) {
 // needed row, items over the needed planes.
 ConvPlan sparse_plan(const Geometry &g, int block, std::vector<int> &lists) {
   ConvPlan p{};
-  lists.assign(3 * (size_t)g.nx, 0);
+  lists.assign(4 * (size_t)g.nx, 0);
   const int iz = g.nz - 12, ix = g.nx - 12, iy = g.ny - 12;
   if (iz <= 0 || ix <= 0 || iy <= 0) return p;  // no interior: nothing to compute
   const std::vector<int> az = anchors(iz, block), ax = anchors(ix, block);
@@ -1562,44 +1684,49 @@ ConvPlan sparse_plan(const Geometry &g, int block, std::vector<int> &lists) {
     p.y_hi[l] = g.ny - 6 + radius;
     add_items(p, l, zs, nt, lists);
   }
+  // conv1: the box 3 rows and planes around the anchors, y within 3 of the interior
+  {
+    int nt = 0;
+    for (int x0 = p.c1_x; x0 < p.c1_x + p.c1_nx; x0 += kCvTX) {
+      const int rows = p.c1_x + p.c1_nx - x0 < kCvTX ? p.c1_x + p.c1_nx - x0 : kCvTX;
+      lists[3 * (size_t)g.nx + nt++] = x0 | (int)(((1u << rows) - 1u) << 16);
+    }
+    std::vector<int> zs(p.c1_nz);
+    for (int i = 0; i < p.c1_nz; ++i) zs[i] = p.c1_z + i;
+    p.y_lo[3] = 3;
+    p.y_hi[3] = g.ny - 3;
+    add_items(p, 3, zs, nt, lists, kC1Y);
+  }
   return p;
 }
 
-int conv1_blocks(const ConvPlan &p, int ny) {
-  const long long items =
-      (long long)p.c1_nz * ((p.c1_nx + kC1Warps - 1) / kC1Warps) * ((ny + 31) / 32);
-  return (int)(items < 16LL * sms() ? items : 16LL * sms());
-}
-
-// conv1's input-MRI half (FP32 sums, before scale and bias), shared by every atlas of the subject.
-cudaError_t run_conv1_img(const Geometry &g, const __nv_bfloat16 *wbf, const float *img,
-                          const ConvPlan &p, const InferScratch &sc, cudaStream_t s) {
-  if (p.c1_nz <= 0 || p.c1_nx <= 0) return cudaSuccess;
-  conv1_kernel<0><<<conv1_blocks(p, g.ny), kC1Warps * 32, 0, s>>>(
-      img, g.ny, wbf, sc.cimg, nullptr, g.nx, g.ny, g.nz, p.c1_z, p.c1_nz, p.c1_x, p.c1_nx);
-  return cudaGetLastError();
-}
-
-// conv1 (atlas half + the shared input half) .. conv4 of one atlas; returns the buffer holding
-// the conv4 features.
-cudaError_t run_convs(const Geometry &g, const __nv_bfloat16 *wbf, const float *atlas_a,
-                      int apitch, const InferScratch &sc, int *err, const ConvPlan &p,
-                      __nv_bfloat16 **features, cudaStream_t s) {
+// conv1 .. conv4 of one (input, atlas) pair; returns the buffer holding the conv4 features.
+cudaError_t run_convs(const Geometry &g, const __nv_bfloat16 *wbf, const float *img,
+                      const float *atlas_a, int apitch, const InferScratch &sc, int *err,
+                      const ConvPlan &p, __nv_bfloat16 **features, cudaStream_t s) {
   const int n_sm = sms();
-  *features = sc.fb;  // conv2 -> fb, conv3 -> fa, conv4 -> fb
-  if (p.c1_nz <= 0 || p.c1_nx <= 0) return cudaSuccess;
-  conv1_kernel<1><<<conv1_blocks(p, g.ny), kC1Warps * 32, 0, s>>>(
-      atlas_a, apitch, wbf, sc.cimg, sc.fa, g.nx, g.ny, g.nz, p.c1_z, p.c1_nz, p.c1_x, p.c1_nx);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  CUtensorMap maps[2];
-  if ((e = make_feature_map(&maps[0], sc.fa, g)) != cudaSuccess) return e;
-  if ((e = make_feature_map(&maps[1], sc.fb, g)) != cudaSuccess) return e;
+  *features = sc.fb;  // conv1 -> fa, conv2 -> fb, conv3 -> fa, conv4 -> fb
+  cudaError_t e;
   ConvGrid cg;
   cg.nx = g.nx;
   cg.ny = g.ny;
   cg.nz = g.nz;
   cg.nvox = g.nvox();
+  if (p.n_items[3] > 0) {
+    cg.xlist = p.dense ? nullptr : sc.lists + 3 * g.nx;
+    cg.items = reinterpret_cast<const int2 *>(sc.lists + p.item_off[3]);
+    cg.n_items = p.n_items[3];
+    cg.y_lo = p.y_lo[3];
+    cg.y_hi = p.y_hi[3];
+    cg.tile_y = kC1Y;
+    const int blocks = cg.n_items < 2 * n_sm ? cg.n_items : 2 * n_sm;
+    conv1_tc_kernel<<<blocks, kC1Threads, kC1Smem, s>>>(
+        img, atlas_a, apitch, sc.frag + 3 * (kFragWords + kRwFragWords), wbf, sc.fa, cg, err);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  CUtensorMap maps[2];
+  if ((e = make_feature_map(&maps[0], sc.fa, g)) != cudaSuccess) return e;
+  if ((e = make_feature_map(&maps[1], sc.fb, g)) != cudaSuccess) return e;
   const int boffs[3] = {kB2, kB3, kB4};
   __nv_bfloat16 *bufs[2] = {sc.fa, sc.fb};
   for (int l = 0; l < 3; ++l) {
@@ -1608,6 +1735,7 @@ cudaError_t run_convs(const Geometry &g, const __nv_bfloat16 *wbf, const float *
     cg.n_items = p.n_items[l];
     cg.y_lo = p.y_lo[l];
     cg.y_hi = p.y_hi[l];
+    cg.tile_y = kCvTY;
     if (cg.n_items <= 0) continue;
     const int blocks = cg.n_items < 2 * n_sm ? cg.n_items : 2 * n_sm;
     if (!p.ring[l]) {
@@ -1640,6 +1768,11 @@ cudaError_t pack_all(const __nv_bfloat16 *wbf, uint32_t *frag, cudaStream_t s) {
         wbf, woffs[l], frag + 3 * kFragWords + l * kRwFragWords);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
+  e0 = cudaFuncSetAttribute(conv1_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)kC1Smem);
+  if (e0 != cudaSuccess) return e0;
+  pack_c1_kernel<<<(kC1FragWords + 255) / 256, 256, 0, s>>>(
+      wbf, frag + 3 * (kFragWords + kRwFragWords));
   return cudaSuccess;
 }
 
@@ -1675,7 +1808,6 @@ cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInp
   if ((e = cudaMemsetAsync(sc.fallbacks, 0, 2 * sizeof(unsigned long long), s)) != cudaSuccess)
     return e;
   if ((e = pack_all(wbf, sc.frag, s)) != cudaSuccess) return e;
-  if ((e = run_conv1_img(g, wbf, in.img, plan, sc, s)) != cudaSuccess) return e;
   const float neg_k = (float)(-1.4426950408889634 / div);
   const float scale = (float)sqrt(1.4426950408889634 / div);
   const int nblk = sms() * 8;
@@ -1693,7 +1825,7 @@ cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInp
   for (int a = 0; a < g.num; ++a) {
     const float *A = in.atlas + a * astride, *L = in.label + a * astride;
     __nv_bfloat16 *f4 = nullptr;
-    if ((e = run_convs(g, wbf, A, in.pitch, sc, err, plan, &f4, s)) != cudaSuccess)
+    if ((e = run_convs(g, wbf, in.img, A, in.pitch, sc, err, plan, &f4, s)) != cudaSuccess)
       return e;
     propose_rows_kernel<<<propose_blocks, kRescoreWarps * 32, 0, s>>>(f4, wbf, g.nx, g.ny, g.nz,
                                                                       block, level, sc.props);
@@ -1733,8 +1865,7 @@ cudaError_t learned_probe(const Geometry &g, const void *weights, const float *i
   if ((e = cudaMemcpyAsync(sc.lists, lists.data(), lists.size() * sizeof(int),
                            cudaMemcpyHostToDevice, s)) != cudaSuccess)
     return e;
-  if ((e = run_conv1_img(g, wbf, img, plan, sc, s)) != cudaSuccess) return e;
-  if ((e = run_convs(g, wbf, atlas_a, g.ny, sc, sc.err, plan, &f4, s)) != cudaSuccess)
+  if ((e = run_convs(g, wbf, img, atlas_a, g.ny, sc, sc.err, plan, &f4, s)) != cudaSuccess)
     return e;
   // the sums area is free here: voxel list, proposals and confidences go there
   int64_t *d_vox = reinterpret_cast<int64_t *>(sc.pacc);
