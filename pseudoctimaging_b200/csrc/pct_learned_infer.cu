@@ -1,9 +1,8 @@
 // Inference side of the learned proposal (EXEC_CHOICE 7).
 //
 // Per atlas, over the whole volume:
-//   conv1 (2 -> 16 channels)            tensor cores: FP16 im2col rows per input channel, FP32
-//                                       accumulation (mma.sync)
-//   conv2..conv4 (16 -> 16 channels)    tensor cores: BF16 implicit GEMM on tcgen05, FP32 in TMEM
+//   conv1 (2 -> 16 channels)            tcgen05: FP16 operands (y taps folded into K), FP32 in TMEM
+//   conv2..conv4 (16 -> 16 channels)    tcgen05: BF16 implicit GEMM, FP32 in TMEM
 //   heads, proposal and rescoring       row segments of 30 voxels along y: per voxel the 33
 //                                       logits and a softmax per axis; the summed probabilities of
 //                                       a block's anchor segment pick 4 offsets per axis and the
