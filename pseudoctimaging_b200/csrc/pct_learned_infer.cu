@@ -1341,20 +1341,23 @@ __device__ __forceinline__ int pick4(const int (&t)[4], int i) {
 // du, yc + dv), `l` at the label voxel (z + dw, x0 + du, yc + dv); row strides are 32-bit.
 __device__ __forceinline__ void eval_offset4(const float *__restrict__ a,
                                              const float *__restrict__ l,
-                                             const float (&in)[3][kRows + 2], int axy, int apitch,
-                                             unsigned take, float s, float (&P)[kRows],
-                                             float (&W)[kRows]) {
+                                             const float2 (&in)[3][(kRows + 2) / 2], int axy,
+                                             int apitch, unsigned take, float2 s2,
+                                             float (&P)[kRows], float (&W)[kRows]) {
+  // x-rows in pairs: packed FP32 FMAs (the same roundings as two scalar FMAs)
   float Z[kRows + 2];
 #pragma unroll
-  for (int xr = 0; xr < kRows + 2; ++xr) {
-    const int ro = xr * apitch;
-    float z = 0.f;
+  for (int xp = 0; xp < (kRows + 2) / 2; ++xp) {
+    const int ro = 2 * xp * apitch;
+    float2 z = make_float2(0.f, 0.f);
 #pragma unroll
     for (int dz = 0; dz < 3; ++dz) {
-      const float t = fmaf(__ldg(a + (ro + dz * axy)), s, in[dz][xr]);
-      z = fmaf(t, t, z);
+      const float2 av = make_float2(__ldg(a + (ro + dz * axy)), __ldg(a + (ro + apitch + dz * axy)));
+      const float2 t = __ffma2_rn(av, s2, in[dz][xp]);
+      z = __ffma2_rn(t, t, z);
     }
-    Z[xr] = z;
+    Z[2 * xp] = z.x;
+    Z[2 * xp + 1] = z.y;
   }
 #pragma unroll
   for (int r = 0; r < kRows; ++r) {
@@ -1426,13 +1429,15 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 4)
     const unsigned any_full = __ballot_sync(0xffffffffu, full);
     if (full) my_fallbacks += __popc(take);
     // input taps I(z+dz-1, x0-1+xr, yc), negated and scaled
-    float in[3][kRows + 2];
+    float2 in[3][(kRows + 2) / 2];
 #pragma unroll
     for (int dz = 0; dz < 3; ++dz)
 #pragma unroll
-      for (int xr = 0; xr < kRows + 2; ++xr)
-        in[dz][xr] =
-            -__ldg(img + (long long)(z + dz - 1) * nxy + (long long)(x0 - 1 + xr) * ny + yc) * scale;
+      for (int xp = 0; xp < (kRows + 2) / 2; ++xp) {
+        const float *pi = img + (long long)(z + dz - 1) * nxy + (long long)(x0 - 1 + 2 * xp) * ny + yc;
+        in[dz][xp] = make_float2(-__ldg(pi) * scale, -__ldg(pi + ny) * scale);
+      }
+    const float2 s2 = make_float2(scale, scale);
     const float *ab = atl + ((long long)(z - 1) * axy + (long long)(x0 - 1) * apitch + yc);
     const float *lb = lab + ((long long)z * axy + (long long)x0 * apitch + yc);
     float P[kRows], W[kRows];
@@ -1443,7 +1448,7 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 4)
 #pragma unroll 2
       for (int c = 0; c < kept; ++c) {
         const int off = w_off[c];
-        eval_offset4(ab + off, lb + off, in, axy, apitch, take, scale, P, W);
+        eval_offset4(ab + off, lb + off, in, axy, apitch, take, s2, P, W);
       }
       my_evals += (unsigned long long)kept * __popc(owned);
     } else {
@@ -1464,7 +1469,7 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 4)
           for (int jv = 0; jv < kAxis; ++jv) {
             const bool mine = full || (ru + (int)((rank[2] >> (4 * jv)) & 0xF) <= LEVEL);
             const int off = (jw - 5) * axy + (ju - 5) * apitch + (jv - 5);
-            eval_offset4(ab + off, lb + off, in, axy, apitch, mine ? take : 0u, scale, P, W);
+            eval_offset4(ab + off, lb + off, in, axy, apitch, mine ? take : 0u, s2, P, W);
           }
         }
       }
