@@ -403,6 +403,7 @@ def time_other_forms(pct, h, d_img, d_mri, d_lab, d_plain, div, stream, args) ->
     h.attach_model(model, 0.0)
     out = {}
     for name, choice, steps, k in (("learned", pct.EXEC_LEARNED, 5, 32),
+                                   ("learned_k20", pct.EXEC_LEARNED, 5, 20),
                                    ("learned_k10", pct.EXEC_LEARNED, 5, 10),
                                    ("tc_fp16", pct.EXEC_TC_FP16, 2, 0),
                                    ("tc_bf16", pct.EXEC_TC_BF16, 2, 0)):
