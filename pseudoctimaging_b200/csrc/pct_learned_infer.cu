@@ -1788,6 +1788,8 @@ cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInp
                            double div, float conf_thr, int block, int level, bool every_voxel,
                            void *scratch, int *err, cudaStream_t s) {
   if (block < 1 || level < 2 || level > 4) return cudaErrorInvalidValue;
+  // work items pack x and z coordinates in 16 bits
+  if (g.nx >= 65536 || g.nz >= 65536) return cudaErrorInvalidValue;
   const __nv_bfloat16 *wbf = static_cast<const __nv_bfloat16 *>(weights);
   const long long nvox = g.nvox();
   const long long astride = (long long)g.nz * g.nx * in.pitch;
@@ -1856,6 +1858,7 @@ cudaError_t learned_probe(const Geometry &g, const void *weights, const float *i
                           const float *atlas_a, void *scratch, const int64_t *voxels, int n,
                           float *features, signed char *top, float *conf, cudaStream_t s) {
   const __nv_bfloat16 *wbf = static_cast<const __nv_bfloat16 *>(weights);
+  if (g.nx >= 65536 || g.nz >= 65536) return cudaErrorInvalidValue;
   InferScratch sc = carve(scratch, g.nvox());
   sc.lists = reinterpret_cast<int *>(reinterpret_cast<unsigned char *>(sc.props) +
                                      prop_table_bytes(g));
