@@ -72,7 +72,7 @@ constexpr int kCvSX = kCvTX + 2, kCvSY = 128;
 constexpr int kCvHalf = kCvSX * kCvSY * 16;                          // 12,288 B
 constexpr int kCvPlane = 2 * kCvHalf;                                // 24,576 B per ring slot
 constexpr int kCvRing = 2;                                           // input-plane slots
-constexpr int kCvChunk = 8;                                          // output planes per item
+constexpr int kCvChunk = 13;                                         // max output planes per item
 constexpr int kCvSeqRows = 144;                                      // 9 blocks of 16 channels
 constexpr int kCvSeq = 2 * kCvSeqRows * 16;                          // 4,608 B per (ky, rho)
 constexpr int kCvWBytes = 9 * kCvSeq;                                // 41,472 B
@@ -1605,7 +1605,8 @@ struct ConvPlan {
 };
 
 // Work items of a layer: every (x tile, y tile) column over each run of consecutive planes of
-// `zs`, cut into pieces of at most kCvChunk planes.
+// `zs`, cut into the fewest pieces of at most kCvChunk planes, of nearly equal length (a 101-plane
+// run: 8 pieces of 12 or 13, which spreads evenly over the persistent grid).
 void add_items(ConvPlan &p, int l, const std::vector<int> &zs, int x_tiles, std::vector<int> &lists,
                int tile_y = kCvTY) {
   const int tiles_y = (p.y_hi[l] - p.y_lo[l] + tile_y - 1) / tile_y;
@@ -1615,9 +1616,14 @@ void add_items(ConvPlan &p, int l, const std::vector<int> &zs, int x_tiles, std:
     for (int ty = 0; ty < tiles_y; ++ty)
       for (size_t i = 0; i < zs.size();) {
         size_t e = i + 1;
-        while (e < zs.size() && zs[e] == zs[e - 1] + 1 && (int)(e - i) < kCvChunk) ++e;
-        lists.push_back(xi | (ty << 16));
-        lists.push_back(zs[i] | ((int)(e - i) << 16));
+        while (e < zs.size() && zs[e] == zs[e - 1] + 1) ++e;  // the run [i, e)
+        const int len = (int)(e - i), pieces = (len + kCvChunk - 1) / kCvChunk;
+        for (int q = 0, at = 0; q < pieces; ++q) {
+          const int n = len / pieces + (q < len % pieces ? 1 : 0);
+          lists.push_back(xi | (ty << 16));
+          lists.push_back(zs[i + at] | (n << 16));
+          at += n;
+        }
         i = e;
       }
   p.n_items[l] = (int)((lists.size() - p.item_off[l]) / 2);
