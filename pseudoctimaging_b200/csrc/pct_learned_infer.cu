@@ -425,7 +425,8 @@ __global__ void __launch_bounds__(kCvThreads, 2)
 // each) instead of forming the three-plane ring, so an output plane costs 54 MMAs of N <= 48 (an
 // input row at one y shift feeds up to 3 output rows of one plane through one MMA, weights stored
 // per (kz, ky) as W(kx = 2) | W(kx = 1) | W(kx = 0)) but no output waits for another's epilogue;
-// input planes stream through a 4-slot ring, so an item's three planes are all in flight.
+// input planes stream through a 4-slot ring, so an item's three planes are all in flight; an item
+// with one output row loads only the 3 input rows it needs (a second TMA map, half the bytes).
 constexpr int kRwRing = 4;
 constexpr int kRwSeq = 2 * 48 * 16;                     // one (kz, ky) weight sequence
 constexpr int kRwWBytes = 9 * kRwSeq;                   // 13,824 B
@@ -451,9 +452,10 @@ __global__ void pack_rows_kernel(const __nv_bfloat16 *__restrict__ wbf, int woff
 // The output region of one layer: work items {x tile | y tile << 16, first plane | planes << 16}
 
 __global__ void __launch_bounds__(kCvThreads, 2)
-    conv16_rows_kernel(const __grid_constant__ CUtensorMap tm, const uint32_t *__restrict__ frag,
-                  const __nv_bfloat16 *__restrict__ wbf, int boff, __nv_bfloat16 *__restrict__ out,
-                  ConvGrid g, int *__restrict__ err) {
+    conv16_rows_kernel(const __grid_constant__ CUtensorMap tm, const __grid_constant__ CUtensorMap tm3,
+                       const uint32_t *__restrict__ frag, const __nv_bfloat16 *__restrict__ wbf,
+                       int boff, __nv_bfloat16 *__restrict__ out, ConvGrid g,
+                       int *__restrict__ err) {
   extern __shared__ unsigned char smem_raw[];
   const uint32_t raw = ptx::smem_u32(smem_raw);
   const uint32_t base = (raw + 127u) & ~127u;
@@ -509,9 +511,11 @@ __global__ void __launch_bounds__(kCvThreads, 2)
             *abort_flag = 1;
             break;
           }
-          ptx::mbar_arrive_expect_tx(full0 + 8 * slot, kCvPlane);
-          ptx::tma_load_4d(base + slot * kCvPlane, &tm, full0 + 8 * slot, 2 * (c.y0 - 1), c.x0 - 1,
-                           c.z0 - 1 + p, 0);
+          // an item of one output row needs 3 input rows: the narrow box
+          const bool narrow = c.mask == 1u;
+          ptx::mbar_arrive_expect_tx(full0 + 8 * slot, narrow ? kCvPlane / 2 : kCvPlane);
+          ptx::tma_load_4d(base + slot * kCvPlane, narrow ? &tm3 : &tm, full0 + 8 * slot,
+                           2 * (c.y0 - 1), c.x0 - 1, c.z0 - 1 + p, 0);
         }
       }
       // planes still landing: wait for the last ring's worth (bounded)
@@ -534,7 +538,8 @@ __global__ void __launch_bounds__(kCvThreads, 2)
             const uint32_t q = j0 + i + kz;
             ok = ok && ptx::mbar_wait_bounded(full0 + 8 * (q % kRwRing), (q / kRwRing) & 1,
                                                kConvTimeoutNs);
-            da[kz] = tc5::desc(base + (q % kRwRing) * kCvPlane, kCvHalf, 128);
+            da[kz] = tc5::desc(base + (q % kRwRing) * kCvPlane,
+                               c.mask == 1u ? kCvHalf / 2 : kCvHalf, 128);
           }
           if (!ok) {
             *abort_flag = 1;
@@ -1574,15 +1579,16 @@ namespace {
 
 // TMA map over a channel-last BF16 feature volume [nz][nx][ny][16]: one box is a conv16 slab
 // (3 z x 6 x x 66 y voxels), 32-byte swizzled, out-of-volume voxels zero.
-cudaError_t make_feature_map(CUtensorMap *map, const __nv_bfloat16 *base, const Geometry &g) {
+cudaError_t make_feature_map(CUtensorMap *map, const __nv_bfloat16 *base, const Geometry &g,
+                             int rows = kCvSX) {
   auto fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(tensor_map_encoder());
   if (!fn) return cudaErrorNotSupported;
   // [half][z][x][y, 8 channels] with each (half, z, x) row as 2 ny 8-byte elements; one box = a
-  // conv16 ring slot (one plane, 6 x-rows of 128 y), out-of-volume voxels zero
+  // conv16 ring slot (one plane, `rows` x-rows of 128 y), out-of-volume voxels zero
   const cuuint64_t dims[4] = {2 * (cuuint64_t)g.ny, (cuuint64_t)g.nx, (cuuint64_t)g.nz, 2};
   const cuuint64_t strides[3] = {16 * (cuuint64_t)g.ny, 16 * (cuuint64_t)g.ny * g.nx,
                                  16 * (cuuint64_t)g.nvox()};
-  const cuuint32_t box[4] = {2 * kCvSY, (cuuint32_t)kCvSX, 1, 2};
+  const cuuint32_t box[4] = {2 * kCvSY, (cuuint32_t)rows, 1, 2};
   const cuuint32_t estr[4] = {1u, 1u, 1u, 1u};
   CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<__nv_bfloat16 *>(base), dims,
                   strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -1734,9 +1740,11 @@ cudaError_t run_convs(const Geometry &g, const __nv_bfloat16 *wbf, const float *
         img, atlas_a, apitch, sc.frag + 3 * (kFragWords + kRwFragWords), wbf, sc.fa, cg, err);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
-  CUtensorMap maps[2];
+  CUtensorMap maps[2], maps3[2];
   if ((e = make_feature_map(&maps[0], sc.fa, g)) != cudaSuccess) return e;
   if ((e = make_feature_map(&maps[1], sc.fb, g)) != cudaSuccess) return e;
+  if ((e = make_feature_map(&maps3[0], sc.fa, g, 3)) != cudaSuccess) return e;
+  if ((e = make_feature_map(&maps3[1], sc.fb, g, 3)) != cudaSuccess) return e;
   const int boffs[3] = {kB2, kB3, kB4};
   __nv_bfloat16 *bufs[2] = {sc.fa, sc.fb};
   for (int l = 0; l < 3; ++l) {
@@ -1750,7 +1758,7 @@ cudaError_t run_convs(const Geometry &g, const __nv_bfloat16 *wbf, const float *
     const int blocks = cg.n_items < 2 * n_sm ? cg.n_items : 2 * n_sm;
     if (!p.ring[l]) {
       conv16_rows_kernel<<<blocks, kCvThreads, kRwSmem, s>>>(
-          maps[l & 1], sc.frag + 3 * kFragWords + l * kRwFragWords, wbf, boffs[l],
+          maps[l & 1], maps3[l & 1], sc.frag + 3 * kFragWords + l * kRwFragWords, wbf, boffs[l],
           bufs[(l + 1) & 1], cg, err);
       if ((e = cudaGetLastError()) != cudaSuccess) return e;
       continue;
