@@ -13,6 +13,9 @@
  * independent (no globals, unlike the reference's nx/ny/nz/num/nh).
  *
  * Streams: every `void *stream` argument is a cudaStream_t; NULL means the CUDA default stream.
+ * A handle's device scratch is shared by its calls, so calls on one handle that may overlap on
+ * the GPU (different streams without an ordering between them) race; order them, or use one
+ * handle per stream.
  */
 #ifndef PCT_B200_H
 #define PCT_B200_H
