@@ -42,6 +42,7 @@ struct pct_handle {
   int learned_level = 4;                // kept rank triples i + j + k <= level (32 offsets)
   DevBuf learned;                       // its feature volumes and sums
   long long learned_nvox = 0;           // volume size of the last learned run (0: none yet)
+  pct::learned::LearnedStreams learned_streams{};  // convolutions beside the rescoring
   cudaStream_t learned_stream = nullptr;
   cudaStream_t copy_stream = nullptr;   // uploads of the pipelined host path
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};  // start, first group staged, rest staged
@@ -166,10 +167,20 @@ int launch_learned_path(pct_handle *h, const pct::Geometry &g, const pct::SlabIn
   int st = ensure(h, h->learned, pct::learned::infer_scratch_bytes(g));
   if (st || (st = ensure(h, h->err, 16))) return st;
   int *err = static_cast<int *>(h->err.ptr);
+  pct::learned::LearnedStreams &ls = h->learned_streams;
+  if (!ls.aux) {
+    // the convolution stream gets the higher priority, so that its CTAs take the SMs the
+    // rescoring's CTAs free
+    int least = 0, greatest = 0;
+    PCT_CUDA(h, cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    PCT_CUDA(h, cudaStreamCreateWithPriority(&ls.aux, cudaStreamNonBlocking, greatest));
+  }
+  for (cudaEvent_t &e : ls.ev)
+    if (!e) PCT_CUDA(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   PCT_CUDA(h, cudaMemsetAsync(err, 0, sizeof(int), s));
   PCT_CUDA(h, pct::learned::launch_learned(g, pct::learned::model_weights(h->model), in, d_out, div,
                                            h->learned_conf, h->learned_block, h->learned_level,
-                                           h->learned_every_voxel, h->learned.ptr, err, s));
+                                           h->learned_every_voxel, h->learned.ptr, err, &ls, s));
   h->learned_nvox = g.nvox();
   h->learned_stream = s;
   return PCT_OK;
@@ -483,6 +494,9 @@ int pct_destroy(pct_handle *h) {
                     &h->stage, &h->batch_stage, &h->batch_meta, &h->learned})
     if (b->ptr) cudaFree(b->ptr);
   if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
+  if (h->learned_streams.aux) cudaStreamDestroy(h->learned_streams.aux);
+  for (cudaEvent_t e : h->learned_streams.ev)
+    if (e) cudaEventDestroy(e);
   for (cudaEvent_t e : h->ev)
     if (e) cudaEventDestroy(e);
   if (h->stream) cudaStreamDestroy(h->stream);

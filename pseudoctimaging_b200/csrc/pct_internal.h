@@ -109,9 +109,17 @@ unsigned long long *infer_counters(void *scratch, long long nvox);
 // rows in (z, x) (1 = every row segment proposes for itself); the kept set of a proposal is the
 // rank triples with i + j + k <= level (2, 3, 4: 10, 20, 32 offsets). The convolutions compute
 // only the outputs the anchor rows need unless `every_voxel` (same result).
+// With `streams` (an auxiliary stream and 5 events), each atlas's convolutions and proposal run
+// on the auxiliary stream while the previous atlas is rescored on `s` (two proposal tables in
+// the scratch); without it everything runs on `s`.
+struct LearnedStreams {
+  cudaStream_t aux;
+  cudaEvent_t ev[5];  // fork, proposal ready [2], rescoring done [2]
+};
 cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInputs &in, float *out,
                            double div, float conf_thr, int block, int level, bool every_voxel,
-                           void *scratch, int *err, cudaStream_t s);
+                           void *scratch, int *err, const LearnedStreams *streams,
+                           cudaStream_t s);
 cudaError_t learned_probe(const Geometry &g, const void *weights, const float *img,
                           const float *atlas_a, void *scratch, const int64_t *voxels, int n,
                           float *features, signed char *top, float *conf, cudaStream_t s);

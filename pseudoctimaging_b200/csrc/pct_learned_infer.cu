@@ -1531,7 +1531,7 @@ struct InferScratch {
   unsigned long long *fallbacks;  // (voxel, atlas) pairs that took the full search
   unsigned long long *evaluated;  // offsets evaluated by warp rows, summed over rows
   int *err;                       // bounded-wait status of the probe hook
-  RowProp *props;                 // row-segment proposals of the block anchor rows
+  RowProp *props;                 // row-segment proposals of the block anchor rows (two tables)
   int *lists;                     // the convolutions' x tiles and work items
 };
 
@@ -1568,7 +1568,7 @@ size_t prop_table_bytes(const Geometry &g) {
 }
 
 size_t infer_scratch_bytes(const Geometry &g) {
-  return infer_base_bytes(g.nvox()) + prop_table_bytes(g) + conv_list_bytes(g) + 256;
+  return infer_base_bytes(g.nvox()) + 2 * prop_table_bytes(g) + conv_list_bytes(g) + 256;
 }
 
 unsigned long long *infer_counters(void *scratch, long long nvox) {
@@ -1800,7 +1800,8 @@ cudaError_t pack_all(const __nv_bfloat16 *wbf, uint32_t *frag, cudaStream_t s) {
 // input MRI contiguous). Writes the interior of `out`; the border is left untouched.
 cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInputs &in, float *out,
                            double div, float conf_thr, int block, int level, bool every_voxel,
-                           void *scratch, int *err, cudaStream_t s) {
+                           void *scratch, int *err, const LearnedStreams *streams,
+                           cudaStream_t s) {
   if (block < 1 || level < 2 || level > 4) return cudaErrorInvalidValue;
   // work items pack x and z coordinates in 16 bits
   if (g.nx >= 65536 || g.nz >= 65536) return cudaErrorInvalidValue;
@@ -1809,7 +1810,7 @@ cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInp
   const long long astride = (long long)g.nz * g.nx * in.pitch;
   InferScratch sc = carve(scratch, nvox);
   sc.lists = reinterpret_cast<int *>(reinterpret_cast<unsigned char *>(sc.props) +
-                                     prop_table_bytes(g));
+                                     2 * prop_table_bytes(g));
   cudaError_t e;
   std::vector<int> lists;
   ConvPlan plan = sparse_plan(g, block, lists);
@@ -1842,26 +1843,46 @@ cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInp
             ((g.ny - 12 + kRowOut - 1) / kRowOut);
   const long long pblk = (prows + kRescoreWarps - 1) / kRescoreWarps;
   const int propose_blocks = (int)(pblk < 1 ? 1 : (pblk > 64LL * sms() ? 64LL * sms() : pblk));
+  // two streams: atlas a's convolutions and proposal (stream cs) run while atlas a - 1 is
+  // rescored (stream s); the proposal tables alternate, the sums are touched by s only
+  const bool two = streams && streams->aux && g.num > 1;
+  const cudaStream_t cs = two ? streams->aux : s;
+  RowProp *tables[2] = {sc.props, reinterpret_cast<RowProp *>(
+                                      reinterpret_cast<unsigned char *>(sc.props) +
+                                      prop_table_bytes(g))};
+  if (two) {
+    if ((e = cudaEventRecord(streams->ev[0], s)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(cs, streams->ev[0], 0)) != cudaSuccess) return e;
+  }
   for (int a = 0; a < g.num; ++a) {
     const float *A = in.atlas + a * astride, *L = in.label + a * astride;
+    RowProp *props = two ? tables[a & 1] : tables[0];
     __nv_bfloat16 *f4 = nullptr;
-    if ((e = run_convs(g, wbf, in.img, A, in.pitch, sc, err, plan, &f4, s)) != cudaSuccess)
+    if ((e = run_convs(g, wbf, in.img, A, in.pitch, sc, err, plan, &f4, cs)) != cudaSuccess)
       return e;
-    propose_rows_kernel<<<propose_blocks, kRescoreWarps * 32, 0, s>>>(f4, wbf, g.nx, g.ny, g.nz,
-                                                                      block, level, sc.props);
+    // the table is free once the rescoring of atlas a - 2 has read it
+    if (two && a >= 2 && (e = cudaStreamWaitEvent(cs, streams->ev[3 + (a & 1)], 0)) != cudaSuccess)
+      return e;
+    propose_rows_kernel<<<propose_blocks, kRescoreWarps * 32, 0, cs>>>(f4, wbf, g.nx, g.ny, g.nz,
+                                                                       block, level, props);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (two) {
+      if ((e = cudaEventRecord(streams->ev[1 + (a & 1)], cs)) != cudaSuccess) return e;
+      if ((e = cudaStreamWaitEvent(s, streams->ev[1 + (a & 1)], 0)) != cudaSuccess) return e;
+    }
     if (block == kRows && g.nx - 12 >= kRows &&
         (long long)g.nz * g.nx * in.pitch < (1LL << 31) - 1) {
       auto k4 = level == 2 ? rescore4_kernel<2> : level == 3 ? rescore4_kernel<3> : rescore4_kernel<4>;
       k4<<<rescore_blocks, kRescoreWarps * 32, 0, s>>>(
-          sc.props, in.img, A, L, g.nx, g.ny, g.nz, in.pitch, scale, conf_thr, sc.pacc, sc.wacc,
+          props, in.img, A, L, g.nx, g.ny, g.nz, in.pitch, scale, conf_thr, sc.pacc, sc.wacc,
           sc.fallbacks, sc.evaluated);
     } else {
       rescore_kernel<<<rescore_blocks, kRescoreWarps * 32, 0, s>>>(
-          sc.props, block, level, in.img, A, L, g.nx, g.ny, g.nz, in.pitch, neg_k, conf_thr, sc.pacc,
+          props, block, level, in.img, A, L, g.nx, g.ny, g.nz, in.pitch, neg_k, conf_thr, sc.pacc,
           sc.wacc, sc.fallbacks, sc.evaluated);
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (two && (e = cudaEventRecord(streams->ev[3 + (a & 1)], s)) != cudaSuccess) return e;
   }
   finalize_kernel<<<nblk, 256, 0, s>>>(sc.pacc, sc.wacc, out, g.nx, g.ny, g.nz);
   return cudaGetLastError();
@@ -1875,7 +1896,7 @@ cudaError_t learned_probe(const Geometry &g, const void *weights, const float *i
   if (g.nx >= 65536 || g.nz >= 65536) return cudaErrorInvalidValue;
   InferScratch sc = carve(scratch, g.nvox());
   sc.lists = reinterpret_cast<int *>(reinterpret_cast<unsigned char *>(sc.props) +
-                                     prop_table_bytes(g));
+                                     2 * prop_table_bytes(g));
   cudaError_t e;
   if ((e = pack_all(wbf, sc.frag, s)) != cudaSuccess) return e;
   __nv_bfloat16 *f4 = nullptr;
