@@ -44,6 +44,21 @@ def test_rank_sum_set():
                      if i + j + k <= 4}
 
 
+@pytest.mark.parametrize("k,level", [(10, 2), (20, 3), (32, 4)])
+def test_rank_sum_set_sizes_nest(k, level):
+    """The smaller kept sets are the rank triples of lower rank sum, each inside the next."""
+    top = np.array([[0, -1, 1, -2], [0, 1, -1, 2], [3, 2, 4, 1]])
+    s = {tuple(o) for o in learned.rank_sum_set(top, k)}
+    assert len(s) == k and learned.KEPT_LEVEL[k] == level
+    ranks = {(list(top[0]).index(a), list(top[1]).index(b), list(top[2]).index(c)) for a, b, c in s}
+    assert ranks == {(i, j, l) for i in range(4) for j in range(4) for l in range(4)
+                     if i + j + l <= level}
+    bigger = {10: 20, 20: 32, 32: 32}[k]
+    assert s <= {tuple(o) for o in learned.rank_sum_set(top, bigger)}
+    with pytest.raises(KeyError):
+        learned.rank_sum_set(top, 16)
+
+
 def test_samplers_stay_in_the_interior():
     shapes = [(40, 44, 30, 3), (36, 50, 28, 2)]
     smp = learned.random_samples(shapes, 5000, 1)
