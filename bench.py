@@ -3,6 +3,9 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
+With --gpus N > 1 and no launcher around it, the command re-runs itself as N ranks under
+torch.distributed.run; every arm checks that the ranks launched equal --gpus.
+
 One step = one pass of the path (patch SSD -> exp weights -> weighted CT fusion) over one
 synthetic subject (seeded generator; the reference's subject data is not public): one
 pct_synthesize_device call on inputs resident in HBM. Timed with CUDA events on the launching
@@ -150,25 +153,45 @@ def profiled_traffic() -> float | None:
 
 # ---------------------------------------------------------------------------------- CPU side
 
-def cpu_reference_rate(target_s: float, threads: int = 0) -> dict:
+def reference_inputs(sub_nz: int, seed: int = 1) -> dict:
+    """The config-1 subject cropped to sub_nz planes, made by the seeded generator in a child
+    process (which loads libpct_b200.so), handed over through a temporary .npz; the caller then
+    loads only the oracle. Labels are normalised and div is computed by the oracle restatement."""
+    import tempfile
+
+    import oracle
+
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "subject.npz")
+        code = ("import sys, numpy as np; sys.path.insert(0, sys.argv[1]); "
+                "import pseudoctimaging_b200 as pct; "
+                "s = pct.synth_subject(*map(int, sys.argv[2:6]), n_blobs=int(sys.argv[6]), "
+                "seed=int(sys.argv[7])); "
+                "np.savez(sys.argv[8], img=s.img, mri=s.atlas_mri, ct=s.atlas_ct)")
+        subprocess.run([sys.executable, "-c", code, str(REPO), str(NX), str(NY), str(sub_nz),
+                        str(NUM), str(N_BLOBS), str(seed), path], check=True, timeout=600)
+        with np.load(path) as z:
+            img, mri, ct = z["img"], z["mri"], z["ct"]
+    return {"img": img, "mri": mri, "label": oracle.normalize_labels_port(ct),
+            "div": oracle.div_port(SIGMA, BETA)}
+
+
+def cpu_reference_rate(target_s: float, threads: int = 0, subject: dict | None = None) -> dict:
     """Times the reference's OpenMP routine on a z/x-cropped slab of the workload (1 interior
     z-plane, enough interior x-rows for about target_s seconds); returns candidates/s."""
     import oracle
-    import pseudoctimaging_b200 as pct
 
     lo = (NH - 1) // 2 + 1
     sub_nz = 2 * lo + 1
-    s = pct.synth_subject(NX, NY, sub_nz, NUM, n_blobs=N_BLOBS, seed=1)
-    label = pct.normalize_labels(s.atlas_ct)
-    div = pct.div_from(SIGMA, BETA)
+    s = subject if subject is not None else reference_inputs(sub_nz)
 
     def run(xrows: int) -> tuple[float, int]:
         nx = 2 * lo + xrows
-        img = np.ascontiguousarray(s.img[:, :nx, :])
-        mri = np.ascontiguousarray(s.atlas_mri[:, :, :nx, :])
-        lab = np.ascontiguousarray(label[:, :, :nx, :])
+        img = np.ascontiguousarray(s["img"][:, :nx, :])
+        mri = np.ascontiguousarray(s["mri"][:, :, :nx, :])
+        lab = np.ascontiguousarray(s["label"][:, :, :nx, :])
         t = time.perf_counter()
-        oracle.fuse_reference(img, mri, lab, NH, div, multicore=True, threads=threads)
+        oracle.fuse_reference(img, mri, lab, NH, s["div"], multicore=True, threads=threads)
         dt = time.perf_counter() - t
         return dt, candidates(nx, NY, sub_nz, NUM, NH)
 
@@ -195,8 +218,9 @@ def run_reference_arm(args) -> None:
     full = candidates()
     step_s = []
     last = None
+    subject = reference_inputs(2 * ((NH - 1) // 2 + 1) + 1)
     for i in range(args.warmup + args.steps):
-        r = cpu_reference_rate(args.ref_step_seconds)
+        r = cpu_reference_rate(args.ref_step_seconds, subject=subject)
         if i >= args.warmup:
             step_s.append(full / r["cand_per_s"])
             last = r
@@ -218,6 +242,49 @@ def run_reference_arm(args) -> None:
 
 
 # ---------------------------------------------------------------------------------- GPU side
+
+FP64_SAMPLE = 4000  # interior voxels per subject checked against the FP64 oracle
+
+
+def sample_interior(nx: int, ny: int, nz: int, nh: int, n: int = FP64_SAMPLE,
+                    seed: int = 7) -> np.ndarray:
+    """Seeded uniform sample of interior voxels, as flat indices z*nx*ny + x*ny + y."""
+    lo = (nh - 1) // 2 + 1
+    rng = np.random.default_rng(seed)
+    z = rng.integers(lo, nz - lo, n)
+    x = rng.integers(lo, nx - lo, n)
+    y = rng.integers(lo, ny - lo, n)
+    return np.unique(z.astype(np.int64) * nx * ny + x.astype(np.int64) * ny + y)
+
+
+class Fp64Check:
+    """The FP64 CPU oracle (the restatement of MultiAtlasPatchBasedSegmentationOpenMP, bit-exact
+    against the reference's own routine) at sampled interior voxels of one subject, and the error
+    of any output volume against it: MAE and max abs in HU, max relative, NaN-mask mismatches."""
+
+    def __init__(self, img, mri, label, nh, div, n=FP64_SAMPLE):
+        import oracle
+
+        nz, nx, ny = img.shape
+        self.vox = sample_interior(nx, ny, nz, nh, n)
+        t = time.perf_counter()
+        out, prod, sumw = oracle.fuse_port_voxels(img, mri, label, nh, div, self.vox)
+        self.seconds = time.perf_counter() - t
+        self.nan = np.isnan(out)
+        with np.errstate(invalid="ignore", divide="ignore"):
+            self.ref = np.where(self.nan, np.nan, prod / sumw)
+
+    def errors(self, vol) -> dict:
+        a = np.asarray(vol).reshape(-1)[self.vox].astype(np.float64)
+        both = np.isfinite(a) & ~self.nan
+        d = np.abs(a[both] - self.ref[both])
+        return {"mae_hu_vs_fp64": float(d.mean() * 4095.0 / 255.0),
+                "max_abs_hu_vs_fp64": float(d.max() * 4095.0 / 255.0),
+                "max_rel_vs_fp64": float((d / np.maximum(np.abs(self.ref[both]), 1e-30)).max()),
+                "nan_mismatch_vs_fp64": int((np.isnan(a) != self.nan).sum()),
+                "fp64_voxels": int(self.vox.size)}
+
+
 
 def measure_e2e(h, s, label, div, sptr, stream, steps, world, dev) -> dict:
     """The drop-in host-pointer entry point (pct_synthesize) on pinned host buffers: every step
@@ -328,9 +395,12 @@ def run_b200_arm(args) -> None:
 
     plan = pct.query_plan(NX, NY, NZ, NUM, NH, local)
     clocks = clk.summary()
+    check = Fp64Check(s.img, s.atlas_mri, label, NH, div)
+    plain_fp64 = check.errors(d_out.cpu().numpy())
     forms = None
     if world == 1 and NH == 11 and not args.no_forms:
-        forms = time_other_forms(pct, h, d_img, d_mri, d_lab, d_out, div, stream, args)
+        forms = time_other_forms(pct, h, d_img, d_mri, d_lab, d_out, div, stream, args, check)
+        forms["batch"] = measure_batch(args, max(3, args.steps // 4), 1)
     peaks = measured_peaks()
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
     mhz = clocks["sm_mhz"] or peaks.get("sm_max_mhz", 1965.0)
@@ -372,6 +442,9 @@ def run_b200_arm(args) -> None:
         },
         "e2e": e2e,
         "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+        "quality": dict(plain_fp64, fp64_seconds=check.seconds,
+                        note="plain FP32 output vs the FP64 CPU oracle at sampled interior "
+                             "voxels of the full-size subject"),
     }
     if forms:
         line["forms"] = forms
@@ -388,10 +461,11 @@ def run_b200_arm(args) -> None:
         print(json.dumps(line))
 
 
-def time_other_forms(pct, h, d_img, d_mri, d_lab, d_plain, div, stream, args) -> dict:
+def time_other_forms(pct, h, d_img, d_mri, d_lab, d_plain, div, stream, args, check) -> dict:
     """The learned proposal (EXEC_CHOICE 7, committed network) and the tensor-core forms
     (5 FP16, 6 BF16) on the same resident subject as the plain kernel: CUDA-event time per step
-    and the error against the plain kernel's output (HU), so one bench line carries every form."""
+    with its own clock record, the error against the plain kernel's output and against the FP64
+    oracle at sampled voxels (HU), so one bench line carries every form."""
     import torch
 
     from pseudoctimaging_b200 import learned
@@ -402,11 +476,12 @@ def time_other_forms(pct, h, d_img, d_mri, d_lab, d_plain, div, stream, args) ->
     model = learned.LearnedModel.load(learned.CHECKPOINT, torch.cuda.current_device())
     h.attach_model(model, 0.0)
     out = {}
-    for name, choice, steps, k in (("learned", pct.EXEC_LEARNED, 5, 32),
-                                   ("learned_k20", pct.EXEC_LEARNED, 5, 20),
-                                   ("learned_k10", pct.EXEC_LEARNED, 5, 10),
-                                   ("tc_fp16", pct.EXEC_TC_FP16, 2, 0),
-                                   ("tc_bf16", pct.EXEC_TC_BF16, 2, 0)):
+    steps_fast = max(5, args.steps // 2)
+    for name, choice, steps, k in (("learned", pct.EXEC_LEARNED, steps_fast, 32),
+                                   ("learned_k20", pct.EXEC_LEARNED, steps_fast, 20),
+                                   ("learned_k10", pct.EXEC_LEARNED, steps_fast, 10),
+                                   ("tc_fp16", pct.EXEC_TC_FP16, 5, 0),
+                                   ("tc_bf16", pct.EXEC_TC_BF16, 5, 0)):
         o = torch.zeros_like(d_img)
         if k:
             h.set_learned_k(k)
@@ -417,19 +492,24 @@ def time_other_forms(pct, h, d_img, d_mri, d_lab, d_plain, div, stream, args) ->
         step()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(steps):
-            step()
-        e1.record(stream)
-        torch.cuda.synchronize()
+        with ClockSampler(torch.cuda.current_device()) as clk:
+            e0.record(stream)
+            for _ in range(steps):
+                step()
+            e1.record(stream)
+            torch.cuda.synchronize()
         h.device_status(stream.cuda_stream)
         ms = e0.elapsed_time(e1) / steps
-        g = o.cpu().numpy()[core].astype(np.float64)
+        vol = o.cpu().numpy()
+        g = vol[core].astype(np.float64)
         both = np.isfinite(g) & np.isfinite(ref)
         e = np.abs(g[both] - ref[both]) * (4095.0 / 255.0)
+        c = clk.summary()
         out[name] = {"ms_per_step": ms, "value": nvox / (ms / 1e3), "steps": steps,
                      "mae_hu_vs_plain": float(e.mean()), "max_abs_hu_vs_plain": float(e.max()),
-                     "nan_mismatch": int((np.isnan(g) != np.isnan(ref)).sum())}
+                     "nan_mismatch": int((np.isnan(g) != np.isnan(ref)).sum()),
+                     **check.errors(vol),
+                     "clocks": {kk: c[kk] for kk in ("sm_mhz", "sm_max_mhz", "reasons")}}
         if k:
             out[name]["offsets_per_row"] = h.learned_stats()["row_offsets"] / (
                 (NZ - 12) * (NX - 12) * -(-(NY - 12) // 30) * NUM)
@@ -447,65 +527,90 @@ def config3_specs(n: int = 16, seed: int = 3) -> list[tuple[int, int, int, int, 
              int(rng.integers(5, 21)), int(rng.choice([7, 9, 11]))) for _ in range(n)]
 
 
-def run_batch_arm(args) -> None:
+def measure_batch(args, steps: int, warmup: int) -> dict:
     """Config 3: all subjects in one persistent launch captured in a CUDA graph, tile set chosen
-    by the autotuner; one step = one graph replay over every subject."""
+    by the autotuner over every compiled set (timings per set reported); one step = one graph
+    replay over every subject. The first subject is checked against the FP64 oracle at sampled
+    voxels."""
     import tempfile
 
     import torch
 
     import pseudoctimaging_b200 as pct
 
-    dev = torch.device("cuda", 0)
+    dev = torch.device("cuda", torch.cuda.current_device())
     specs = config3_specs(args.batch_subjects)
     subs, keep = [], []
     nvox = cand = 0
+    check = None
+    div = pct.div_from(SIGMA, BETA)
     for i, (nx, ny, nz, num, nh) in enumerate(specs):
         s = pct.synth_subject(nx, ny, nz, num, n_blobs=N_BLOBS, seed=100 + i)
         lab = pct.normalize_labels(s.atlas_ct)
+        if i == 0:
+            check = (Fp64Check(s.img, s.atlas_mri, lab, nh, div, n=1000), (nz, nx, ny))
         d = [torch.from_numpy(x).to(dev) for x in (s.img, s.atlas_mri, lab)]
         out = torch.zeros_like(d[0])
         keep.append((d, out))
         subs.append(pct.SubjectDesc(img=d[0].data_ptr(), atlas=d[1].data_ptr(),
                                     atlas_label=d[2].data_ptr(), out=out.data_ptr(), nx=nx, ny=ny,
-                                    nz=nz, num_atlas=num, nh=nh, div=pct.div_from(SIGMA, BETA)))
+                                    nz=nz, num_atlas=num, nh=nh, div=div))
         nvox += nx * ny * nz
         cand += candidates(nx, ny, nz, num, nh)
         del s
-    h = pct.Handle(0)
+    h = pct.Handle(dev.index)
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
-    cache = os.path.join(tempfile.gettempdir(), "pct_b200_tune.jsonl")
+    cache = os.path.join(tempfile.gettempdir(), f"pct_b200_tune_{os.getpid()}.jsonl")
     chosen, tune_ms = h.autotune(subs, cache)
     g = h.batch_graph(subs, stream.cuda_stream)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         g.launch(stream.cuda_stream)
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(0) as clk:
+    with ClockSampler(dev.index) as clk:
         ev0.record(stream)
-        for _ in range(args.steps):
+        for _ in range(steps):
             g.launch(stream.cuda_stream)
         ev1.record(stream)
         torch.cuda.synchronize()
     g.status(stream.cuda_stream)
-    ms = ev0.elapsed_time(ev1) / args.steps
+    ms = ev0.elapsed_time(ev1) / steps
     clocks = clk.summary()
-    line = {
-        "metric": f"pseudo-CT voxels/s, config 3 batch ({len(specs)} subjects, one persistent "
-                  "launch in a CUDA graph)",
-        "value": nvox / (ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator, config 3)",
-        "config": {"workload": "config 3 batch", "subjects": specs,
-                   "voxels": nvox, "candidates": cand, "tile_set": chosen,
-                   "autotune_ms_per_set": tune_ms},
-        "candidates_per_s": cand / (ms / 1e3),
-        "gpu_launches": args.steps * 1,
-        "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
-    }
+    fp64 = check[0].errors(keep[0][1].cpu().numpy())
     g.close()
     h.close()
+    try:
+        os.remove(cache)
+    except OSError:
+        pass
+    return {"workload": f"config 3: {len(specs)} subjects (x, y 96..222, z 64..112, 5..20 atlases, "
+                        "NH 7/9/11), one persistent launch replayed as a CUDA graph",
+            "ms_per_step": ms, "value": nvox / (ms / 1e3), "unit": UNIT, "steps": steps,
+            "voxels": nvox, "candidates": cand, "candidates_per_s": cand / (ms / 1e3),
+            "tile_set": chosen, "autotune_ms_per_set": tune_ms, "subjects": specs,
+            "fp64_subject0": fp64,
+            "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")}}
+
+
+def run_batch_arm(args) -> None:
+    """Config 3 as its own bench line (see measure_batch)."""
+    b = measure_batch(args, args.steps, args.warmup)
+    line = {
+        "metric": f"pseudo-CT voxels/s, config 3 batch ({args.batch_subjects} subjects, one "
+                  "persistent launch in a CUDA graph)",
+        "value": b["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": b["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded generator, config 3)",
+        "config": {"workload": "config 3 batch", "subjects": b["subjects"], "voxels": b["voxels"],
+                   "candidates": b["candidates"], "tile_set": b["tile_set"],
+                   "autotune_ms_per_set": b["autotune_ms_per_set"]},
+        "candidates_per_s": b["candidates_per_s"],
+        "fp64_subject0": b["fp64_subject0"],
+        "gpu_launches": args.steps * 1,
+        "clocks": b["clocks"],
+    }
     print(json.dumps(line))
 
 
@@ -611,9 +716,9 @@ def run_sharded_arm(args) -> None:
 def run_tc_arm(args) -> None:
     """Config 2: the tensor-core form (EXEC_CHOICE 5 FP16 and 6 BF16: tcgen05 correlation, top-16
     per (voxel, atlas), exact FP32 rescoring) on a 222x222x112 subject with 20 atlases, NH = 11,
-    against the plain FP32 kernel on the same inputs: voxels/s of each and the error against the
-    plain method in HU (the error against the FP64 oracle is measured by the tests at small sizes;
-    a full-size FP64 run takes about half an hour of CPU)."""
+    against the plain FP32 kernel on the same inputs: voxels/s of each, the error against the
+    plain method in HU, and the error of every form against the FP64 CPU oracle at sampled
+    interior voxels of the full-size subject."""
     import torch
 
     import pseudoctimaging_b200 as pct
@@ -651,6 +756,7 @@ def run_tc_arm(args) -> None:
     core = (slice(6, -6),) * 3
     ref = outs[pct.EXEC_B200_FP32][core].astype(np.float64)
     nvox = NX * NY * NZ
+    check = Fp64Check(s.img, s.atlas_mri, label, 11, div)
     forms = {}
     for choice, name in ((pct.EXEC_TC_FP16, "fp16"), (pct.EXEC_TC_BF16, "bf16")):
         g = outs[choice][core].astype(np.float64)
@@ -658,7 +764,8 @@ def run_tc_arm(args) -> None:
         e = np.abs(g[both] - ref[both]) * (4095.0 / 255.0)
         forms[name] = {"ms_per_step": times[choice], "value": nvox / (times[choice] / 1e3),
                        "mae_hu_vs_plain": float(e.mean()), "max_abs_hu_vs_plain": float(e.max()),
-                       "nan_mismatch": int((np.isnan(g) != np.isnan(ref)).sum())}
+                       "nan_mismatch": int((np.isnan(g) != np.isnan(ref)).sum()),
+                       **check.errors(outs[choice])}
     # tensor work: 128 x 128 x 32 per chunk, 28 chunks per tile and atlas
     tiles = -(-(NZ - 12) // 4) * -(-(NX - 12) // 4) * -(-(NY - 12) // 8)
     flop = 2.0 * 128 * 128 * 32 * 28 * tiles * num
@@ -676,7 +783,8 @@ def run_tc_arm(args) -> None:
                    "volume": [NX, NY, NZ], "atlases": num, "nh": 11},
         "forms": forms,
         "plain": {"ms_per_step": times[pct.EXEC_B200_FP32],
-                  "value": nvox / (times[pct.EXEC_B200_FP32] / 1e3)},
+                  "value": nvox / (times[pct.EXEC_B200_FP32] / 1e3),
+                  **check.errors(outs[pct.EXEC_B200_FP32])},
         "gpu_launches": args.steps,
         "roofline": {"bound": "tensor", "unit": "TFLOP/s", "achieved": flop / (ms / 1e3) / 1e12,
                      "peak": peaks.get("bf16_tflops"),
@@ -754,8 +862,10 @@ def run_learned_arm(args) -> None:
         ms = timed(pct.EXEC_LEARNED, o_learn, args.steps, args.warmup)
     st = h.learned_stats()
     core = (slice(6, -6),) * 3
-    a = o_learn.cpu().numpy()[core].astype(np.float64)
-    b = o_plain.cpu().numpy()[core].astype(np.float64)
+    check = Fp64Check(s.img, s.atlas_mri, label, 11, div)
+    vol_learn, vol_plain = o_learn.cpu().numpy(), o_plain.cpu().numpy()
+    a = vol_learn[core].astype(np.float64)
+    b = vol_plain[core].astype(np.float64)
     both = np.isfinite(a) & np.isfinite(b)
     err = np.abs(a[both] - b[both]) * (4095.0 / 255.0)
     nvox = NX * NY * NZ
@@ -776,10 +886,12 @@ def run_learned_arm(args) -> None:
         "config": {"workload": f"config 4: learned proposal, k = {args.k} per row segment",
                    "checkpoint": learned.CHECKPOINT.name, "conf_threshold": args.conf,
                    "volume": [NX, NY, NZ], "atlases": NUM, "nh": 11},
-        "plain": {"ms_per_step": ms_plain, "value": nvox / (ms_plain / 1e3)},
+        "plain": {"ms_per_step": ms_plain, "value": nvox / (ms_plain / 1e3),
+                  **check.errors(vol_plain)},
         "speedup_vs_plain": ms_plain / ms,
         "quality_vs_plain": {"mae_hu": float(err.mean()), "max_abs_hu": float(err.max()),
                              "nan_mismatch": int((np.isnan(a) != np.isnan(b)).sum())},
+        "quality_vs_fp64": check.errors(vol_learn),
         "fallback_share": st["fallback_pairs"] / pairs,
         "offsets_per_row": st["row_offsets"] / rows,
         "gpu_launches": args.steps * (7 + 6 * NUM + 1),
@@ -796,6 +908,45 @@ def run_learned_arm(args) -> None:
     model.close()
     h.close()
     print(json.dumps(line))
+
+
+def spawn_ranks(n: int) -> int:
+    """Re-runs this command as n ranks under torch.distributed.run (one process per GPU) when
+    --gpus asks for more than one GPU and no launcher started us; returns its exit code."""
+    import socket
+
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = ["timeout", "-k", "60", "1800", sys.executable, "-m", "torch.distributed.run",
+           "--nnodes=1", f"--nproc-per-node={n}", "--master-addr", "127.0.0.1",
+           "--master-port", str(port), str(pathlib.Path(__file__).resolve()), *sys.argv[1:]]
+    return subprocess.run(cmd).returncode
+
+
+def run_dry_arm(args) -> None:
+    """The launcher and rank logic without a GPU: every rank joins a gloo group, takes the same
+    barrier and max-reduction as the timed arms, and rank 0 prints n_gpus and the ranks seen."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1:
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+        dist.barrier()
+    t = torch.tensor([float(rank)], dtype=torch.float64)
+    ranks = torch.zeros(world, dtype=torch.float64)
+    ranks[rank] = 1.0
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(ranks, op=dist.ReduceOp.SUM)
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps({"dry": True, "n_gpus": world, "gpus_requested": args.gpus,
+                          "max_rank": int(t.item()), "ranks_seen": int(ranks.sum().item())}))
 
 
 def main() -> None:
@@ -828,11 +979,22 @@ def main() -> None:
                     help="CPU-baseline sample length (rank 0, N=1 only)")
     ap.add_argument("--ref-step-seconds", type=float, default=4.0,
                     help="length of each reference-arm step")
+    ap.add_argument("--dry", action="store_true",
+                    help="launcher and rank logic only (gloo, no GPU work)")
     args = ap.parse_args()
+    if args.gpus < 1:
+        ap.error("--gpus must be at least 1")
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        sys.exit(spawn_ranks(args.gpus))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world != args.gpus:
+        raise SystemExit(f"bench.py: --gpus {args.gpus} but {world} rank(s) were launched")
     NZ = args.nz
     NH = args.nh
     METRIC = f"pseudo-CT voxels/s at {NX}x{NY}x{NZ}, 10 atlases, NH={NH}"
-    if args.impl == "reference":
+    if args.dry:
+        run_dry_arm(args)
+    elif args.impl == "reference":
         run_reference_arm(args)
     elif args.workload == "batch":
         run_batch_arm(args)

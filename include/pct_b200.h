@@ -320,9 +320,12 @@ int pct_regularize_device(pct_handle *h, float *d_vol, int nx, int ny, int nz, i
  * the reference. Same result as pct_regularize_device; needs no handle and calls no allocator:
  * its scratch is a fixed 64 MiB array inside the library, held by every GPU that loads the
  * library until the process exits. Volumes of more than 2^23 voxels (8,388,608) are rejected
- * with PCT_ERR_TOO_LARGE. Runs on the current device; its first call on a device looks up the
- * array's device address, so make that first call before any stream capture. Calls share the
- * array: calls whose work overlaps on the GPU race and must be issued one after another.
+ * with PCT_ERR_TOO_LARGE. Runs on the current device. CUDA loads the library's device code
+ * lazily, so the array is reserved on a device by the first call of this entry point (or of any
+ * other kernel of the library) there: make that first call at start-up, before the caller's pool
+ * takes the device memory and before any stream capture, or set CUDA_MODULE_LOADING=EAGER. Every
+ * call looks up the array's device address on the current device. Calls share the array: calls
+ * whose work overlaps on the GPU race and must be issued one after another.
  * Synchronous on `stream`.
  */
 int pct_regularize_device_noalloc(float *d_vol, int nx, int ny, int nz, int nh, int64_t *fills,

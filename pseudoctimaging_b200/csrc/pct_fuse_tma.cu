@@ -190,6 +190,133 @@ __device__ __forceinline__ void sweep_dw(const float2 (&In)[TZ + 2][RX + 2], flo
   }
 }
 
+// ------------------------------------------------------------- y-pair layout (LY = 1)
+//
+// Same warp tile (30 y x RX x x 2*TZ z) and the same shared-memory slabs as above, mapped
+// differently: half-warp h = lane / 16 owns the z planes [z0 + h*TZ, z0 + h*TZ + TZ), and lane
+// j = lane % 16 owns the two adjacent y positions (y0 - 1 + 2j, y0 + 2j), packed in a float2.
+//  * y-box: each output needs one neighbour value from each side (the left lane's .y, the right
+//    lane's .x): 2 shuffles per voxel pair instead of 4.
+//  * x-box: the squares are folded into the first additions as FMAs
+//    (g = d0*d0 + (d1*d1 + d2*d2) with the inner pair shared by two outputs), 6 instructions per
+//    plane of 3 outputs instead of 5 multiplies + 5 adds.
+//  * labels ride a register ring like the atlas planes: one new plane per dw step.
+//  * a pair's shared-memory address is 8-byte aligned for every other dv (the parity of
+//    dv + HW): those sweeps load pairs with one 64-bit LDS, the others with two 32-bit LDS.
+
+template <bool AL>
+__device__ __forceinline__ float2 lds_pair(uint32_t addr) {
+  if constexpr (AL) {
+    return lds_f32x2(addr);
+  } else {
+    return make_float2(lds_f32(addr), lds_f32(addr + 4));
+  }
+}
+
+// g[x] = d[x]^2 + d[x+1]^2 + d[x+2]^2 for x < RX, two outputs at a time sharing d[x+1]^2 + d[x+2]^2.
+template <int RX>
+__device__ __forceinline__ void xbox_squares(const float2 (&d)[RX + 2], float2 (&g)[RX]) {
+  float2 u = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int x = 0; x < RX; x += 2) {
+    if (x + 1 < RX) {
+      u = mul2(d[x + 2], d[x + 2]);
+      const float2 m = fma2(d[x + 1], d[x + 1], u);
+      g[x] = fma2(d[x], d[x], m);
+      g[x + 1] = fma2(d[x + 3], d[x + 3], m);
+    } else if (x >= 2) {  // odd RX: u holds d[x]^2 from the previous pair
+      g[x] = fma2(d[x + 2], d[x + 2], fma2(d[x + 1], d[x + 1], u));
+    } else {
+      g[x] = fma2(d[x], d[x], fma2(d[x + 1], d[x + 1], mul2(d[x + 2], d[x + 2])));
+    }
+  }
+}
+
+// One dw sweep (all dw for fixed atlas, du, dv) of the lane's voxels, y-pair layout.
+// rowA[r] / rowL[r]: the lane's pair in plane 0 of its half's slab rows, at this dv.
+template <int HW, int RX, int TZ, bool AL, bool LR>
+__device__ __forceinline__ void sweep_dw_yp(const float2 (&In)[TZ + 2][RX + 2],
+                                            float2 (&P)[TZ][RX], float2 (&W)[TZ][RX],
+                                            const uint32_t (&rowA)[RX + 2],
+                                            const uint32_t (&rowL)[RX], const float2 scale2) {
+  using C = Cfg<HW, RX, TZ>;
+  constexpr int NQ = C::NQ, NR = C::NR;
+  // Atlas plane t (= step + D plane) and label plane t (= step + output plane) live in slot
+  // (t + OFF) % NQ; at virtual step v = c*NQ + jj that is slot (jj + plane) % NQ.
+  float2 Aw[NQ][NR];
+  float2 Lw[NQ][RX];
+#pragma unroll
+  for (int t = 0; t < NQ - 1; ++t)
+#pragma unroll
+    for (int r = 0; r < NR; ++r) Aw[(t + C::OFF) % NQ][r] = lds_pair<AL>(rowA[r] + t * C::PLANE);
+  if constexpr (LR) {
+#pragma unroll
+    for (int t = 0; t < TZ - 1; ++t)
+#pragma unroll
+      for (int r = 0; r < RX; ++r)
+        Lw[(t + C::OFF) % NQ][r] = lds_pair<AL>(rowL[r] + t * C::PLANE);
+  }
+#pragma unroll 1
+  for (int c = 0; c < C::NCH; ++c) {
+#pragma unroll
+    for (int jj = 0; jj < NQ; ++jj) {
+      if (jj < C::OFF && c == 0) continue;
+      const uint32_t so = (uint32_t)(c * NQ + jj - C::OFF) * C::PLANE;  // real step s = dw + HW
+      {
+        const int sa = (jj + NQ - 1) % NQ;
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+          Aw[sa][r] = lds_pair<AL>(rowA[r] + so + (NQ - 1) * C::PLANE);
+        if constexpr (LR) {
+          const int sl = (jj + TZ - 1) % NQ;
+#pragma unroll
+          for (int r = 0; r < RX; ++r)
+            Lw[sl][r] = lds_pair<AL>(rowL[r] + so + (TZ - 1) * C::PLANE);
+        }
+      }
+      // Output planes two at a time: the x-box of D = (s A - s I)^2 for the planes they need
+      // (computed once, as late as possible, to keep few x-box sums live), then the z-box, the
+      // y-box (half-warp shuffles), the weight and the accumulators.
+      float2 g[NQ][RX];
+#pragma unroll
+      for (int q = 0; q < TZ; q += 2) {
+#pragma unroll
+        for (int pq = (q == 0 ? 0 : q + 2); pq < (q + 4 < NQ ? q + 4 : NQ); ++pq) {
+          const int sq = (pq + jj) % NQ;
+          float2 d[NR];
+#pragma unroll
+          for (int r = 0; r < NR; ++r) d[r] = fma2(Aw[sq][r], scale2, In[pq][r]);  // s * (A - I)
+          xbox_squares<RX>(d, g[pq]);
+        }
+#pragma unroll
+        for (int x = 0; x < RX; ++x) {
+          float2 S[2];
+          if (q + 1 < TZ) {
+            const float2 mid = add2(g[q + 1][x], g[q + 2][x]);
+            S[0] = add2(g[q][x], mid);
+            S[1] = add2(mid, g[q + 3][x]);
+          } else {
+            S[0] = add2(add2(g[q][x], g[q + 1][x]), g[q + 2][x]);
+          }
+#pragma unroll
+          for (int k = 0; k < 2; ++k) {
+            if (q + k >= TZ) break;
+            const float2 cc = S[k];
+            const float lft = __shfl_up_sync(0xffffffffu, cc.y, 1, 16);
+            const float rgt = __shfl_down_sync(0xffffffffu, cc.x, 1, 16);
+            const float m = cc.x + cc.y;
+            const float2 w = make_float2(ex2_approx(-(m + lft)), ex2_approx(-(m + rgt)));
+            const float2 lab = LR ? Lw[(q + k + jj) % NQ][x]
+                                  : lds_pair<AL>(rowL[x] + so + (q + k) * C::PLANE);
+            P[q + k][x] = fma2(w, lab, P[q + k][x]);
+            W[q + k][x] = add2(W[q + k][x], w);
+          }
+        }
+      }
+    }
+  }
+}
+
 // Pipeline state of one CTA, carried across its work items.
 struct Pipe {
   uint32_t base;              // 128-byte aligned start of the dynamic shared memory
@@ -198,9 +325,10 @@ struct Pipe {
   volatile int *abort_flag;
 };
 
-// Processes work item `item` (tile x atlas group) of subject `sv` with register tile (RX, TZ).
-// Returns false when a bounded wait gave up (the CTA must stop).
-template <int HW, int RX, int TZ>
+// Processes work item `item` (tile x atlas group) of subject `sv` with register tile (RX, TZ) in
+// layout LY (0: z-halves packed; 1: y-pairs, labels read per use; 2: y-pairs, labels in a
+// register ring). Returns false when a bounded wait gave up (the CTA must stop).
+template <int HW, int RX, int TZ, int LY>
 __device__ __forceinline__ bool run_item(const SubjectView &sv, int item, Pipe &pp, int *err,
                                          unsigned long long timeout_ns, int withhold_cta) {
   using C = Cfg<HW, RX, TZ>;
@@ -228,7 +356,11 @@ __device__ __forceinline__ bool run_item(const SubjectView &sv, int item, Pipe &
   const int xw = X0 + warp * RX;   // this warp's first output row
   const int xA = X0 - 1 - HW, zA = z0 - 1 - HW;  // MRI slab origin (row k=0)
   const int xL = X0 - HW, zL = z0 - HW;          // CT slab origin
-  const uint32_t lane_off = (uint32_t)(lane + HW + e) * 4u;
+  // y-pair layout: half-warp hh stacks in z, lane jj owns y positions yp, yp + 1.
+  const int hh = lane >> 4, jj = lane & 15;
+  const int yp = y0 - 1 + 2 * jj;
+  const uint32_t lane_off = LY == 0 ? (uint32_t)(lane + HW + e) * 4u
+                                    : (uint32_t)(2 * jj + HW + e) * 4u + hh * TZ * C::PLANE;
 
   // Input patch values, negated and scaled (D = (s A + In)^2 = s^2 (A - I)^2), zero outside.
   float2 In[NQ][NR];
@@ -238,10 +370,11 @@ __device__ __forceinline__ bool run_item(const SubjectView &sv, int item, Pipe &
     for (int r = 0; r < NR; ++r) {
       float v[2];
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int zz = z0 + h * TZ - 1 + q, xx = xw - 1 + r;
-        v[h] = (zz < sv.nz && xx < sv.nx && y < sv.ny)
-                   ? -__ldg(sv.img + (long long)zz * sv.nxy + (long long)xx * sv.ny + y) * sv.scale
+      for (int k = 0; k < 2; ++k) {
+        const int zz = (LY == 0 ? z0 + k * TZ : z0 + hh * TZ) - 1 + q, xx = xw - 1 + r;
+        const int yy = LY == 0 ? y : yp + k;
+        v[k] = (zz < sv.nz && xx < sv.nx && yy < sv.ny)
+                   ? -__ldg(sv.img + (long long)zz * sv.nxy + (long long)xx * sv.ny + yy) * sv.scale
                    : 0.f;
       }
       In[q][r] = make_float2(v[0], v[1]);
@@ -299,41 +432,66 @@ __device__ __forceinline__ bool run_item(const SubjectView &sv, int item, Pipe &
 #pragma unroll
     for (int r = 0; r < RX; ++r)
       rowL[r] = ringL + (uint32_t)((warp * RX + r + j) % C::RL) * C::SLOT_L + lane_off;
+    if constexpr (LY == 0) {
 #pragma unroll 1
-    for (int dv = -HW; dv <= HW; ++dv) {
-      uint32_t ra[NR], rl[RX];
+      for (int dv = -HW; dv <= HW; ++dv) {
+        uint32_t ra[NR], rl[RX];
 #pragma unroll
-      for (int r = 0; r < NR; ++r) ra[r] = rowA[r] + (uint32_t)(dv * 4);
+        for (int r = 0; r < NR; ++r) ra[r] = rowA[r] + (uint32_t)(dv * 4);
 #pragma unroll
-      for (int r = 0; r < RX; ++r) rl[r] = rowL[r] + (uint32_t)(dv * 4);
-      sweep_dw<HW, RX, TZ>(In, P, W, ra, rl, scale2);
+        for (int r = 0; r < RX; ++r) rl[r] = rowL[r] + (uint32_t)(dv * 4);
+        sweep_dw<HW, RX, TZ>(In, P, W, ra, rl, scale2);
+      }
+    } else {
+      // Pairs are 8-byte aligned when dv + HW is even: those sweeps first, then the others (the
+      // order of the offsets only changes the FP32 summation order).
+#pragma unroll 1
+      for (int sv2 = 0; sv2 < NS; sv2 += 2) {
+        uint32_t ra[NR], rl[RX];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) ra[r] = rowA[r] + (uint32_t)((sv2 - HW) * 4);
+#pragma unroll
+        for (int r = 0; r < RX; ++r) rl[r] = rowL[r] + (uint32_t)((sv2 - HW) * 4);
+        sweep_dw_yp<HW, RX, TZ, true, LY == 2>(In, P, W, ra, rl, scale2);
+      }
+#pragma unroll 1
+      for (int sv2 = 1; sv2 < NS; sv2 += 2) {
+        uint32_t ra[NR], rl[RX];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) ra[r] = rowA[r] + (uint32_t)((sv2 - HW) * 4);
+#pragma unroll
+        for (int r = 0; r < RX; ++r) rl[r] = rowL[r] + (uint32_t)((sv2 - HW) * 4);
+        sweep_dw_yp<HW, RX, TZ, false, LY == 2>(In, P, W, ra, rl, scale2);
+      }
     }
   }
   __syncthreads();  // a timeout in the item's last step is seen here
   if (*pp.abort_flag) return false;
 
-  if (lane >= 1 && lane <= kOutY && y < sv.ny - lo) {
 #pragma unroll
-    for (int h = 0; h < 2; ++h)
+  for (int k = 0; k < 2; ++k) {
+    // LY 0: k is the z half, the lane's y is y; LY 1: k is the y of the pair, the half is hh.
+    const int yy = LY == 0 ? y : yp + k;
+    if (yy < y0 || yy >= y0 + kOutY || yy >= sv.ny - lo) continue;
 #pragma unroll
-      for (int q = 0; q < TZ; ++q) {
-        const int z = z0 + h * TZ + q;
-        if (z >= sv.nz - lo) continue;
+    for (int q = 0; q < TZ; ++q) {
+      const int z = (LY == 0 ? z0 + k * TZ : z0 + hh * TZ) + q;
+      if (z >= sv.nz - lo) continue;
 #pragma unroll
-        for (int r = 0; r < RX; ++r) {
-          const int x = xw + r;
-          if (x >= sv.nx - lo) continue;
-          const float pr = h ? P[q][r].y : P[q][r].x;
-          const float sw = h ? W[q][r].y : W[q][r].x;
-          const long long v = (long long)z * sv.nxy + (long long)x * sv.ny + y;
-          if (sv.groups == 1) {
-            sv.out[v] = fuse_result(pr, sw);
-          } else {
-            sv.partial[(2LL * grp) * sv.nvox + v] = pr;
-            sv.partial[(2LL * grp + 1) * sv.nvox + v] = sw;
-          }
+      for (int r = 0; r < RX; ++r) {
+        const int x = xw + r;
+        if (x >= sv.nx - lo) continue;
+        const float pr = k ? P[q][r].y : P[q][r].x;
+        const float sw = k ? W[q][r].y : W[q][r].x;
+        const long long v = (long long)z * sv.nxy + (long long)x * sv.ny + yy;
+        if (sv.groups == 1) {
+          sv.out[v] = fuse_result(pr, sw);
+        } else {
+          sv.partial[(2LL * grp) * sv.nvox + v] = pr;
+          sv.partial[(2LL * grp + 1) * sv.nvox + v] = sw;
         }
       }
+    }
   }
   return true;
 }
@@ -366,9 +524,9 @@ __device__ __forceinline__ void pipe_drain(const Pipe &pp, unsigned long long ti
     mbar_wait_bounded((pp.gstep & 1) ? bar1 : bar0, (pp.gstep >> 1) & 1, timeout_ns);
 }
 
-// One subject, persistent over its work items.
-template <int HW, int RX, int TZ>
-__global__ void __launch_bounds__(kThreads, 1)
+// One subject, persistent over its work items. MB = CTAs per SM the register budget is sized for.
+template <int HW, int RX, int TZ, int LY, int MB>
+__global__ void __launch_bounds__(kThreads, MB)
     fuse_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmL,
                     TmaParams p) {
   extern __shared__ unsigned char smem_raw[];
@@ -376,23 +534,31 @@ __global__ void __launch_bounds__(kThreads, 1)
   p.sv.tmA = &tmA;
   p.sv.tmL = &tmL;
   for (int item = p.item_begin + blockIdx.x; item < p.item_end; item += gridDim.x) {
-    if (!run_item<HW, RX, TZ>(p.sv, item, pp, p.err, p.timeout_ns, p.withhold_cta)) {
+    if (!run_item<HW, RX, TZ, LY>(p.sv, item, pp, p.err, p.timeout_ns, p.withhold_cta)) {
       pipe_drain(pp, p.timeout_ns);
       return;
     }
   }
 }
 
-// Register tiles (x rows RX, z planes per half TZ) by half window, in two sets the autotuner
-// chooses between. Each compiles to at most 255 registers without spilling more than a few bytes.
-template <int SET, int HW> struct TileOf { static constexpr int RX = 3, TZ = 4; };
-template <> struct TileOf<0, 2> { static constexpr int RX = 3, TZ = 3; };
-template <> struct TileOf<0, 1> { static constexpr int RX = 4, TZ = 2; };
-template <> struct TileOf<1, 5> { static constexpr int RX = 3, TZ = 3; };
-template <> struct TileOf<1, 4> { static constexpr int RX = 4, TZ = 2; };
-template <> struct TileOf<1, 3> { static constexpr int RX = 4, TZ = 2; };
-template <> struct TileOf<1, 2> { static constexpr int RX = 3, TZ = 3; };
-template <> struct TileOf<1, 1> { static constexpr int RX = 4, TZ = 2; };
+// Register tiles (x rows RX, z planes per half TZ, layout LY, CTAs per SM MB) by half window, in
+// sets the autotuner chooses between. Set 0 is the fastest measured shape per window on one B200
+// (222x222x112, 10 atlases): y-pairs (3,4) for NH 7 and 11, y-pairs with the label ring (3,3)
+// for NH 9. Set 1 is the z-pair layout (3,4), set 2 the z-pair (3,3)/(4,2) tiles, set 3 y-pairs
+// with the label ring (3,4), set 4 y-pairs (2,3) at three CTAs per SM (168 registers).
+template <int SET, int HW> struct TileOf { static constexpr int RX = 3, TZ = 4, LY = 1, MB = 1; };
+template <> struct TileOf<0, 4> { static constexpr int RX = 3, TZ = 3, LY = 2, MB = 1; };
+template <> struct TileOf<0, 2> { static constexpr int RX = 3, TZ = 3, LY = 1, MB = 1; };
+template <> struct TileOf<0, 1> { static constexpr int RX = 4, TZ = 2, LY = 1, MB = 1; };
+template <int HW> struct TileOf<1, HW> { static constexpr int RX = 3, TZ = 4, LY = 0, MB = 1; };
+template <> struct TileOf<1, 2> { static constexpr int RX = 3, TZ = 3, LY = 0, MB = 1; };
+template <> struct TileOf<1, 1> { static constexpr int RX = 4, TZ = 2, LY = 0, MB = 1; };
+template <int HW> struct TileOf<2, HW> { static constexpr int RX = 4, TZ = 2, LY = 0, MB = 1; };
+template <> struct TileOf<2, 5> { static constexpr int RX = 3, TZ = 3, LY = 0, MB = 1; };
+template <> struct TileOf<2, 2> { static constexpr int RX = 3, TZ = 3, LY = 0, MB = 1; };
+template <int HW> struct TileOf<3, HW> { static constexpr int RX = 3, TZ = 4, LY = 2, MB = 1; };
+template <> struct TileOf<3, 1> { static constexpr int RX = 4, TZ = 2, LY = 2, MB = 1; };
+template <int HW> struct TileOf<4, HW> { static constexpr int RX = 2, TZ = 3, LY = 1, MB = 3; };
 template <int SET, int HW>
 constexpr int smem_of() {
   return Cfg<HW, TileOf<SET, HW>::RX, TileOf<SET, HW>::TZ>::SMEM;
@@ -416,7 +582,7 @@ struct BatchParams {
 // items of all subjects are numbered consecutively; each CTA walks the list with a grid stride
 // and dispatches every item to the tile code of its subject's window.
 template <int SET>
-__global__ void __launch_bounds__(kThreads, 1) fuse_batch_kernel(const BatchParams bp) {
+__global__ void __launch_bounds__(kThreads, TileOf<SET, 5>::MB) fuse_batch_kernel(const BatchParams bp) {
   extern __shared__ unsigned char smem_raw[];
   Pipe pp = pipe_init(smem_raw);
   int s = 0;
@@ -426,9 +592,9 @@ __global__ void __launch_bounds__(kThreads, 1) fuse_batch_kernel(const BatchPara
     const int local = item - sv.item_begin;
     bool ok = true;
     switch (sv.hw) {
-      case 5: ok = run_item<5, TileOf<SET, 5>::RX, TileOf<SET, 5>::TZ>(sv, local, pp, bp.err, bp.timeout_ns, -1); break;
-      case 4: ok = run_item<4, TileOf<SET, 4>::RX, TileOf<SET, 4>::TZ>(sv, local, pp, bp.err, bp.timeout_ns, -1); break;
-      default: ok = run_item<3, TileOf<SET, 3>::RX, TileOf<SET, 3>::TZ>(sv, local, pp, bp.err, bp.timeout_ns, -1); break;
+      case 5: ok = run_item<5, TileOf<SET, 5>::RX, TileOf<SET, 5>::TZ, TileOf<SET, 5>::LY>(sv, local, pp, bp.err, bp.timeout_ns, -1); break;
+      case 4: ok = run_item<4, TileOf<SET, 4>::RX, TileOf<SET, 4>::TZ, TileOf<SET, 4>::LY>(sv, local, pp, bp.err, bp.timeout_ns, -1); break;
+      default: ok = run_item<3, TileOf<SET, 3>::RX, TileOf<SET, 3>::TZ, TileOf<SET, 3>::LY>(sv, local, pp, bp.err, bp.timeout_ns, -1); break;
     }
     if (!ok) {
       pipe_drain(pp, bp.timeout_ns);
@@ -538,9 +704,9 @@ struct Plan {
 
 template <int SET, int HW>
 cudaError_t plan_hw(const Geometry &g, Plan *pl) {
-  constexpr int RX = TileOf<SET, HW>::RX, TZ = TileOf<SET, HW>::TZ;
+  constexpr int RX = TileOf<SET, HW>::RX, TZ = TileOf<SET, HW>::TZ, LY = TileOf<SET, HW>::LY;
   using C = Cfg<HW, RX, TZ>;
-  auto kern = fuse_tma_kernel<HW, RX, TZ>;
+  auto kern = fuse_tma_kernel<HW, RX, TZ, LY, TileOf<SET, HW>::MB>;
   cudaError_t e;
   if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM)) !=
       cudaSuccess)
@@ -620,7 +786,8 @@ cudaError_t launch_hw(const Geometry &g, const SlabInputs &in, float *out, doubl
   p.item_begin = group_begin * pl.ntiles;
   p.item_end = group_end * pl.ntiles;
   const int blocks = std::min(pl.blocks, p.item_end - p.item_begin);
-  fuse_tma_kernel<HW, RX, TZ><<<blocks, kThreads, C::SMEM, stream>>>(tmA, tmL, p);
+  fuse_tma_kernel<HW, RX, TZ, TileOf<SET, HW>::LY, TileOf<SET, HW>::MB>
+      <<<blocks, kThreads, C::SMEM, stream>>>(tmA, tmL, p);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (whole && pl.groups > 1) return launch_combine_groups(g, partial, pl.groups, out, stream);
   return cudaSuccess;
@@ -639,7 +806,14 @@ cudaError_t plan_set(const Geometry &g, Plan *pl) {
 }
 
 cudaError_t plan_any(const Geometry &g, int set, Plan *pl) {
-  return set == 1 ? plan_set<1>(g, pl) : plan_set<0>(g, pl);
+  switch (set) {
+    case 0: return plan_set<0>(g, pl);
+    case 1: return plan_set<1>(g, pl);
+    case 2: return plan_set<2>(g, pl);
+    case 3: return plan_set<3>(g, pl);
+    case 4: return plan_set<4>(g, pl);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 template <int SET>
@@ -756,8 +930,14 @@ cudaError_t prepare_batch(const BatchSubjectIn *subs, int n, int set, void *dev_
                           cudaStream_t stream, BatchSetup *setup) {
   for (int i = 0; i < n; ++i)
     if (subs[i].geom.hw < 3 || subs[i].geom.hw > 5) return cudaErrorInvalidValue;
-  return set == 1 ? launch_batch_set<1>(subs, n, dev_scratch, err, stream, setup)
-                  : launch_batch_set<0>(subs, n, dev_scratch, err, stream, setup);
+  switch (set) {
+    case 0: return launch_batch_set<0>(subs, n, dev_scratch, err, stream, setup);
+    case 1: return launch_batch_set<1>(subs, n, dev_scratch, err, stream, setup);
+    case 2: return launch_batch_set<2>(subs, n, dev_scratch, err, stream, setup);
+    case 3: return launch_batch_set<3>(subs, n, dev_scratch, err, stream, setup);
+    case 4: return launch_batch_set<4>(subs, n, dev_scratch, err, stream, setup);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 cudaError_t launch_prepared_batch(const BatchSetup &setup, cudaStream_t stream) {
@@ -765,10 +945,14 @@ cudaError_t launch_prepared_batch(const BatchSetup &setup, cudaStream_t stream) 
   if (setup.items == 0) return cudaSuccess;
   BatchParams bp{static_cast<const SubjectView *>(setup.bp_subjects), setup.bp_nsub, setup.items,
                  setup.bp_err, 2000000000ull};
-  if (setup.set == 1)
-    fuse_batch_kernel<1><<<setup.blocks, kThreads, setup.smem, stream>>>(bp);
-  else
-    fuse_batch_kernel<0><<<setup.blocks, kThreads, setup.smem, stream>>>(bp);
+  switch (setup.set) {
+    case 0: fuse_batch_kernel<0><<<setup.blocks, kThreads, setup.smem, stream>>>(bp); break;
+    case 1: fuse_batch_kernel<1><<<setup.blocks, kThreads, setup.smem, stream>>>(bp); break;
+    case 2: fuse_batch_kernel<2><<<setup.blocks, kThreads, setup.smem, stream>>>(bp); break;
+    case 3: fuse_batch_kernel<3><<<setup.blocks, kThreads, setup.smem, stream>>>(bp); break;
+    case 4: fuse_batch_kernel<4><<<setup.blocks, kThreads, setup.smem, stream>>>(bp); break;
+    default: return cudaErrorInvalidValue;
+  }
   return cudaGetLastError();
 }
 
@@ -799,8 +983,14 @@ cudaError_t launch_fuse_tma(const Geometry &g, const SlabInputs &in, float *out,
                             float *partial, int *err, const WaitTest &wt, int set,
                             cudaStream_t stream) {
   if (g.ix <= 0 || g.iy <= 0 || g.iz <= 0) return cudaSuccess;
-  return set == 1 ? launch_set<1>(g, in, out, div, partial, err, wt, -1, -1, stream)
-                  : launch_set<0>(g, in, out, div, partial, err, wt, -1, -1, stream);
+  switch (set) {
+    case 0: return launch_set<0>(g, in, out, div, partial, err, wt, -1, -1, stream);
+    case 1: return launch_set<1>(g, in, out, div, partial, err, wt, -1, -1, stream);
+    case 2: return launch_set<2>(g, in, out, div, partial, err, wt, -1, -1, stream);
+    case 3: return launch_set<3>(g, in, out, div, partial, err, wt, -1, -1, stream);
+    case 4: return launch_set<4>(g, in, out, div, partial, err, wt, -1, -1, stream);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 cudaError_t launch_fuse_tma_groups(const Geometry &g, const SlabInputs &in, double div,
@@ -808,9 +998,14 @@ cudaError_t launch_fuse_tma_groups(const Geometry &g, const SlabInputs &in, doub
                                    int group_end, cudaStream_t stream) {
   if (g.ix <= 0 || g.iy <= 0 || g.iz <= 0) return cudaSuccess;
   const WaitTest wt{0};
-  return set == 1
-             ? launch_set<1>(g, in, nullptr, div, partial, err, wt, group_begin, group_end, stream)
-             : launch_set<0>(g, in, nullptr, div, partial, err, wt, group_begin, group_end, stream);
+  switch (set) {
+    case 0: return launch_set<0>(g, in, nullptr, div, partial, err, wt, group_begin, group_end, stream);
+    case 1: return launch_set<1>(g, in, nullptr, div, partial, err, wt, group_begin, group_end, stream);
+    case 2: return launch_set<2>(g, in, nullptr, div, partial, err, wt, group_begin, group_end, stream);
+    case 3: return launch_set<3>(g, in, nullptr, div, partial, err, wt, group_begin, group_end, stream);
+    case 4: return launch_set<4>(g, in, nullptr, div, partial, err, wt, group_begin, group_end, stream);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 cudaError_t launch_fuse_tma_combine(const Geometry &g, const float *partial, int set, float *out,

@@ -40,7 +40,7 @@ struct WaitTest {
 };
 
 // Tile-shape sets compiled into the library (chosen per handle, see pct_autotune).
-constexpr int kTileSets = 2;
+constexpr int kTileSets = 5;
 size_t fuse_tma_partial_bytes(const Geometry &g, int set);
 struct FusePlanInfo {
   int groups, tiles, ctas, rx, tz;

@@ -8,16 +8,18 @@
 // which allocates on first use; this one uses a fixed array that lives in the library instead.
 //
 // The array below is allocated when the CUDA runtime loads this library's device code on a GPU,
-// and every GPU that loads it keeps it until the process exits. Host code cannot use the
-// array's name as a device address, so the first call on each device (with that device
-// current) looks the address up with cudaGetSymbolAddress; make that first call before any
-// stream capture. All calls share the array and it keeps the last call's contents; the counters
-// that must start at zero are cleared by every call. Calls whose work overlaps on the GPU race on
-// the array: issue them one after another.
+// and every GPU that loads it keeps it until the process exits. CUDA loads modules lazily by
+// default, so on each device that happens at the first call of this entry point (or of any
+// other kernel of the library): make that first call at start-up, before the caller's own pool
+// takes the device memory and before any stream capture (or set CUDA_MODULE_LOADING=EAGER, which
+// loads the array with the library). Host code cannot use the array's name as a device address,
+// so every call looks the address up with cudaGetSymbolAddress on the current device; after the
+// first call on a device that lookup allocates nothing, and it stays correct if the caller resets
+// the device. All calls share the array and it keeps the last call's contents; the counters that
+// must start at zero are cleared by every call. Calls whose work overlaps on the GPU race on the
+// array: issue them one after another.
 #include <cuda_runtime.h>
 #include <stdint.h>
-
-#include <mutex>
 
 #include "pct_b200.h"
 #include "pct_internal.h"
@@ -31,24 +33,13 @@ constexpr size_t kScratchBytes = 64 + 2 * (size_t)kMaxVoxels * sizeof(int);
 
 static __device__ __align__(256) unsigned char g_fill_scratch[kScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-void *g_addr[kMaxDevices] = {};
-
-// Device address of g_fill_scratch for the current device, looked up once per device.
+// Device address of g_fill_scratch on the current device. Looked up on every call (it is cheap),
+// so that a cudaDeviceReset between calls cannot leave a stale address behind.
 cudaError_t scratch_address(void **out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  void *p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_fill_scratch);
   if (e != cudaSuccess) return e;
-  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_addr[dev]) {
-    void *p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_fill_scratch);
-    if (e != cudaSuccess) return e;
-    g_addr[dev] = p;
-  }
-  *out = g_addr[dev];
+  *out = p;
   return cudaSuccess;
 }
 
@@ -58,7 +49,9 @@ extern "C" int pct_regularize_device_noalloc(float *d_vol, int nx, int ny, int n
                                              int64_t *fills, void *stream) {
   if (!d_vol || nx <= 0 || ny <= 0 || nz <= 0 || nh < 1 || (nh % 2) == 0)
     return PCT_ERR_INVALID_ARG;
-  if ((long long)nx * ny * nz > kMaxVoxels) return PCT_ERR_TOO_LARGE;
+  // Compared factor by factor, so no product can overflow before the check.
+  if (nx > kMaxVoxels || ny > kMaxVoxels / nx || nz > kMaxVoxels / ((long long)nx * ny))
+    return PCT_ERR_TOO_LARGE;
   static_assert(kScratchBytes >= 64 + 2 * (size_t)kMaxVoxels * sizeof(int), "scratch too small");
   void *scratch = nullptr;
   if (scratch_address(&scratch) != cudaSuccess) {

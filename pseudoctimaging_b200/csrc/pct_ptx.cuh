@@ -79,6 +79,13 @@ __device__ __forceinline__ float lds_f32(uint32_t addr) {
   return v;
 }
 
+// Two consecutive floats at an 8-byte aligned shared-memory address.
+__device__ __forceinline__ float2 lds_f32x2(uint32_t addr) {
+  float2 v;
+  asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr));
+  return v;
+}
+
 __device__ __forceinline__ float ex2_approx(float x) {
   float r;
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));

@@ -92,3 +92,21 @@ def test_div_and_host_label_normalisation():
     assert pct.div_from(2.5, 1.0) == 337.5
     ct = np.array([-1024.0, 0.0, 3071.0], np.float32)
     np.testing.assert_array_equal(pct.normalize_labels(ct), np.float32(255.0) * ((ct + 1024) / np.float32(4095.0)))
+
+
+@pytest.mark.parametrize("dims", [(1 << 21, 1 << 21, 1 << 21),   # product 2^63 wraps negative
+                                  ((1 << 31) - 1, (1 << 31) - 1, 4),
+                                  (3, 1 << 30, 1 << 30),
+                                  (2048, 2048, 3)])                # 12.6M > 2^23, no overflow
+def test_noalloc_fill_rejects_oversized_shapes_before_any_device_work(dims):
+    """The size check of the allocation-free fill compares factor by factor, so shapes whose
+    voxel count overflows 64 bits are rejected too. Run only where no GPU is visible: the
+    rejection must come before any CUDA call, and without a GPU nothing could run if it did not."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("host-only check; shapes like these are never sent to a GPU entry point")
+    fills = ctypes.c_int64(-1)
+    st = pct.lib.pct_regularize_device_noalloc(ctypes.c_void_p(16), *dims, 7,
+                                               ctypes.byref(fills), None)
+    assert st == -8, pct.STATUS.get(st, st)  # PCT_ERR_TOO_LARGE
+    assert fills.value == -1
