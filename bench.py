@@ -400,6 +400,9 @@ def run_b200_arm(args) -> None:
     forms = None
     if world == 1 and NH == 11 and not args.no_forms:
         forms = time_other_forms(pct, h, d_img, d_mri, d_lab, d_out, div, stream, args, check)
+        fb = forms["learned_conf0.05"]
+        # what the fallback may cost: its share of the plain method's time plus the learned form
+        fb["bound_ms"] = fb["fallback_share"] * ms + forms["learned"]["ms_per_step"]
         forms["batch"] = measure_batch(args, max(3, args.steps // 4), 1)
     peaks = measured_peaks()
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
@@ -477,14 +480,26 @@ def time_other_forms(pct, h, d_img, d_mri, d_lab, d_plain, div, stream, args, ch
     h.attach_model(model, 0.0)
     out = {}
     steps_fast = max(5, args.steps // 2)
-    for name, choice, steps, k in (("learned", pct.EXEC_LEARNED, steps_fast, 32),
-                                   ("learned_k20", pct.EXEC_LEARNED, steps_fast, 20),
-                                   ("learned_k10", pct.EXEC_LEARNED, steps_fast, 10),
-                                   ("tc_fp16", pct.EXEC_TC_FP16, 5, 0),
-                                   ("tc_bf16", pct.EXEC_TC_BF16, 5, 0)):
+    # prior_kN: the same rescoring without the network (the N window offsets nearest the
+    # centre for every voxel), for comparing what the network buys at equal time
+    # learned_conf0.05: the confidence fallback (tiles holding a voxel below the threshold run
+    # the plain full search)
+    for name, choice, steps, k, prior, conf in (
+            ("learned", pct.EXEC_LEARNED, steps_fast, 32, 0, 0.0),
+            ("learned_k20", pct.EXEC_LEARNED, steps_fast, 20, 0, 0.0),
+            ("learned_k10", pct.EXEC_LEARNED, steps_fast, 10, 0, 0.0),
+            ("learned_conf0.05", pct.EXEC_LEARNED, 3, 32, 0, 0.05),
+            ("prior_k32", pct.EXEC_LEARNED, steps_fast, 0, 32, 0.0),
+            ("prior_k57", pct.EXEC_LEARNED, steps_fast, 0, 57, 0.0),
+            ("prior_k81", pct.EXEC_LEARNED, steps_fast, 0, 81, 0.0),
+            ("prior_k123", pct.EXEC_LEARNED, steps_fast, 0, 123, 0.0),
+            ("tc_fp16", pct.EXEC_TC_FP16, 5, 0, 0, 0.0),
+            ("tc_bf16", pct.EXEC_TC_BF16, 5, 0, 0, 0.0)):
         o = torch.zeros_like(d_img)
         if k:
             h.set_learned_k(k)
+        h.set_learned_prior(prior)
+        h.attach_model(model, conf)
 
         def step():
             h.synthesize_device(d_img.data_ptr(), d_mri.data_ptr(), d_lab.data_ptr(), o.data_ptr(),
@@ -510,9 +525,13 @@ def time_other_forms(pct, h, d_img, d_mri, d_lab, d_plain, div, stream, args, ch
                      "nan_mismatch": int((np.isnan(g) != np.isnan(ref)).sum()),
                      **check.errors(vol),
                      "clocks": {kk: c[kk] for kk in ("sm_mhz", "sm_max_mhz", "reasons")}}
-        if k:
-            out[name]["offsets_per_row"] = h.learned_stats()["row_offsets"] / (
+        if k or prior:
+            st = h.learned_stats()
+            out[name]["offsets_per_row"] = st["row_offsets"] / (
                 (NZ - 12) * (NX - 12) * -(-(NY - 12) // 30) * NUM)
+            out[name]["fallback_share"] = st["fallback_pairs"] / (
+                (NZ - 12) * (NX - 12) * (NY - 12) * NUM)
+    h.set_learned_prior(0)
     h.set_learned_k(32)
     h.attach_model(None)
     model.close()

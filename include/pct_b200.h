@@ -272,6 +272,17 @@ int pct_set_learned_convs(pct_handle *h, int every_voxel);
 int pct_set_learned_k(pct_handle *h, int k);
 
 /*
+ * The proposal baseline without a network, for measuring what the network gains: with k > 0,
+ * EXEC_CHOICE 7 runs no convolutions and no proposal kernel and needs no attached model; every
+ * voxel rescores the same k offsets, those of the 11^3 window nearest its centre (by squared
+ * distance, ties in (dw, du, dv) order), with the learned form's exact FP32 rescoring; no
+ * confidence fallback. k = 0 (the default) uses the attached network. 0 <= k <= 125. No
+ * counterpart in the reference (its search is always the full window,
+ * NewPatchedBrainPureC.cpp:1283-1331).
+ */
+int pct_set_learned_prior(pct_handle *h, int k);
+
+/*
  * Tensor-core form (EXEC_CHOICE 5 = FP16, 6 = BF16; NH = 11) runs through pct_synthesize /
  * pct_synthesize_device / pct_run_pipeline. Per (voxel, atlas) the SSD of all 11^3 positions is
  * ranked by a tcgen05 correlation of 16-bit patches (the tile's mean removed, scaled by 1/64,

@@ -151,6 +151,7 @@ SIGNATURES = {
     "pct_set_learned_block": (_I, [_P, _I]),
     "pct_set_learned_convs": (_I, [_P, _I]),
     "pct_set_learned_k": (_I, [_P, _I]),
+    "pct_set_learned_prior": (_I, [_P, _I]),
     "pct_tc_survivors": (_I, [_P, _I, _P, _P, _P, _P, _I, _I, _I, _D, _P, _P]),
     "pct_learned_stats": (_I, [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
     "pct_model_probe": (_I, [_P, _P, _P, _I, _I, _I, _P, _I, _P, _P, _P]),
@@ -265,6 +266,10 @@ class Handle:
         """Offsets rescored per proposal for EXEC_LEARNED: 32 (default; rank triples i + j + k <=
         4 of the 4 best offsets per axis), 20 (<= 3) or 10 (<= 2)."""
         self._check(lib.pct_set_learned_k(self._h, int(k)), "pct_set_learned_k")
+
+    def set_learned_prior(self, k: int) -> None:
+        """k > 0: EXEC_CHOICE 7 runs the no-network centre prior with k offsets; 0: the network."""
+        self._check(lib.pct_set_learned_prior(self._h, k), "pct_set_learned_prior")
 
     def set_learned_convs(self, every_voxel: bool) -> None:
         """Diagnostic: True = EXEC_LEARNED's convolutions over every voxel instead of only the

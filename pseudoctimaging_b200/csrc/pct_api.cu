@@ -40,10 +40,11 @@ struct pct_handle {
   int learned_block = 4;                // rows per proposal block along z and x
   bool learned_every_voxel = false;     // convolutions over the whole volume (diagnostic)
   int learned_level = 4;                // kept rank triples i + j + k <= level (32 offsets)
+  int learned_prior_k = 0;              // > 0: EXEC_CHOICE 7 runs the no-network centre prior
   DevBuf learned;                       // its feature volumes and sums
   long long learned_nvox = 0;           // volume size of the last learned run (0: none yet)
   pct::learned::LearnedStreams learned_streams{};  // convolutions beside the rescoring
-  cudaStream_t learned_stream = nullptr;
+  cudaEvent_t learned_done = nullptr;   // recorded after the last learned run's kernels
   cudaStream_t copy_stream = nullptr;   // uploads of the pipelined host path
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};  // start, first group staged, rest staged
   std::string last_error;
@@ -104,9 +105,10 @@ int check_choice(pct_handle *h, int exec_choice) {
       return fail(h, PCT_ERR_UNSUPPORTED,
                   "exec_choice 8 (batched) runs through pct_synthesize_batch / pct_batch_create");
     case PCT_EXEC_LEARNED:
-      if (h && h->model) return PCT_OK;
+      if (h && (h->model || h->learned_prior_k > 0)) return PCT_OK;
       return fail(h, PCT_ERR_UNSUPPORTED,
-                  "exec_choice 7 (learned proposal) needs a model attached with pct_attach_model");
+                  "exec_choice 7 (learned proposal) needs a model attached with pct_attach_model "
+                  "(or the centre prior, pct_set_learned_prior)");
     case PCT_EXEC_TC_FP16:
     case PCT_EXEC_TC_BF16:
       return PCT_OK;
@@ -155,6 +157,16 @@ int launch_fusion(pct_handle *h, const pct::Geometry &g, const pct::SlabInputs &
 }
 
 // Reads (and clears) the device status word after `s` has drained.
+// Marks the end of a learned run on `s`, so that pct_learned_stats can read its counters later
+// without touching the caller's stream (which may be gone by then).
+int learned_ran(pct_handle *h, const pct::Geometry &g, cudaStream_t s) {
+  if (!h->learned_done)
+    PCT_CUDA(h, cudaEventCreateWithFlags(&h->learned_done, cudaEventDisableTiming));
+  PCT_CUDA(h, cudaEventRecord(h->learned_done, s));
+  h->learned_nvox = g.nvox();
+  return PCT_OK;
+}
+
 // The learned form: conv features, proposal and exact rescoring over all atlases (NH = 11).
 int launch_learned_path(pct_handle *h, const pct::Geometry &g, const pct::SlabInputs &in,
                         float *d_out, double div, cudaStream_t s) {
@@ -162,6 +174,14 @@ int launch_learned_path(pct_handle *h, const pct::Geometry &g, const pct::SlabIn
     return fail(h, PCT_ERR_UNSUPPORTED,
                 "exec_choice 7 (learned proposal) is trained for NH = 11 only, got NH = " +
                     std::to_string(g.nh));
+  if (h->learned_prior_k > 0) {
+    if (g.nx - 12 < 4)
+      return fail(h, PCT_ERR_UNSUPPORTED, "the centre prior needs at least 4 interior x-rows");
+    int st = ensure(h, h->learned, pct::learned::infer_scratch_bytes(g));
+    if (st) return st;
+    PCT_CUDA(h, pct::learned::launch_prior(g, in, d_out, div, h->learned_prior_k, h->learned.ptr, s));
+    return learned_ran(h, g, s);
+  }
   if (pct::learned::model_device(h->model) != h->device)
     return fail(h, PCT_ERR_INVALID_ARG, "the attached model lives on another device");
   int st = ensure(h, h->learned, pct::learned::infer_scratch_bytes(g));
@@ -181,9 +201,7 @@ int launch_learned_path(pct_handle *h, const pct::Geometry &g, const pct::SlabIn
   PCT_CUDA(h, pct::learned::launch_learned(g, pct::learned::model_weights(h->model), in, d_out, div,
                                            h->learned_conf, h->learned_block, h->learned_level,
                                            h->learned_every_voxel, h->learned.ptr, err, &ls, s));
-  h->learned_nvox = g.nvox();
-  h->learned_stream = s;
-  return PCT_OK;
+  return learned_ran(h, g, s);
 }
 
 // The tensor-core form (NH = 11).
@@ -203,6 +221,13 @@ int launch_tc_path(pct_handle *h, const pct::Geometry &g, const pct::SlabInputs 
 
 // Whether a choice runs the TMA-staged plain kernel (which needs 16-byte row strides).
 bool uses_tma_rows(int exec_choice) { return exec_choice <= PCT_EXEC_B200_FP32; }
+
+// The learned form with a confidence threshold sends low-confidence tiles to the plain kernel,
+// whose TMA maps need the same 16-byte row strides.
+bool needs_tma_rows(const pct_handle *h, int exec_choice) {
+  return uses_tma_rows(exec_choice) ||
+         (exec_choice == PCT_EXEC_LEARNED && h->learned_prior_k == 0 && h->learned_conf > 0.f);
+}
 
 int launch_path(pct_handle *h, const pct::Geometry &g, const pct::SlabInputs &in, float *d_out,
                 double div, int exec_choice, cudaStream_t s) {
@@ -494,6 +519,7 @@ int pct_destroy(pct_handle *h) {
                     &h->stage, &h->batch_stage, &h->batch_meta, &h->learned})
     if (b->ptr) cudaFree(b->ptr);
   if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
+  if (h->learned_done) cudaEventDestroy(h->learned_done);
   if (h->learned_streams.aux) cudaStreamDestroy(h->learned_streams.aux);
   for (cudaEvent_t e : h->learned_streams.ev)
     if (e) cudaEventDestroy(e);
@@ -563,6 +589,14 @@ int pct_set_learned_k(pct_handle *h, int k) {
   return PCT_OK;
 }
 
+int pct_set_learned_prior(pct_handle *h, int k) {
+  if (!h) return PCT_ERR_INVALID_ARG;
+  if (k < 0 || k > 125)
+    return fail(h, PCT_ERR_INVALID_ARG, "centre prior k must be 0 (use the network) .. 125");
+  h->learned_prior_k = k;
+  return PCT_OK;
+}
+
 int pct_set_learned_convs(pct_handle *h, int every_voxel) {
   if (!h) return PCT_ERR_INVALID_ARG;
   if (every_voxel != 0 && every_voxel != 1)
@@ -579,9 +613,10 @@ int pct_learned_stats(pct_handle *h, uint64_t *fallback_pairs, uint64_t *row_off
   int st = select_device(h);
   if (st) return st;
   unsigned long long v[2] = {0, 0};
+  if (h->learned_done) PCT_CUDA(h, cudaEventSynchronize(h->learned_done));
   PCT_CUDA(h, cudaMemcpyAsync(v, pct::learned::infer_counters(h->learned.ptr, h->learned_nvox),
-                              sizeof(v), cudaMemcpyDeviceToHost, h->learned_stream));
-  PCT_CUDA(h, cudaStreamSynchronize(h->learned_stream));
+                              sizeof(v), cudaMemcpyDeviceToHost, h->stream));
+  PCT_CUDA(h, cudaStreamSynchronize(h->stream));
   if (fallback_pairs) *fallback_pairs = v[0];
   if (row_offsets) *row_offsets = v[1];
   return PCT_OK;
@@ -605,7 +640,7 @@ int pct_synthesize_device(pct_handle *h, const float *d_img, const float *d_atla
   pct::SlabInputs in{d_img, d_atlas, d_atlas_label, g.ny};
   const bool aligned = (g.ny % 4 == 0) && (reinterpret_cast<uintptr_t>(d_atlas) % 16 == 0) &&
                        (reinterpret_cast<uintptr_t>(d_atlas_label) % 16 == 0);
-  if (!aligned && uses_tma_rows(exec_choice)) {  // TMA needs 16-byte row strides: stage a pitched copy on the handle
+  if (!aligned && needs_tma_rows(h, exec_choice)) {  // TMA needs 16-byte row strides: stage a pitched copy on the handle
     const int pitch = pct::slab_pitch(g.ny);
     const long long rows = (long long)g.num * g.nz * g.nx;
     const size_t bytes = (size_t)rows * pitch * sizeof(float);

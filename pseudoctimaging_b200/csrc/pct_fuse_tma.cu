@@ -96,6 +96,8 @@ struct SubjectView {
   int groups, atlases_per_group;  // items = groups * ntiles (group-major)
   int hw;             // half window of this subject (batched kernel dispatch)
   int item_begin;     // first global item of this subject (batched kernel)
+  int atlas_base;     // first atlas of group 0 (a single-atlas launch over a tile list)
+  float *acc_p, *acc_w;  // non-null: add each voxel's (product, sum_weight) into these instead
 };
 
 struct TmaParams {
@@ -342,7 +344,7 @@ __device__ __forceinline__ bool run_item(const SubjectView &sv, int item, Pipe &
   const int T = sv.atlases_per_group * NS;  // du steps per item (atlas-major)
 
   const int grp = item / sv.ntiles;
-  const int a_first = grp * sv.atlases_per_group;
+  const int a_first = sv.atlas_base + grp * sv.atlases_per_group;
   int t = item - grp * sv.ntiles;
   const int ty = t % sv.tiles_y;
   t /= sv.tiles_y;
@@ -484,7 +486,10 @@ __device__ __forceinline__ bool run_item(const SubjectView &sv, int item, Pipe &
         const float pr = k ? P[q][r].y : P[q][r].x;
         const float sw = k ? W[q][r].y : W[q][r].x;
         const long long v = (long long)z * sv.nxy + (long long)x * sv.ny + yy;
-        if (sv.groups == 1) {
+        if (sv.acc_p) {
+          sv.acc_p[v] += pr;
+          sv.acc_w[v] += sw;
+        } else if (sv.groups == 1) {
           sv.out[v] = fuse_result(pr, sw);
         } else {
           sv.partial[(2LL * grp) * sv.nvox + v] = pr;
@@ -535,6 +540,25 @@ __global__ void __launch_bounds__(kThreads, MB)
   p.sv.tmL = &tmL;
   for (int item = p.item_begin + blockIdx.x; item < p.item_end; item += gridDim.x) {
     if (!run_item<HW, RX, TZ, LY>(p.sv, item, pp, p.err, p.timeout_ns, p.withhold_cta)) {
+      pipe_drain(pp, p.timeout_ns);
+      return;
+    }
+  }
+}
+
+// The full search of one atlas over a device-side list of tiles (count on the device, so the
+// launch needs no host round trip), adding each voxel's sums into sv.acc_p / sv.acc_w.
+template <int HW, int RX, int TZ, int LY, int MB>
+__global__ void __launch_bounds__(kThreads, MB)
+    fuse_list_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmL,
+                     TmaParams p, const int *__restrict__ tiles, const int *__restrict__ count) {
+  extern __shared__ unsigned char smem_raw[];
+  Pipe pp = pipe_init(smem_raw);
+  p.sv.tmA = &tmA;
+  p.sv.tmL = &tmL;
+  const int n = *count;
+  for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    if (!run_item<HW, RX, TZ, LY>(p.sv, tiles[i], pp, p.err, p.timeout_ns, -1)) {
       pipe_drain(pp, p.timeout_ns);
       return;
     }
@@ -953,6 +977,63 @@ cudaError_t launch_prepared_batch(const BatchSetup &setup, cudaStream_t stream) 
     case 4: fuse_batch_kernel<4><<<setup.blocks, kThreads, setup.smem, stream>>>(bp); break;
     default: return cudaErrorInvalidValue;
   }
+  return cudaGetLastError();
+}
+
+TileShape fuse_tile_shape(const Geometry &g) {
+  using T = TileOf<0, 5>;
+  TileShape t{};
+  t.out_y = kOutY;
+  t.xc = kWarps * T::RX;
+  t.zt = 2 * T::TZ;
+  if (g.ix > 0 && g.iy > 0 && g.iz > 0) {
+    t.tiles_y = (g.iy + kOutY - 1) / kOutY;
+    t.tiles_x = (g.ix + t.xc - 1) / t.xc;
+    t.tiles_z = (g.iz + t.zt - 1) / t.zt;
+  }
+  return t;
+}
+
+cudaError_t launch_fuse_tiles(const Geometry &g, const SlabInputs &in, double div, int atlas,
+                              const int *tiles, const int *count, float *acc_p, float *acc_w,
+                              int *err, cudaStream_t stream) {
+  if (g.hw != 5 || atlas < 0 || atlas >= g.num) return cudaErrorInvalidValue;
+  if (g.ix <= 0 || g.iy <= 0 || g.iz <= 0) return cudaSuccess;
+  using T = TileOf<0, 5>;
+  using C = Cfg<5, T::RX, T::TZ>;
+  auto kern = fuse_list_kernel<5, T::RX, T::TZ, T::LY, T::MB>;
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM)) !=
+      cudaSuccess)
+    return e;
+  int per_sm = 1;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, C::SMEM)) !=
+      cudaSuccess)
+    return e;
+  if (per_sm < 1) return cudaErrorLaunchOutOfResources;
+  CUtensorMap tmA, tmL;
+  if ((e = make_slab_map(&tmA, in.atlas, g.nx, g.ny, g.nz, g.num, in.pitch, C::YB, C::ZA)) !=
+      cudaSuccess)
+    return e;
+  if ((e = make_slab_map(&tmL, in.label, g.nx, g.ny, g.nz, g.num, in.pitch, C::YB, C::ZL)) !=
+      cudaSuccess)
+    return e;
+  const TileShape ts = fuse_tile_shape(g);
+  Plan pl{};
+  pl.tiles_y = ts.tiles_y;
+  pl.tiles_x = ts.tiles_x;
+  pl.tiles_z = ts.tiles_z;
+  pl.ntiles = ts.tiles_y * ts.tiles_x * ts.tiles_z;
+  pl.groups = g.num;  // atlases_per_group = 1; only group 0 (atlas_base) is run
+  TmaParams p{};
+  p.sv = subject_view(g, in, nullptr, div, nullptr, pl);
+  p.sv.atlas_base = atlas;
+  p.sv.acc_p = acc_p;
+  p.sv.acc_w = acc_w;
+  p.err = err;
+  p.timeout_ns = 2000000000ull;
+  p.withhold_cta = -1;
+  kern<<<sm_count() * per_sm, kThreads, C::SMEM, stream>>>(tmA, tmL, p, tiles, count);
   return cudaGetLastError();
 }
 

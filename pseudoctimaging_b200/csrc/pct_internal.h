@@ -59,6 +59,20 @@ cudaError_t launch_fuse_tma_groups(const Geometry &g, const SlabInputs &in, doub
 cudaError_t launch_fuse_tma_combine(const Geometry &g, const float *partial, int set, float *out,
                                     cudaStream_t stream);
 
+// Tiles of the plain kernel as the learned form's fallback sees them (NH = 11, tile set 0): tile
+// t = (tz * tiles_x + tx) * tiles_y + ty covers interior y [30 ty, 30 ty + 30), x rows
+// [xc tx, xc tx + xc) and z planes [zt tz, zt tz + zt), counted from the first interior voxel.
+struct TileShape {
+  int out_y, xc, zt;
+  int tiles_y, tiles_x, tiles_z;
+};
+TileShape fuse_tile_shape(const Geometry &g);
+// The plain full search of atlas `atlas` (NH = 11) over the *count tiles listed in `tiles` (both
+// on the device), adding every voxel's product and weight sums into acc_p / acc_w.
+cudaError_t launch_fuse_tiles(const Geometry &g, const SlabInputs &in, double div, int atlas,
+                              const int *tiles, const int *count, float *acc_p, float *acc_w,
+                              int *err, cudaStream_t stream);
+
 // Batched form: many subjects (NH 7/9/11), one persistent launch.
 struct BatchSubjectIn {
   Geometry geom;
@@ -120,6 +134,11 @@ cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInp
                            double div, float conf_thr, int block, int level, bool every_voxel,
                            void *scratch, int *err, const LearnedStreams *streams,
                            cudaStream_t s);
+// The proposal baseline without a network (no convolutions, no proposal kernel): every voxel
+// rescores the k offsets of the window nearest its centre (1 <= k <= 125), with the same exact
+// FP32 rescoring as the learned form. Writes the interior of out.
+cudaError_t launch_prior(const Geometry &g, const SlabInputs &in, float *out, double div, int k,
+                         void *scratch, cudaStream_t s);
 cudaError_t learned_probe(const Geometry &g, const void *weights, const float *img,
                           const float *atlas_a, void *scratch, const int64_t *voxels, int n,
                           float *features, signed char *top, float *conf, cudaStream_t s);

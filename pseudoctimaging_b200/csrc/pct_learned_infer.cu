@@ -22,6 +22,8 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <array>
+#include <algorithm>
 #include <vector>
 
 #include "pct_internal.h"
@@ -271,7 +273,8 @@ __global__ void __launch_bounds__(kCvThreads, 2)
       }
       // planes still landing: wait for the last ring's worth (bounded)
       for (uint32_t q = j > kCvRing ? j - kCvRing : 0; q < j; ++q)
-        ptx::mbar_wait_bounded(full0 + 8 * (q % kCvRing), (q / kCvRing) & 1, kConvTimeoutNs);
+        if (!ptx::mbar_wait_bounded(full0 + 8 * (q % kCvRing), (q / kCvRing) & 1, kConvTimeoutNs))
+          *abort_flag = 1;  // reported as a timeout
     }
   } else if (warp == 5) {
     // MMA issuer: the whole warp runs the loop, one elected lane issues
@@ -325,7 +328,8 @@ __global__ void __launch_bounds__(kCvThreads, 2)
       }
     }
     // let every issued MMA finish before the accumulators are released (bounded)
-    if (j > 0) ptx::mbar_wait_bounded(mdone, (j - 1) & 1, kConvTimeoutNs);
+    if (j > 0 && !ptx::mbar_wait_bounded(mdone, (j - 1) & 1, kConvTimeoutNs))
+      *abort_flag = 1;  // reported as a timeout
   } else {
     // epilogue: warp w reads TMEM lanes 32w..32w+31 = output y0 + 32w + lane
     const uint32_t lane_addr = tmem + ((uint32_t)(32 * warp) << 16);
@@ -520,7 +524,8 @@ __global__ void __launch_bounds__(kCvThreads, 2)
       }
       // planes still landing: wait for the last ring's worth (bounded)
       for (uint32_t q = j > kRwRing ? j - kRwRing : 0; q < j; ++q)
-        ptx::mbar_wait_bounded(full0 + 8 * (q % kRwRing), (q / kRwRing) & 1, kConvTimeoutNs);
+        if (!ptx::mbar_wait_bounded(full0 + 8 * (q % kRwRing), (q / kRwRing) & 1, kConvTimeoutNs))
+          *abort_flag = 1;  // reported as a timeout
     }
   } else if (warp == 5) {
     // MMA issuer: the whole warp runs the loop, one elected lane issues
@@ -576,7 +581,9 @@ __global__ void __launch_bounds__(kCvThreads, 2)
         j0 += c.planes + 2;
       }
       // let every issued MMA finish before the accumulators are released (bounded)
-      if (t > 0) ptx::mbar_wait_bounded(dfull0 + 8 * ((t - 1) & 1), ((t - 1) >> 1) & 1, kConvTimeoutNs);
+      if (t > 0 &&
+          !ptx::mbar_wait_bounded(dfull0 + 8 * ((t - 1) & 1), ((t - 1) >> 1) & 1, kConvTimeoutNs))
+        *abort_flag = 1;  // reported as a timeout
     }
   } else {
     // epilogue: warp w reads TMEM lanes 32w..32w+31 = output y0 + 32w + lane
@@ -841,7 +848,8 @@ __global__ void __launch_bounds__(kC1Threads, 2)
         }
       }
     }
-    if (j > 0) ptx::mbar_wait_bounded(mdone, (j - 1) & 1, kConvTimeoutNs);
+    if (j > 0 && !ptx::mbar_wait_bounded(mdone, (j - 1) & 1, kConvTimeoutNs))
+      *abort_flag = 1;  // reported as a timeout
   } else {
     // epilogue: warp w reads TMEM lanes 32w..32w+31 = output y0 + 32w + lane
     const uint32_t lane_addr = tmem + ((uint32_t)(32 * warp) << 16);
@@ -1096,6 +1104,7 @@ __global__ void proposal_hook_kernel(const __nv_bfloat16 *__restrict__ f4,
 }
 
 constexpr int kRowOut = 30;       // output voxels per warp row (lanes 1..30)
+constexpr int kMaxPrior = 125;    // offsets of the no-network prior (5 x 5 x 5 around the centre)
 constexpr int kRescoreWarps = 4;  // warps per CTA
 constexpr int kProbStride = kHeads;  // 33 floats per lane row: column reads are conflict-free
 
@@ -1386,7 +1395,8 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 4)
                     const float *__restrict__ atl, const float *__restrict__ lab, int nx, int ny,
                     int nz, int apitch, float scale, float conf_thr, float *__restrict__ pacc,
                     float *__restrict__ wacc, unsigned long long *__restrict__ fallbacks,
-                    unsigned long long *__restrict__ evaluated) {
+                    unsigned long long *__restrict__ evaluated,
+                    const unsigned char *__restrict__ tile_flag, const TileShape ts) {
   __shared__ int s_off[kRescoreWarps][kTopK];  // per warp: the item's kept offsets, 32-bit
   const int lane = threadIdx.x & 31;
   int *w_off = s_off[threadIdx.x >> 5];
@@ -1405,6 +1415,10 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 4)
     const long long r0 = it / segs;
     const int bx = (int)(r0 % nbx), z = (int)(r0 / nbx) + lo;
     const int xb = lo + bx * kRows;
+    // items of tiles that fell back to the plain kernel are left to it (warp-uniform)
+    if (tile_flag &&
+        tile_flag[((z - lo) / ts.zt * ts.tiles_x + (xb - lo) / ts.xc) * ts.tiles_y + seg])
+      continue;
     const int x0 = min(xb, nx - lo - kRows);
     const int y0 = lo + seg * kRowOut;
     const int y = y0 - 1 + lane;
@@ -1492,6 +1506,117 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 4)
   if (lane == 0 && my_evals) atomicAdd(evaluated, my_evals);
 }
 
+// The confidence fallback at the plain kernel's tile granularity (blocks of 4 x 4 rows share a
+// proposal and its per-voxel confidences): a tile falls back when any of its interior voxels has
+// a confidence below the threshold. Flagged tiles are listed (any order: each tile's result does
+// not depend on it) for the plain kernel, which runs the full search on them; the rescoring skips
+// them. Counts the fallback (voxel, atlas) pairs and the offsets evaluated by their rows.
+__global__ void flag_tiles_kernel(const RowProp *__restrict__ props, int nx, int ny, int nz,
+                                  float conf_thr, const TileShape ts,
+                                  unsigned char *__restrict__ flag, int *__restrict__ list,
+                                  int *__restrict__ count,
+                                  unsigned long long *__restrict__ fallbacks,
+                                  unsigned long long *__restrict__ evaluated) {
+  const int lo = 6;
+  const int ix = nx - 2 * lo, iy = ny - 2 * lo, iz = nz - 2 * lo;
+  const int nbx = (ix + kRows - 1) / kRows, segs = (iy + kRowOut - 1) / kRowOut;
+  const int ntiles = ts.tiles_y * ts.tiles_x * ts.tiles_z;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += gridDim.x * blockDim.x) {
+    const int ty = t % ts.tiles_y, r = t / ts.tiles_y;
+    const int tx = r % ts.tiles_x, tz = r / ts.tiles_x;
+    const int x0 = tx * ts.xc, x1 = min(x0 + ts.xc, ix);  // interior-relative
+    const int z0 = tz * ts.zt, z1 = min(z0 + ts.zt, iz);
+    const int nyv = min(kRowOut, iy - ty * kRowOut);
+    bool any = false;
+    for (int zb = z0 / kRows; zb <= (z1 - 1) / kRows && !any; ++zb)
+      for (int bx = x0 / kRows; bx <= (x1 - 1) / kRows && !any; ++bx) {
+        const RowProp &rp = props[((long long)zb * nbx + bx) * segs + ty];
+        for (int l = 0; l < nyv; ++l)
+          if (rp.conf[l] < conf_thr) {
+            any = true;
+            break;
+          }
+      }
+    flag[t] = any ? 1 : 0;
+    if (any) {
+      list[atomicAdd(count, 1)] = t;
+      const unsigned long long rows = (unsigned long long)(z1 - z0) * (x1 - x0);
+      atomicAdd(fallbacks, rows * nyv);
+      atomicAdd(evaluated, rows * kAxis * kAxis * kAxis);
+    }
+  }
+}
+
+// The proposal baseline without a network: every voxel rescores the same k offsets, the ones of
+// the window nearest its centre. Same items, taps and arithmetic as rescore4_kernel; the offsets
+// (32-bit element offsets into the atlas volume) come from the kernel parameters.
+struct PriorList {
+  int n;
+  int off[kMaxPrior];
+};
+
+__global__ void __launch_bounds__(kRescoreWarps * 32, 4)
+    rescore_prior_kernel(const __grid_constant__ PriorList pl, const float *__restrict__ img,
+                         const float *__restrict__ atl, const float *__restrict__ lab, int nx,
+                         int ny, int nz, int apitch, float scale, float *__restrict__ pacc,
+                         float *__restrict__ wacc, unsigned long long *__restrict__ evaluated) {
+  const int lane = threadIdx.x & 31;
+  const int lo = 6;
+  const int ix = nx - 2 * lo, iz = nz - 2 * lo, iy = ny - 2 * lo;
+  if (ix < kRows || iy <= 0 || iz <= 0) return;
+  const int segs = (iy + kRowOut - 1) / kRowOut;
+  const int nbx = (ix + kRows - 1) / kRows;
+  const long long items = (long long)iz * nbx * segs;
+  const int nxy = nx * ny;
+  const int axy = nx * apitch;
+  unsigned long long my_evals = 0;
+  for (long long it = (long long)blockIdx.x * kRescoreWarps + (threadIdx.x >> 5); it < items;
+       it += (long long)gridDim.x * kRescoreWarps) {
+    const int seg = (int)(it % segs);
+    const long long r0 = it / segs;
+    const int bx = (int)(r0 % nbx), z = (int)(r0 / nbx) + lo;
+    const int xb = lo + bx * kRows;
+    const int x0 = min(xb, nx - lo - kRows);
+    const int y0 = lo + seg * kRowOut;
+    const int y = y0 - 1 + lane;
+    const bool out_lane = lane >= 1 && lane <= kRowOut && y < ny - lo;
+    const int yc = min(y, ny - lo);
+    unsigned owned = 0;
+#pragma unroll
+    for (int r = 0; r < kRows; ++r)
+      if (x0 + r >= xb) owned |= 1u << r;
+    const unsigned take = out_lane ? owned : 0u;
+    float2 in[3][(kRows + 2) / 2];
+#pragma unroll
+    for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+      for (int xp = 0; xp < (kRows + 2) / 2; ++xp) {
+        const float *pi = img + (long long)(z + dz - 1) * nxy + (long long)(x0 - 1 + 2 * xp) * ny + yc;
+        in[dz][xp] = make_float2(-__ldg(pi) * scale, -__ldg(pi + ny) * scale);
+      }
+    const float2 s2 = make_float2(scale, scale);
+    const float *ab = atl + ((long long)(z - 1) * axy + (long long)(x0 - 1) * apitch + yc);
+    const float *lb = lab + ((long long)z * axy + (long long)x0 * apitch + yc);
+    float P[kRows], W[kRows];
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) P[r] = W[r] = 0.f;
+#pragma unroll 2
+    for (int c = 0; c < pl.n; ++c) {
+      const int off = pl.off[c];
+      eval_offset4(ab + off, lb + off, in, axy, apitch, take, s2, P, W);
+    }
+    my_evals += (unsigned long long)pl.n * __popc(owned);
+#pragma unroll
+    for (int r = 0; r < kRows; ++r)
+      if ((take >> r) & 1u) {
+        const long long v = (long long)z * nxy + (long long)(x0 + r) * ny + y;
+        pacc[v] += P[r];
+        wacc[v] += W[r];
+      }
+  }
+  if (lane == 0 && my_evals) atomicAdd(evaluated, my_evals);
+}
+
 __global__ void finalize_kernel(const float *__restrict__ pacc, const float *__restrict__ wacc,
                                 float *__restrict__ out, int nx, int ny, int nz) {
   const int lo = 6;
@@ -1567,8 +1692,16 @@ size_t prop_table_bytes(const Geometry &g) {
   return (rows * sizeof(RowProp) + 255) / 256 * 256;
 }
 
+// The confidence fallback's tile flags, list and count (after the convolutions' lists).
+size_t fallback_bytes(const Geometry &g) {
+  const TileShape ts = fuse_tile_shape(g);
+  const size_t ntiles = (size_t)ts.tiles_y * ts.tiles_x * ts.tiles_z;
+  return 16 + ntiles * sizeof(int) + ntiles + 256;
+}
+
 size_t infer_scratch_bytes(const Geometry &g) {
-  return infer_base_bytes(g.nvox()) + 2 * prop_table_bytes(g) + conv_list_bytes(g) + 256;
+  return infer_base_bytes(g.nvox()) + 2 * prop_table_bytes(g) + conv_list_bytes(g) +
+         fallback_bytes(g) + 256;
 }
 
 unsigned long long *infer_counters(void *scratch, long long nvox) {
@@ -1825,6 +1958,18 @@ cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInp
   if ((e = cudaMemcpyAsync(sc.lists, lists.data(), lists.size() * sizeof(int),
                            cudaMemcpyHostToDevice, s)) != cudaSuccess)
     return e;
+  // Confidence fallback through the plain kernel's tiles, where its TMA maps can read the stacks
+  // (16-byte row strides); otherwise the rescoring runs the full window for low-confidence rows.
+  const TileShape ts = fuse_tile_shape(g);
+  const int ntiles = ts.tiles_y * ts.tiles_x * ts.tiles_z;
+  const bool tile_fallback =
+      conf_thr > 0.f && block == kRows && g.hw == 5 && ntiles > 0 && in.pitch % 4 == 0 &&
+      reinterpret_cast<uintptr_t>(in.atlas) % 16 == 0 &&
+      reinterpret_cast<uintptr_t>(in.label) % 16 == 0;
+  unsigned char *fb_region = reinterpret_cast<unsigned char *>(sc.lists) + conv_list_bytes(g);
+  int *fb_count = reinterpret_cast<int *>(fb_region);
+  int *fb_list = reinterpret_cast<int *>(fb_region + 16);
+  unsigned char *fb_flag = fb_region + 16 + (size_t)ntiles * sizeof(int);
   if ((e = cudaMemsetAsync(sc.pacc, 0, (size_t)nvox * 4 * 2, s)) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(sc.fallbacks, 0, 2 * sizeof(unsigned long long), s)) != cudaSuccess)
     return e;
@@ -1854,37 +1999,105 @@ cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInp
     if ((e = cudaEventRecord(streams->ev[0], s)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(cs, streams->ev[0], 0)) != cudaSuccess) return e;
   }
+  // Every exit after the fork joins the auxiliary stream back into s (the last atlas's wait for
+  // its proposal already does on success; on an error the work queued on cs must not outlive
+  // the call unordered).
+  auto join = [&](cudaError_t status) {
+    if (two && cudaEventRecord(streams->ev[0], cs) == cudaSuccess)
+      cudaStreamWaitEvent(s, streams->ev[0], 0);
+    return status;
+  };
   for (int a = 0; a < g.num; ++a) {
     const float *A = in.atlas + a * astride, *L = in.label + a * astride;
     RowProp *props = two ? tables[a & 1] : tables[0];
     __nv_bfloat16 *f4 = nullptr;
     if ((e = run_convs(g, wbf, in.img, A, in.pitch, sc, err, plan, &f4, cs)) != cudaSuccess)
-      return e;
+      return join(e);
     // the table is free once the rescoring of atlas a - 2 has read it
     if (two && a >= 2 && (e = cudaStreamWaitEvent(cs, streams->ev[3 + (a & 1)], 0)) != cudaSuccess)
-      return e;
+      return join(e);
     propose_rows_kernel<<<propose_blocks, kRescoreWarps * 32, 0, cs>>>(f4, wbf, g.nx, g.ny, g.nz,
                                                                        block, level, props);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = cudaGetLastError()) != cudaSuccess) return join(e);
     if (two) {
-      if ((e = cudaEventRecord(streams->ev[1 + (a & 1)], cs)) != cudaSuccess) return e;
-      if ((e = cudaStreamWaitEvent(s, streams->ev[1 + (a & 1)], 0)) != cudaSuccess) return e;
+      if ((e = cudaEventRecord(streams->ev[1 + (a & 1)], cs)) != cudaSuccess) return join(e);
+      if ((e = cudaStreamWaitEvent(s, streams->ev[1 + (a & 1)], 0)) != cudaSuccess) return join(e);
     }
     if (block == kRows && g.nx - 12 >= kRows &&
         (long long)g.nz * g.nx * in.pitch < (1LL << 31) - 1) {
+      if (tile_fallback) {
+        if ((e = cudaMemsetAsync(fb_count, 0, sizeof(int), s)) != cudaSuccess) return join(e);
+        flag_tiles_kernel<<<(ntiles + 255) / 256, 256, 0, s>>>(
+            props, g.nx, g.ny, g.nz, conf_thr, ts, fb_flag, fb_list, fb_count, sc.fallbacks,
+            sc.evaluated);
+        if ((e = cudaGetLastError()) != cudaSuccess) return join(e);
+      }
       auto k4 = level == 2 ? rescore4_kernel<2> : level == 3 ? rescore4_kernel<3> : rescore4_kernel<4>;
       k4<<<rescore_blocks, kRescoreWarps * 32, 0, s>>>(
-          props, in.img, A, L, g.nx, g.ny, g.nz, in.pitch, scale, conf_thr, sc.pacc, sc.wacc,
-          sc.fallbacks, sc.evaluated);
+          props, in.img, A, L, g.nx, g.ny, g.nz, in.pitch, scale, tile_fallback ? 0.f : conf_thr,
+          sc.pacc, sc.wacc, sc.fallbacks, sc.evaluated, tile_fallback ? fb_flag : nullptr, ts);
+      if (tile_fallback) {
+        if ((e = cudaGetLastError()) != cudaSuccess) return join(e);
+        if ((e = launch_fuse_tiles(g, in, div, a, fb_list, fb_count, sc.pacc, sc.wacc, err, s)) !=
+            cudaSuccess)
+          return join(e);
+      }
     } else {
       rescore_kernel<<<rescore_blocks, kRescoreWarps * 32, 0, s>>>(
           props, block, level, in.img, A, L, g.nx, g.ny, g.nz, in.pitch, neg_k, conf_thr, sc.pacc,
           sc.wacc, sc.fallbacks, sc.evaluated);
     }
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if (two && (e = cudaEventRecord(streams->ev[3 + (a & 1)], s)) != cudaSuccess) return e;
+    if ((e = cudaGetLastError()) != cudaSuccess) return join(e);
+    if (two && (e = cudaEventRecord(streams->ev[3 + (a & 1)], s)) != cudaSuccess) return join(e);
   }
   finalize_kernel<<<nblk, 256, 0, s>>>(sc.pacc, sc.wacc, out, g.nx, g.ny, g.nz);
+  return cudaGetLastError();
+}
+
+// The k offsets (dw, du, dv) of the 11^3 window nearest its centre, by squared distance, ties
+// in (dw, du, dv) order.
+std::vector<std::array<int, 3>> prior_offsets(int k) {
+  std::vector<std::array<int, 3>> all;
+  for (int dw = -5; dw <= 5; ++dw)
+    for (int du = -5; du <= 5; ++du)
+      for (int dv = -5; dv <= 5; ++dv) all.push_back({dw, du, dv});
+  std::stable_sort(all.begin(), all.end(), [](const std::array<int, 3> &a, const std::array<int, 3> &b) {
+    return a[0] * a[0] + a[1] * a[1] + a[2] * a[2] < b[0] * b[0] + b[1] * b[1] + b[2] * b[2];
+  });
+  all.resize(k);
+  return all;
+}
+
+cudaError_t launch_prior(const Geometry &g, const SlabInputs &in, float *out, double div, int k,
+                         void *scratch, cudaStream_t s) {
+  if (k < 1 || k > kMaxPrior) return cudaErrorInvalidValue;
+  if (g.nx - 12 < kRows || (long long)g.nz * g.nx * in.pitch >= (1LL << 31) - 1)
+    return cudaErrorInvalidValue;
+  const long long nvox = g.nvox();
+  InferScratch sc = carve(scratch, nvox);
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(sc.pacc, 0, (size_t)nvox * 4 * 2, s)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(sc.fallbacks, 0, 2 * sizeof(unsigned long long), s)) != cudaSuccess)
+    return e;
+  PriorList pl{};
+  pl.n = k;
+  const int axy = g.nx * in.pitch;
+  const auto offs = prior_offsets(k);
+  for (int c = 0; c < k; ++c) pl.off[c] = offs[c][0] * axy + offs[c][1] * in.pitch + offs[c][2];
+  const float scale = (float)sqrt(1.4426950408889634 / div);
+  long long rows = 0;
+  if (g.nx > 12 && g.ny > 12 && g.nz > 12)
+    rows = (long long)(g.nz - 12) * (g.nx - 12) * ((g.ny - 12 + kRowOut - 1) / kRowOut);
+  const long long rblk = (rows + kRescoreWarps - 1) / kRescoreWarps;
+  const int blocks = (int)(rblk < 1 ? 1 : (rblk > 64LL * sms() ? 64LL * sms() : rblk));
+  const long long astride = (long long)g.nz * g.nx * in.pitch;
+  for (int a = 0; a < g.num; ++a) {
+    rescore_prior_kernel<<<blocks, kRescoreWarps * 32, 0, s>>>(
+        pl, in.img, in.atlas + a * astride, in.label + a * astride, g.nx, g.ny, g.nz, in.pitch,
+        scale, sc.pacc, sc.wacc, sc.evaluated);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  finalize_kernel<<<sms() * 8, 256, 0, s>>>(sc.pacc, sc.wacc, out, g.nx, g.ny, g.nz);
   return cudaGetLastError();
 }
 

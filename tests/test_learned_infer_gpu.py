@@ -131,6 +131,43 @@ def test_full_fallback_is_the_plain_method(shape):
     assert st["row_offsets"] == rows_of(nx, ny, nz) * 1331 * num
 
 
+def centre_offsets(k):
+    """The k offsets of the 11^3 window nearest its centre, by squared distance, ties in
+    (dw, du, dv) order (a stable sort of the lexicographic enumeration)."""
+    import itertools
+    return sorted(itertools.product(range(-5, 6), repeat=3),
+                  key=lambda o: o[0] ** 2 + o[1] ** 2 + o[2] ** 2)[:k]
+
+
+@pytest.mark.parametrize("k", [1, 7, 32, 57, 125])
+def test_centre_prior_without_network_exact(k):
+    """The no-network baseline (pct_set_learned_prior): no convolutions, no proposal, every voxel
+    rescores the k centre offsets; exact against the float64 fusion over those offsets."""
+    nx, ny, nz, num = 36, 41, 30, 2
+    img, atl, lab = subject(nx, ny, nz, num, 21)
+    ref, prod, sumw = fuse_offsets_f64(img, atl, lab, centre_offsets(k), DIV)
+    with pct.Handle(0) as h:
+        h.set_learned_prior(k)  # no model attached: the prior needs none
+        got = h.synthesize(img, atl, lab, NH, DIV, pct.EXEC_LEARNED)
+        st = h.learned_stats()
+        with learned.LearnedModel(0, seed=3) as m:  # an attached model does not change it
+            h.attach_model(m, 0.5)
+            again = h.synthesize(img, atl, lab, NH, DIV, pct.EXEC_LEARNED)
+            h.attach_model(None)
+        h.set_learned_prior(0)
+        with pytest.raises(pct.PctError) as e:  # back to the network, which is not attached
+            h.synthesize(img, atl, lab, NH, DIV, pct.EXEC_LEARNED)
+        assert e.value.status == -4
+        for bad in (-1, 126):
+            with pytest.raises(pct.PctError) as e:
+                h.set_learned_prior(bad)
+            assert e.value.status == -1
+    compare_fused(got, ref, NH, 1e-4, prod, sumw)
+    assert np.array_equal(got.view(np.uint32), again.view(np.uint32))
+    assert st["fallback_pairs"] == 0
+    assert st["row_offsets"] == rows_of(nx, ny, nz) * k * num
+
+
 @pytest.mark.parametrize("k,block", [(32, 4), (20, 4), (10, 4), (20, 1)])
 def test_prior_proposal_exact(k, block):
     nx, ny, nz, num = 40, 47, 32, 2
@@ -165,6 +202,45 @@ def test_confidence_threshold(k):
         got = h.synthesize(img, atl, lab, NH, DIV, pct.EXEC_LEARNED)
         assert h.learned_stats()["fallback_pairs"] == interior(nx, ny, nz) * num
     compare_fused(got, ref, NH, 1e-4)
+
+
+def test_partial_fallback_runs_whole_tiles_through_the_plain_kernel():
+    """Low-confidence voxels send their whole tile of the plain kernel (30 y x 12 x x 8 z voxels
+    from the first interior voxel, tile set 0 at NH = 11) to its full search: every tile of the
+    result equals either the no-fallback run bit for bit or the FP64 oracle within the plain gate,
+    and the fallback count is the interior voxels of the tiles that fell back."""
+    nx, ny, nz, num = 40, 70, 36, 1
+    img, atl, lab = subject(nx, ny, nz, num, 51)
+    ref, prod, sumw = oracle.fuse_port(img, atl, lab, NH, DIV, with_sums=True)
+    core = (slice(LO, nz - LO), slice(LO, nx - LO), slice(LO, ny - LO))
+    with pct.Handle(0) as h, learned.LearnedModel(0, seed=9) as m:
+        h.attach_model(m, 0.0)
+        base = h.synthesize(img, atl, lab, NH, DIV, pct.EXEC_LEARNED)
+        partial = None
+        for thr in np.geomspace(1e-3, 0.5, 40):
+            h.attach_model(m, float(thr))
+            got = h.synthesize(img, atl, lab, NH, DIV, pct.EXEC_LEARNED)
+            st = h.learned_stats()
+            if 0 < st["fallback_pairs"] < interior(nx, ny, nz) * num:
+                partial = (got, st)
+                break
+    assert partial is not None, "no threshold gave a partial fallback"
+    got, st = partial
+    iz, ix, iy = nz - 2 * LO, nx - 2 * LO, ny - 2 * LO
+    g, b, r = got[core], base[core], ref[core]
+    fell = 0
+    for tz in range(0, iz, 8):
+        for tx in range(0, ix, 12):
+            for ty in range(0, iy, 30):
+                t = (slice(tz, tz + 8), slice(tx, tx + 12), slice(ty, ty + 30))
+                if np.array_equal(g[t].view(np.uint32), b[t].view(np.uint32)):
+                    continue
+                fin = np.isfinite(r[t])
+                assert np.array_equal(np.isnan(g[t]), np.isnan(r[t]))
+                rel = np.abs(g[t][fin] - r[t][fin]) / np.abs(r[t][fin])
+                assert rel.max() <= 1e-4
+                fell += g[t].size
+    assert fell * num == st["fallback_pairs"]
 
 
 def test_probe_matches_float64_network():
