@@ -356,6 +356,8 @@ def run_b200_arm(args) -> None:
     d_lab = torch.from_numpy(label).to(dev)
     d_out = torch.zeros_like(d_img)
     h = pct.Handle(local)
+    if args.tile_set is not None:
+        h.set_tile_set(args.tile_set)
     stream = torch.cuda.Stream(dev)  # a real stream handle, so events and kernels share it
     torch.cuda.set_stream(stream)
     sptr = stream.cuda_stream
@@ -428,7 +430,8 @@ def run_b200_arm(args) -> None:
                    "nh": NH, "atlases": NUM, "volume": [NX, NY, NZ],
                    "l2": f"inputs larger than L2 ({1 + 2 * NUM} volumes, "
                          f"{4 * nvox * (1 + 2 * NUM) / 1e6:.0f} MB per subject)",
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "tile_set": h.tile_set},
         "candidates_per_s": world * cand / (ms / 1e3),
         "gpu_launches": args.steps * plan["launches"],
         "plan": plan,
@@ -785,9 +788,10 @@ def run_tc_arm(args) -> None:
                        "mae_hu_vs_plain": float(e.mean()), "max_abs_hu_vs_plain": float(e.max()),
                        "nan_mismatch": int((np.isnan(g) != np.isnan(ref)).sum()),
                        **check.errors(outs[choice])}
-    # tensor work: 128 x 128 x 32 per chunk, 28 chunks per tile and atlas
+    # tensor work: three K = 16 MMAs of 128 x 128 per chunk (the patch taps and norms, then the
+    # window penalty and the voxel norm), 28 chunks per tile and atlas
     tiles = -(-(NZ - 12) // 4) * -(-(NX - 12) // 4) * -(-(NY - 12) // 8)
-    flop = 2.0 * 128 * 128 * 32 * 28 * tiles * num
+    flop = 2.0 * 128 * 128 * 48 * 28 * tiles * num
     peaks = measured_peaks()
     clocks = clk.summary()
     ms = times[pct.EXEC_TC_FP16]
@@ -810,9 +814,9 @@ def run_tc_arm(args) -> None:
                      "frac": flop / (ms / 1e3) / 1e12 / peaks["bf16_tflops"]
                      if peaks.get("bf16_tflops") else None,
                      "traffic": None,
-                     "note": "dense correlation FLOPs (128 x 128 x 32 per chunk, 28 chunks per "
-                             "tile and atlas) over the FP16 step; the selection epilogue, not the "
-                             "tensor pipe, bounds this kernel"},
+                     "note": "dense correlation FLOPs (128 x 128 x 48 per chunk, 28 chunks per "
+                             "tile and atlas) over the FP16 step; MMAs of N = 128 are issue-rate "
+                             "bound, and the selection epilogue runs beside them"},
         "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
     }
     h.close()
@@ -998,6 +1002,9 @@ def main() -> None:
                     help="CPU-baseline sample length (rank 0, N=1 only)")
     ap.add_argument("--ref-step-seconds", type=float, default=4.0,
                     help="length of each reference-arm step")
+    ap.add_argument("--tile-set", type=int, default=None,
+                    help="single workload: the plain kernel's register-tile set (default: the "
+                         "handle's, set 0)")
     ap.add_argument("--dry", action="store_true",
                     help="launcher and rank logic only (gloo, no GPU work)")
     args = ap.parse_args()

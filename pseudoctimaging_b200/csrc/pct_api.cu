@@ -42,6 +42,7 @@ struct pct_handle {
   int learned_level = 4;                // kept rank triples i + j + k <= level (32 offsets)
   int learned_prior_k = 0;              // > 0: EXEC_CHOICE 7 runs the no-network centre prior
   DevBuf learned;                       // its feature volumes and sums
+  DevBuf tcbuf;                         // tensor-core form: 16-bit patch rows, sums, offset
   long long learned_nvox = 0;           // volume size of the last learned run (0: none yet)
   pct::learned::LearnedStreams learned_streams{};  // convolutions beside the rescoring
   cudaEvent_t learned_done = nullptr;   // recorded after the last learned run's kernels
@@ -204,7 +205,8 @@ int launch_learned_path(pct_handle *h, const pct::Geometry &g, const pct::SlabIn
   return learned_ran(h, g, s);
 }
 
-// The tensor-core form (NH = 11).
+// The tensor-core form (NH = 11). Its TMA loads need 16-byte row strides: unaligned stacks are
+// repacked into the handle's pitched buffers first.
 int launch_tc_path(pct_handle *h, const pct::Geometry &g, const pct::SlabInputs &in, float *d_out,
                    double div, bool bf16, int16_t *dbg_top, cudaStream_t s) {
   if (g.nh != 11)
@@ -212,10 +214,28 @@ int launch_tc_path(pct_handle *h, const pct::Geometry &g, const pct::SlabInputs 
                 "exec_choice 5/6 (tensor-core form) is built for NH = 11 only, got NH = " +
                     std::to_string(g.nh));
   int st = ensure(h, h->err, 16);
-  if (st) return st;
+  if (st || (st = ensure(h, h->tcbuf, pct::tc::scratch_bytes(g)))) return st;
+  pct::SlabInputs tin = in;
+  const bool aligned = (in.pitch % 4 == 0) && (reinterpret_cast<uintptr_t>(in.atlas) % 16 == 0) &&
+                       (reinterpret_cast<uintptr_t>(in.label) % 16 == 0);
+  if (!aligned) {
+    const int pitch = pct::slab_pitch(g.ny);
+    const long long rows = (long long)g.num * g.nz * g.nx;
+    const size_t bytes = (size_t)rows * pitch * sizeof(float);
+    if ((st = ensure(h, h->atlas, bytes)) || (st = ensure(h, h->label, bytes))) return st;
+    // copies read rows `in.pitch` floats apart
+    PCT_CUDA(h, cudaMemcpy2DAsync(h->atlas.ptr, pitch * sizeof(float), in.atlas,
+                                  in.pitch * sizeof(float), g.ny * sizeof(float), rows,
+                                  cudaMemcpyDeviceToDevice, s));
+    PCT_CUDA(h, cudaMemcpy2DAsync(h->label.ptr, pitch * sizeof(float), in.label,
+                                  in.pitch * sizeof(float), g.ny * sizeof(float), rows,
+                                  cudaMemcpyDeviceToDevice, s));
+    tin = pct::SlabInputs{in.img, static_cast<const float *>(h->atlas.ptr),
+                          static_cast<const float *>(h->label.ptr), pitch};
+  }
   int *err = static_cast<int *>(h->err.ptr);
   PCT_CUDA(h, cudaMemsetAsync(err, 0, sizeof(int), s));
-  PCT_CUDA(h, pct::tc::launch_tc(g, in, d_out, div, bf16, err, dbg_top, s));
+  PCT_CUDA(h, pct::tc::launch_tc(g, tin, d_out, div, bf16, err, dbg_top, h->tcbuf.ptr, s));
   return PCT_OK;
 }
 
@@ -516,7 +536,7 @@ int pct_destroy(pct_handle *h) {
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   for (DevBuf *b : {&h->img, &h->atlas, &h->label, &h->out, &h->scratch, &h->err, &h->partial,
-                    &h->stage, &h->batch_stage, &h->batch_meta, &h->learned})
+                    &h->stage, &h->batch_stage, &h->batch_meta, &h->learned, &h->tcbuf})
     if (b->ptr) cudaFree(b->ptr);
   if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
   if (h->learned_done) cudaEventDestroy(h->learned_done);

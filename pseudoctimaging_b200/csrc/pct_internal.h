@@ -149,9 +149,12 @@ int model_device(const pct_model *m);
 namespace tc {
 // Tensor-core form (NH = 11): FP16 or BF16 correlation on tcgen05, top-16 per (voxel, atlas),
 // exact FP32 rescoring. Writes interior voxels of out. *err (device) is set if a bounded wait
-// gives up. dbg_top (optional, device [nvox][16]) receives atlas 0's survivors per voxel.
+// gives up. dbg_top (optional, device [nvox][16]) receives atlas 0's survivors per voxel. The
+// atlas stacks must be TMA-ready (pitch % 4 == 0, 16-byte aligned); scratch holds
+// scratch_bytes(g) bytes (one atlas's 16-bit patch rows, the sums, the subject's offset).
+size_t scratch_bytes(const Geometry &g);
 cudaError_t launch_tc(const Geometry &g, const SlabInputs &in, float *out, double div, bool bf16,
-                      int *err, int16_t *dbg_top, cudaStream_t s);
+                      int *err, int16_t *dbg_top, void *scratch, cudaStream_t s);
 }  // namespace tc
 
 }  // namespace pct

@@ -13,7 +13,8 @@
 // With a non-NaN border every NaN has a non-NaN earlier neighbour by the time it is ready, so
 // one sweep's worth of rounds fills everything; the number of rounds is the longest chain of
 // NaN voxels that follow each other in sweep order. Rounds are bounded by the number of NaN
-// voxels; a round that fills nothing stops the loop (only possible with NaN in the border).
+// voxels; a batch of rounds that fills nothing stops the loop (only possible with NaN in the
+// border).
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -131,25 +132,33 @@ cudaError_t launch_regularize(float *vol, int nx, int ny, int nz, int nh, void *
       cudaSuccess)
     return e;
   if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return e;
+  // Rounds are enqueued in batches (4, 8, ... 64) between host reads: a round reads its list's
+  // length on the device, so rounds after the last NaN cost only an empty launch, and the host
+  // waits once per batch instead of once per round.
   const int max_rounds = pending + 1;
-  int cur = 0, rounds = 0;
+  int cur = 0, rounds = 0, batch = 4;
   while (pending > 0) {
     if (rounds >= max_rounds) return cudaErrorUnknown;
-    const int nxt = cur ^ 1;
-    if ((e = cudaMemsetAsync(&counters[nxt], 0, sizeof(int), stream)) != cudaSuccess) return e;
     const int blocks = (int)((pending + 255) / 256 < sms * 8 ? (pending + 255) / 256 : sms * 8);
-    fill_round_kernel<<<blocks, 256, 0, stream>>>(vol, nx, ny, nz, lo, list[cur], &counters[cur],
-                                                  list[nxt], &counters[nxt], fills);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    for (int r = 0; r < batch; ++r) {
+      const int nxt = cur ^ 1;
+      if ((e = cudaMemsetAsync(&counters[nxt], 0, sizeof(int), stream)) != cudaSuccess) return e;
+      fill_round_kernel<<<blocks, 256, 0, stream>>>(vol, nx, ny, nz, lo, list[cur], &counters[cur],
+                                                    list[nxt], &counters[nxt], fills);
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+      cur = nxt;
+    }
     int left = 0;
-    if ((e = cudaMemcpyAsync(&left, &counters[nxt], sizeof(int), cudaMemcpyDeviceToHost,
+    if ((e = cudaMemcpyAsync(&left, &counters[cur], sizeof(int), cudaMemcpyDeviceToHost,
                              stream)) != cudaSuccess)
       return e;
     if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return e;
-    ++rounds;
-    if (left == pending) break;  // nothing filled: only NaN-bordered voxels remain
+    rounds += batch;
+    // a batch that filled nothing means only voxels with no non-NaN neighbour remain (possible
+    // only with NaN in the border), and no later round could fill them either
+    if (left == pending) break;
     pending = left;
-    cur = nxt;
+    if (batch < 64) batch *= 2;
   }
   unsigned long long f = 0;
   if ((e = cudaMemcpyAsync(&f, fills, sizeof(f), cudaMemcpyDeviceToHost, stream)) != cudaSuccess)
