@@ -70,6 +70,12 @@ constexpr float kPenalty = 60000.0f;
 // Below every in-window score (-|a - b|^2/2 of 16-bit patches stays above -1e9 for any MRI
 // intensities up to ~10^5) and above every penalised one (about -3.6e9): the initial 16th best.
 constexpr float kFloorScore = -1.0e9f;
+// A later atlas's selection starts at this multiple of the lowest 16th best score of the voxel
+// over the atlases before it (scores are -|a - b|^2/2 <= 0, so the start lies below it): the
+// atlases of one subject differ little there, and a voxel whose own 16th best is lower sends its
+// tile to the exact redo launch (1.08 of the previous atlas's value alone sent so many tiles
+// there that the step took 380 ms instead of 209 ms on config 2).
+constexpr float kWarmMargin = 1.25f;
 constexpr float kDblEpsilonF = 2.220446049250313080847e-16f;
 constexpr unsigned long long kTimeoutNs = 2000000000ULL;
 
@@ -78,10 +84,12 @@ constexpr int kOffSlots = 0;
 constexpr int kOffA = kOffSlots + kStages * kSlot;          // [6 K groups][128 rows][16 B]
 constexpr int kOffMask = kOffA + 6 * kAKg;                  // [2 halves][2 K groups][128][16 B]
 constexpr int kOffRegion = kOffMask + 4 * kAKg;             // FP32 [16][16][20]
-constexpr int kOffBars = kOffRegion + kRZ * kRX * kRY * 4;
+constexpr int kStashStride = 33;
+constexpr int kOffStash = kOffRegion + kRZ * kRX * kRY * 4; // [128][33] floats
+constexpr int kOffBars = kOffStash + kEpi * kStashStride * 4;
 constexpr int kNumBars = 2 * kStages + 4 + 3;               // full, empty, tfull[2], tempty[2],
                                                             // a_ready, reg_full, reg_empty
-constexpr int kOffMisc = kOffBars + 8 * kNumBars;           // TMEM slot, abort flag
+constexpr int kOffMisc = kOffBars + 8 * kNumBars;           // TMEM slot, abort and redo flags
 constexpr int kSmemBytes = kOffMisc + 16 + 1024;            // + alignment slack
 
 struct Params {
@@ -93,7 +101,22 @@ struct Params {
   const float *mu;    // device: the subject's offset
   int *err;
   int16_t *dbg_top;   // optional: this atlas's survivors per voxel [nvox][16], best first
+  // Warm start: s16[v] holds the lowest 16th-best score of voxel v over the atlases done so far;
+  // with `warm`, this atlas's selection starts from kWarmMargin x that value instead of -1e9. A
+  // tile
+  // where a voxel ends with fewer than 16 candidates above its start is not accumulated; it is
+  // listed in redo_list for an exact second launch over that list (`list`, `list_count`).
+  float *s16;
+  int warm;
+  const int *list, *list_count;  // null: every tile; else the tiles list[0 .. *list_count)
+  int *redo_list, *redo_count;
 };
+
+__device__ __forceinline__ int tiles_of(const Params &p) {
+  return p.list ? *p.list_count : p.ntiles;
+}
+
+__device__ __forceinline__ int tile_at(const Params &p, int i) { return p.list ? p.list[i] : i; }
 
 // ------------------------------------------------------------------ tcgen05 wrappers
 
@@ -158,6 +181,11 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
 __device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap *map, uint32_t bar,
                                             int c0, int c1, int c2, int c3) {
   ptx::tma_load_4d(dst, map, bar, c0, c1, c2, c3);
+}
+
+// Barrier among the 128 selecting threads only (warps 0-3); the other warps never join it.
+__device__ __forceinline__ void named_barrier_epilogue() {
+  asm volatile("bar.sync 1, 128;" ::: "memory");
 }
 
 // ------------------------------------------------------------------ operand rows
@@ -343,6 +371,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     ptx::mbar_init(bar.reg_full, 1);
     ptx::mbar_init(bar.reg_empty, kEpi);
     *abort_flag = 0;
+    abort_flag[1] = 0;  // the redo flag of the tile being selected
     ptx::fence_mbarrier_init();
   }
   if (warp == 0) {
@@ -391,7 +420,9 @@ __global__ void __launch_bounds__(kThreads, 2)
     if (lane == 0) {
       uint32_t g = 0;  // chunks issued
       int k = 0;       // tiles started by this CTA
-      for (int t = blockIdx.x; t < p.ntiles && !*abort_flag; t += gridDim.x, ++k) {
+      const int n_tiles = tiles_of(p);
+      for (int i = blockIdx.x; i < n_tiles && !*abort_flag; i += gridDim.x, ++k) {
+        const int t = tile_at(p, i);
         const int ty = t % p.tiles_y, r = t / p.tiles_y;
         const int tx = r % p.tiles_x, tz = r / p.tiles_x;
         const int oz = lo + tz * kTZ, ox = lo + tx * kTX, oy = lo + ty * kTY;
@@ -432,7 +463,8 @@ __global__ void __launch_bounds__(kThreads, 2)
     uint32_t g = 0, u = 0;
     int k = 0;
     bool stop = false;
-    for (int t = blockIdx.x; t < p.ntiles && !stop; t += gridDim.x, ++k) {
+    const int n_tiles = tiles_of(p);
+    for (int i = blockIdx.x; i < n_tiles && !stop; i += gridDim.x, ++k) {
       const bool a_ok = ptx::mbar_wait_bounded(bar.a_ready, k & 1, kTimeoutNs);
       if (!__all_sync(0xffffffffu, a_ok && !*abort_flag)) {
         if (lane == 0) {
@@ -533,15 +565,22 @@ __global__ void __launch_bounds__(kThreads, 2)
       ptx::fence_proxy_async_smem();
       ptx::mbar_arrive(bar.a_ready);
     };
-    if ((int)blockIdx.x < p.ntiles) build_a(blockIdx.x, in);
-    for (int t = blockIdx.x; t < p.ntiles && !stop; t += gridDim.x, ++k) {
+    float *row = reinterpret_cast<float *>(sbase + kOffStash) + m * kStashStride;
+    volatile int *redo_flag = abort_flag + 1;
+    const int n_tiles = tiles_of(p);
+    if ((int)blockIdx.x < n_tiles) build_a(tile_at(p, blockIdx.x), in);
+    for (int i = blockIdx.x; i < n_tiles && !stop; i += gridDim.x, ++k) {
+      const int t = tile_at(p, i);
       const int ty = t % p.tiles_y, r = t / p.tiles_y;
       const int tx = r % p.tiles_x, tz = r / p.tiles_x;
       const int gz = lo + tz * kTZ + vz, gx = lo + tx * kTX + vx, gy = lo + ty * kTY + vy;
       const bool valid = gz < p.nz - lo && gx < p.nx - lo && gy < p.ny - lo;
+      const long long vox = (long long)gz * nxy + (long long)gx * p.ny + gy;
+      // the selection's start: the 16th best found so far must beat it
+      const float start = (p.warm && valid) ? kWarmMargin * p.s16[vox] : kFloorScore;
       float tv[kTop];
 #pragma unroll
-      for (int j = 0; j < kTop; ++j) tv[j] = kFloorScore;
+      for (int j = 0; j < kTop; ++j) tv[j] = start;
       for (int c = 0; c < kChunks; ++c, ++u) {
         const uint32_t b = u & 1;
         const bool ok = ptx::mbar_wait_bounded(bar.tfull + 8 * b, (u >> 1) & 1, kTimeoutNs);
@@ -562,16 +601,27 @@ __global__ void __launch_bounds__(kThreads, 2)
           for (int grp = 0; grp < 4; ++grp) {
             float v[32];
             tmem_ld32(my_tmem + b * 128 + grp * 32, v);
-            if (__any_sync(0xffffffffu, max32(v) > tv[kTop - 1])) {
-              // columns in order; a column some lane's 16th best does not stop is inserted by
-              // those lanes (warp-uniform branch per column, the top-16 stays in registers)
+            const float thr = tv[kTop - 1];
+            if (__any_sync(0xffffffffu, max32(v) > thr)) {
+              // each lane walks its own columns above its 16th best (parked in shared memory,
+              // so that the lanes need not agree on a column): the warp loops as often as its
+              // busiest lane has candidates, not once per column any lane wants
+              uint32_t msk = 0;
 #pragma unroll
-              for (int i = 0; i < 32; ++i) {
-                const bool c = v[i] > tv[kTop - 1];
-                if (__any_sync(0xffffffffu, c) && c) {
-                  const int n = grp * 32 + i;
-                  const int px = half * kHalfX + n / kPY, py = n % kPY;
-                  insert_key(tv, pack_key(v[i], ((dz + 5) * 11 + (px - vx)) * 11 + (py - vy)));
+              for (int q = 0; q < 32; ++q) {
+                msk |= (v[q] > thr ? 1u : 0u) << q;
+                row[q] = v[q];
+              }
+              while (__any_sync(0xffffffffu, msk != 0u)) {
+                if (msk) {
+                  const int q = __ffs(msk) - 1;
+                  msk &= msk - 1;
+                  const float val = row[q];
+                  if (val > tv[kTop - 1]) {
+                    const int n = grp * 32 + q;
+                    const int px = half * kHalfX + n / kPY, py = n % kPY;
+                    insert_key(tv, pack_key(val, ((dz + 5) * 11 + (px - vx)) * 11 + (py - vy)));
+                  }
                 }
               }
             }
@@ -584,8 +634,13 @@ __global__ void __launch_bounds__(kThreads, 2)
       // the MMAs of this tile are complete (its last accumulator was read): the next tile's
       // voxel operand may replace this one while this tile is rescored
       float nin[27];
-      const int tn = t + gridDim.x;
-      if (tn < p.ntiles) build_a(tn, nin);
+      const int inext = i + gridDim.x;
+      if (inext < n_tiles) build_a(tile_at(p, inext), nin);
+      // a voxel whose start held back part of its 16 sends the tile to the exact redo launch
+      const bool short_list = p.warm && valid && !(tv[kTop - 1] > start);
+      if (short_list) *redo_flag = 1;
+      named_barrier_epilogue();
+      const bool redo = *redo_flag != 0;
       // exact FP32 rescoring of the survivors from the FP32 region
       if (!ptx::mbar_wait_bounded(bar.reg_full, k & 1, kTimeoutNs)) {
         *abort_flag = 1;
@@ -593,35 +648,44 @@ __global__ void __launch_bounds__(kThreads, 2)
         break;
       }
       float P = 0.f, W = 0.f;
+      if (!redo) {
 #pragma unroll
-      for (int j = 0; j < kTop; ++j) {  // unrolled: the top-16 must stay in registers
-        const int o = __float_as_int(tv[j]) & 0x7FF;
-        // an entry never replaced (only inputs whose 16-bit scores leave (-1e9, 1e9) can leave
-        // one) holds no offset
-        if (!(tv[j] > kFloorScore) || o > 1330) continue;
-        const int dzz = o / 121 - 5, dx = (o / 11) % 11 - 5, dy = o % 11 - 5;
-        // position (vz + dz, vx + dx, vy + dy) + 5 in box coordinates; the region starts at -6
-        const int rz = vz + dzz + 5, rx = vx + dx + 5, ry = vy + dy + 5;
-        float ssd = 0.f;
+        for (int j = 0; j < kTop; ++j) {  // unrolled: the top-16 must stay in registers
+          const int o = __float_as_int(tv[j]) & 0x7FF;
+          // an entry never replaced (only inputs whose 16-bit scores leave (-1e9, 1e9) can
+          // leave one) holds no offset
+          if (!(tv[j] > kFloorScore) || o > 1330) continue;
+          const int dzz = o / 121 - 5, dx = (o / 11) % 11 - 5, dy = o % 11 - 5;
+          // position (vz + dz, vx + dx, vy + dy) + 5 in box coordinates; the region starts at -6
+          const int rz = vz + dzz + 5, rx = vx + dx + 5, ry = vy + dy + 5;
+          float ssd = 0.f;
 #pragma unroll
-        for (int q = 0; q < 27; ++q) {
-          const float d = in[q] - region[((rz + q / 9) * kRX + (rx + (q / 3) % 3)) * kRY + ry + q % 3];
-          ssd = fmaf(d, d, ssd);
-        }
-        if (valid) {
-          const float w = ptx::ex2_approx(ssd * p.neg_k);
-          P = fmaf(w, __ldg(L + ((long long)(gz + dzz) * p.nx + gx + dx) * p.apitch + gy + dy), P);
-          W += w;
-          if (p.dbg_top)
-            p.dbg_top[((long long)gz * nxy + (long long)gx * p.ny + gy) * kTop + j] = (int16_t)o;
+          for (int q = 0; q < 27; ++q) {
+            const float d =
+                in[q] - region[((rz + q / 9) * kRX + (rx + (q / 3) % 3)) * kRY + ry + q % 3];
+            ssd = fmaf(d, d, ssd);
+          }
+          if (valid) {
+            const float w = ptx::ex2_approx(ssd * p.neg_k);
+            P = fmaf(w, __ldg(L + ((long long)(gz + dzz) * p.nx + gx + dx) * p.apitch + gy + dy),
+                     P);
+            W += w;
+            if (p.dbg_top) p.dbg_top[vox * kTop + j] = (int16_t)o;
+          }
         }
       }
       ptx::mbar_arrive(bar.reg_empty);
-      if (valid) {
-        const long long v = (long long)gz * nxy + (long long)gx * p.ny + gy;
-        p.pacc[v] += P;
-        p.wacc[v] += W;
+      if (redo) {
+        if (m == 0) p.redo_list[atomicAdd(p.redo_count, 1)] = t;
+      } else if (valid) {
+        p.pacc[vox] += P;
+        p.wacc[vox] += W;
+        // the lowest 16th best so far: the next atlas starts below it
+        const float s16v = __int_as_float(__float_as_int(tv[kTop - 1]) & ~0x7FF);
+        p.s16[vox] = (p.warm || p.list) ? fminf(p.s16[vox], s16v) : s16v;
       }
+      named_barrier_epilogue();  // every lane has read the flag: it may be cleared
+      if (m == 0) *redo_flag = 0;
 #pragma unroll
       for (int q = 0; q < 27; ++q) in[q] = nin[q];
     }
@@ -678,21 +742,42 @@ int sm_count() {
   return n;
 }
 
+struct Scratch {
+  uint4 *feat;
+  float *pacc, *wacc, *mu, *s16;
+  int *redo_count, *redo_list;
+};
+
+Scratch carve(void *scratch, const Geometry &g) {
+  const long long nvox = g.nvox();
+  unsigned char *sc = static_cast<unsigned char *>(scratch);
+  Scratch r;
+  r.feat = reinterpret_cast<uint4 *>(sc);
+  r.pacc = reinterpret_cast<float *>(sc + 64 * (size_t)nvox);
+  r.wacc = r.pacc + nvox;
+  r.s16 = r.wacc + nvox;
+  r.mu = r.s16 + nvox;                                   // 16 bytes
+  r.redo_count = reinterpret_cast<int *>(r.mu + 4);      // 16 bytes
+  r.redo_list = r.redo_count + 4;
+  return r;
+}
+
+int num_tiles(const Geometry &g) {
+  if (g.ix <= 0 || g.iy <= 0 || g.iz <= 0) return 0;
+  return ((g.iz + kTZ - 1) / kTZ) * ((g.ix + kTX - 1) / kTX) * ((g.iy + kTY - 1) / kTY);
+}
+
 template <bool BF16>
 cudaError_t launch_all(const Geometry &g, const SlabInputs &in, float *out, double div, int *err,
                        int16_t *dbg_top, void *scratch, cudaStream_t s) {
   const long long nvox = g.nvox();
-  unsigned char *sc = static_cast<unsigned char *>(scratch);
-  uint4 *feat = reinterpret_cast<uint4 *>(sc);
-  float *pacc = reinterpret_cast<float *>(sc + 64 * (size_t)nvox);
-  float *wacc = pacc + nvox;
-  float *mu = wacc + nvox;
+  const Scratch sc = carve(scratch, g);
   cudaError_t e;
-  if ((e = cudaMemsetAsync(pacc, 0, 8 * (size_t)nvox, s)) != cudaSuccess) return e;
-  mean_kernel<<<1, 1024, 0, s>>>(in.img, nvox, mu);
+  if ((e = cudaMemsetAsync(sc.pacc, 0, 8 * (size_t)nvox, s)) != cudaSuccess) return e;
+  mean_kernel<<<1, 1024, 0, s>>>(in.img, nvox, sc.mu);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   CUtensorMap tm_feat, tm_atlas;
-  if ((e = make_feature_map(&tm_feat, feat, g)) != cudaSuccess) return e;
+  if ((e = make_feature_map(&tm_feat, sc.feat, g)) != cudaSuccess) return e;
   if ((e = make_region_map(&tm_atlas, in.atlas, g, in.pitch)) != cudaSuccess) return e;
   auto kern = tc_fuse_kernel<BF16>;
   if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes)) !=
@@ -701,8 +786,8 @@ cudaError_t launch_all(const Geometry &g, const SlabInputs &in, float *out, doub
   Params p{};
   p.img = in.img;
   p.label = in.label;
-  p.pacc = pacc;
-  p.wacc = wacc;
+  p.pacc = sc.pacc;
+  p.wacc = sc.wacc;
   p.nx = g.nx;
   p.ny = g.ny;
   p.nz = g.nz;
@@ -712,26 +797,43 @@ cudaError_t launch_all(const Geometry &g, const SlabInputs &in, float *out, doub
   p.tiles_y = (g.iy + kTY - 1) / kTY;
   p.ntiles = p.tiles_z * p.tiles_x * p.tiles_y;
   p.neg_k = (float)(-1.4426950408889634 / div);
-  p.mu = mu;
+  p.mu = sc.mu;
   p.err = err;
+  p.s16 = sc.s16;
+  p.redo_list = sc.redo_list;
+  p.redo_count = sc.redo_count;
   const int blocks = std::min(p.ntiles, 2 * sm_count());
   const long long astride = (long long)g.nz * g.nx * in.pitch;
   for (int a = 0; a < g.num; ++a) {
     features_kernel<BF16><<<sm_count() * 8, 256, 0, s>>>(in.atlas + a * astride, g.nx, g.ny, g.nz,
-                                                         in.pitch, mu, feat);
+                                                         in.pitch, sc.mu, sc.feat);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(sc.redo_count, 0, sizeof(int), s)) != cudaSuccess) return e;
     p.atlas = a;
     p.dbg_top = a == 0 ? dbg_top : nullptr;
+    // atlas 0 selects from scratch; later atlases start from their voxels' 16th best so far
+    p.warm = a > 0;
+    p.list = p.list_count = nullptr;
     kern<<<blocks, kThreads, kSmemBytes, s>>>(tm_feat, tm_atlas, p);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (a > 0) {  // the tiles whose start was too high, exactly (count read on the device)
+      Params q = p;
+      q.warm = 0;
+      q.list = sc.redo_list;
+      q.list_count = sc.redo_count;
+      kern<<<blocks, kThreads, kSmemBytes, s>>>(tm_feat, tm_atlas, q);
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
   }
-  finalize_kernel<<<sm_count() * 8, 256, 0, s>>>(pacc, wacc, out, g.nx, g.ny, g.nz);
+  finalize_kernel<<<sm_count() * 8, 256, 0, s>>>(sc.pacc, sc.wacc, out, g.nx, g.ny, g.nz);
   return cudaGetLastError();
 }
 
 }  // namespace
 
-size_t scratch_bytes(const Geometry &g) { return 72 * (size_t)g.nvox() + 256; }
+size_t scratch_bytes(const Geometry &g) {
+  return 76 * (size_t)g.nvox() + 32 + 4 * (size_t)num_tiles(g) + 256;
+}
 
 cudaError_t launch_tc(const Geometry &g, const SlabInputs &in, float *out, double div, bool bf16,
                       int *err, int16_t *dbg_top, void *scratch, cudaStream_t s) {
