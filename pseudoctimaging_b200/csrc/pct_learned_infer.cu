@@ -1353,6 +1353,10 @@ __device__ __forceinline__ int pick4(const int (&t)[4], int i) {
 
 // One offset for the 4 rows of a warp item. `a` points at the atlas voxel (z - 1 + dw, x0 - 1 +
 // du, yc + dv), `l` at the label voxel (z + dw, x0 + du, yc + dv); row strides are 32-bit.
+// MASKED: only the rows set in `take` accumulate (the full-search path, whose rows differ in
+// which offsets they keep); otherwise every row accumulates and the caller stores only the rows
+// it owns.
+template <bool MASKED>
 __device__ __forceinline__ void eval_offset4(const float *__restrict__ a,
                                              const float *__restrict__ l,
                                              const float2 (&in)[3][(kRows + 2) / 2], int axy,
@@ -1378,7 +1382,7 @@ __device__ __forceinline__ void eval_offset4(const float *__restrict__ a,
     const float x = Z[r] + Z[r + 1] + Z[r + 2];
     const float e =
         __shfl_up_sync(0xffffffffu, x, 1) + x + __shfl_down_sync(0xffffffffu, x, 1);
-    if ((take >> r) & 1u) {
+    if (!MASKED || ((take >> r) & 1u)) {
       const float w = ptx::ex2_approx(-e);
       P[r] = fmaf(w, __ldg(l + r * apitch), P[r]);
       W[r] += w;
@@ -1467,7 +1471,7 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 4)
 #pragma unroll 2
       for (int c = 0; c < kept; ++c) {
         const int off = w_off[c];
-        eval_offset4(ab + off, lb + off, in, axy, apitch, take, s2, P, W);
+        eval_offset4<false>(ab + off, lb + off, in, axy, apitch, take, s2, P, W);
       }
       my_evals += (unsigned long long)kept * __popc(owned);
     } else {
@@ -1488,7 +1492,7 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 4)
           for (int jv = 0; jv < kAxis; ++jv) {
             const bool mine = full || (ru + (int)((rank[2] >> (4 * jv)) & 0xF) <= LEVEL);
             const int off = (jw - 5) * axy + (ju - 5) * apitch + (jv - 5);
-            eval_offset4(ab + off, lb + off, in, axy, apitch, mine ? take : 0u, s2, P, W);
+            eval_offset4<true>(ab + off, lb + off, in, axy, apitch, mine ? take : 0u, s2, P, W);
           }
         }
       }
@@ -1603,7 +1607,7 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 4)
 #pragma unroll 2
     for (int c = 0; c < pl.n; ++c) {
       const int off = pl.off[c];
-      eval_offset4(ab + off, lb + off, in, axy, apitch, take, s2, P, W);
+      eval_offset4<false>(ab + off, lb + off, in, axy, apitch, take, s2, P, W);
     }
     my_evals += (unsigned long long)pl.n * __popc(owned);
 #pragma unroll
