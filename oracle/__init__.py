@@ -28,10 +28,18 @@ _I = ctypes.c_int
 _D = ctypes.c_double
 
 
+# Where the build container keeps the reference checkout (read-only); PCT_REFERENCE_DIR overrides.
+_DEFAULT_REF_DIR = "/root/reference"
+
+
 def build() -> None:
     """Builds the restatement and, where the reference checkout exists, the reference library."""
     make = "/usr/bin/make" if os.path.exists("/usr/bin/make") else "make"
-    subprocess.run([make, "-s", "-C", str(HERE), "all"], check=True)
+    ref = os.environ.get("PCT_REFERENCE_DIR") or _DEFAULT_REF_DIR
+    args = [make, "-s", "-C", str(HERE), "all"]
+    if os.path.isdir(ref):
+        args.append(f"REF={ref}")
+    subprocess.run(args, check=True)
 
 
 def _load(path: pathlib.Path) -> ctypes.CDLL:

@@ -29,11 +29,14 @@ INCLUDE = REPO / "include"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 HOST_CXX = shutil.which("g++", path="/usr/bin") or "g++"
 COMMON = ["-O3", "-std=c++17", "-lineinfo", f"-ccbin={HOST_CXX}", "-Xcompiler", "-fPIC",
-          f"-I{INCLUDE}", f"-I{CSRC}"]
+          f"-I{INCLUDE}", f"-I{CSRC}", f"-I{OBJ}"]
 # Sources that make up the shared library; the CLI main is linked separately against it.
 LIB_SOURCES = ["pct_api.cu", "pct_fuse_tma.cu", "pct_pointwise.cu", "pct_regularize.cu",
                "pct_noalloc.cu", "pct_synth.cpp", "pct_io.cpp", "pct_learned_train.cu",
-               "pct_learned_api.cu", "pct_learned_infer.cu", "pct_tc_fuse.cu"]
+               "pct_learned_api.cu", "pct_learned_infer.cu", "pct_tc_fuse.cu", "pct_jit.cpp"]
+# Device sources that are also compiled at run time (NVRTC): each is embedded as a string in
+# _build/<stem>_src.inc, which the library sources include.
+EMBEDDED = ["pct_rescore.cuh"]
 CLI_SOURCES = ["pct_cli.cpp"]
 
 
@@ -45,7 +48,22 @@ def nvcc() -> str:
 
 
 def _headers() -> list[pathlib.Path]:
-    return sorted(CSRC.glob("*.h")) + sorted(INCLUDE.glob("*.h"))
+    return sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cuh")) + sorted(INCLUDE.glob("*.h"))
+
+
+def _embed(name: str) -> pathlib.Path:
+    """Writes _build/<stem>_src.inc: the file's text as a C++ raw string constant."""
+    src = CSRC / name
+    stem = src.name.split(".")[0]
+    out = OBJ / f"{stem}_src.inc"
+    text = src.read_text()
+    if ")pct_src\"" in text:
+        raise RuntimeError(f"{src} contains the raw-string delimiter")
+    body = (f"// Generated from csrc/{src.name} by build.py; do not edit.\n"
+            f"static const char k_{stem}_source[] = R\"pct_src({text})pct_src\";\n")
+    if not out.exists() or out.read_text() != body:
+        out.write_text(body)
+    return out
 
 
 def _stale(target: pathlib.Path, deps: list[pathlib.Path]) -> bool:
@@ -79,6 +97,8 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     OBJ.mkdir(parents=True, exist_ok=True)
     LIB.parent.mkdir(parents=True, exist_ok=True)
     CLI.parent.mkdir(parents=True, exist_ok=True)
+    for name in EMBEDDED:
+        _embed(name)
     srcs = [CSRC / s for s in LIB_SOURCES]
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         results = list(ex.map(lambda s: _compile(s, force, verbose, ptxas_info), srcs))
@@ -88,7 +108,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
             if log:
                 sys.stdout.write(log)
     if force or _stale(LIB, objs):
-        _run([nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lpthread"], verbose)
+        _run([nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lpthread", "-ldl"], verbose)
     cli_src = [CSRC / s for s in CLI_SOURCES if (CSRC / s).exists()]
     if cli_src:
         cli_objs = [_compile(s, force, verbose, False)[0] for s in cli_src]

@@ -4,6 +4,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string>
+#include <vector>
+
 struct pct_model;
 
 namespace pct {
@@ -99,6 +102,17 @@ cudaError_t launch_pitch_copy(const float *src, float *dst, long long rows, int 
                               cudaStream_t stream);
 
 inline int slab_pitch(int ny) { return (ny + 3) / 4 * 4; }
+
+// Run-time compiled kernels (NVRTC; pct_jit.cpp): the entry point `entry_name` of `source`
+// built for the current device with `options` (typically -D constants), cached per (context,
+// source name, options, entry point). nullptr when NVRTC or the driver's module calls are
+// unavailable or the build failed; callers then launch their ahead-of-time build.
+namespace jit {
+void *kernel(const char *source, const char *file_name, const std::vector<std::string> &options,
+             const char *entry_name);
+// 1-D launch of a kernel returned by kernel() (no dynamic shared memory).
+cudaError_t launch(void *fn, unsigned grid, unsigned block, cudaStream_t stream, void **args);
+}  // namespace jit
 
 // cuTensorMapEncodeTiled of the driver (a PFN_cuTensorMapEncodeTiled_v12000), found through the
 // runtime's entry-point query; NULL if the driver does not provide it.

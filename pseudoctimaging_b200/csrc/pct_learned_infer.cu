@@ -17,6 +17,7 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
+#include <stdlib.h>
 #include <stdint.h>
 
 #include <cuda.h>
@@ -1103,21 +1104,12 @@ __global__ void proposal_hook_kernel(const __nv_bfloat16 *__restrict__ f4,
   conf[i] = pr.conf;
 }
 
-constexpr int kRowOut = 30;       // output voxels per warp row (lanes 1..30)
-constexpr int kMaxPrior = 125;    // offsets of the no-network prior (5 x 5 x 5 around the centre)
-constexpr int kRescoreWarps = 4;  // warps per CTA
+// Rescoring device code (RowProp, the kept rank triples, the tap evaluation and both rescoring
+// kernels' bodies); the same text is compiled again per geometry at run time.
+#include "pct_rescore.cuh"
+static_assert(kRsAxis == kAxis && kRsTopK == kTopK, "rescoring constants follow the network's");
+
 constexpr int kProbStride = kHeads;  // 33 floats per lane row: column reads are conflict-free
-
-
-// The proposal of one row segment (30 voxels along y) of a block anchor row: the segment's
-// per-axis probabilities summed over its voxels, the 4 most probable offsets per axis of the sums
-// (offset index 0..10, ties to the lower offset), and each voxel's own probability mass on the
-// resulting rank triples (i + j + k <= level). Rows share the proposal of their block's anchor row: blocks of
-// `block` x `block` rows in (z, x), anchored at their middle row (clamped to the interior).
-struct RowProp {
-  signed char top[12];  // [axis][rank]
-  float conf[kRowOut];  // per output voxel of the segment (lane - 1)
-};
 
 __device__ __forceinline__ int anchor_of(int b, int block, int extent) {
   const int a = b * block + block / 2;
@@ -1335,64 +1327,8 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 3)
   if (lane == 0 && my_evals) atomicAdd(evaluated, my_evals);
 }
 
-// Blocks of 4 rows: the 4 x-rows of a block (one z plane) share their proposal, so one warp
-// rescores them together. Per offset it loads the 3 z x 6 x tap rows the 4 rows need once
-// (instead of 4 x 9), forms D = s^2 (A - I)^2 with the scale folded into the differences,
-// sums z in registers, x across the shared rows and y by warp shuffles.
-constexpr int kRows = 4;
-
-// The kept set's rank triples (i, j, k), i + j + k <= 4, packed as i | j << 2 | k << 4, in
-// order of rank sum: the first 10, 20 or 32 are the kept sets of levels 2, 3 and 4.
-__constant__ unsigned char kRankTriples[kTopK] = {
-    0x00, 0x01, 0x04, 0x10, 0x02, 0x05, 0x08, 0x11, 0x14, 0x20, 0x03, 0x06, 0x09, 0x0c, 0x12, 0x15,
-    0x18, 0x21, 0x24, 0x30, 0x07, 0x0a, 0x0d, 0x13, 0x16, 0x19, 0x1c, 0x22, 0x25, 0x28, 0x31, 0x34};
-
-__device__ __forceinline__ int pick4(const int (&t)[4], int i) {
-  return i == 0 ? t[0] : i == 1 ? t[1] : i == 2 ? t[2] : t[3];
-}
-
-// One offset for the 4 rows of a warp item. `a` points at the atlas voxel (z - 1 + dw, x0 - 1 +
-// du, yc + dv), `l` at the label voxel (z + dw, x0 + du, yc + dv); row strides are 32-bit.
-// MASKED: only the rows set in `take` accumulate (the full-search path, whose rows differ in
-// which offsets they keep); otherwise every row accumulates and the caller stores only the rows
-// it owns.
-template <bool MASKED>
-__device__ __forceinline__ void eval_offset4(const float *__restrict__ a,
-                                             const float *__restrict__ l,
-                                             const float2 (&in)[3][(kRows + 2) / 2], int axy,
-                                             int apitch, unsigned take, float2 s2,
-                                             float (&P)[kRows], float (&W)[kRows]) {
-  // x-rows in pairs: packed FP32 FMAs (the same roundings as two scalar FMAs)
-  float Z[kRows + 2];
-#pragma unroll
-  for (int xp = 0; xp < (kRows + 2) / 2; ++xp) {
-    const int ro = 2 * xp * apitch;
-    float2 z = make_float2(0.f, 0.f);
-#pragma unroll
-    for (int dz = 0; dz < 3; ++dz) {
-      const float2 av = make_float2(__ldg(a + (ro + dz * axy)), __ldg(a + (ro + apitch + dz * axy)));
-      const float2 t = __ffma2_rn(av, s2, in[dz][xp]);
-      z = __ffma2_rn(t, t, z);
-    }
-    Z[2 * xp] = z.x;
-    Z[2 * xp + 1] = z.y;
-  }
-#pragma unroll
-  for (int r = 0; r < kRows; ++r) {
-    const float x = Z[r] + Z[r + 1] + Z[r + 2];
-    const float e =
-        __shfl_up_sync(0xffffffffu, x, 1) + x + __shfl_down_sync(0xffffffffu, x, 1);
-    if (!MASKED || ((take >> r) & 1u)) {
-      const float w = ptx::ex2_approx(-e);
-      P[r] = fmaf(w, __ldg(l + r * apitch), P[r]);
-      W[r] += w;
-    }
-  }
-}
-
-// Items are 4 x-rows of one z plane; the last item of an x-row band is shifted back to end at
-// the last interior row, the rows the previous item owns left out, so no load needs a clamp.
-// Needs at least 4 interior x-rows and an atlas volume below 2^31 voxels (32-bit offsets).
+// Proposal rescoring, library build (run-time strides); launch_rescore4 prefers the per-geometry
+// run-time compiled module of the same code.
 template <int LEVEL>
 __global__ void __launch_bounds__(kRescoreWarps * 32, 4)
     rescore4_kernel(const RowProp *__restrict__ props, const float *__restrict__ img,
@@ -1400,114 +1336,9 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 4)
                     int nz, int apitch, float scale, float conf_thr, float *__restrict__ pacc,
                     float *__restrict__ wacc, unsigned long long *__restrict__ fallbacks,
                     unsigned long long *__restrict__ evaluated,
-                    const unsigned char *__restrict__ tile_flag, const TileShape ts) {
-  __shared__ int s_off[kRescoreWarps][kTopK];  // per warp: the item's kept offsets, 32-bit
-  const int lane = threadIdx.x & 31;
-  int *w_off = s_off[threadIdx.x >> 5];
-  const int lo = 6;
-  const int ix = nx - 2 * lo, iz = nz - 2 * lo, iy = ny - 2 * lo;
-  if (ix < kRows || iy <= 0 || iz <= 0) return;
-  const int segs = (iy + kRowOut - 1) / kRowOut;
-  const int nbx = (ix + kRows - 1) / kRows;
-  const long long items = (long long)iz * nbx * segs;
-  const int nxy = nx * ny;
-  const int axy = nx * apitch;
-  unsigned long long my_fallbacks = 0, my_evals = 0;
-  for (long long it = (long long)blockIdx.x * kRescoreWarps + (threadIdx.x >> 5); it < items;
-       it += (long long)gridDim.x * kRescoreWarps) {
-    const int seg = (int)(it % segs);
-    const long long r0 = it / segs;
-    const int bx = (int)(r0 % nbx), z = (int)(r0 / nbx) + lo;
-    const int xb = lo + bx * kRows;
-    // items of tiles that fell back to the plain kernel are left to it (warp-uniform)
-    if (tile_flag &&
-        tile_flag[((z - lo) / ts.zt * ts.tiles_x + (xb - lo) / ts.xc) * ts.tiles_y + seg])
-      continue;
-    const int x0 = min(xb, nx - lo - kRows);
-    const int y0 = lo + seg * kRowOut;
-    const int y = y0 - 1 + lane;
-    const bool out_lane = lane >= 1 && lane <= kRowOut && y < ny - lo;
-    const int yc = min(y, ny - lo);
-    const RowProp &rp = props[((long long)((z - lo) / kRows) * nbx + bx) * segs + seg];
-    int top[3][4];
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-      for (int r = 0; r < 4; ++r) top[a][r] = rp.top[a * 4 + r];
-    // lane c: the offset of kept triple c
-    {
-      const int code = kRankTriples[lane];
-      const int dw = pick4(top[0], code & 3) - 5, du = pick4(top[1], (code >> 2) & 3) - 5,
-                dv = pick4(top[2], code >> 4) - 5;
-      __syncwarp();
-      w_off[lane] = dw * axy + du * apitch + dv;
-      __syncwarp();
-    }
-    unsigned owned = 0;
-#pragma unroll
-    for (int r = 0; r < kRows; ++r)
-      if (x0 + r >= xb) owned |= 1u << r;
-    const unsigned take = out_lane ? owned : 0u;
-    const bool full = out_lane && conf_thr > 0.f && rp.conf[lane - 1] < conf_thr;
-    const unsigned any_full = __ballot_sync(0xffffffffu, full);
-    if (full) my_fallbacks += __popc(take);
-    // input taps I(z+dz-1, x0-1+xr, yc), negated and scaled
-    float2 in[3][(kRows + 2) / 2];
-#pragma unroll
-    for (int dz = 0; dz < 3; ++dz)
-#pragma unroll
-      for (int xp = 0; xp < (kRows + 2) / 2; ++xp) {
-        const float *pi = img + (long long)(z + dz - 1) * nxy + (long long)(x0 - 1 + 2 * xp) * ny + yc;
-        in[dz][xp] = make_float2(-__ldg(pi) * scale, -__ldg(pi + ny) * scale);
-      }
-    const float2 s2 = make_float2(scale, scale);
-    const float *ab = atl + ((long long)(z - 1) * axy + (long long)(x0 - 1) * apitch + yc);
-    const float *lb = lab + ((long long)z * axy + (long long)x0 * apitch + yc);
-    float P[kRows], W[kRows];
-#pragma unroll
-    for (int r = 0; r < kRows; ++r) P[r] = W[r] = 0.f;
-    if (!any_full) {
-      constexpr int kept = LEVEL <= 2 ? 10 : LEVEL == 3 ? 20 : 32;
-#pragma unroll 2
-      for (int c = 0; c < kept; ++c) {
-        const int off = w_off[c];
-        eval_offset4<false>(ab + off, lb + off, in, axy, apitch, take, s2, P, W);
-      }
-      my_evals += (unsigned long long)kept * __popc(owned);
-    } else {
-      unsigned long long rank[3];
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        rank[a] = 0x77777777777ULL;  // nibble j: rank of offset j - 5 on axis a, 7 = not kept
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          rank[a] &= ~(0xFULL << (4 * top[a][r]));
-          rank[a] |= (unsigned long long)r << (4 * top[a][r]);
-        }
-      }
-      for (int jw = 0; jw < kAxis; ++jw) {
-        const int rw = (int)((rank[0] >> (4 * jw)) & 0xF);
-        for (int ju = 0; ju < kAxis; ++ju) {
-          const int ru = rw + (int)((rank[1] >> (4 * ju)) & 0xF);
-          for (int jv = 0; jv < kAxis; ++jv) {
-            const bool mine = full || (ru + (int)((rank[2] >> (4 * jv)) & 0xF) <= LEVEL);
-            const int off = (jw - 5) * axy + (ju - 5) * apitch + (jv - 5);
-            eval_offset4<true>(ab + off, lb + off, in, axy, apitch, mine ? take : 0u, s2, P, W);
-          }
-        }
-      }
-      my_evals += (unsigned long long)kAxis * kAxis * kAxis * __popc(owned);
-    }
-#pragma unroll
-    for (int r = 0; r < kRows; ++r)
-      if ((take >> r) & 1u) {
-        const long long v = (long long)z * nxy + (long long)(x0 + r) * ny + y;
-        pacc[v] += P[r];
-        wacc[v] += W[r];
-      }
-  }
-  if (my_fallbacks) atomicAdd(fallbacks, my_fallbacks);
-  if (lane == 0 && my_evals) atomicAdd(evaluated, my_evals);
+                    const unsigned char *__restrict__ tile_flag, const RescoreTiles ts) {
+  rescore4_body<LEVEL>(props, img, atl, lab, nx, ny, nz, apitch, scale, conf_thr, pacc, wacc,
+                       fallbacks, evaluated, tile_flag, ts);
 }
 
 // The confidence fallback at the plain kernel's tile granularity (blocks of 4 x 4 rows share a
@@ -1551,74 +1382,13 @@ __global__ void flag_tiles_kernel(const RowProp *__restrict__ props, int nx, int
   }
 }
 
-// The proposal baseline without a network: every voxel rescores the same k offsets, the ones of
-// the window nearest its centre. Same items, taps and arithmetic as rescore4_kernel; the offsets
-// (32-bit element offsets into the atlas volume) come from the kernel parameters.
-struct PriorList {
-  int n;
-  int off[kMaxPrior];
-};
-
+// The no-network centre prior, library build (run-time strides).
 __global__ void __launch_bounds__(kRescoreWarps * 32, 4)
     rescore_prior_kernel(const __grid_constant__ PriorList pl, const float *__restrict__ img,
                          const float *__restrict__ atl, const float *__restrict__ lab, int nx,
                          int ny, int nz, int apitch, float scale, float *__restrict__ pacc,
                          float *__restrict__ wacc, unsigned long long *__restrict__ evaluated) {
-  const int lane = threadIdx.x & 31;
-  const int lo = 6;
-  const int ix = nx - 2 * lo, iz = nz - 2 * lo, iy = ny - 2 * lo;
-  if (ix < kRows || iy <= 0 || iz <= 0) return;
-  const int segs = (iy + kRowOut - 1) / kRowOut;
-  const int nbx = (ix + kRows - 1) / kRows;
-  const long long items = (long long)iz * nbx * segs;
-  const int nxy = nx * ny;
-  const int axy = nx * apitch;
-  unsigned long long my_evals = 0;
-  for (long long it = (long long)blockIdx.x * kRescoreWarps + (threadIdx.x >> 5); it < items;
-       it += (long long)gridDim.x * kRescoreWarps) {
-    const int seg = (int)(it % segs);
-    const long long r0 = it / segs;
-    const int bx = (int)(r0 % nbx), z = (int)(r0 / nbx) + lo;
-    const int xb = lo + bx * kRows;
-    const int x0 = min(xb, nx - lo - kRows);
-    const int y0 = lo + seg * kRowOut;
-    const int y = y0 - 1 + lane;
-    const bool out_lane = lane >= 1 && lane <= kRowOut && y < ny - lo;
-    const int yc = min(y, ny - lo);
-    unsigned owned = 0;
-#pragma unroll
-    for (int r = 0; r < kRows; ++r)
-      if (x0 + r >= xb) owned |= 1u << r;
-    const unsigned take = out_lane ? owned : 0u;
-    float2 in[3][(kRows + 2) / 2];
-#pragma unroll
-    for (int dz = 0; dz < 3; ++dz)
-#pragma unroll
-      for (int xp = 0; xp < (kRows + 2) / 2; ++xp) {
-        const float *pi = img + (long long)(z + dz - 1) * nxy + (long long)(x0 - 1 + 2 * xp) * ny + yc;
-        in[dz][xp] = make_float2(-__ldg(pi) * scale, -__ldg(pi + ny) * scale);
-      }
-    const float2 s2 = make_float2(scale, scale);
-    const float *ab = atl + ((long long)(z - 1) * axy + (long long)(x0 - 1) * apitch + yc);
-    const float *lb = lab + ((long long)z * axy + (long long)x0 * apitch + yc);
-    float P[kRows], W[kRows];
-#pragma unroll
-    for (int r = 0; r < kRows; ++r) P[r] = W[r] = 0.f;
-#pragma unroll 2
-    for (int c = 0; c < pl.n; ++c) {
-      const int off = pl.off[c];
-      eval_offset4<false>(ab + off, lb + off, in, axy, apitch, take, s2, P, W);
-    }
-    my_evals += (unsigned long long)pl.n * __popc(owned);
-#pragma unroll
-    for (int r = 0; r < kRows; ++r)
-      if ((take >> r) & 1u) {
-        const long long v = (long long)z * nxy + (long long)(x0 + r) * ny + y;
-        pacc[v] += P[r];
-        wacc[v] += W[r];
-      }
-  }
-  if (lane == 0 && my_evals) atomicAdd(evaluated, my_evals);
+  rescore_prior_body(pl, img, atl, lab, nx, ny, nz, apitch, scale, pacc, wacc, evaluated);
 }
 
 __global__ void finalize_kernel(const float *__restrict__ pacc, const float *__restrict__ wacc,
@@ -1931,6 +1701,57 @@ cudaError_t pack_all(const __nv_bfloat16 *wbf, uint32_t *frag, cudaStream_t s) {
   return cudaSuccess;
 }
 
+#include "pct_rescore_src.inc"  // k_pct_rescore_source: the text of pct_rescore.cuh
+
+// An entry point of the rescoring module compiled for this x extent and atlas row pitch, or
+// nullptr: the environment variable PCT_RESCORE_JIT=0 keeps the library build, as does a
+// missing NVRTC.
+void *rescore_jit(const char *entry, int nx, int pitch) {
+  const char *env = getenv("PCT_RESCORE_JIT");
+  if (env && env[0] == '0') return nullptr;
+  const std::vector<std::string> opts = {"-DPCT_RS_JIT", "-DPCT_RS_NX=" + std::to_string(nx),
+                                         "-DPCT_RS_PITCH=" + std::to_string(pitch)};
+  return jit::kernel(k_pct_rescore_source, "pct_rescore.cuh", opts, entry);
+}
+
+// One atlas's proposal rescoring: the geometry's compiled module where there is one, else the
+// library's kernel (same code, run-time strides).
+cudaError_t launch_rescore4(int level, int blocks, const RowProp *props, const float *img,
+                            const float *atl, const float *lab, int nx, int ny, int nz,
+                            int apitch, float scale, float conf_thr, float *pacc, float *wacc,
+                            unsigned long long *fallbacks, unsigned long long *evaluated,
+                            const unsigned char *tile_flag, RescoreTiles ts, cudaStream_t s) {
+  void *fn = rescore_jit(level == 2 ? "pct_rescore4_l2" : level == 3 ? "pct_rescore4_l3"
+                                                                      : "pct_rescore4_l4",
+                         nx, apitch);
+  if (fn) {
+    void *args[] = {&props, &img,  &atl,  &lab,       &nx,        &ny,       &nz,       &apitch,
+                    &scale, &conf_thr, &pacc, &wacc, &fallbacks, &evaluated, &tile_flag, &ts};
+    return jit::launch(fn, blocks, kRescoreWarps * 32, s, args);
+  }
+  auto k4 = level == 2 ? rescore4_kernel<2> : level == 3 ? rescore4_kernel<3> : rescore4_kernel<4>;
+  k4<<<blocks, kRescoreWarps * 32, 0, s>>>(props, img, atl, lab, nx, ny, nz, apitch, scale,
+                                            conf_thr, pacc, wacc, fallbacks, evaluated, tile_flag,
+                                            ts);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rescore_prior(int blocks, const PriorList &pl, const float *img,
+                                 const float *atl, const float *lab, int nx, int ny, int nz,
+                                 int apitch, float scale, float *pacc, float *wacc,
+                                 unsigned long long *evaluated, cudaStream_t s) {
+  void *fn = rescore_jit("pct_rescore_prior", nx, apitch);
+  if (fn) {
+    PriorList copy = pl;
+    void *args[] = {&copy, &img, &atl, &lab, &nx, &ny, &nz, &apitch, &scale, &pacc, &wacc,
+                    &evaluated};
+    return jit::launch(fn, blocks, kRescoreWarps * 32, s, args);
+  }
+  rescore_prior_kernel<<<blocks, kRescoreWarps * 32, 0, s>>>(pl, img, atl, lab, nx, ny, nz, apitch,
+                                                             scale, pacc, wacc, evaluated);
+  return cudaGetLastError();
+}
+
 }  // namespace
 
 // The learned form over all atlases of `in` (atlas and label rows `in.pitch` floats apart, the
@@ -2036,12 +1857,13 @@ cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInp
             sc.evaluated);
         if ((e = cudaGetLastError()) != cudaSuccess) return join(e);
       }
-      auto k4 = level == 2 ? rescore4_kernel<2> : level == 3 ? rescore4_kernel<3> : rescore4_kernel<4>;
-      k4<<<rescore_blocks, kRescoreWarps * 32, 0, s>>>(
-          props, in.img, A, L, g.nx, g.ny, g.nz, in.pitch, scale, tile_fallback ? 0.f : conf_thr,
-          sc.pacc, sc.wacc, sc.fallbacks, sc.evaluated, tile_fallback ? fb_flag : nullptr, ts);
+      if ((e = launch_rescore4(level, rescore_blocks, props, in.img, A, L, g.nx, g.ny, g.nz,
+                               in.pitch, scale, tile_fallback ? 0.f : conf_thr, sc.pacc, sc.wacc,
+                               sc.fallbacks, sc.evaluated, tile_fallback ? fb_flag : nullptr,
+                               RescoreTiles{ts.zt, ts.xc, ts.tiles_x, ts.tiles_y}, s)) !=
+          cudaSuccess)
+        return join(e);
       if (tile_fallback) {
-        if ((e = cudaGetLastError()) != cudaSuccess) return join(e);
         if ((e = launch_fuse_tiles(g, in, div, a, fb_list, fb_count, sc.pacc, sc.wacc, err, s)) !=
             cudaSuccess)
           return join(e);
@@ -2096,10 +1918,10 @@ cudaError_t launch_prior(const Geometry &g, const SlabInputs &in, float *out, do
   const int blocks = (int)(rblk < 1 ? 1 : (rblk > 64LL * sms() ? 64LL * sms() : rblk));
   const long long astride = (long long)g.nz * g.nx * in.pitch;
   for (int a = 0; a < g.num; ++a) {
-    rescore_prior_kernel<<<blocks, kRescoreWarps * 32, 0, s>>>(
-        pl, in.img, in.atlas + a * astride, in.label + a * astride, g.nx, g.ny, g.nz, in.pitch,
-        scale, sc.pacc, sc.wacc, sc.evaluated);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = launch_rescore_prior(blocks, pl, in.img, in.atlas + a * astride,
+                                  in.label + a * astride, g.nx, g.ny, g.nz, in.pitch, scale,
+                                  sc.pacc, sc.wacc, sc.evaluated, s)) != cudaSuccess)
+      return e;
   }
   finalize_kernel<<<sms() * 8, 256, 0, s>>>(sc.pacc, sc.wacc, out, g.nx, g.ny, g.nz);
   return cudaGetLastError();

@@ -386,3 +386,25 @@ def test_trained_network_gain():
     assert res["trained"]["mae_hu"] < res["prior"]["mae_hu"] < res["untrained"]["mae_hu"]
     assert res["trained"]["mae_hu"] <= 5.0
     assert res["trained"]["offsets_per_row"] == 32.0
+
+
+@pytest.mark.parametrize("mode", ["network", "network_conf", "prior"])
+def test_runtime_compiled_rescoring_matches_library_build(mode, monkeypatch):
+    """The rescoring runs from a module compiled at run time for the volume's x extent and row
+    pitch; PCT_RESCORE_JIT=0 keeps the library's own build of the same code. Both give the same
+    output bit for bit (odd sizes; with a confidence threshold the atlas rows are repacked to a
+    16-byte pitch, a second geometry)."""
+    nx, ny, nz, num = 41, 53, 31, 2
+    img, atl, lab = subject(nx, ny, nz, num, 61)
+    outs = []
+    for jit in ("1", "0"):
+        monkeypatch.setenv("PCT_RESCORE_JIT", jit)
+        with pct.Handle(0) as h, learned.LearnedModel(0, seed=5) as m:
+            if mode == "prior":
+                h.set_learned_prior(32)
+            else:
+                h.attach_model(m, 0.02 if mode == "network_conf" else 0.0)
+            outs.append((h.synthesize(img, atl, lab, NH, DIV, pct.EXEC_LEARNED), h.learned_stats()))
+    (a, sa), (b, sb) = outs
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert sa == sb

@@ -162,7 +162,7 @@ def full_subject():
     return s, pct.normalize_labels(s.atlas_ct)
 
 
-@pytest.mark.parametrize("nh", [7, 11])
+@pytest.mark.parametrize("nh", [7, 9, 11])
 def test_full_size_sampled_voxels(handle, full_subject, nh):
     """Full config-1 volume on the GPU; the oracle recomputes 1500 random interior voxels."""
     s, label = full_subject
