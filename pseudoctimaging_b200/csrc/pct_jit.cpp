@@ -7,7 +7,8 @@
 // loaded function for the life of the process. NVRTC is opened with dlopen, the driver's module
 // calls through the runtime's entry-point query, so the library neither links against them nor
 // fails to load without them: jit::kernel then returns nullptr and the caller launches its
-// ahead-of-time build of the same code. A failed compile or load is remembered and not retried.
+// ahead-of-time build of the same code. A failed compile or load is remembered and not retried;
+// at most kMaxModules are built per process.
 //
 // The cache key holds the context's unique id (cuCtxGetId), so a cudaDeviceReset, which
 // destroys the modules with the context, leads to a fresh compile rather than a stale handle.
@@ -93,8 +94,13 @@ const Driver &driver() {
   return d;
 }
 
+// Compiled modules stay loaded for the life of their context; past this many (distinct
+// geometries) new ones are not built and callers use their ahead-of-time kernels.
+constexpr int kMaxModules = 64;
+
 std::mutex g_mu;
 std::map<std::string, CUfunction> g_cache;  // nullptr entries: failed, not retried
+int g_modules = 0;
 
 // Compiles `source` for the current device and returns the loaded `entry_name`, or nullptr.
 CUfunction build(const char *source, const char *file_name, const std::vector<std::string> &options,
@@ -149,8 +155,10 @@ void *kernel(const char *source, const char *file_name, const std::vector<std::s
   std::lock_guard<std::mutex> lock(g_mu);
   auto it = g_cache.find(key);
   if (it != g_cache.end()) return it->second;
+  if (g_modules >= kMaxModules) return nullptr;
   CUfunction fn = build(source, file_name, options, entry_name);
   g_cache[key] = fn;
+  if (fn) ++g_modules;
   return fn;
 }
 

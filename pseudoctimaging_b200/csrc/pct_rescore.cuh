@@ -23,15 +23,16 @@
 // plain kernel's arithmetic (the reference's PatchSimilarity and weighted sums,
 // NewPatchedBrainPureC.cpp:1184-1212,1350-1449), over the kept offsets only.
 
-// Offsets in flight per warp: with constant strides two offsets' loads fit the registers (5.59
-// against 5.99 ms per learned step at 222x222x112, 10 atlases); with run-time strides the
-// address registers leave room for one (6.28 against 6.44 ms).
+// Offsets in flight per warp (unroll of the offset loop) and CTAs per SM, measured on the learned
+// step at 222x222x112, 10 atlases, k = 32. Constant strides: one offset at 7 CTAs (72 registers)
+// 5.33 ms; 1/6 5.55, 1/8 5.63, 2/6 5.44, 2/7 5.66, 2/4 5.59, 3/4 5.52, 3/6 5.75. Run-time
+// strides (the library build; its address registers need 128): one offset at 4 CTAs 6.28 ms,
+// two 6.44.
 #ifndef PCT_RS_UNROLL
-#ifdef PCT_RS_NX
-#define PCT_RS_UNROLL 2
-#else
 #define PCT_RS_UNROLL 1
 #endif
+#ifndef PCT_RS_MIN_CTAS
+#define PCT_RS_MIN_CTAS 7  // of the run-time compiled entry points
 #endif
 
 constexpr int kRsAxis = 11;       // offsets per axis of the NH = 11 window
@@ -320,7 +321,7 @@ __device__ __forceinline__ void rescore_prior_body(
 #ifdef PCT_RS_JIT
 // Entry points of the run-time compiled module (same parameters as the library's kernels).
 #define PCT_RS_ENTRY(NAME, LEVEL)                                                                 \
-  extern "C" __global__ void __launch_bounds__(kRescoreWarps * 32, 4) NAME(                       \
+  extern "C" __global__ void __launch_bounds__(kRescoreWarps * 32, PCT_RS_MIN_CTAS) NAME(         \
       const RowProp *__restrict__ props, const float *__restrict__ img,                           \
       const float *__restrict__ atl, const float *__restrict__ lab, int nx, int ny, int nz,       \
       int apitch, float scale, float conf_thr, float *__restrict__ pacc,                          \
@@ -335,7 +336,7 @@ PCT_RS_ENTRY(pct_rescore4_l3, 3)
 PCT_RS_ENTRY(pct_rescore4_l4, 4)
 #undef PCT_RS_ENTRY
 
-extern "C" __global__ void __launch_bounds__(kRescoreWarps * 32, 4)
+extern "C" __global__ void __launch_bounds__(kRescoreWarps * 32, PCT_RS_MIN_CTAS)
     pct_rescore_prior(const __grid_constant__ PriorList pl, const float *__restrict__ img,
                       const float *__restrict__ atl, const float *__restrict__ lab, int nx, int ny,
                       int nz, int apitch, float scale, float *__restrict__ pacc,
