@@ -386,6 +386,24 @@ int pct_raw_read(const char *path, float *out, size_t n);
 int pct_raw_write(const char *path, const float *data, size_t n);
 
 /*
+ * MATLAB level-5 MAT-files, the reference's data and result files (ReadMatFile / FindDimension /
+ * WriteOutputMatFile, PatchBasedPseudoCT.cu:1047-1370; read there through MATLAB's libmat).
+ * A data file holds `img` ([nx ny nz] single) and the structs `atlas` and `atlas_label` whose
+ * fields are the atlases' [nx ny nz] single volumes, atlas i = field i. pct_mat_dims gives
+ * {num, nx, ny, nz}; pct_mat_read fills img (n_img = nx*ny*nz) and the atlas MRI and CT stacks
+ * (n_atlas = num*nx*ny*nz) in this library's [atlas][z][x][y] layout (x = MATLAB dimension 1,
+ * y = dimension 2, as the reference's ConvertToRowBased). Compressed (level-7) elements are
+ * read; little-endian files only. pct_mat_write stores one [nx ny nz] single variable named
+ * `variable` (uncompressed), from the [z][x][y] layout. PCT_ERR_INVALID_ARG for unreadable or
+ * malformed files and for sizes that do not match.
+ */
+int pct_mat_dims(const char *path, int dims[4]);
+int pct_mat_read(const char *path, float *img, float *atlas_mri, float *atlas_ct, size_t n_img,
+                 size_t n_atlas);
+int pct_mat_write(const char *path, const char *variable, const float *vol, int nx, int ny,
+                  int nz);
+
+/*
  * Normalised cross-correlation of two device volumes over the interior of an NH window, counting
  * only voxels finite in both (FP64 sums); the quality measure the reference reports for its
  * pseudo-CTs against the real CT (imgs/Correlation.png). *ncc is NaN if fewer than two voxels

@@ -130,6 +130,9 @@ SIGNATURES = {
     "pct_matrixio_write": (_I, [ctypes.c_char_p, _P, _I, _I, _I, _I]),
     "pct_raw_read": (_I, [ctypes.c_char_p, _P, _SZ]),
     "pct_raw_write": (_I, [ctypes.c_char_p, _P, _SZ]),
+    "pct_mat_dims": (_I, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)]),
+    "pct_mat_read": (_I, [ctypes.c_char_p, _P, _P, _P, _SZ, _SZ]),
+    "pct_mat_write": (_I, [ctypes.c_char_p, ctypes.c_char_p, _P, _I, _I, _I]),
     "pct_ncc_device": (_I, [_P, _P, _P, _I, _I, _I, _I, ctypes.POINTER(ctypes.c_double),
                             ctypes.POINTER(ctypes.c_int64), _P]),
     "pct_test_wait_timeout": (_I, [_P, _D]),
@@ -485,6 +488,33 @@ def write_matrixio(path, vol) -> None:
     st = lib.pct_matrixio_write(str(path).encode(), _ptr(v), num, rows, cols, depth)
     if st != PCT_OK:
         raise PctError(st, f"pct_matrixio_write({path})")
+
+
+def read_mat(path):
+    """The reference's MAT data file (img, atlas, atlas_label): (img [z][x][y], atlas MRI
+    [num][z][x][y], atlas CT [num][z][x][y]) as float32, x = MATLAB dimension 1."""
+    dims = (ctypes.c_int * 4)()
+    st = lib.pct_mat_dims(str(path).encode(), dims)
+    if st != PCT_OK:
+        raise PctError(st, f"pct_mat_dims({path})")
+    num, nx, ny, nz = dims
+    img = np.empty((nz, nx, ny), np.float32)
+    atl = np.empty((num, nz, nx, ny), np.float32)
+    ct = np.empty((num, nz, nx, ny), np.float32)
+    st = lib.pct_mat_read(str(path).encode(), _ptr(img), _ptr(atl), _ptr(ct), img.size, atl.size)
+    if st != PCT_OK:
+        raise PctError(st, f"pct_mat_read({path})")
+    return img, atl, ct
+
+
+def write_mat(path, variable: str, vol) -> None:
+    """Writes a [z][x][y] float32 volume as one [nx ny nz] single variable of a MAT-file, as the
+    reference writes its result."""
+    v = np.ascontiguousarray(vol, np.float32)
+    nz, nx, ny = v.shape
+    st = lib.pct_mat_write(str(path).encode(), variable.encode(), _ptr(v), nx, ny, nz)
+    if st != PCT_OK:
+        raise PctError(st, f"pct_mat_write({path})")
 
 
 @dataclass

@@ -33,7 +33,8 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", f"-ccbin={HOST_CXX}", "-Xcompiler", 
 # Sources that make up the shared library; the CLI main is linked separately against it.
 LIB_SOURCES = ["pct_api.cu", "pct_fuse_tma.cu", "pct_pointwise.cu", "pct_regularize.cu",
                "pct_noalloc.cu", "pct_synth.cpp", "pct_io.cpp", "pct_learned_train.cu",
-               "pct_learned_api.cu", "pct_learned_infer.cu", "pct_tc_fuse.cu", "pct_jit.cpp"]
+               "pct_learned_api.cu", "pct_learned_infer.cu", "pct_tc_fuse.cu", "pct_jit.cpp",
+               "pct_mat.cpp"]
 # Device sources that are also compiled at run time (NVRTC): each is embedded as a string in
 # _build/<stem>_src.inc, which the library sources include.
 EMBEDDED = ["pct_rescore.cuh"]
@@ -108,7 +109,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
             if log:
                 sys.stdout.write(log)
     if force or _stale(LIB, objs):
-        _run([nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lpthread", "-ldl"], verbose)
+        _run([nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lpthread", "-ldl", "-lz"], verbose)
     cli_src = [CSRC / s for s in CLI_SOURCES if (CSRC / s).exists()]
     if cli_src:
         cli_objs = [_compile(s, force, verbose, False)[0] for s in cli_src]

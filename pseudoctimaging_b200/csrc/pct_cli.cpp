@@ -10,7 +10,10 @@
 // the learned proposal (NH = 11; the network from $PCT_LEARNED_MODEL, else the checkpoint
 // shipped beside the program, with the fallback threshold $PCT_LEARNED_CONF, default 0).
 //
-// <data> is the reference's non-MATLAB configuration file (PatchBasedPseudoCT.cu:1376-1488):
+// <data> is the reference's MATLAB data file (a name ending in .mat: variables img, atlas and
+// atlas_label, ReadMatFile, PatchBasedPseudoCT.cu:1047-1169; the result goes to
+// <output name>.mat as one single variable named after the result, WriteOutputMatFile,
+// :1310-1370), or its non-MATLAB configuration file (PatchBasedPseudoCT.cu:1376-1488):
 //   line 1: 0 -> lines 2-4: atlas MRI, atlas CT, input MRI as MatrixIO text files
 //           1 -> lines 2-5: num, nx, ny, nz; volumes of uniform [0,10) values (the reference's
 //                test mode; seeded here, so runs are reproducible)
@@ -39,7 +42,13 @@ struct Subject {
   int nx = 0, ny = 0, nz = 0, num = 0;
   std::vector<float> img, atlas, ct;
   bool raw_output = false;
+  bool mat_output = false;
 };
+
+bool ends_with(const std::string &s, const char *suffix) {
+  const size_t n = strlen(suffix);
+  return s.size() >= n && s.compare(s.size() - n, n, suffix) == 0;
+}
 
 std::vector<std::string> read_lines(const char *path) {
   std::vector<std::string> lines;
@@ -67,6 +76,30 @@ bool load_matrixio(const std::string &path, std::vector<float> &out, int dims[4]
 }
 
 bool load_subject(const char *config, Subject *s, std::string *err) {
+  if (ends_with(config, ".mat") || ends_with(config, ".MAT")) {
+    // the reference's MATLAB data file: img, atlas, atlas_label (ReadMatFile)
+    int d[4];
+    if (pct_mat_dims(config, d) != PCT_OK) {
+      *err = std::string("cannot read the MAT data file ") + config +
+             " (img, atlas and atlas_label of equal [nx ny nz] single volumes)";
+      return false;
+    }
+    s->num = d[0];
+    s->nx = d[1];
+    s->ny = d[2];
+    s->nz = d[3];
+    const size_t n = (size_t)s->nx * s->ny * s->nz;
+    s->img.resize(n);
+    s->atlas.resize(n * s->num);
+    s->ct.resize(n * s->num);
+    if (pct_mat_read(config, s->img.data(), s->atlas.data(), s->ct.data(), n, n * s->num) !=
+        PCT_OK) {
+      *err = std::string("cannot read the MAT data file ") + config;
+      return false;
+    }
+    s->mat_output = true;
+    return true;
+  }
   const std::vector<std::string> L = read_lines(config);
   if (L.empty()) {
     *err = std::string("cannot read configuration file ") + config;
@@ -242,9 +275,16 @@ int main(int argc, char **argv) {
     const double ms =
         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     if (st == PCT_OK) {
-      const std::string file = out_name + (s.raw_output ? ".f32" : ".txt");
-      const int wst = s.raw_output ? pct_raw_write(file.c_str(), out.data(), n)
-                                   : pct_matrixio_write(file.c_str(), out.data(), 1, s.nx, s.ny, s.nz);
+      const std::string file =
+          out_name + (s.mat_output ? ".mat" : s.raw_output ? ".f32" : ".txt");
+      // a MAT result holds one variable named after the result, as the reference's
+      // WriteOutputMatFile; a directory part of the name is not part of the variable's name
+      const size_t slash = out_name.find_last_of("/\\");
+      const std::string var = slash == std::string::npos ? out_name : out_name.substr(slash + 1);
+      const int wst =
+          s.mat_output ? pct_mat_write(file.c_str(), var.c_str(), out.data(), s.nx, s.ny, s.nz)
+          : s.raw_output ? pct_raw_write(file.c_str(), out.data(), n)
+                         : pct_matrixio_write(file.c_str(), out.data(), 1, s.nx, s.ny, s.nz);
       if (wst != PCT_OK) {
         fprintf(stderr, "cannot write %s\n", file.c_str());
         st = wst;

@@ -83,3 +83,28 @@ def test_cli_tensor_core_and_learned_choices(tmp_path):
                          capture_output=True, text=True, timeout=300,
                          env={"PCT_LEARNED_MODEL": str(tmp_path / "missing.pctl")})
     assert res.returncode != 0 and "missing.pctl" in res.stderr
+
+
+def test_cli_mat_data_file(tmp_path):
+    """The reference's own data-file format: a MAT-file with img and the structs atlas and
+    atlas_label (one field per atlas), written here by scipy.io in MATLAB's column-major
+    [nx ny nz] layout, compressed; the result comes back as <output>.mat with one single variable
+    named after the result. Same output as the raw-file mode on the same volumes."""
+    sio = pytest.importorskip("scipy.io")
+    s = pct.synth_subject(30, 28, 26, 2, n_blobs=6, seed=9)
+    col = lambda v: np.ascontiguousarray(np.transpose(v, (1, 2, 0)))  # [z][x][y] -> [nx ny nz]
+    sio.savemat(tmp_path / "Subject.mat", {
+        "atlas": {f"MRI{i + 1}": col(s.atlas_mri[i]) for i in range(2)},
+        "atlas_label": {f"MRI{i + 1}": col(s.atlas_ct[i]) for i in range(2)},
+        "img": col(s.img)}, do_compression=True, format="5")
+    run_cli(tmp_path / "Subject.mat", tmp_path / "Subject_result", 2, 7, 2.5, 1.0)
+    m = sio.loadmat(tmp_path / "Subject_result.mat")
+    got = np.ascontiguousarray(np.transpose(m["Subject_result"], (2, 0, 1)))
+    s.atlas_mri.tofile(tmp_path / "a.f32")
+    s.atlas_ct.tofile(tmp_path / "c.f32")
+    s.img.tofile(tmp_path / "i.f32")
+    cfg = tmp_path / "raw.cfg"
+    cfg.write_text(f"2\n2\n30\n28\n26\n{tmp_path/'a.f32'}\n{tmp_path/'c.f32'}\n{tmp_path/'i.f32'}\n")
+    run_cli(cfg, tmp_path / "raw", 2, 7, 2.5, 1.0)
+    ref = np.fromfile(str(tmp_path / "raw") + ".f32", np.float32).reshape(26, 30, 28)
+    assert np.array_equal(got, ref)
