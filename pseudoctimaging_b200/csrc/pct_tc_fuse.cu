@@ -74,7 +74,9 @@ constexpr float kFloorScore = -1.0e9f;
 // over the atlases before it (scores are -|a - b|^2/2 <= 0, so the start lies below it): the
 // atlases of one subject differ little there, and a voxel whose own 16th best is lower sends its
 // tile to the exact redo launch (1.08 of the previous atlas's value alone sent so many tiles
-// there that the step took 380 ms instead of 209 ms on config 2).
+// there that the step took 380 ms instead of 209 ms on config 2; of the running minimum, margins
+// 1.10 / 1.15 / 1.25 / 1.40 took 219.5 / 208.3 / 209.0 / 216.5 ms: fewer redos against fewer
+// insertions, flat between 1.15 and 1.25).
 constexpr float kWarmMargin = 1.25f;
 constexpr float kDblEpsilonF = 2.220446049250313080847e-16f;
 constexpr unsigned long long kTimeoutNs = 2000000000ULL;
