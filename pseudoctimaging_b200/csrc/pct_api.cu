@@ -365,8 +365,8 @@ int fuse_pipelined(pct_handle *h, const pct::Geometry &g, const float *img, cons
   PCT_CUDA(h, pct::launch_fuse_tma_groups(g, in, div, partial, err, h->tile_set, 0, 1, s));
   // The second group runs as soon as it has landed, the remaining groups in one launch once
   // everything has (config 1 end to end: 34.0 ms against 34.2 with groups 2.. in one launch; a
-  // launch per group 34.0; pitched 2-D host copies instead of the repack kernel, which would free
-  // the SMs of the repack, run the copy engine at a quarter of its speed: 82.9 ms).
+  // launch per group 34.0; pitched 2-D host copies of the 888-byte rows instead of the repack
+  // kernel made the uploads several times slower: 82.9 ms).
   int next = 1;
   if (pl.groups >= 3) {
     if ((st = stage_group(per, 2 * per))) return st;
