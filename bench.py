@@ -808,7 +808,9 @@ def run_tc_arm(args) -> None:
         "plain": {"ms_per_step": times[pct.EXEC_B200_FP32],
                   "value": nvox / (times[pct.EXEC_B200_FP32] / 1e3),
                   **check.errors(outs[pct.EXEC_B200_FP32])},
-        "gpu_launches": args.steps,
+        # per FP16 step: the input mean, per atlas the patch rows and the main launch, per atlas
+        # after the first the redo launch, and the finalisation
+        "gpu_launches": args.steps * (3 * num + 1),
         "roofline": {"bound": "tensor", "unit": "TFLOP/s", "achieved": flop / (ms / 1e3) / 1e12,
                      "peak": peaks.get("bf16_tflops"),
                      "frac": flop / (ms / 1e3) / 1e12 / peaks["bf16_tflops"]
