@@ -239,16 +239,17 @@ int pct_model_train(pct_model *m, pct_train_set *ts, int batch, int steps, float
 
 /*
  * Learned-proposal form, inference side. pct_attach_model makes EXEC_CHOICE 7 available on the
- * handle's pct_synthesize / pct_synthesize_device / pct_run_pipeline calls (NH must be 11; the
+ * handle's pct_synthesize / pct_synthesize_device / pct_run_pipeline calls (NH 7, 9 or 11; the
  * model must live on the handle's device and outlive its use; m = NULL detaches). Per atlas and
  * per row segment of 30 interior voxels along y, the network's per-axis offset probabilities
- * of the segment's voxels are summed; the 4 most probable offsets per axis are kept and, of their
+ * of the segment's voxels are summed (for NH 7 and 9 each axis's softmax runs over the offsets
+ * inside the window only); the 4 most probable offsets per axis are kept and, of their
  * 64 combinations, the 32 whose per-axis ranks sum to at most 4 (ties: lower offset first). Only
  * those 32 offsets get the exact FP32 SSD and a weight. A voxel whose own probability mass
- * (p_w*p_u*p_v summed over the 32) is below `conf_threshold` falls back to all 11^3 offsets for
+ * (p_w*p_u*p_v summed over the 32) is below `conf_threshold` falls back to all NH^3 offsets for
  * that atlas. conf_threshold = 0 never falls back; a threshold above 1 always does (every
  * candidate, as the plain method). Output: the same interior, border and NaN rule as the plain
- * method (voxels 6 or more from every face). No counterpart in the reference.
+ * method (voxels (NH+1)/2 or more from every face). No counterpart in the reference.
  */
 int pct_attach_model(pct_handle *h, pct_model *m, float conf_threshold);
 /* Proposal sharing (default 4): row segments share the proposal of their block's anchor row,
@@ -274,7 +275,7 @@ int pct_set_learned_k(pct_handle *h, int k);
 /*
  * The proposal baseline without a network, for measuring what the network gains: with k > 0,
  * EXEC_CHOICE 7 runs no convolutions and no proposal kernel and needs no attached model; every
- * voxel rescores the same k offsets, those of the 11^3 window nearest its centre (by squared
+ * voxel rescores the same k offsets, those of the NH^3 window nearest its centre (by squared
  * distance, ties in (dw, du, dv) order), with the learned form's exact FP32 rescoring; no
  * confidence fallback. k = 0 (the default) uses the attached network. 0 <= k <= 125. No
  * counterpart in the reference (its search is always the full window,

@@ -281,7 +281,7 @@ class Handle:
                     "pct_set_learned_convs")
 
     def attach_model(self, model, conf_threshold: float = 0.0) -> None:
-        """Makes EXEC_LEARNED available (NH = 11) with a :class:`learned.LearnedModel` (None
+        """Makes EXEC_LEARNED available (NH 7, 9, 11) with a :class:`learned.LearnedModel` (None
         detaches). Pairs whose 32 proposals hold less than ``conf_threshold`` of the proposal's
         probability mass fall back to the full search. The model must outlive its use."""
         self._model = model

@@ -171,12 +171,20 @@ int learned_ran(pct_handle *h, const pct::Geometry &g, cudaStream_t s) {
 // The learned form: conv features, proposal and exact rescoring over all atlases (NH = 11).
 int launch_learned_path(pct_handle *h, const pct::Geometry &g, const pct::SlabInputs &in,
                         float *d_out, double div, cudaStream_t s) {
-  if (g.nh != 11)
+  // The network scores the 11 offsets of each axis; smaller windows keep the offsets inside them
+  // (NH 7 and 9). Below 7 the interior would start fewer than 4 voxels from a face, inside the
+  // reach of the network's four 3x3x3 layers.
+  if (g.nh != 7 && g.nh != 9 && g.nh != 11)
     return fail(h, PCT_ERR_UNSUPPORTED,
-                "exec_choice 7 (learned proposal) is trained for NH = 11 only, got NH = " +
+                "exec_choice 7 (learned proposal) runs NH = 7, 9 or 11, got NH = " +
                     std::to_string(g.nh));
   if (h->learned_prior_k > 0) {
-    if (g.nx - 12 < 4)
+    const int window = g.nh * g.nh * g.nh;
+    if (h->learned_prior_k > window)
+      return fail(h, PCT_ERR_INVALID_ARG,
+                  "the centre prior's k = " + std::to_string(h->learned_prior_k) +
+                      " exceeds the NH^3 = " + std::to_string(window) + " window");
+    if (g.ix < 4)
       return fail(h, PCT_ERR_UNSUPPORTED, "the centre prior needs at least 4 interior x-rows");
     int st = ensure(h, h->learned, pct::learned::infer_scratch_bytes(g));
     if (st) return st;

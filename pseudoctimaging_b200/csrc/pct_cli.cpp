@@ -7,7 +7,7 @@
 // device 0, as in the reference). EXEC_CHOICE 0/1/2/3 run the path (the reference's GM, GM2, SM
 // and this library's plain FP32 kernel, which compute the same function); 4 times it like the
 // reference's GpuTestTime (10 samples of 10 calls); 5/6 run the tensor-core FP16/BF16 form and 7
-// the learned proposal (NH = 11; the network from $PCT_LEARNED_MODEL, else the checkpoint
+// the learned proposal (NH = 7, 9 or 11; the network from $PCT_LEARNED_MODEL, else the checkpoint
 // shipped beside the program, with the fallback threshold $PCT_LEARNED_CONF, default 0).
 //
 // <data> is the reference's MATLAB data file (a name ending in .mat: variables img, atlas and
@@ -188,7 +188,7 @@ void usage() {
       "[device]\n"
       "  EXEC_CHOICE {GM=0, GM2=1, SM=2, B200 FP32=3: the path; GpuTestTime=4: timing;\n"
       "               5/6: tensor-core FP16/BF16 form; 7: learned proposal}\n"
-      "  NH {3,5,7,9,11} (11 for 5, 6, 7); sigma, beta default 1; device default 0\n"
+      "  NH {3,5,7,9,11} (11 for 5 and 6; 7, 9 or 11 for 7); sigma, beta default 1; device 0\n"
       "  EXEC_CHOICE 7 reads the network from $PCT_LEARNED_MODEL (default: the checkpoint\n"
       "  shipped beside this program, ../checkpoints/learned_nh11.pctl) and the full-search\n"
       "  confidence threshold from $PCT_LEARNED_CONF (default 0)\n");

@@ -963,10 +963,14 @@ __device__ __forceinline__ void stage_heads(const __nv_bfloat16 *__restrict__ wb
 }
 
 // Per-axis offset probabilities of one (voxel, atlas) pair from its 16 conv4 features: the three
-// softmaxes over dw, du, dv of the heads' logits, p[a * 11 + j] for offset j - 5 on axis a.
+// softmaxes over dw, du, dv of the heads' logits, p[a * 11 + j] for offset j - 5 on axis a. For a
+// window NH = 2 half + 1 below 11 each softmax runs over the window's offsets only
+// (|j - 5| <= half) and the others get probability 0; at NH = 11 every offset takes part.
+__device__ __forceinline__ bool in_window(int j, int half) { return (unsigned)(j - 5 + half) <= 2u * half; }
+
 __device__ __forceinline__ void axis_probs(const __nv_bfloat16 *__restrict__ f4, long long v,
                                            long long nvox, const float *__restrict__ hw,
-                                           float (&p)[kHeads]) {
+                                           float (&p)[kHeads], int half) {
   float f[kC];
   {
     __align__(16) __nv_bfloat16 fb[kC];
@@ -992,13 +996,14 @@ __device__ __forceinline__ void axis_probs(const __nv_bfloat16 *__restrict__ f4,
   for (int o = 0; o < kHeads; ++o) p[o] = (o & 1) ? acc[o / 2].y : acc[o / 2].x;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    float m = p[a * kAxis];
+    float m = -INFINITY;
 #pragma unroll
-    for (int j = 1; j < kAxis; ++j) m = fmaxf(m, p[a * kAxis + j]);
+    for (int j = 0; j < kAxis; ++j)
+      if (in_window(j, half)) m = fmaxf(m, p[a * kAxis + j]);
     float sum = 0.f;
 #pragma unroll
     for (int j = 0; j < kAxis; ++j) {
-      p[a * kAxis + j] = __expf(p[a * kAxis + j] - m);
+      p[a * kAxis + j] = in_window(j, half) ? __expf(p[a * kAxis + j] - m) : 0.f;
       sum += p[a * kAxis + j];
     }
     const float inv = 1.f / sum;
@@ -1007,16 +1012,17 @@ __device__ __forceinline__ void axis_probs(const __nv_bfloat16 *__restrict__ f4,
   }
 }
 
-// The 4 largest of p[a * 11 .. a * 11 + 10] in order, ties to the lower offset: indices 0..10.
-__device__ __forceinline__ void top4(const float (&p)[kHeads], int a, int (&idx)[4]) {
+// The 4 largest of p[a * 11 .. a * 11 + 10] within the window in order, ties to the lower
+// offset: indices 0..10.
+__device__ __forceinline__ void top4(const float (&p)[kHeads], int a, int (&idx)[4], int half) {
   unsigned used = 0;
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
-    int bi = 0;
+    int bi = 5;
     float bp = -1.f;
 #pragma unroll
     for (int j = 0; j < kAxis; ++j)
-      if (!((used >> j) & 1u) && p[a * kAxis + j] > bp) {
+      if (in_window(j, half) && !((used >> j) & 1u) && p[a * kAxis + j] > bp) {
         bp = p[a * kAxis + j];
         bi = j;
       }
@@ -1074,13 +1080,13 @@ struct Proposal {
 
 __device__ __forceinline__ void propose(const __nv_bfloat16 *__restrict__ f4, long long v,
                                         long long nvox, const float *__restrict__ hw,
-                                        Proposal &pr) {
+                                        Proposal &pr, int half) {
   float p[kHeads];
-  axis_probs(f4, v, nvox, hw, p);
+  axis_probs(f4, v, nvox, hw, p, half);
   int top[3][4];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    top4(p, a, top[a]);
+    top4(p, a, top[a], half);
 #pragma unroll
     for (int r = 0; r < 4; ++r) pr.top[a][r] = (signed char)(top[a][r] - 5);
   }
@@ -1091,14 +1097,15 @@ __device__ __forceinline__ void propose(const __nv_bfloat16 *__restrict__ f4, lo
 __global__ void proposal_hook_kernel(const __nv_bfloat16 *__restrict__ f4,
                                      const __nv_bfloat16 *__restrict__ wbf,
                                      const int64_t *__restrict__ voxels, int n, long long nvox,
-                                     signed char *__restrict__ top, float *__restrict__ conf) {
+                                     signed char *__restrict__ top, float *__restrict__ conf,
+                                     int half) {
   __shared__ __align__(16) float hw[kHeadFloats];
   stage_heads(wbf, hw);
   __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   Proposal pr;
-  propose(f4, voxels[i], nvox, hw, pr);
+  propose(f4, voxels[i], nvox, hw, pr, half);
   for (int a = 0; a < 3; ++a)
     for (int r = 0; r < 4; ++r) top[i * 12 + a * 4 + r] = pr.top[a][r];
   conf[i] = pr.conf;
@@ -1119,7 +1126,7 @@ __device__ __forceinline__ int anchor_of(int b, int block, int extent) {
 __global__ void __launch_bounds__(kRescoreWarps * 32)
     propose_rows_kernel(const __nv_bfloat16 *__restrict__ f4, const __nv_bfloat16 *__restrict__ wbf,
                         int nx, int ny, int nz, int block, int level,
-                        RowProp *__restrict__ props) {
+                        RowProp *__restrict__ props, int half) {
   __shared__ __align__(16) float hw[kHeadFloats];
   __shared__ float s_prob[kRescoreWarps * 32 * kProbStride];
   __shared__ float s_sum[kRescoreWarps * 36];
@@ -1127,7 +1134,7 @@ __global__ void __launch_bounds__(kRescoreWarps * 32)
   stage_heads(wbf, hw);
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  const int lo = 6;
+  const int lo = half + 1;
   const int ix = nx - 2 * lo, iz = nz - 2 * lo, iy = ny - 2 * lo;
   if (ix <= 0 || iy <= 0 || iz <= 0) return;
   const int segs = (iy + kRowOut - 1) / kRowOut;
@@ -1144,7 +1151,7 @@ __global__ void __launch_bounds__(kRescoreWarps * 32)
     const bool out_lane = lane >= 1 && lane <= kRowOut && y < ny - lo;
     float p[kHeads];
     if (out_lane) {
-      axis_probs(f4, (long long)z * nxy + (long long)x * ny + y, (long long)nz * nxy, hw, p);
+      axis_probs(f4, (long long)z * nxy + (long long)x * ny + y, (long long)nz * nxy, hw, p, half);
     } else {
 #pragma unroll
       for (int o = 0; o < kHeads; ++o) p[o] = 0.f;
@@ -1175,11 +1182,11 @@ __global__ void __launch_bounds__(kRescoreWarps * 32)
       unsigned used = 0;
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
-        int bi = 0;
+        int bi = 5;
         float bp = -1.f;
 #pragma unroll
         for (int j = 0; j < kAxis; ++j)
-          if (!((used >> j) & 1u) && q[j] > bp) {
+          if (in_window(j, half) && !((used >> j) & 1u) && q[j] > bp) {
             bp = q[j];
             bi = j;
           }
@@ -1239,9 +1246,9 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 3)
                    const float *__restrict__ atl, const float *__restrict__ lab, int nx, int ny,
                    int nz, int apitch, float neg_k, float conf_thr, float *__restrict__ pacc,
                    float *__restrict__ wacc, unsigned long long *__restrict__ fallbacks,
-                   unsigned long long *__restrict__ evaluated) {
+                   unsigned long long *__restrict__ evaluated, int half) {
   const int lane = threadIdx.x & 31;
-  const int lo = 6;
+  const int lo = half + 1;
   const int ix = nx - 2 * lo, iz = nz - 2 * lo, iy = ny - 2 * lo;
   if (ix <= 0 || iy <= 0 || iz <= 0) return;
   const int segs = (iy + kRowOut - 1) / kRowOut;
@@ -1304,18 +1311,18 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 3)
           rank[a] |= (unsigned long long)r << (4 * top[a][r]);
         }
       }
-      for (int jw = 0; jw < kAxis; ++jw) {
+      for (int jw = 5 - half; jw <= 5 + half; ++jw) {
         const int rw = (int)((rank[0] >> (4 * jw)) & 0xF);
-        for (int ju = 0; ju < kAxis; ++ju) {
+        for (int ju = 5 - half; ju <= 5 + half; ++ju) {
           const int ru = rw + (int)((rank[1] >> (4 * ju)) & 0xF);
-          for (int jv = 0; jv < kAxis; ++jv) {
+          for (int jv = 5 - half; jv <= 5 + half; ++jv) {
             const bool mine = full || (ru + (int)((rank[2] >> (4 * jv)) & 0xF) <= level);
             eval_offset(atl, lab, in, vz + axy + apitch, axy, apitch, yc, jw - 5, ju - 5, jv - 5,
                         mine && out_lane, P, W, neg_k);
           }
         }
       }
-      my_evals += kAxis * kAxis * kAxis;
+      my_evals += (unsigned long long)(2 * half + 1) * (2 * half + 1) * (2 * half + 1);
     }
     if (out_lane) {
       const long long v = (long long)z * nxy + (long long)x * ny + y;
@@ -1336,9 +1343,9 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 4)
                     int nz, int apitch, float scale, float conf_thr, float *__restrict__ pacc,
                     float *__restrict__ wacc, unsigned long long *__restrict__ fallbacks,
                     unsigned long long *__restrict__ evaluated,
-                    const unsigned char *__restrict__ tile_flag, const RescoreTiles ts) {
+                    const unsigned char *__restrict__ tile_flag, const RescoreTiles ts, int hw) {
   rescore4_body<LEVEL>(props, img, atl, lab, nx, ny, nz, apitch, scale, conf_thr, pacc, wacc,
-                       fallbacks, evaluated, tile_flag, ts);
+                       fallbacks, evaluated, tile_flag, ts, hw);
 }
 
 // The confidence fallback at the plain kernel's tile granularity (blocks of 4 x 4 rows share a
@@ -1352,7 +1359,7 @@ __global__ void flag_tiles_kernel(const RowProp *__restrict__ props, int nx, int
                                   int *__restrict__ count,
                                   unsigned long long *__restrict__ fallbacks,
                                   unsigned long long *__restrict__ evaluated) {
-  const int lo = 6;
+  const int lo = 6;  // NH = 11 only: the plain kernel's tiles of that window
   const int ix = nx - 2 * lo, iy = ny - 2 * lo, iz = nz - 2 * lo;
   const int nbx = (ix + kRows - 1) / kRows, segs = (iy + kRowOut - 1) / kRowOut;
   const int ntiles = ts.tiles_y * ts.tiles_x * ts.tiles_z;
@@ -1387,13 +1394,13 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 4)
     rescore_prior_kernel(const __grid_constant__ PriorList pl, const float *__restrict__ img,
                          const float *__restrict__ atl, const float *__restrict__ lab, int nx,
                          int ny, int nz, int apitch, float scale, float *__restrict__ pacc,
-                         float *__restrict__ wacc, unsigned long long *__restrict__ evaluated) {
-  rescore_prior_body(pl, img, atl, lab, nx, ny, nz, apitch, scale, pacc, wacc, evaluated);
+                         float *__restrict__ wacc, unsigned long long *__restrict__ evaluated,
+                         int hw) {
+  rescore_prior_body(pl, img, atl, lab, nx, ny, nz, apitch, scale, pacc, wacc, evaluated, hw);
 }
 
 __global__ void finalize_kernel(const float *__restrict__ pacc, const float *__restrict__ wacc,
-                                float *__restrict__ out, int nx, int ny, int nz) {
-  const int lo = 6;
+                                float *__restrict__ out, int nx, int ny, int nz, int lo) {
   const int ix = nx - 2 * lo, iy = ny - 2 * lo, iz = nz - 2 * lo;
   const long long total = (ix > 0 && iy > 0 && iz > 0) ? (long long)ix * iy * iz : 0;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
@@ -1563,9 +1570,9 @@ ConvPlan dense_plan(const Geometry &g, std::vector<int> &lists) {
 }
 
 // Anchor rows of blocks of `block` rows along an axis with `extent` interior rows from row 6.
-std::vector<int> anchors(int extent, int block) {
+std::vector<int> anchors(int extent, int block, int lo) {
   std::vector<int> a;
-  for (int b = 0; b * block < extent; ++b) a.push_back(6 + anchor_of_host(b, block, extent));
+  for (int b = 0; b * block < extent; ++b) a.push_back(lo + anchor_of_host(b, block, extent));
   return a;
 }
 
@@ -1586,9 +1593,9 @@ std::vector<int> rows_near(const std::vector<int> &anc, int radius, int n) {
 ConvPlan sparse_plan(const Geometry &g, int block, std::vector<int> &lists) {
   ConvPlan p{};
   lists.assign(4 * (size_t)g.nx, 0);
-  const int iz = g.nz - 12, ix = g.nx - 12, iy = g.ny - 12;
+  const int iz = g.iz, ix = g.ix, iy = g.iy;
   if (iz <= 0 || ix <= 0 || iy <= 0) return p;  // no interior: nothing to compute
-  const std::vector<int> az = anchors(iz, block), ax = anchors(ix, block);
+  const std::vector<int> az = anchors(iz, block, g.lo), ax = anchors(ix, block, g.lo);
   p.c1_z = az.front() - 3;
   p.c1_nz = az.back() + 4 - p.c1_z;
   p.c1_x = ax.front() - 3;
@@ -1603,8 +1610,8 @@ ConvPlan sparse_plan(const Geometry &g, int block, std::vector<int> &lists) {
       while (i < xs.size() && xs[i] < x0 + kCvTX) mask |= 1u << (xs[i++] - x0);
       lists[(size_t)l * g.nx + nt++] = x0 | (int)(mask << 16);
     }
-    p.y_lo[l] = 6 - radius;
-    p.y_hi[l] = g.ny - 6 + radius;
+    p.y_lo[l] = g.lo - radius;
+    p.y_hi[l] = g.ny - g.lo + radius;
     add_items(p, l, zs, nt, lists);
   }
   // conv1: the box 3 rows and planes around the anchors, y within 3 of the interior
@@ -1616,8 +1623,8 @@ ConvPlan sparse_plan(const Geometry &g, int block, std::vector<int> &lists) {
     }
     std::vector<int> zs(p.c1_nz);
     for (int i = 0; i < p.c1_nz; ++i) zs[i] = p.c1_z + i;
-    p.y_lo[3] = 3;
-    p.y_hi[3] = g.ny - 3;
+    p.y_lo[3] = g.lo - 3;
+    p.y_hi[3] = g.ny - g.lo + 3;
     add_items(p, 3, zs, nt, lists, kC1Y);
   }
   return p;
@@ -1706,11 +1713,12 @@ cudaError_t pack_all(const __nv_bfloat16 *wbf, uint32_t *frag, cudaStream_t s) {
 // An entry point of the rescoring module compiled for this x extent and atlas row pitch, or
 // nullptr: the environment variable PCT_RESCORE_JIT=0 keeps the library build, as does a
 // missing NVRTC.
-void *rescore_jit(const char *entry, int nx, int pitch) {
+void *rescore_jit(const char *entry, int nx, int pitch, int hw) {
   const char *env = getenv("PCT_RESCORE_JIT");
   if (env && env[0] == '0') return nullptr;
   const std::vector<std::string> opts = {"-DPCT_RS_JIT", "-DPCT_RS_NX=" + std::to_string(nx),
-                                         "-DPCT_RS_PITCH=" + std::to_string(pitch)};
+                                         "-DPCT_RS_PITCH=" + std::to_string(pitch),
+                                         "-DPCT_RS_HW=" + std::to_string(hw)};
   return jit::kernel(k_pct_rescore_source, "pct_rescore.cuh", opts, entry);
 }
 
@@ -1720,35 +1728,37 @@ cudaError_t launch_rescore4(int level, int blocks, const RowProp *props, const f
                             const float *atl, const float *lab, int nx, int ny, int nz,
                             int apitch, float scale, float conf_thr, float *pacc, float *wacc,
                             unsigned long long *fallbacks, unsigned long long *evaluated,
-                            const unsigned char *tile_flag, RescoreTiles ts, cudaStream_t s) {
+                            const unsigned char *tile_flag, RescoreTiles ts, int hw,
+                            cudaStream_t s) {
   void *fn = rescore_jit(level == 2 ? "pct_rescore4_l2" : level == 3 ? "pct_rescore4_l3"
                                                                       : "pct_rescore4_l4",
-                         nx, apitch);
+                         nx, apitch, hw);
   if (fn) {
-    void *args[] = {&props, &img,  &atl,  &lab,       &nx,        &ny,       &nz,       &apitch,
-                    &scale, &conf_thr, &pacc, &wacc, &fallbacks, &evaluated, &tile_flag, &ts};
+    void *args[] = {&props, &img,     &atl,  &lab,  &nx,        &ny,        &nz,        &apitch,
+                    &scale, &conf_thr, &pacc, &wacc, &fallbacks, &evaluated, &tile_flag, &ts,
+                    &hw};
     return jit::launch(fn, blocks, kRescoreWarps * 32, s, args);
   }
   auto k4 = level == 2 ? rescore4_kernel<2> : level == 3 ? rescore4_kernel<3> : rescore4_kernel<4>;
   k4<<<blocks, kRescoreWarps * 32, 0, s>>>(props, img, atl, lab, nx, ny, nz, apitch, scale,
                                             conf_thr, pacc, wacc, fallbacks, evaluated, tile_flag,
-                                            ts);
+                                            ts, hw);
   return cudaGetLastError();
 }
 
 cudaError_t launch_rescore_prior(int blocks, const PriorList &pl, const float *img,
                                  const float *atl, const float *lab, int nx, int ny, int nz,
                                  int apitch, float scale, float *pacc, float *wacc,
-                                 unsigned long long *evaluated, cudaStream_t s) {
-  void *fn = rescore_jit("pct_rescore_prior", nx, apitch);
+                                 unsigned long long *evaluated, int hw, cudaStream_t s) {
+  void *fn = rescore_jit("pct_rescore_prior", nx, apitch, hw);
   if (fn) {
     PriorList copy = pl;
     void *args[] = {&copy, &img, &atl, &lab, &nx, &ny, &nz, &apitch, &scale, &pacc, &wacc,
-                    &evaluated};
+                    &evaluated, &hw};
     return jit::launch(fn, blocks, kRescoreWarps * 32, s, args);
   }
   rescore_prior_kernel<<<blocks, kRescoreWarps * 32, 0, s>>>(pl, img, atl, lab, nx, ny, nz, apitch,
-                                                             scale, pacc, wacc, evaluated);
+                                                             scale, pacc, wacc, evaluated, hw);
   return cudaGetLastError();
 }
 
@@ -1803,14 +1813,14 @@ cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInp
   const float scale = (float)sqrt(1.4426950408889634 / div);
   const int nblk = sms() * 8;
   long long rows = 0;
-  if (g.nx > 12 && g.ny > 12 && g.nz > 12)
-    rows = (long long)(g.nz - 12) * (g.nx - 12) * ((g.ny - 12 + kRowOut - 1) / kRowOut);
+  if (g.ix > 0 && g.iy > 0 && g.iz > 0)
+    rows = (long long)g.iz * g.ix * ((g.iy + kRowOut - 1) / kRowOut);
   const long long rblk = (rows + kRescoreWarps - 1) / kRescoreWarps;
   const int rescore_blocks = (int)(rblk < 1 ? 1 : (rblk > 64LL * sms() ? 64LL * sms() : rblk));
   long long prows = 0;
-  if (g.nx > 12 && g.ny > 12 && g.nz > 12)
-    prows = (long long)((g.nz - 12 + block - 1) / block) * ((g.nx - 12 + block - 1) / block) *
-            ((g.ny - 12 + kRowOut - 1) / kRowOut);
+  if (g.ix > 0 && g.iy > 0 && g.iz > 0)
+    prows = (long long)((g.iz + block - 1) / block) * ((g.ix + block - 1) / block) *
+            ((g.iy + kRowOut - 1) / kRowOut);
   const long long pblk = (prows + kRescoreWarps - 1) / kRescoreWarps;
   const int propose_blocks = (int)(pblk < 1 ? 1 : (pblk > 64LL * sms() ? 64LL * sms() : pblk));
   // two streams: atlas a's convolutions and proposal (stream cs) run while atlas a - 1 is
@@ -1842,13 +1852,13 @@ cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInp
     if (two && a >= 2 && (e = cudaStreamWaitEvent(cs, streams->ev[3 + (a & 1)], 0)) != cudaSuccess)
       return join(e);
     propose_rows_kernel<<<propose_blocks, kRescoreWarps * 32, 0, cs>>>(f4, wbf, g.nx, g.ny, g.nz,
-                                                                       block, level, props);
+                                                                       block, level, props, g.hw);
     if ((e = cudaGetLastError()) != cudaSuccess) return join(e);
     if (two) {
       if ((e = cudaEventRecord(streams->ev[1 + (a & 1)], cs)) != cudaSuccess) return join(e);
       if ((e = cudaStreamWaitEvent(s, streams->ev[1 + (a & 1)], 0)) != cudaSuccess) return join(e);
     }
-    if (block == kRows && g.nx - 12 >= kRows &&
+    if (block == kRows && g.ix >= kRows &&
         (long long)g.nz * g.nx * in.pitch < (1LL << 31) - 1) {
       if (tile_fallback) {
         if ((e = cudaMemsetAsync(fb_count, 0, sizeof(int), s)) != cudaSuccess) return join(e);
@@ -1860,7 +1870,7 @@ cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInp
       if ((e = launch_rescore4(level, rescore_blocks, props, in.img, A, L, g.nx, g.ny, g.nz,
                                in.pitch, scale, tile_fallback ? 0.f : conf_thr, sc.pacc, sc.wacc,
                                sc.fallbacks, sc.evaluated, tile_fallback ? fb_flag : nullptr,
-                               RescoreTiles{ts.zt, ts.xc, ts.tiles_x, ts.tiles_y}, s)) !=
+                               RescoreTiles{ts.zt, ts.xc, ts.tiles_x, ts.tiles_y}, g.hw, s)) !=
           cudaSuccess)
         return join(e);
       if (tile_fallback) {
@@ -1871,22 +1881,22 @@ cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInp
     } else {
       rescore_kernel<<<rescore_blocks, kRescoreWarps * 32, 0, s>>>(
           props, block, level, in.img, A, L, g.nx, g.ny, g.nz, in.pitch, neg_k, conf_thr, sc.pacc,
-          sc.wacc, sc.fallbacks, sc.evaluated);
+          sc.wacc, sc.fallbacks, sc.evaluated, g.hw);
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return join(e);
     if (two && (e = cudaEventRecord(streams->ev[3 + (a & 1)], s)) != cudaSuccess) return join(e);
   }
-  finalize_kernel<<<nblk, 256, 0, s>>>(sc.pacc, sc.wacc, out, g.nx, g.ny, g.nz);
+  finalize_kernel<<<nblk, 256, 0, s>>>(sc.pacc, sc.wacc, out, g.nx, g.ny, g.nz, g.lo);
   return cudaGetLastError();
 }
 
-// The k offsets (dw, du, dv) of the 11^3 window nearest its centre, by squared distance, ties
-// in (dw, du, dv) order.
-std::vector<std::array<int, 3>> prior_offsets(int k) {
+// The k offsets (dw, du, dv) of the NH^3 window (half width hw) nearest its centre, by squared
+// distance, ties in (dw, du, dv) order.
+std::vector<std::array<int, 3>> prior_offsets(int k, int hw) {
   std::vector<std::array<int, 3>> all;
-  for (int dw = -5; dw <= 5; ++dw)
-    for (int du = -5; du <= 5; ++du)
-      for (int dv = -5; dv <= 5; ++dv) all.push_back({dw, du, dv});
+  for (int dw = -hw; dw <= hw; ++dw)
+    for (int du = -hw; du <= hw; ++du)
+      for (int dv = -hw; dv <= hw; ++dv) all.push_back({dw, du, dv});
   std::stable_sort(all.begin(), all.end(), [](const std::array<int, 3> &a, const std::array<int, 3> &b) {
     return a[0] * a[0] + a[1] * a[1] + a[2] * a[2] < b[0] * b[0] + b[1] * b[1] + b[2] * b[2];
   });
@@ -1896,8 +1906,9 @@ std::vector<std::array<int, 3>> prior_offsets(int k) {
 
 cudaError_t launch_prior(const Geometry &g, const SlabInputs &in, float *out, double div, int k,
                          void *scratch, cudaStream_t s) {
-  if (k < 1 || k > kMaxPrior) return cudaErrorInvalidValue;
-  if (g.nx - 12 < kRows || (long long)g.nz * g.nx * in.pitch >= (1LL << 31) - 1)
+  const long long window = (2LL * g.hw + 1) * (2 * g.hw + 1) * (2 * g.hw + 1);
+  if (k < 1 || k > kMaxPrior || k > window) return cudaErrorInvalidValue;
+  if (g.ix < kRows || (long long)g.nz * g.nx * in.pitch >= (1LL << 31) - 1)
     return cudaErrorInvalidValue;
   const long long nvox = g.nvox();
   InferScratch sc = carve(scratch, nvox);
@@ -1908,22 +1919,22 @@ cudaError_t launch_prior(const Geometry &g, const SlabInputs &in, float *out, do
   PriorList pl{};
   pl.n = k;
   const int axy = g.nx * in.pitch;
-  const auto offs = prior_offsets(k);
+  const auto offs = prior_offsets(k, g.hw);
   for (int c = 0; c < k; ++c) pl.off[c] = offs[c][0] * axy + offs[c][1] * in.pitch + offs[c][2];
   const float scale = (float)sqrt(1.4426950408889634 / div);
   long long rows = 0;
-  if (g.nx > 12 && g.ny > 12 && g.nz > 12)
-    rows = (long long)(g.nz - 12) * (g.nx - 12) * ((g.ny - 12 + kRowOut - 1) / kRowOut);
+  if (g.ix > 0 && g.iy > 0 && g.iz > 0)
+    rows = (long long)g.iz * g.ix * ((g.iy + kRowOut - 1) / kRowOut);
   const long long rblk = (rows + kRescoreWarps - 1) / kRescoreWarps;
   const int blocks = (int)(rblk < 1 ? 1 : (rblk > 64LL * sms() ? 64LL * sms() : rblk));
   const long long astride = (long long)g.nz * g.nx * in.pitch;
   for (int a = 0; a < g.num; ++a) {
     if ((e = launch_rescore_prior(blocks, pl, in.img, in.atlas + a * astride,
                                   in.label + a * astride, g.nx, g.ny, g.nz, in.pitch, scale,
-                                  sc.pacc, sc.wacc, sc.evaluated, s)) != cudaSuccess)
+                                  sc.pacc, sc.wacc, sc.evaluated, g.hw, s)) != cudaSuccess)
       return e;
   }
-  finalize_kernel<<<sms() * 8, 256, 0, s>>>(sc.pacc, sc.wacc, out, g.nx, g.ny, g.nz);
+  finalize_kernel<<<sms() * 8, 256, 0, s>>>(sc.pacc, sc.wacc, out, g.nx, g.ny, g.nz, g.lo);
   return cudaGetLastError();
 }
 
@@ -1956,7 +1967,8 @@ cudaError_t learned_probe(const Geometry &g, const void *weights, const float *i
   if ((e = cudaMemcpyAsync(d_vox, voxels, n * sizeof(int64_t), cudaMemcpyHostToDevice, s)) !=
       cudaSuccess)
     return e;
-  proposal_hook_kernel<<<(n + 127) / 128, 128, 0, s>>>(f4, wbf, d_vox, n, g.nvox(), d_top, d_conf);
+  proposal_hook_kernel<<<(n + 127) / 128, 128, 0, s>>>(f4, wbf, d_vox, n, g.nvox(), d_top, d_conf,
+                                                       g.hw);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (top && (e = cudaMemcpyAsync(top, d_top, 12 * (size_t)n, cudaMemcpyDeviceToHost, s)) !=
                  cudaSuccess)

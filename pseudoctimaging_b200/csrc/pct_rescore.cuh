@@ -4,8 +4,9 @@
 // This text is compiled twice:
 //  * by the library build, included inside its namespace: the volume's x extent and the atlas
 //    row pitch are kernel arguments;
-//  * at run time by NVRTC, once per (device, x extent, pitch), with PCT_RS_NX and PCT_RS_PITCH
-//    defined and PCT_RS_JIT selecting the extern "C" entry points at the end. Both strides are
+//  * at run time by NVRTC, once per (device, x extent, pitch, window), with PCT_RS_NX,
+//    PCT_RS_PITCH and PCT_RS_HW defined and PCT_RS_JIT selecting the extern "C" entry points at
+//    the end. Both strides are
 //    then constants, so each of an offset's 22 tap loads is one base address plus an immediate
 //    (the run-time strides cost about 45 % of the instructions in address arithmetic).
 // So it includes nothing, opens no namespace and uses CUDA built-ins only.
@@ -123,10 +124,10 @@ struct RsItem {
   unsigned owned, take;
 };
 
-// Item `it` of the interior grid: false when its z plane lies past the interior.
-__device__ __forceinline__ bool rs_place(long long it, int nx, int ny, int nz, int segs, int nbx,
-                                         int lane, RsItem &t) {
-  const int lo = 6;
+// Item `it` of the interior grid (first interior index lo): false when its z plane lies past
+// the interior.
+__device__ __forceinline__ bool rs_place(long long it, int nx, int ny, int nz, int lo, int segs,
+                                         int nbx, int lane, RsItem &t) {
   const long long r0 = it / kRows;
   t.seg = (int)(r0 % segs);
   const long long r1 = r0 / segs;
@@ -173,8 +174,8 @@ __device__ __forceinline__ void rs_store(const RsItem &t, int nx, int ny, const 
 }
 
 // Rescoring of the kept offsets of each row segment's block proposal (LEVEL 2, 3, 4: 10, 20 or
-// 32 rank triples). A voxel whose confidence is below conf_thr sends its item through all 11^3
-// offsets (rows keep what the proposal kept, or everything for the low-confidence voxels);
+// 32 rank triples) for the NH = 2 hw + 1 window (hw 3, 4 or 5; the interior starts at hw + 1).
+// A voxel whose confidence is below conf_thr sends its item through all NH^3 offsets (rows keep what the proposal kept, or everything for the low-confidence voxels);
 // items of tiles flagged in tile_flag were left to the plain kernel and are skipped.
 template <int LEVEL>
 __device__ __forceinline__ void rescore4_body(
@@ -182,7 +183,7 @@ __device__ __forceinline__ void rescore4_body(
     const float *__restrict__ lab, int nx, int ny, int nz, int apitch, float scale, float conf_thr,
     float *__restrict__ pacc, float *__restrict__ wacc, unsigned long long *__restrict__ fallbacks,
     unsigned long long *__restrict__ evaluated, const unsigned char *__restrict__ tile_flag,
-    const RescoreTiles ts) {
+    const RescoreTiles ts, int hw) {
   __shared__ int s_off[kRescoreWarps][kRsTopK];  // per warp: the item's kept offsets, 32-bit
 #ifdef PCT_RS_NX
   nx = PCT_RS_NX;
@@ -190,9 +191,12 @@ __device__ __forceinline__ void rescore4_body(
 #ifdef PCT_RS_PITCH
   apitch = PCT_RS_PITCH;
 #endif
+#ifdef PCT_RS_HW
+  hw = PCT_RS_HW;
+#endif
   const int lane = threadIdx.x & 31;
   int *w_off = s_off[threadIdx.x >> 5];
-  const int lo = 6;
+  const int lo = hw + 1;  // first interior index of the NH = 2 hw + 1 window
   const int ix = nx - 2 * lo, iz = nz - 2 * lo, iy = ny - 2 * lo;
   if (ix < kRows || iy <= 0 || iz <= 0) return;
   const int segs = (iy + kRowOut - 1) / kRowOut;
@@ -203,7 +207,7 @@ __device__ __forceinline__ void rescore4_body(
   for (long long it = (long long)blockIdx.x * kRescoreWarps + (threadIdx.x >> 5); it < items;
        it += (long long)gridDim.x * kRescoreWarps) {
     RsItem t;
-    if (!rs_place(it, nx, ny, nz, segs, nbx, lane, t)) continue;
+    if (!rs_place(it, nx, ny, nz, lo, segs, nbx, lane, t)) continue;
     // items of tiles that fell back to the plain kernel are left to it (warp-uniform)
     if (tile_flag &&
         tile_flag[((t.z - lo) / ts.zt * ts.tiles_x + (t.xb - lo) / ts.xc) * ts.tiles_y + t.seg])
@@ -254,18 +258,20 @@ __device__ __forceinline__ void rescore4_body(
           rank[a] |= (unsigned long long)r << (4 * top[a][r]);
         }
       }
-      for (int jw = 0; jw < kRsAxis; ++jw) {
+      // the NH^3 window: offset indices 5 - hw .. 5 + hw of each axis
+      for (int jw = 5 - hw; jw <= 5 + hw; ++jw) {
         const int rw = (int)((rank[0] >> (4 * jw)) & 0xF);
-        for (int ju = 0; ju < kRsAxis; ++ju) {
+        for (int ju = 5 - hw; ju <= 5 + hw; ++ju) {
           const int ru = rw + (int)((rank[1] >> (4 * ju)) & 0xF);
-          for (int jv = 0; jv < kRsAxis; ++jv) {
+          for (int jv = 5 - hw; jv <= 5 + hw; ++jv) {
             const bool mine = full || (ru + (int)((rank[2] >> (4 * jv)) & 0xF) <= LEVEL);
             const int off = (jw - 5) * axy + (ju - 5) * apitch + (jv - 5);
             eval_offset4<true>(ab + off, lb + off, in, axy, apitch, mine ? t.take : 0u, s2, P, W);
           }
         }
       }
-      my_evals += (unsigned long long)kRsAxis * kRsAxis * kRsAxis * __popc(t.owned);
+      const unsigned long long nw = 2 * hw + 1;
+      my_evals += nw * nw * nw * __popc(t.owned);
     }
     rs_store(t, nx, ny, P, W, pacc, wacc);
   }
@@ -278,15 +284,19 @@ __device__ __forceinline__ void rescore4_body(
 __device__ __forceinline__ void rescore_prior_body(
     const PriorList &pl, const float *__restrict__ img, const float *__restrict__ atl,
     const float *__restrict__ lab, int nx, int ny, int nz, int apitch, float scale,
-    float *__restrict__ pacc, float *__restrict__ wacc, unsigned long long *__restrict__ evaluated) {
+    float *__restrict__ pacc, float *__restrict__ wacc, unsigned long long *__restrict__ evaluated,
+    int hw) {
 #ifdef PCT_RS_NX
   nx = PCT_RS_NX;
 #endif
 #ifdef PCT_RS_PITCH
   apitch = PCT_RS_PITCH;
 #endif
+#ifdef PCT_RS_HW
+  hw = PCT_RS_HW;
+#endif
   const int lane = threadIdx.x & 31;
-  const int lo = 6;
+  const int lo = hw + 1;
   const int ix = nx - 2 * lo, iz = nz - 2 * lo, iy = ny - 2 * lo;
   if (ix < kRows || iy <= 0 || iz <= 0) return;
   const int segs = (iy + kRowOut - 1) / kRowOut;
@@ -297,7 +307,7 @@ __device__ __forceinline__ void rescore_prior_body(
   for (long long it = (long long)blockIdx.x * kRescoreWarps + (threadIdx.x >> 5); it < items;
        it += (long long)gridDim.x * kRescoreWarps) {
     RsItem t;
-    if (!rs_place(it, nx, ny, nz, segs, nbx, lane, t)) continue;
+    if (!rs_place(it, nx, ny, nz, lo, segs, nbx, lane, t)) continue;
     const int yc = min(t.y, ny - lo);
     float2 in[3][(kRows + 2) / 2];
     rs_inputs(img, nx, ny, t, yc, scale, in);
@@ -327,9 +337,9 @@ __device__ __forceinline__ void rescore_prior_body(
       int apitch, float scale, float conf_thr, float *__restrict__ pacc,                          \
       float *__restrict__ wacc, unsigned long long *__restrict__ fallbacks,                       \
       unsigned long long *__restrict__ evaluated, const unsigned char *__restrict__ tile_flag,    \
-      const RescoreTiles ts) {                                                                    \
+      const RescoreTiles ts, int hw) {                                                            \
     rescore4_body<LEVEL>(props, img, atl, lab, nx, ny, nz, apitch, scale, conf_thr, pacc, wacc,   \
-                         fallbacks, evaluated, tile_flag, ts);                                    \
+                         fallbacks, evaluated, tile_flag, ts, hw);                                \
   }
 PCT_RS_ENTRY(pct_rescore4_l2, 2)
 PCT_RS_ENTRY(pct_rescore4_l3, 3)
@@ -340,7 +350,7 @@ extern "C" __global__ void __launch_bounds__(kRescoreWarps * 32, PCT_RS_MIN_CTAS
     pct_rescore_prior(const __grid_constant__ PriorList pl, const float *__restrict__ img,
                       const float *__restrict__ atl, const float *__restrict__ lab, int nx, int ny,
                       int nz, int apitch, float scale, float *__restrict__ pacc,
-                      float *__restrict__ wacc, unsigned long long *__restrict__ evaluated) {
-  rescore_prior_body(pl, img, atl, lab, nx, ny, nz, apitch, scale, pacc, wacc, evaluated);
+                      float *__restrict__ wacc, unsigned long long *__restrict__ evaluated, int hw) {
+  rescore_prior_body(pl, img, atl, lab, nx, ny, nz, apitch, scale, pacc, wacc, evaluated, hw);
 }
 #endif

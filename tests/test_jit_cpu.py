@@ -47,12 +47,12 @@ def test_embedded_source_is_the_header():
     assert inc[start:end] == text
 
 
-@pytest.mark.parametrize("nx,pitch", [(222, 222), (222, 224), (64, 64), (17, 20)])
-def test_rescore_module_compiles_for_sm100a(nx, pitch):
+@pytest.mark.parametrize("nx,pitch,hw", [(222, 222, 5), (222, 224, 5), (64, 64, 4), (17, 20, 3)])
+def test_rescore_module_compiles_for_sm100a(nx, pitch, hw):
     lib = _nvrtc()
     src = (CSRC / "pct_rescore.cuh").read_bytes()
     opts = [b"-DPCT_RS_JIT", b"-DPCT_RS_NX=%d" % nx, b"-DPCT_RS_PITCH=%d" % pitch,
-            b"--gpu-architecture=sm_100a", b"-std=c++17"]
+            b"-DPCT_RS_HW=%d" % hw, b"--gpu-architecture=sm_100a", b"-std=c++17"]
     rc, log, cubin = _compile(lib, src, opts)
     assert rc == 0, log
     assert cubin > 0

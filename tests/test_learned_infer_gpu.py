@@ -53,8 +53,9 @@ def prior_proposal(scales=(0.7, 0.5, 0.3), k=32):
     return np.array(top), conf
 
 
-def fuse_offsets_f64(img, atlas, label, offsets, div):
-    """Float64 fusion over a fixed offset list at every interior voxel; (out, prod, sumw)."""
+def fuse_offsets_f64(img, atlas, label, offsets, div, LO=LO):
+    """Float64 fusion over a fixed offset list at every interior voxel (interior from LO);
+    (out, prod, sumw)."""
     nz, nx, ny = img.shape
     I = img.astype(np.float64)
     shape = (nz - 2 * LO, nx - 2 * LO, ny - 2 * LO)
@@ -84,12 +85,12 @@ def fuse_offsets_f64(img, atlas, label, offsets, div):
     return out, prod, sumw
 
 
-def rows_of(nx, ny, nz):
-    return (nz - 2 * LO) * (nx - 2 * LO) * -(-(ny - 2 * LO) // 30)
+def rows_of(nx, ny, nz, lo=LO):
+    return (nz - 2 * lo) * (nx - 2 * lo) * -(-(ny - 2 * lo) // 30)
 
 
-def interior(nx, ny, nz):
-    return (nz - 2 * LO) * (nx - 2 * LO) * (ny - 2 * LO)
+def interior(nx, ny, nz, lo=LO):
+    return (nz - 2 * lo) * (nx - 2 * lo) * (ny - 2 * lo)
 
 
 def test_attach_rules():
@@ -103,8 +104,8 @@ def test_attach_rules():
                 h.attach_model(m, -0.5)
             assert e.value.status == -1
             h.attach_model(m, 0.0)
-            with pytest.raises(pct.PctError) as e:
-                h.synthesize(img, atl, lab, 9, DIV, pct.EXEC_LEARNED)
+            with pytest.raises(pct.PctError) as e:  # NH 7, 9 and 11 only
+                h.synthesize(img, atl, lab, 5, DIV, pct.EXEC_LEARNED)
             assert e.value.status == -4
             out = h.synthesize(img, atl, lab, NH, DIV, pct.EXEC_LEARNED)
             assert np.all(out[:LO] == 0) and np.all(out[:, :, -LO:] == 0)
@@ -388,8 +389,9 @@ def test_trained_network_gain():
     assert res["trained"]["offsets_per_row"] == 32.0
 
 
-@pytest.mark.parametrize("mode", ["network", "network_conf", "prior"])
-def test_runtime_compiled_rescoring_matches_library_build(mode, monkeypatch):
+@pytest.mark.parametrize("mode,nh", [("network", 11), ("network_conf", 11), ("prior", 11),
+                                     ("network_conf", 9), ("prior", 7)])
+def test_runtime_compiled_rescoring_matches_library_build(mode, nh, monkeypatch):
     """The rescoring runs from a module compiled at run time for the volume's x extent and row
     pitch; PCT_RESCORE_JIT=0 keeps the library's own build of the same code. Both give the same
     output bit for bit (odd sizes; with a confidence threshold the atlas rows are repacked to a
@@ -404,7 +406,92 @@ def test_runtime_compiled_rescoring_matches_library_build(mode, monkeypatch):
                 h.set_learned_prior(32)
             else:
                 h.attach_model(m, 0.02 if mode == "network_conf" else 0.0)
-            outs.append((h.synthesize(img, atl, lab, NH, DIV, pct.EXEC_LEARNED), h.learned_stats()))
+            outs.append((h.synthesize(img, atl, lab, nh, DIV, pct.EXEC_LEARNED), h.learned_stats()))
     (a, sa), (b, sb) = outs
     assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
     assert sa == sb
+
+
+
+def window_proposal(nh, k, scales=(0.7, 0.5, 0.3)):
+    """The prior network's proposal for an NH window: per axis the softmax of its biases over the
+    window's offsets, the 4 most probable (ties: lower offset first), the kept rank triples and
+    their probability mass, in float64."""
+    hw = (nh - 1) // 2
+    top, probs = [], []
+    for c in scales:
+        d = np.arange(-hw, hw + 1)
+        logits = -c * d.astype(np.float64) ** 2
+        p = np.exp(logits - logits.max())
+        p /= p.sum()
+        order = sorted(range(len(d)), key=lambda j: (-p[j], j))[:4]
+        top.append([int(d[j]) for j in order])
+        probs.append([p[j] for j in order])
+    level = learned.KEPT_LEVEL[k]
+    conf = sum(probs[0][i] * probs[1][j] * probs[2][l] for i in range(4) for j in range(4)
+               for l in range(4) if i + j + l <= level)
+    return np.array(top), conf
+
+
+@pytest.mark.parametrize("nh,k,block", [(7, 32, 4), (9, 32, 4), (9, 20, 1), (7, 10, 4)])
+def test_prior_proposal_exact_small_windows(nh, k, block):
+    """NH 7 and 9: the network's softmaxes run over the window's offsets only; with the prior
+    network every row keeps the same k offsets, exactly the float64 fusion over them, on the
+    larger interior of the smaller window."""
+    lo = (nh - 1) // 2 + 1
+    nx, ny, nz, num = 38, 45, 30, 2
+    img, atl, lab = subject(nx, ny, nz, num, 23)
+    top, _ = window_proposal(nh, k)
+    offsets = learned.rank_sum_set(top, k)
+    assert len({tuple(o) for o in offsets}) == k
+    ref, prod, sumw = fuse_offsets_f64(img, atl, lab, offsets, DIV, LO=lo)
+    with pct.Handle(0) as h, learned.LearnedModel(0, params=prior_params()) as m:
+        h.attach_model(m, 0.0)
+        h.set_learned_k(k)
+        h.set_learned_block(block)
+        got = h.synthesize(img, atl, lab, nh, DIV, pct.EXEC_LEARNED)
+        st = h.learned_stats()
+    compare_fused(got, ref, nh, 1e-4, prod, sumw)
+    assert np.all(got[:lo] == 0) and np.all(got[:, :, -lo:] == 0)
+    assert st["fallback_pairs"] == 0
+    assert st["row_offsets"] == rows_of(nx, ny, nz, lo) * k * num
+
+
+@pytest.mark.parametrize("nh", [7, 9])
+def test_confidence_and_full_fallback_small_windows(nh):
+    """Below the prior's own confidence nothing falls back; above 1 every pair takes the full
+    NH^3 window, which is the plain method."""
+    lo = (nh - 1) // 2 + 1
+    nx, ny, nz, num = 34, 37, 29, 2
+    img, atl, lab = subject(nx, ny, nz, num, 33)
+    _, conf = window_proposal(nh, 32)
+    ref, prod, sumw = oracle.fuse_port(img, atl, lab, nh, DIV, with_sums=True)
+    with pct.Handle(0) as h, learned.LearnedModel(0, params=prior_params()) as m:
+        h.attach_model(m, conf * (1 - 1e-3))
+        h.synthesize(img, atl, lab, nh, DIV, pct.EXEC_LEARNED)
+        assert h.learned_stats()["fallback_pairs"] == 0
+        h.attach_model(m, 2.0)
+        got = h.synthesize(img, atl, lab, nh, DIV, pct.EXEC_LEARNED)
+        st = h.learned_stats()
+    compare_fused(got, ref, nh, 1e-4, prod, sumw)
+    assert st["fallback_pairs"] == interior(nx, ny, nz, lo) * num
+    assert st["row_offsets"] == rows_of(nx, ny, nz, lo) * nh ** 3 * num
+
+
+@pytest.mark.parametrize("nh", [7, 9])
+def test_centre_prior_small_windows(nh):
+    """The no-network centre prior at NH 7 and 9: the 32 and 57 offsets nearest the centre of the
+    window, exactly the float64 fusion over them."""
+    import itertools
+    lo, hw = (nh - 1) // 2 + 1, (nh - 1) // 2
+    nx, ny, nz, num = 36, 41, 30, 2
+    img, atl, lab = subject(nx, ny, nz, num, 21)
+    with pct.Handle(0) as h:
+        for k in (32, 57):
+            offs = sorted(itertools.product(range(-hw, hw + 1), repeat=3),
+                          key=lambda o: o[0] ** 2 + o[1] ** 2 + o[2] ** 2)[:k]
+            ref, prod, sumw = fuse_offsets_f64(img, atl, lab, offs, DIV, LO=lo)
+            h.set_learned_prior(k)
+            got = h.synthesize(img, atl, lab, nh, DIV, pct.EXEC_LEARNED)
+            compare_fused(got, ref, nh, 1e-4, prod, sumw)
+            assert h.learned_stats()["row_offsets"] == rows_of(nx, ny, nz, lo) * k * num
