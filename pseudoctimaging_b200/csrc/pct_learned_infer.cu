@@ -1123,10 +1123,14 @@ __device__ __forceinline__ int anchor_of(int b, int block, int extent) {
   return a < extent ? a : extent - 1;
 }
 
+// HALF: the window's half width (5, 4, 3), a template so that NH = 11 compiles without the
+// window tests.
+template <int HALF>
 __global__ void __launch_bounds__(kRescoreWarps * 32)
     propose_rows_kernel(const __nv_bfloat16 *__restrict__ f4, const __nv_bfloat16 *__restrict__ wbf,
                         int nx, int ny, int nz, int block, int level,
-                        RowProp *__restrict__ props, int half) {
+                        RowProp *__restrict__ props) {
+  constexpr int half = HALF;
   __shared__ __align__(16) float hw[kHeadFloats];
   __shared__ float s_prob[kRescoreWarps * 32 * kProbStride];
   __shared__ float s_sum[kRescoreWarps * 36];
@@ -1851,8 +1855,10 @@ cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInp
     // the table is free once the rescoring of atlas a - 2 has read it
     if (two && a >= 2 && (e = cudaStreamWaitEvent(cs, streams->ev[3 + (a & 1)], 0)) != cudaSuccess)
       return join(e);
-    propose_rows_kernel<<<propose_blocks, kRescoreWarps * 32, 0, cs>>>(f4, wbf, g.nx, g.ny, g.nz,
-                                                                       block, level, props, g.hw);
+    auto kp = g.hw == 5 ? propose_rows_kernel<5> : g.hw == 4 ? propose_rows_kernel<4>
+                                                              : propose_rows_kernel<3>;
+    kp<<<propose_blocks, kRescoreWarps * 32, 0, cs>>>(f4, wbf, g.nx, g.ny, g.nz, block, level,
+                                                      props);
     if ((e = cudaGetLastError()) != cudaSuccess) return join(e);
     if (two) {
       if ((e = cudaEventRecord(streams->ev[1 + (a & 1)], cs)) != cudaSuccess) return join(e);
