@@ -106,10 +106,11 @@ inline int slab_pitch(int ny) { return (ny + 3) / 4 * 4; }
 // Run-time compiled kernels (NVRTC; pct_jit.cpp): the entry point `entry_name` of `source`
 // built for the current device with `options` (typically -D constants), cached per (context,
 // source name, options, entry point). nullptr when NVRTC or the driver's module calls are
-// unavailable or the build failed; callers then launch their ahead-of-time build.
+// unavailable, the build failed, or it is not built yet and `build` is false (a lookup only);
+// callers then launch their ahead-of-time build.
 namespace jit {
 void *kernel(const char *source, const char *file_name, const std::vector<std::string> &options,
-             const char *entry_name);
+             const char *entry_name, bool build = true);
 // 1-D launch of a kernel returned by kernel() (no dynamic shared memory).
 cudaError_t launch(void *fn, unsigned grid, unsigned block, cudaStream_t stream, void **args);
 }  // namespace jit

@@ -12,8 +12,8 @@
 //
 // The cache key holds the context's unique id (cuCtxGetId), so a cudaDeviceReset, which
 // destroys the modules with the context, leads to a fresh compile rather than a stale handle.
-// Loading a module is not a stream operation; the first call for a geometry belongs outside a
-// stream capture (later calls only launch).
+// Loading a module is not a stream operation: callers pass build = false while their stream is
+// being captured, and the ahead-of-time kernel runs until a call outside capture has built it.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
@@ -144,7 +144,7 @@ CUfunction build(const char *source, const char *file_name, const std::vector<st
 }  // namespace
 
 void *kernel(const char *source, const char *file_name, const std::vector<std::string> &options,
-             const char *entry_name) {
+             const char *entry_name, bool build_allowed) {
   if (!nvrtc().ok || !driver().ok) return nullptr;
   CUcontext ctx = nullptr;  // the runtime's context, current once the caller has used the device
   unsigned long long ctx_id = 0;
@@ -155,7 +155,7 @@ void *kernel(const char *source, const char *file_name, const std::vector<std::s
   std::lock_guard<std::mutex> lock(g_mu);
   auto it = g_cache.find(key);
   if (it != g_cache.end()) return it->second;
-  if (g_modules >= kMaxModules) return nullptr;
+  if (!build_allowed || g_modules >= kMaxModules) return nullptr;
   CUfunction fn = build(source, file_name, options, entry_name);
   g_cache[key] = fn;
   if (fn) ++g_modules;

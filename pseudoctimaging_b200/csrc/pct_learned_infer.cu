@@ -1717,13 +1717,17 @@ cudaError_t pack_all(const __nv_bfloat16 *wbf, uint32_t *frag, cudaStream_t s) {
 // An entry point of the rescoring module compiled for this x extent and atlas row pitch, or
 // nullptr: the environment variable PCT_RESCORE_JIT=0 keeps the library build, as does a
 // missing NVRTC.
-void *rescore_jit(const char *entry, int nx, int pitch, int hw) {
+void *rescore_jit(const char *entry, int nx, int pitch, int hw, cudaStream_t s) {
   const char *env = getenv("PCT_RESCORE_JIT");
   if (env && env[0] == '0') return nullptr;
   const std::vector<std::string> opts = {"-DPCT_RS_JIT", "-DPCT_RS_NX=" + std::to_string(nx),
                                          "-DPCT_RS_PITCH=" + std::to_string(pitch),
                                          "-DPCT_RS_HW=" + std::to_string(hw)};
-  return jit::kernel(k_pct_rescore_source, "pct_rescore.cuh", opts, entry);
+  // while `s` is being captured a module is only looked up, never built (loading one is not a
+  // stream operation)
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  const bool build = cudaStreamIsCapturing(s, &cap) == cudaSuccess && cap == cudaStreamCaptureStatusNone;
+  return jit::kernel(k_pct_rescore_source, "pct_rescore.cuh", opts, entry, build);
 }
 
 // One atlas's proposal rescoring: the geometry's compiled module where there is one, else the
@@ -1736,7 +1740,7 @@ cudaError_t launch_rescore4(int level, int blocks, const RowProp *props, const f
                             cudaStream_t s) {
   void *fn = rescore_jit(level == 2 ? "pct_rescore4_l2" : level == 3 ? "pct_rescore4_l3"
                                                                       : "pct_rescore4_l4",
-                         nx, apitch, hw);
+                         nx, apitch, hw, s);
   if (fn) {
     void *args[] = {&props, &img,     &atl,  &lab,  &nx,        &ny,        &nz,        &apitch,
                     &scale, &conf_thr, &pacc, &wacc, &fallbacks, &evaluated, &tile_flag, &ts,
@@ -1754,7 +1758,7 @@ cudaError_t launch_rescore_prior(int blocks, const PriorList &pl, const float *i
                                  const float *atl, const float *lab, int nx, int ny, int nz,
                                  int apitch, float scale, float *pacc, float *wacc,
                                  unsigned long long *evaluated, int hw, cudaStream_t s) {
-  void *fn = rescore_jit("pct_rescore_prior", nx, apitch, hw);
+  void *fn = rescore_jit("pct_rescore_prior", nx, apitch, hw, s);
   if (fn) {
     PriorList copy = pl;
     void *args[] = {&copy, &img, &atl, &lab, &nx, &ny, &nz, &apitch, &scale, &pacc, &wacc,
