@@ -22,11 +22,14 @@ def device_run(h, img, atl, lab, nh, div):
     return out.cpu().numpy()
 
 
-@pytest.mark.parametrize("shape,nh", [((64, 70, 48, 6), 11), ((90, 61, 40, 4), 7)])
-def test_pipelined_host_path_equals_device_path(shape, nh):
+@pytest.mark.parametrize("shape,nh,min_groups", [((64, 70, 48, 6), 11, 2), ((90, 61, 40, 4), 7, 2),
+                                                ((40, 45, 30, 10), 11, 3)])
+def test_pipelined_host_path_equals_device_path(shape, nh, min_groups):
+    """With three or more groups the second group runs in a launch of its own as soon as it has
+    landed, the rest in a third."""
     nx, ny, nz, num = shape
     plan = pct.query_plan(nx, ny, nz, num, nh)
-    assert plan["groups"] >= 2, plan  # the shape must take the pipelined path
+    assert plan["groups"] >= min_groups, plan  # the shape must take the pipelined path
     s = pct.synth_subject(nx, ny, nz, num, n_blobs=10, seed=nh)
     lab = pct.normalize_labels(s.atlas_ct)
     div = pct.div_from(2.5, 1.0)
