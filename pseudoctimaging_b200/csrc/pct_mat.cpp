@@ -174,6 +174,10 @@ bool parse_file(const std::vector<unsigned char> &file, std::vector<Array> *vars
     *why = "not a little-endian level-5 MAT-file";
     return false;
   }
+  if (file[125] != 0x01 || file[124] != 0x00) {  // 0x0200: a version 7.3 (HDF5) file
+    *why = "not a level-5 MAT-file (version 7.3 files are HDF5; save with -v7 or -v6)";
+    return false;
+  }
   size_t pos = 128;
   while (pos + 8 <= file.size()) {
     Element e;

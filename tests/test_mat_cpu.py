@@ -69,6 +69,11 @@ def test_rejects_malformed(tmp_path, compress):
     trunc.write_bytes(path.read_bytes()[:300])
     with pytest.raises(pct.PctError):
         pct.read_mat(trunc)
+    v73 = bytearray(path.read_bytes())  # a version 7.3 header (HDF5 files) is refused
+    v73[124:126] = b"\x00\x02"
+    (tmp_path / "v73.mat").write_bytes(bytes(v73))
+    with pytest.raises(pct.PctError):
+        pct.read_mat(tmp_path / "v73.mat")
     with pytest.raises(pct.PctError):
         pct.read_mat(tmp_path / "missing.mat")
 
