@@ -307,27 +307,30 @@ def test_host_device_and_pipeline_paths_agree():
     np.testing.assert_array_equal(np.nan_to_num(host), np.nan_to_num(dev))
 
 
-@pytest.mark.parametrize("block,shape", [(4, (47, 53, 35)), (3, (41, 70, 30)), (1, (33, 42, 29)),
-                                         (5, (26, 40, 22))])
-def test_restricted_convs_match_every_voxel(block, shape):
+@pytest.mark.parametrize("block,shape,nh", [(4, (47, 53, 35), 11), (3, (41, 70, 30), 11),
+                                            (1, (33, 42, 29), 11), (5, (26, 40, 22), 11),
+                                            (4, (39, 44, 27), 7), (1, (30, 37, 25), 9)])
+def test_restricted_convs_match_every_voxel(block, shape, nh):
     """The convolutions compute only what the anchor rows need (conv4 on the anchor rows, each
     earlier layer one row, plane and y further out); every needed value must be the one the
-    whole-volume convolutions give, so the results are bit-identical."""
+    whole-volume convolutions give, so the results are bit-identical (also with the interior of
+    the smaller windows, which starts 4 and 5 voxels from the faces)."""
     nx, ny, nz = shape
+    lo = (nh - 1) // 2 + 1
     img, atl, lab = subject(nx, ny, nz, 2, 60 + block)
     with pct.Handle(0) as h, learned.LearnedModel.load(learned.CHECKPOINT) as m:
         h.attach_model(m, 0.2)
         h.set_learned_block(block)
-        sparse = h.synthesize(img, atl, lab, NH, DIV, pct.EXEC_LEARNED)
+        sparse = h.synthesize(img, atl, lab, nh, DIV, pct.EXEC_LEARNED)
         st_sparse = h.learned_stats()
         h.set_learned_convs(True)
-        full = h.synthesize(img, atl, lab, NH, DIV, pct.EXEC_LEARNED)
+        full = h.synthesize(img, atl, lab, nh, DIV, pct.EXEC_LEARNED)
         st_full = h.learned_stats()
         h.set_learned_convs(False)
     np.testing.assert_array_equal(np.isnan(sparse), np.isnan(full))
     np.testing.assert_array_equal(np.nan_to_num(sparse), np.nan_to_num(full))
     assert st_sparse == st_full
-    assert np.isfinite(sparse[LO:-LO, LO:-LO, LO:-LO]).mean() > 0.5
+    assert np.isfinite(sparse[lo:-lo, lo:-lo, lo:-lo]).mean() > 0.5
 
 
 def test_checkpoint_round_trip(tmp_path):

@@ -88,3 +88,12 @@ def test_write_result_round_trip(tmp_path):
     got = m["Subject_08_result"]
     assert got.dtype == np.float32 and got.shape == (7, 6, 5)  # [nx ny nz]
     assert np.array_equal(row_based(got), vol, equal_nan=True)
+
+
+def test_write_rejects_bad_arguments(tmp_path):
+    vol = np.zeros((2, 3, 4), np.float32)
+    for name in ("", "x" * 64):
+        with pytest.raises(pct.PctError):
+            pct.write_mat(tmp_path / "a.mat", name, vol)
+    with pytest.raises(pct.PctError):  # unwritable path
+        pct.write_mat(tmp_path / "missing_dir" / "a.mat", "v", vol)
