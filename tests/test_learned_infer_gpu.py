@@ -498,3 +498,53 @@ def test_centre_prior_small_windows(nh):
             got = h.synthesize(img, atl, lab, nh, DIV, pct.EXEC_LEARNED)
             compare_fused(got, ref, nh, 1e-4, prod, sumw)
             assert h.learned_stats()["row_offsets"] == rows_of(nx, ny, nz, lo) * k * num
+
+
+def sampled_fusion_f64(img, atlas, label, offsets, div, vox):
+    """Float64 fusion over a fixed offset list at the flat voxels `vox` only; (out, prod, sumw)."""
+    nz, nx, ny = img.shape
+    z, r = np.divmod(vox, nx * ny)
+    x, y = np.divmod(r, ny)
+    taps = [(dz, dx, dy) for dz in (-1, 0, 1) for dx in (-1, 0, 1) for dy in (-1, 0, 1)]
+    I = np.stack([img[z + dz, x + dx, y + dy] for dz, dx, dy in taps]).astype(np.float64)
+    P = np.zeros(len(vox))
+    W = np.zeros(len(vox))
+    for a in range(atlas.shape[0]):
+        A, L = atlas[a], label[a]
+        for dw, du, dv in offsets:
+            Ab = np.stack([A[z + dw + dz, x + du + dx, y + dv + dy] for dz, dx, dy in taps])
+            ssd = ((I - Ab.astype(np.float64)) ** 2).sum(axis=0)
+            w = np.exp(-ssd / div)
+            P += w * L[z + dw, x + du, y + dv]
+            W += w
+    ok = (np.abs(P) > DBL_EPS) & (np.abs(W) > DBL_EPS)
+    return np.where(ok, P / np.where(ok, W, 1.0), np.nan), P, W
+
+
+@pytest.mark.parametrize("k", [32, 10])
+def test_full_size_prior_network_sampled_voxels(k):
+    """The learned form at the full config-1 geometry (222x222x112, 10 atlases, the run-time
+    compiled rescoring for nx = 222 and pitch 222) with the prior network: every row keeps the
+    same k offsets, so 1,500 sampled interior voxels must equal the float64 fusion over them."""
+    s = pct.synth_subject(222, 222, 112, 10, n_blobs=60, seed=1)
+    lab = pct.normalize_labels(s.atlas_ct)
+    top, _ = prior_proposal(k=k)
+    offsets = learned.rank_sum_set(top, k)
+    with pct.Handle(0) as h, learned.LearnedModel(0, params=prior_params()) as m:
+        h.attach_model(m, 0.0)
+        h.set_learned_k(k)
+        got = h.synthesize(s.img, s.atlas_mri, lab, NH, DIV, pct.EXEC_LEARNED)
+    nz, nx, ny = s.img.shape
+    rng = np.random.default_rng(k)
+    vox = (rng.integers(LO, nz - LO, 1500) * nx * ny + rng.integers(LO, nx - LO, 1500) * ny
+           + rng.integers(LO, ny - LO, 1500))
+    ref, P, W = sampled_fusion_f64(s.img, s.atlas_mri, lab, offsets, DIV, vox)
+    g = got.reshape(-1)[vox]
+    gn, rn = np.isnan(g), np.isnan(ref)
+    mism = gn != rn
+    if mism.any():  # only where a float64 sum sits at the DBL_EPSILON threshold
+        near = (np.abs(np.abs(P[mism]) / DBL_EPS - 1) < 1e-3) | (np.abs(np.abs(W[mism]) / DBL_EPS - 1) < 1e-3)
+        assert near.all()
+    both = ~gn & ~rn
+    rel = np.abs(g[both].astype(np.float64) - ref[both]) / np.maximum(np.abs(ref[both]), 1e-30)
+    assert rel.max() <= 1e-4, rel.max()
