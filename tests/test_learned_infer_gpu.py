@@ -548,3 +548,26 @@ def test_full_size_prior_network_sampled_voxels(k):
     both = ~gn & ~rn
     rel = np.abs(g[both].astype(np.float64) - ref[both]) / np.maximum(np.abs(ref[both]), 1e-30)
     assert rel.max() <= 1e-4, rel.max()
+
+
+def test_full_size_centre_prior_sampled_voxels():
+    """The no-network centre prior at the full config-1 geometry (k = 57): 1,500 sampled interior
+    voxels against the float64 fusion over the 57 offsets nearest the window's centre."""
+    s = pct.synth_subject(222, 222, 112, 10, n_blobs=60, seed=1)
+    lab = pct.normalize_labels(s.atlas_ct)
+    with pct.Handle(0) as h:
+        h.set_learned_prior(57)
+        got = h.synthesize(s.img, s.atlas_mri, lab, NH, DIV, pct.EXEC_LEARNED)
+    nz, nx, ny = s.img.shape
+    rng = np.random.default_rng(57)
+    vox = (rng.integers(LO, nz - LO, 1500) * nx * ny + rng.integers(LO, nx - LO, 1500) * ny
+           + rng.integers(LO, ny - LO, 1500))
+    ref, P, W = sampled_fusion_f64(s.img, s.atlas_mri, lab, centre_offsets(57), DIV, vox)
+    g = got.reshape(-1)[vox]
+    both = ~np.isnan(g) & ~np.isnan(ref)
+    mism = np.isnan(g) != np.isnan(ref)
+    if mism.any():
+        near = (np.abs(np.abs(P[mism]) / DBL_EPS - 1) < 1e-3) | (np.abs(np.abs(W[mism]) / DBL_EPS - 1) < 1e-3)
+        assert near.all()
+    rel = np.abs(g[both].astype(np.float64) - ref[both]) / np.maximum(np.abs(ref[both]), 1e-30)
+    assert rel.max() <= 1e-4, rel.max()
