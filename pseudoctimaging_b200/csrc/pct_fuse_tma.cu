@@ -608,11 +608,25 @@ struct BatchParams {
 template <int SET>
 __global__ void __launch_bounds__(kThreads, TileOf<SET, 5>::MB) fuse_batch_kernel(const BatchParams bp) {
   extern __shared__ unsigned char smem_raw[];
+  // The current subject's view, copied into shared memory when the subject changes: the tile
+  // code then reads its fields from there as it needs them instead of keeping the values it
+  // loaded from global memory in registers (the single-subject kernel reads them from its
+  // parameters).
+  __shared__ __align__(16) SubjectView s_sv;
+  static_assert(sizeof(SubjectView) % 4 == 0 && sizeof(SubjectView) <= 4 * kThreads, "copy");
   Pipe pp = pipe_init(smem_raw);
-  int s = 0;
+  int s = 0, cur = -1;
   for (int item = blockIdx.x; item < bp.total_items; item += gridDim.x) {
     while (s + 1 < bp.nsub && bp.subjects[s + 1].item_begin <= item) ++s;
-    const SubjectView &sv = bp.subjects[s];
+    if (s != cur) {  // uniform over the CTA
+      __syncthreads();  // every thread is done with the previous subject's view
+      if (threadIdx.x < sizeof(SubjectView) / 4)
+        reinterpret_cast<int *>(&s_sv)[threadIdx.x] =
+            reinterpret_cast<const int *>(bp.subjects + s)[threadIdx.x];
+      __syncthreads();
+      cur = s;
+    }
+    const SubjectView &sv = s_sv;
     const int local = item - sv.item_begin;
     bool ok = true;
     switch (sv.hw) {
