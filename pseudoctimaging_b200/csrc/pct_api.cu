@@ -46,8 +46,9 @@ struct pct_handle {
   long long learned_nvox = 0;           // volume size of the last learned run (0: none yet)
   pct::learned::LearnedStreams learned_streams{};  // convolutions beside the rescoring
   cudaEvent_t learned_done = nullptr;   // recorded after the last learned run's kernels
-  cudaStream_t copy_stream = nullptr;   // uploads of the pipelined host path
-  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};  // start, first group staged, rest staged
+  cudaStream_t copy_stream = nullptr;     // uploads of the pipelined host path
+  cudaStream_t compute_stream = nullptr;  // its second compute stream
+  std::vector<cudaEvent_t> pipe_ev;       // its fork, one per uploaded part, two joins
   std::string last_error;
 };
 
@@ -299,34 +300,44 @@ int stage_pitched_h2d(pct_handle *h, DevBuf &buf, const float *src, const pct::G
   return PCT_OK;
 }
 
-// Uploads atlases [a0, a1) of a host stack into the pitched device stack `buf`; `stage` (the
-// same [num][nz][nx][ny] shape as the host stack) holds the contiguous copy before the repack
-// when the pitch differs from ny.
+// Uploads planes [z0, z1) of atlases [a0, a1) of a host stack into the pitched device stack
+// `buf`; `stage` (the same [num][nz][nx][ny] shape as the host stack) holds the contiguous copy
+// before the repack when the pitch differs from ny. Whole atlases are one run of rows, a plane
+// range one run per atlas.
 int stage_pitched_slice(pct_handle *h, DevBuf &buf, float *stage_base, const float *src,
-                        const pct::Geometry &g, int a0, int a1, bool normalize, cudaStream_t s) {
+                        const pct::Geometry &g, int a0, int a1, int z0, int z1, bool normalize,
+                        cudaStream_t s) {
   const int pitch = pct::slab_pitch(g.ny);
-  const size_t rows = (size_t)(a1 - a0) * g.nz * g.nx;
-  const size_t first_row = (size_t)a0 * g.nz * g.nx;
-  float *dst = static_cast<float *>(buf.ptr) + first_row * pitch;
-  const float *from = src + first_row * g.ny;
-  const size_t bytes = rows * g.ny * sizeof(float);
-  if (pitch == g.ny) {
-    PCT_CUDA(h, cudaMemcpyAsync(dst, from, bytes, cudaMemcpyHostToDevice, s));
-  } else {
-    float *stage = stage_base + first_row * g.ny;
-    PCT_CUDA(h, cudaMemcpyAsync(stage, from, bytes, cudaMemcpyHostToDevice, s));
-    PCT_CUDA(h, pct::launch_pitch_copy(stage, dst, (long long)rows, g.ny, pitch, s));
+  const bool whole = z0 == 0 && z1 == g.nz;
+  for (int a = a0; a < (whole ? a0 + 1 : a1); ++a) {
+    const size_t rows = whole ? (size_t)(a1 - a0) * g.nz * g.nx : (size_t)(z1 - z0) * g.nx;
+    const size_t first_row = ((size_t)a * g.nz + z0) * g.nx;
+    float *dst = static_cast<float *>(buf.ptr) + first_row * pitch;
+    const float *from = src + first_row * g.ny;
+    const size_t bytes = rows * g.ny * sizeof(float);
+    if (pitch == g.ny) {
+      PCT_CUDA(h, cudaMemcpyAsync(dst, from, bytes, cudaMemcpyHostToDevice, s));
+    } else {
+      float *stage = stage_base + first_row * g.ny;
+      PCT_CUDA(h, cudaMemcpyAsync(stage, from, bytes, cudaMemcpyHostToDevice, s));
+      PCT_CUDA(h, pct::launch_pitch_copy(stage, dst, (long long)rows, g.ny, pitch, s));
+    }
+    if (normalize) PCT_CUDA(h, pct::launch_normalize_labels(dst, rows * pitch, s));
   }
-  if (normalize) PCT_CUDA(h, pct::launch_normalize_labels(dst, rows * pitch, s));
   return PCT_OK;
 }
 
-// The host-pointer path with uploads overlapped with the fusion: the input MRI and the first
-// atlas group are uploaded and repacked on the handle's copy stream, the fusion of that group
-// starts on `s`, the remaining groups upload meanwhile and run in a second launch, then the
-// group sums are combined into d_out. Used when the plan has two or more atlas groups; returns
+// The host-pointer path with uploads overlapped with the fusion. The handle's copy stream
+// uploads (and repacks) the subject in parts, each part's fusion items starting as soon as it has
+// landed: the first atlas group with the input MRI in up to three plane ranges (the first holds
+// the planes read by just enough z-tiles to give every CTA of the grid an item, the second as
+// many z-tiles again, the third the rest), then one part per further group. The launches
+// alternate between `s` and the handle's second compute stream, so that the last round of one
+// launch overlaps the first round of the next; both streams join `s` before the group sums are
+// combined into d_out. Used when the plan has two or more atlas groups; returns
 // PCT_ERR_UNSUPPORTED (nothing enqueued) otherwise. `normalize` applies the label normalisation
-// to the CT stack on the device (the pipeline entry point).
+// to the CT stack on the device (the pipeline entry point). The items and the combine's group
+// order are those of the one-launch path, so the result is the same bit for bit.
 int fuse_pipelined(pct_handle *h, const pct::Geometry &g, const float *img, const float *atlas,
                    const float *atlas_ct, float *d_out, double div, bool normalize,
                    cudaStream_t s) {
@@ -344,49 +355,92 @@ int fuse_pipelined(pct_handle *h, const pct::Geometry &g, const float *img, cons
     h->last_error.clear();  // over the handle's memory cap: the one-upload path needs half
     return PCT_ERR_UNSUPPORTED;
   }
+  struct Part {
+    bool with_img;
+    int a0, a1, z0, z1;  // atlases [a0, a1), planes [z0, z1)
+    int i0, i1;          // work items that may run once it has landed
+  };
+  std::vector<Part> parts;
+  const int per = g.num / pl.groups;
+  {
+    // z-tile ends of the first group's leading parts; part k reads planes [0, planes_read(end))
+    const int a = std::min(pl.tiles_z, (pl.ctas + pl.tiles_xy - 1) / pl.tiles_xy);
+    const int ends[2] = {a, std::min(pl.tiles_z, 2 * a)};
+    int z0 = 0, t0 = 0;
+    for (const int e : ends) {
+      if (e <= t0 || e >= pl.tiles_z) continue;
+      const int z1 = pct::fuse_tma_planes_read(g, pl, e);
+      if (z1 >= g.nz) continue;
+      parts.push_back(Part{true, 0, per, z0, z1, t0 * pl.tiles_xy, e * pl.tiles_xy});
+      z0 = z1;
+      t0 = e;
+    }
+    parts.push_back(Part{true, 0, per, z0, g.nz, t0 * pl.tiles_xy, pl.tiles});
+    for (int grp = 1; grp < pl.groups; ++grp)
+      parts.push_back(Part{false, grp * per, (grp + 1) * per, 0, g.nz, grp * pl.tiles,
+                           (grp + 1) * pl.tiles});
+  }
   if (!h->copy_stream)
     PCT_CUDA(h, cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
-  for (cudaEvent_t &e : h->ev)
-    if (!e) PCT_CUDA(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  if (!h->compute_stream)
+    PCT_CUDA(h, cudaStreamCreateWithFlags(&h->compute_stream, cudaStreamNonBlocking));
+  // events: the fork, one per part, two joins
+  while (h->pipe_ev.size() < parts.size() + 3) {
+    cudaEvent_t e = nullptr;
+    PCT_CUDA(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    h->pipe_ev.push_back(e);
+  }
   const cudaStream_t cs = h->copy_stream;
-  const int per = g.num / pl.groups;
+  const cudaStream_t lanes[2] = {s, h->compute_stream};
   int *err = static_cast<int *>(h->err.ptr);
   PCT_CUDA(h, cudaMemsetAsync(err, 0, sizeof(int), s));
-  PCT_CUDA(h, cudaEventRecord(h->ev[0], s));
-  PCT_CUDA(h, cudaStreamWaitEvent(cs, h->ev[0], 0));
-  PCT_CUDA(h, cudaMemcpyAsync(h->img.ptr, img, (size_t)g.nvox() * sizeof(float),
-                              cudaMemcpyHostToDevice, cs));
-  // staging: the MRI stack, then the CT stack (both in flight at once)
+  // fork: the copy stream and the second compute stream follow the work already on s
+  PCT_CUDA(h, cudaEventRecord(h->pipe_ev[0], s));
+  PCT_CUDA(h, cudaStreamWaitEvent(cs, h->pipe_ev[0], 0));
+  PCT_CUDA(h, cudaStreamWaitEvent(lanes[1], h->pipe_ev[0], 0));
+  const size_t plane = (size_t)g.nx * g.ny;
   float *stage_mri = static_cast<float *>(h->stage.ptr);
   float *stage_ct = stage_mri ? stage_mri + rows * g.ny : nullptr;
-  auto stage_group = [&](int a0, int a1) -> int {
-    const int r = stage_pitched_slice(h, h->atlas, stage_mri, atlas, g, a0, a1, false, cs);
-    return r ? r : stage_pitched_slice(h, h->label, stage_ct, atlas_ct, g, a0, a1, normalize, cs);
-  };
-  if ((st = stage_group(0, per))) return st;
-  PCT_CUDA(h, cudaEventRecord(h->ev[1], cs));
-  PCT_CUDA(h, cudaStreamWaitEvent(s, h->ev[1], 0));
   const pct::SlabInputs in{static_cast<const float *>(h->img.ptr),
                            static_cast<const float *>(h->atlas.ptr),
                            static_cast<const float *>(h->label.ptr), pitch};
   float *partial = static_cast<float *>(h->partial.ptr);
-  PCT_CUDA(h, pct::launch_fuse_tma_groups(g, in, div, partial, err, h->tile_set, 0, 1, s));
-  // The second group runs as soon as it has landed, the remaining groups in one launch once
-  // everything has (config 1 end to end: 34.0 ms against 34.2 with groups 2.. in one launch; a
-  // launch per group 34.0; pitched 2-D host copies of the 888-byte rows instead of the repack
-  // kernel made the uploads several times slower: 82.9 ms).
-  int next = 1;
-  if (pl.groups >= 3) {
-    if ((st = stage_group(per, 2 * per))) return st;
-    PCT_CUDA(h, cudaEventRecord(h->ev[2], cs));
-    PCT_CUDA(h, cudaStreamWaitEvent(s, h->ev[2], 0));
-    PCT_CUDA(h, pct::launch_fuse_tma_groups(g, in, div, partial, err, h->tile_set, 1, 2, s));
-    next = 2;
+  // (config 1 end to end: 34.0 ms with the first group whole and the group launches on s alone;
+  // pitched 2-D host copies of the 888-byte rows instead of the repack kernel made the uploads
+  // several times slower: 82.9 ms)
+  auto run_part = [&](size_t k) -> int {
+    const Part &p = parts[k];
+    if (p.with_img)
+      PCT_CUDA(h, cudaMemcpyAsync(static_cast<float *>(h->img.ptr) + p.z0 * plane,
+                                  img + p.z0 * plane, (size_t)(p.z1 - p.z0) * plane * sizeof(float),
+                                  cudaMemcpyHostToDevice, cs));
+    int r = stage_pitched_slice(h, h->atlas, stage_mri, atlas, g, p.a0, p.a1, p.z0, p.z1, false,
+                                cs);
+    if (!r)
+      r = stage_pitched_slice(h, h->label, stage_ct, atlas_ct, g, p.a0, p.a1, p.z0, p.z1,
+                              normalize, cs);
+    if (r) return r;
+    const cudaStream_t ls = lanes[k & 1];
+    PCT_CUDA(h, cudaEventRecord(h->pipe_ev[1 + k], cs));
+    PCT_CUDA(h, cudaStreamWaitEvent(ls, h->pipe_ev[1 + k], 0));
+    PCT_CUDA(h, pct::launch_fuse_tma_items(g, in, div, partial, err, h->tile_set, p.i0, p.i1, ls));
+    return PCT_OK;
+  };
+  st = PCT_OK;
+  for (size_t k = 0; k < parts.size() && !st; ++k) st = run_part(k);
+  // join (on failure too, so that nothing of this call is still running on the other streams
+  // when the caller's next call reuses the buffers)
+  const cudaStream_t others[2] = {lanes[1], cs};
+  for (int k = 0; k < 2; ++k) {
+    const cudaEvent_t joined = h->pipe_ev[1 + parts.size() + k];
+    if (st) {  // best effort: the call already failed
+      if (cudaEventRecord(joined, others[k]) == cudaSuccess) cudaStreamWaitEvent(s, joined, 0);
+      continue;
+    }
+    PCT_CUDA(h, cudaEventRecord(joined, others[k]));
+    PCT_CUDA(h, cudaStreamWaitEvent(s, joined, 0));
   }
-  if ((st = stage_group(next * per, g.num))) return st;
-  PCT_CUDA(h, cudaEventRecord(h->ev[2], cs));
-  PCT_CUDA(h, cudaStreamWaitEvent(s, h->ev[2], 0));
-  PCT_CUDA(h, pct::launch_fuse_tma_groups(g, in, div, partial, err, h->tile_set, next, pl.groups, s));
+  if (st) return st;
   PCT_CUDA(h, pct::launch_fuse_tma_combine(g, partial, h->tile_set, d_out, s));
   return PCT_OK;
 }
@@ -559,11 +613,12 @@ int pct_destroy(pct_handle *h) {
                     &h->stage, &h->batch_stage, &h->batch_meta, &h->learned, &h->tcbuf})
     if (b->ptr) cudaFree(b->ptr);
   if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
+  if (h->compute_stream) cudaStreamDestroy(h->compute_stream);
   if (h->learned_done) cudaEventDestroy(h->learned_done);
   if (h->learned_streams.aux) cudaStreamDestroy(h->learned_streams.aux);
   for (cudaEvent_t e : h->learned_streams.ev)
     if (e) cudaEventDestroy(e);
-  for (cudaEvent_t e : h->ev)
+  for (cudaEvent_t e : h->pipe_ev)
     if (e) cudaEventDestroy(e);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;

@@ -790,7 +790,7 @@ SubjectView subject_view(const Geometry &g, const SlabInputs &in, float *out, do
 
 template <int SET, int HW>
 cudaError_t launch_hw(const Geometry &g, const SlabInputs &in, float *out, double div,
-                      float *partial, int *err, const WaitTest &wt, int group_begin, int group_end,
+                      float *partial, int *err, const WaitTest &wt, int item_begin, int item_end,
                       cudaStream_t stream) {
   constexpr int RX = TileOf<SET, HW>::RX, TZ = TileOf<SET, HW>::TZ;
   using C = Cfg<HW, RX, TZ>;
@@ -798,12 +798,12 @@ cudaError_t launch_hw(const Geometry &g, const SlabInputs &in, float *out, doubl
   cudaError_t e = plan_hw<SET, HW>(g, &pl);
   if (e != cudaSuccess) return e;
   if (pl.groups > 1 && !partial) return cudaErrorInvalidValue;
-  const bool whole = group_begin < 0;  // all groups, then the combine
+  const bool whole = item_begin < 0;  // every item, then the combine
   if (whole) {
-    group_begin = 0;
-    group_end = pl.groups;
-  } else if (pl.groups < 2 || group_begin >= group_end || group_end > pl.groups) {
-    return cudaErrorInvalidValue;  // a group range needs partial sums and a later combine
+    item_begin = 0;
+    item_end = pl.groups * pl.ntiles;
+  } else if (pl.groups < 2 || item_begin >= item_end || item_end > pl.groups * pl.ntiles) {
+    return cudaErrorInvalidValue;  // an item range needs partial sums and a later combine
   }
   CUtensorMap tmA, tmL;
   if ((e = make_slab_map(&tmA, in.atlas, g.nx, g.ny, g.nz, g.num, in.pitch, C::YB, C::ZA)) !=
@@ -821,8 +821,8 @@ cudaError_t launch_hw(const Geometry &g, const SlabInputs &in, float *out, doubl
     p.timeout_ns = wt.timeout_ns;
     p.withhold_cta = 0;
   }
-  p.item_begin = group_begin * pl.ntiles;
-  p.item_end = group_end * pl.ntiles;
+  p.item_begin = item_begin;
+  p.item_end = item_end;
   const int blocks = std::min(pl.blocks, p.item_end - p.item_begin);
   fuse_tma_kernel<HW, RX, TZ, TileOf<SET, HW>::LY, TileOf<SET, HW>::MB>
       <<<blocks, kThreads, C::SMEM, stream>>>(tmA, tmL, p);
@@ -856,14 +856,14 @@ cudaError_t plan_any(const Geometry &g, int set, Plan *pl) {
 
 template <int SET>
 cudaError_t launch_set(const Geometry &g, const SlabInputs &in, float *out, double div,
-                       float *partial, int *err, const WaitTest &wt, int gb, int ge,
+                       float *partial, int *err, const WaitTest &wt, int ib, int ie,
                        cudaStream_t stream) {
   switch (g.hw) {
-    case 1: return launch_hw<SET, 1>(g, in, out, div, partial, err, wt, gb, ge, stream);
-    case 2: return launch_hw<SET, 2>(g, in, out, div, partial, err, wt, gb, ge, stream);
-    case 3: return launch_hw<SET, 3>(g, in, out, div, partial, err, wt, gb, ge, stream);
-    case 4: return launch_hw<SET, 4>(g, in, out, div, partial, err, wt, gb, ge, stream);
-    case 5: return launch_hw<SET, 5>(g, in, out, div, partial, err, wt, gb, ge, stream);
+    case 1: return launch_hw<SET, 1>(g, in, out, div, partial, err, wt, ib, ie, stream);
+    case 2: return launch_hw<SET, 2>(g, in, out, div, partial, err, wt, ib, ie, stream);
+    case 3: return launch_hw<SET, 3>(g, in, out, div, partial, err, wt, ib, ie, stream);
+    case 4: return launch_hw<SET, 4>(g, in, out, div, partial, err, wt, ib, ie, stream);
+    case 5: return launch_hw<SET, 5>(g, in, out, div, partial, err, wt, ib, ie, stream);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -1059,7 +1059,7 @@ size_t fuse_tma_partial_bytes(const Geometry &g, int set) {
 }
 
 cudaError_t fuse_tma_plan(const Geometry &g, int set, FusePlanInfo *info) {
-  *info = FusePlanInfo{0, 0, 0, 0, 0, 0};
+  *info = FusePlanInfo{0, 0, 0, 0, 0, 0, 0, 0};
   if (g.ix <= 0 || g.iy <= 0 || g.iz <= 0) return cudaSuccess;
   Plan pl;
   cudaError_t e = plan_any(g, set, &pl);
@@ -1071,7 +1071,16 @@ cudaError_t fuse_tma_plan(const Geometry &g, int set, FusePlanInfo *info) {
   info->tz = pl.tz;
   info->partial_bytes =
       pl.groups > 1 ? (size_t)pl.groups * 2 * (size_t)g.nvox() * sizeof(float) : 0;
+  info->tiles_z = pl.tiles_z;
+  info->tiles_xy = pl.tiles_y * pl.tiles_x;
   return cudaSuccess;
+}
+
+int fuse_tma_planes_read(const Geometry &g, const FusePlanInfo &info, int ztiles) {
+  // z-tile tz reads the atlas MRI slab [2 tz TZ, 2 tz TZ + 2 TZ + 2 + 2 HW) (its first output
+  // plane minus the box and window reach), the CT slab and the input taps lie inside it
+  const long long n = (long long)ztiles * 2 * info.tz + 2 + 2 * g.hw;
+  return ztiles <= 0 ? 0 : (int)(n < g.nz ? n : g.nz);
 }
 
 cudaError_t launch_fuse_tma(const Geometry &g, const SlabInputs &in, float *out, double div,
@@ -1088,17 +1097,18 @@ cudaError_t launch_fuse_tma(const Geometry &g, const SlabInputs &in, float *out,
   }
 }
 
-cudaError_t launch_fuse_tma_groups(const Geometry &g, const SlabInputs &in, double div,
-                                   float *partial, int *err, int set, int group_begin,
-                                   int group_end, cudaStream_t stream) {
+cudaError_t launch_fuse_tma_items(const Geometry &g, const SlabInputs &in, double div,
+                                  float *partial, int *err, int set, int item_begin, int item_end,
+                                  cudaStream_t stream) {
   if (g.ix <= 0 || g.iy <= 0 || g.iz <= 0) return cudaSuccess;
+  if (item_begin < 0) return cudaErrorInvalidValue;
   const WaitTest wt{0};
   switch (set) {
-    case 0: return launch_set<0>(g, in, nullptr, div, partial, err, wt, group_begin, group_end, stream);
-    case 1: return launch_set<1>(g, in, nullptr, div, partial, err, wt, group_begin, group_end, stream);
-    case 2: return launch_set<2>(g, in, nullptr, div, partial, err, wt, group_begin, group_end, stream);
-    case 3: return launch_set<3>(g, in, nullptr, div, partial, err, wt, group_begin, group_end, stream);
-    case 4: return launch_set<4>(g, in, nullptr, div, partial, err, wt, group_begin, group_end, stream);
+    case 0: return launch_set<0>(g, in, nullptr, div, partial, err, wt, item_begin, item_end, stream);
+    case 1: return launch_set<1>(g, in, nullptr, div, partial, err, wt, item_begin, item_end, stream);
+    case 2: return launch_set<2>(g, in, nullptr, div, partial, err, wt, item_begin, item_end, stream);
+    case 3: return launch_set<3>(g, in, nullptr, div, partial, err, wt, item_begin, item_end, stream);
+    case 4: return launch_set<4>(g, in, nullptr, div, partial, err, wt, item_begin, item_end, stream);
     default: return cudaErrorInvalidValue;
   }
 }

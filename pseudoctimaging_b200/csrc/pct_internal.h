@@ -48,17 +48,21 @@ size_t fuse_tma_partial_bytes(const Geometry &g, int set);
 struct FusePlanInfo {
   int groups, tiles, ctas, rx, tz;
   size_t partial_bytes;
+  int tiles_z, tiles_xy;  // tiles are numbered z-major: tile t has z-tile t / tiles_xy
 };
 cudaError_t fuse_tma_plan(const Geometry &g, int set, FusePlanInfo *info);
 cudaError_t launch_fuse_tma(const Geometry &g, const SlabInputs &in, float *out, double div,
                             float *partial, int *err, const WaitTest &wt, int set,
                             cudaStream_t stream);
-// Pipelined form of the same (plans with 2 or more atlas groups only): the work items of atlas
-// groups [group_begin, group_end) into the partial sums, and, once every group has run, the
-// combine into out. Lets the host start on the first groups while later groups are uploaded.
-cudaError_t launch_fuse_tma_groups(const Geometry &g, const SlabInputs &in, double div,
-                                   float *partial, int *err, int set, int group_begin,
-                                   int group_end, cudaStream_t stream);
+// Pipelined form of the same (plans with 2 or more atlas groups only): the work items
+// [item_begin, item_end) into the partial sums (item = group * tiles + tile);
+// launch_fuse_tma_combine adds the groups into out once every item has run. Lets the host start
+// on the first planes of the first group while the rest is uploaded.
+cudaError_t launch_fuse_tma_items(const Geometry &g, const SlabInputs &in, double div,
+                                  float *partial, int *err, int set, int item_begin, int item_end,
+                                  cudaStream_t stream);
+// Planes [0, n) of the input and atlas volumes that the items of z-tiles [0, ztiles) read.
+int fuse_tma_planes_read(const Geometry &g, const FusePlanInfo &info, int ztiles);
 cudaError_t launch_fuse_tma_combine(const Geometry &g, const float *partial, int set, float *out,
                                     cudaStream_t stream);
 

@@ -22,14 +22,29 @@ def device_run(h, img, atl, lab, nh, div):
     return out.cpu().numpy()
 
 
-@pytest.mark.parametrize("shape,nh,min_groups", [((64, 70, 48, 6), 11, 2), ((90, 61, 40, 4), 7, 2),
-                                                ((40, 45, 30, 10), 11, 3)])
-def test_pipelined_host_path_equals_device_path(shape, nh, min_groups):
-    """With three or more groups the second group runs in a launch of its own as soon as it has
-    landed, the rest in a third."""
+def first_group_split(plan, nx, ny, nz, nh):
+    """Whether the first atlas group uploads in plane ranges: the z-tiles that give every CTA of
+    the grid an item read fewer planes than the volume has."""
+    lo = (nh - 1) // 2 + 1
+    tiles_xy = -(-(ny - 2 * lo) // 30) * -(-(nx - 2 * lo) // (4 * plan["tile_rows"]))
+    zt = 2 * plan["tile_planes"]
+    tiles_z = -(-(nz - 2 * lo) // zt)
+    first = -(-plan["ctas"] // tiles_xy)
+    return first < tiles_z and first * zt + 2 + 2 * (lo - 1) < nz
+
+
+@pytest.mark.parametrize("shape,nh,min_groups,split",
+                         [((64, 70, 48, 6), 11, 2, False), ((90, 61, 40, 4), 7, 2, False),
+                          ((40, 45, 30, 10), 11, 3, False), ((222, 222, 112, 4), 11, 3, True),
+                          ((64, 70, 252, 4), 7, 3, True)])
+def test_pipelined_host_path_equals_device_path(shape, nh, min_groups, split):
+    """Every atlas group after the first runs in a launch of its own as soon as it has landed;
+    on volumes with more z-tiles than one round of the grid needs, the first group's first
+    z-tiles start before the rest of its planes have landed."""
     nx, ny, nz, num = shape
     plan = pct.query_plan(nx, ny, nz, num, nh)
     assert plan["groups"] >= min_groups, plan  # the shape must take the pipelined path
+    assert first_group_split(plan, nx, ny, nz, nh) == split, plan
     s = pct.synth_subject(nx, ny, nz, num, n_blobs=10, seed=nh)
     lab = pct.normalize_labels(s.atlas_ct)
     div = pct.div_from(2.5, 1.0)
