@@ -1124,14 +1124,27 @@ cudaError_t launch_fuse_tma_combine(const Geometry &g, const float *partial, int
 }
 
 namespace {
+// One warp per row (grid-stride over rows), so that no element index is divided by the row
+// length; PAIRS copies 8-byte pairs (even ny and an 8-byte aligned source; the destination's
+// pitch is a multiple of 4 floats).
+template <bool PAIRS>
 __global__ void pitch_copy_kernel(const float *__restrict__ src, float *__restrict__ dst,
                                   long long rows, int ny, int pitch) {
-  const long long total = rows * ny;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-       i += (long long)gridDim.x * blockDim.x) {
-    const long long r = i / ny;
-    const int c = (int)(i - r * ny);
-    dst[r * pitch + c] = src[i];
+  const int lane = threadIdx.x & 31;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long r = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows;
+       r += nwarps) {
+    const float *s = src + r * ny;
+    float *d = dst + r * pitch;
+    if constexpr (PAIRS) {
+      const float2 *s2 = reinterpret_cast<const float2 *>(s);
+      float2 *d2 = reinterpret_cast<float2 *>(d);
+#pragma unroll 4
+      for (int c = lane; c < ny / 2; c += 32) d2[c] = s2[c];
+    } else {
+#pragma unroll 4
+      for (int c = lane; c < ny; c += 32) d[c] = s[c];
+    }
   }
 }
 }  // namespace
@@ -1142,7 +1155,11 @@ cudaError_t launch_pitch_copy(const float *src, float *dst, long long rows, int 
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  pitch_copy_kernel<<<sms * 8, 256, 0, stream>>>(src, dst, rows, ny, pitch);
+  if (ny % 2 == 0 && reinterpret_cast<uintptr_t>(src) % 8 == 0 &&
+      reinterpret_cast<uintptr_t>(dst) % 16 == 0 && pitch % 4 == 0)
+    pitch_copy_kernel<true><<<sms * 8, 256, 0, stream>>>(src, dst, rows, ny, pitch);
+  else
+    pitch_copy_kernel<false><<<sms * 8, 256, 0, stream>>>(src, dst, rows, ny, pitch);
   return cudaGetLastError();
 }
 
