@@ -188,6 +188,18 @@ int pct_autotune(pct_handle *h, const pct_subject *subjects, int n, const char *
                  double *ms_per_set, int *chosen);
 
 /*
+ * Device time of the plain path's fusion kernel (EXEC_CHOICE 0-3 through pct_synthesize_device,
+ * or pct_synthesize when it uploads in one piece): while timing is on, CUDA events are recorded
+ * on the call's stream right before and after each fusion launch (the group combine and the
+ * repack are outside). pct_kernel_time waits for the last of them and returns the launches
+ * timed since the previous read and their summed device time in milliseconds, then starts over.
+ * At most 4096 launches are kept between reads; later ones run untimed. No counterpart in the
+ * reference (its timing is host wall clock around the whole call).
+ */
+int pct_set_kernel_timing(pct_handle *h, int on);
+int pct_kernel_time(pct_handle *h, double *ms_total, int *launches);
+
+/*
  * Learned-proposal form (EXEC_CHOICE 7), training side. The model is a small 3D CNN over the
  * co-located 9x9x9 patches of the input MRI and one atlas MRI (conv 2->16, 3 x conv 16->16, all
  * 3x3x3 valid + ReLU, then three linear heads 16->11 scoring dw, du and dv); it proposes, per

@@ -115,6 +115,8 @@ SIGNATURES = {
     "pct_batch_destroy": (_I, [_P]),
     "pct_tile_sets": (_I, []),
     "pct_set_tile_set": (_I, [_P, _I]),
+    "pct_set_kernel_timing": (_I, [_P, _I]),
+    "pct_kernel_time": (_I, [_P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]),
     "pct_get_tile_set": (_I, [_P]),
     "pct_autotune": (_I, [_P, ctypes.POINTER(SubjectDesc), _I, ctypes.c_char_p,
                           ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]),
@@ -364,6 +366,17 @@ class Handle:
 
     def batch_graph(self, subjects, stream: int = 0) -> "BatchGraph":
         return BatchGraph(self, subjects, stream)
+
+    def set_kernel_timing(self, on: bool) -> None:
+        """Record CUDA events around every fusion launch of the plain path from now on."""
+        self._check(lib.pct_set_kernel_timing(self._h, int(bool(on))), "pct_set_kernel_timing")
+
+    def kernel_time(self) -> tuple[float, int]:
+        """(summed device ms, launches) of the fusion launches timed since the last read."""
+        ms, n = ctypes.c_double(), ctypes.c_int()
+        self._check(lib.pct_kernel_time(self._h, ctypes.byref(ms), ctypes.byref(n)),
+                    "pct_kernel_time")
+        return float(ms.value), int(n.value)
 
     def set_tile_set(self, k: int) -> None:
         self._check(lib.pct_set_tile_set(self._h, k), "pct_set_tile_set")

@@ -49,6 +49,9 @@ struct pct_handle {
   cudaStream_t copy_stream = nullptr;     // uploads of the pipelined host path
   cudaStream_t compute_stream = nullptr;  // its second compute stream
   std::vector<cudaEvent_t> pipe_ev;       // its fork, one per uploaded part, two joins
+  bool time_kernels = false;              // pct_set_kernel_timing
+  std::vector<cudaEvent_t> kt_ev;         // start / stop pairs around timed fusion launches
+  size_t kt_used = 0;                     // pairs recorded since the last pct_kernel_time
   std::string last_error;
 };
 
@@ -142,6 +145,8 @@ int select_device(pct_handle *h) {
   return PCT_OK;
 }
 
+constexpr size_t kMaxTimedLaunches = 4096;  // pct_set_kernel_timing: pairs kept between reads
+
 // Zeroes the device status word and enqueues the TMA-staged fusion kernel.
 int launch_fusion(pct_handle *h, const pct::Geometry &g, const pct::SlabInputs &in, float *d_out,
                   double div, cudaStream_t s) {
@@ -151,8 +156,18 @@ int launch_fusion(pct_handle *h, const pct::Geometry &g, const pct::SlabInputs &
   const size_t pbytes = pct::fuse_tma_partial_bytes(g, h->tile_set);
   if (pbytes && (st = ensure(h, h->partial, pbytes))) return st;
   PCT_CUDA(h, cudaMemsetAsync(err, 0, sizeof(int), s));
-  const pct::WaitTest wt{h->wait_test_ns};
+  pct::LaunchHooks wt{h->wait_test_ns, nullptr, nullptr};
   h->wait_test_ns = 0;
+  if (h->time_kernels && h->kt_used < kMaxTimedLaunches) {
+    while (h->kt_ev.size() < 2 * (h->kt_used + 1)) {
+      cudaEvent_t e = nullptr;
+      PCT_CUDA(h, cudaEventCreate(&e));
+      h->kt_ev.push_back(e);
+    }
+    wt.start = h->kt_ev[2 * h->kt_used];
+    wt.stop = h->kt_ev[2 * h->kt_used + 1];
+    ++h->kt_used;
+  }
   PCT_CUDA(h, pct::launch_fuse_tma(g, in, d_out, div, static_cast<float *>(h->partial.ptr), err, wt,
                                    h->tile_set, s));
   return PCT_OK;
@@ -207,10 +222,17 @@ int launch_learned_path(pct_handle *h, const pct::Geometry &g, const pct::SlabIn
   }
   for (cudaEvent_t &e : ls.ev)
     if (!e) PCT_CUDA(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  // the confidence fallback's full search writes per-pair partial sums (NH = 11 tiles only)
+  float *fb_partial = nullptr;
+  if (h->learned_conf > 0.f && g.nh == 11) {
+    if ((st = ensure(h, h->partial, pct::learned::fallback_partial_bytes(g)))) return st;
+    fb_partial = static_cast<float *>(h->partial.ptr);
+  }
   PCT_CUDA(h, cudaMemsetAsync(err, 0, sizeof(int), s));
   PCT_CUDA(h, pct::learned::launch_learned(g, pct::learned::model_weights(h->model), in, d_out, div,
                                            h->learned_conf, h->learned_block, h->learned_level,
-                                           h->learned_every_voxel, h->learned.ptr, err, &ls, s));
+                                           h->learned_every_voxel, h->learned.ptr, fb_partial, err,
+                                           &ls, s));
   return learned_ran(h, g, s);
 }
 
@@ -620,6 +642,8 @@ int pct_destroy(pct_handle *h) {
     if (e) cudaEventDestroy(e);
   for (cudaEvent_t e : h->pipe_ev)
     if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : h->kt_ev)
+    if (e) cudaEventDestroy(e);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return PCT_OK;
@@ -697,6 +721,34 @@ int pct_set_learned_convs(pct_handle *h, int every_voxel) {
   if (every_voxel != 0 && every_voxel != 1)
     return fail(h, PCT_ERR_INVALID_ARG, "every_voxel must be 0 or 1");
   h->learned_every_voxel = every_voxel == 1;
+  return PCT_OK;
+}
+
+int pct_set_kernel_timing(pct_handle *h, int on) {
+  if (!h) return PCT_ERR_INVALID_ARG;
+  h->time_kernels = on != 0;
+  return PCT_OK;
+}
+
+int pct_kernel_time(pct_handle *h, double *ms_total, int *launches) {
+  if (!h || !ms_total || !launches) return PCT_ERR_INVALID_ARG;
+  h->last_error.clear();
+  *ms_total = 0.0;
+  *launches = 0;
+  const size_t n = h->kt_used;
+  h->kt_used = 0;
+  if (n == 0) return PCT_OK;
+  int st = select_device(h);
+  if (st) return st;
+  PCT_CUDA(h, cudaEventSynchronize(h->kt_ev[2 * n - 1]));
+  double total = 0.0;
+  for (size_t i = 0; i < n; ++i) {
+    float ms = 0.f;
+    PCT_CUDA(h, cudaEventElapsedTime(&ms, h->kt_ev[2 * i], h->kt_ev[2 * i + 1]));
+    total += ms;
+  }
+  *ms_total = total;
+  *launches = (int)n;
   return PCT_OK;
 }
 

@@ -98,6 +98,9 @@ struct SubjectView {
   int item_begin;     // first global item of this subject (batched kernel)
   int atlas_base;     // first atlas of group 0 (a single-atlas launch over a tile list)
   float *acc_p, *acc_w;  // non-null: add each voxel's (product, sum_weight) into these instead
+  // non-null (masked items): item = pair << 24 | tile, over the atlases atlas_base + i for the
+  // set bits i of atlas_mask[tile], two per pair in bit order; pair k's sums go to partial slot k
+  const uint32_t *atlas_mask;
 };
 
 struct TmaParams {
@@ -330,7 +333,7 @@ struct Pipe {
 // Processes work item `item` (tile x atlas group) of subject `sv` with register tile (RX, TZ) in
 // layout LY (0: z-halves packed; 1: y-pairs, labels read per use; 2: y-pairs, labels in a
 // register ring). Returns false when a bounded wait gave up (the CTA must stop).
-template <int HW, int RX, int TZ, int LY>
+template <int HW, int RX, int TZ, int LY, bool MASKED = false>
 __device__ __forceinline__ bool run_item(const SubjectView &sv, int item, Pipe &pp, int *err,
                                          unsigned long long timeout_ns, int withhold_cta) {
   using C = Cfg<HW, RX, TZ>;
@@ -341,11 +344,23 @@ __device__ __forceinline__ bool run_item(const SubjectView &sv, int item, Pipe &
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int lo = HW + 1;
   const float2 scale2 = make_float2(sv.scale, sv.scale);
-  const int T = sv.atlases_per_group * NS;  // du steps per item (atlas-major)
-
-  const int grp = item / sv.ntiles;
-  const int a_first = sv.atlas_base + grp * sv.atlases_per_group;
-  int t = item - grp * sv.ntiles;
+  int grp, t, a_first, natl;
+  uint32_t later = 0;  // masked items: the pair's atlases after the current one (bits)
+  if constexpr (MASKED) {
+    grp = (int)((uint32_t)item >> 24);
+    t = item & 0xffffff;
+    uint32_t m = sv.atlas_mask[t];
+    for (int k = 0; k < 2 * grp; ++k) m &= m - 1;  // drop the earlier pairs' atlases
+    natl = min(2, __popc(m));
+    a_first = sv.atlas_base + __ffs(m) - 1;
+    later = m & (m - 1);
+  } else {
+    grp = item / sv.ntiles;
+    t = item - grp * sv.ntiles;
+    a_first = sv.atlas_base + grp * sv.atlases_per_group;
+    natl = sv.atlases_per_group;
+  }
+  const int T = natl * NS;  // du steps per item (atlas-major)
   const int ty = t % sv.tiles_y;
   t /= sv.tiles_y;
   const int txc = t % sv.tiles_x;
@@ -390,9 +405,17 @@ __device__ __forceinline__ bool run_item(const SubjectView &sv, int item, Pipe &
       W[q][r] = make_float2(0.f, 0.f);
     }
 
+  int a = a_first;
   for (int i = 0; i < T; ++i, ++pp.gstep) {
     const int ai = i / NS, j = i - ai * NS;
-    const int a = a_first + ai;
+    if constexpr (MASKED) {
+      if (j == 0 && i > 0) {  // the pair's second atlas
+        a = sv.atlas_base + __ffs(later) - 1;
+        later &= later - 1;
+      }
+    } else {
+      a = a_first + ai;
+    }
     __syncthreads();  // every warp is done with step i-1: its ring rows may be refilled
     if (*pp.abort_flag) return false;
     const uint32_t gstep = pp.gstep;
@@ -546,19 +569,20 @@ __global__ void __launch_bounds__(kThreads, MB)
   }
 }
 
-// The full search of one atlas over a device-side list of tiles (count on the device, so the
-// launch needs no host round trip), adding each voxel's sums into sv.acc_p / sv.acc_w.
+// The full search over a device-side list of masked items (count on the device, so the launch
+// needs no host round trip): each item is up to two flagged atlases of one tile, its sums written
+// to the partial slot of its pair.
 template <int HW, int RX, int TZ, int LY, int MB>
 __global__ void __launch_bounds__(kThreads, MB)
     fuse_list_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmL,
-                     TmaParams p, const int *__restrict__ tiles, const int *__restrict__ count) {
+                     TmaParams p, const int *__restrict__ items, const int *__restrict__ count) {
   extern __shared__ unsigned char smem_raw[];
   Pipe pp = pipe_init(smem_raw);
   p.sv.tmA = &tmA;
   p.sv.tmL = &tmL;
   const int n = *count;
   for (int i = blockIdx.x; i < n; i += gridDim.x) {
-    if (!run_item<HW, RX, TZ, LY>(p.sv, tiles[i], pp, p.err, p.timeout_ns, -1)) {
+    if (!run_item<HW, RX, TZ, LY, true>(p.sv, items[i], pp, p.err, p.timeout_ns, -1)) {
       pipe_drain(pp, p.timeout_ns);
       return;
     }
@@ -790,7 +814,7 @@ SubjectView subject_view(const Geometry &g, const SlabInputs &in, float *out, do
 
 template <int SET, int HW>
 cudaError_t launch_hw(const Geometry &g, const SlabInputs &in, float *out, double div,
-                      float *partial, int *err, const WaitTest &wt, int item_begin, int item_end,
+                      float *partial, int *err, const LaunchHooks &wt, int item_begin, int item_end,
                       cudaStream_t stream) {
   constexpr int RX = TileOf<SET, HW>::RX, TZ = TileOf<SET, HW>::TZ;
   using C = Cfg<HW, RX, TZ>;
@@ -824,9 +848,11 @@ cudaError_t launch_hw(const Geometry &g, const SlabInputs &in, float *out, doubl
   p.item_begin = item_begin;
   p.item_end = item_end;
   const int blocks = std::min(pl.blocks, p.item_end - p.item_begin);
+  if (wt.start && (e = cudaEventRecord(wt.start, stream)) != cudaSuccess) return e;
   fuse_tma_kernel<HW, RX, TZ, TileOf<SET, HW>::LY, TileOf<SET, HW>::MB>
       <<<blocks, kThreads, C::SMEM, stream>>>(tmA, tmL, p);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (wt.stop && (e = cudaEventRecord(wt.stop, stream)) != cudaSuccess) return e;
   if (whole && pl.groups > 1) return launch_combine_groups(g, partial, pl.groups, out, stream);
   return cudaSuccess;
 }
@@ -856,7 +882,7 @@ cudaError_t plan_any(const Geometry &g, int set, Plan *pl) {
 
 template <int SET>
 cudaError_t launch_set(const Geometry &g, const SlabInputs &in, float *out, double div,
-                       float *partial, int *err, const WaitTest &wt, int ib, int ie,
+                       float *partial, int *err, const LaunchHooks &wt, int ib, int ie,
                        cudaStream_t stream) {
   switch (g.hw) {
     case 1: return launch_hw<SET, 1>(g, in, out, div, partial, err, wt, ib, ie, stream);
@@ -1008,10 +1034,53 @@ TileShape fuse_tile_shape(const Geometry &g) {
   return t;
 }
 
-cudaError_t launch_fuse_tiles(const Geometry &g, const SlabInputs &in, double div, int atlas,
-                              const int *tiles, const int *count, float *acc_p, float *acc_w,
-                              int *err, cudaStream_t stream) {
-  if (g.hw != 5 || atlas < 0 || atlas >= g.num) return cudaErrorInvalidValue;
+namespace {
+
+// One masked item per pair of flagged atlases of every tile with a non-empty mask (any order:
+// each item writes its own partial slot).
+__global__ void masked_items_kernel(const uint32_t *__restrict__ masks, int ntiles,
+                                    int *__restrict__ items, int *__restrict__ count) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += gridDim.x * blockDim.x) {
+    const uint32_t m = masks[t];
+    if (!m) continue;
+    const int pairs = (__popc(m) + 1) / 2;
+    const int at = atomicAdd(count, pairs);
+    for (int k = 0; k < pairs; ++k) items[at + k] = (k << 24) | t;
+  }
+}
+
+// Adds the pair slots of every interior voxel of a masked tile into acc_p / acc_w, in pair order.
+__global__ void masked_combine_kernel(const uint32_t *__restrict__ masks, const TileShape ts,
+                                      int nx, int ny, int nz, int lo, long long nvox,
+                                      const float *__restrict__ partial, float *__restrict__ acc_p,
+                                      float *__restrict__ acc_w) {
+  const int ix = nx - 2 * lo, iy = ny - 2 * lo, iz = nz - 2 * lo;
+  const long long total = (long long)ix * iy * iz;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int yi = (int)(i % iy);
+    const long long r = i / iy;
+    const int xi = (int)(r % ix), zi = (int)(r / ix);
+    const int t = ((zi / ts.zt) * ts.tiles_x + xi / ts.xc) * ts.tiles_y + yi / ts.out_y;
+    const uint32_t m = masks[t];
+    if (!m) continue;
+    const long long v = (long long)(zi + lo) * nx * ny + (long long)(xi + lo) * ny + (yi + lo);
+    float p = acc_p[v], w = acc_w[v];
+    for (int k = 0; k < (__popc(m) + 1) / 2; ++k) {
+      p += partial[(2LL * k) * nvox + v];
+      w += partial[(2LL * k + 1) * nvox + v];
+    }
+    acc_p[v] = p;
+    acc_w[v] = w;
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_fuse_masked(const Geometry &g, const SlabInputs &in, double div, int atlas_base,
+                               const uint32_t *masks, int *items, int *count, float *partial,
+                               float *acc_p, float *acc_w, int *err, cudaStream_t stream) {
+  if (g.hw != 5 || atlas_base < 0 || atlas_base >= g.num) return cudaErrorInvalidValue;
   if (g.ix <= 0 || g.iy <= 0 || g.iz <= 0) return cudaSuccess;
   using T = TileOf<0, 5>;
   using C = Cfg<5, T::RX, T::TZ>;
@@ -1033,21 +1102,28 @@ cudaError_t launch_fuse_tiles(const Geometry &g, const SlabInputs &in, double di
       cudaSuccess)
     return e;
   const TileShape ts = fuse_tile_shape(g);
+  const int ntiles = ts.tiles_y * ts.tiles_x * ts.tiles_z;
+  if (ntiles >= (1 << 24)) return cudaErrorInvalidValue;  // items pack the tile in 24 bits
+  if ((e = cudaMemsetAsync(count, 0, sizeof(int), stream)) != cudaSuccess) return e;
+  masked_items_kernel<<<(ntiles + 255) / 256, 256, 0, stream>>>(masks, ntiles, items, count);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
   Plan pl{};
   pl.tiles_y = ts.tiles_y;
   pl.tiles_x = ts.tiles_x;
   pl.tiles_z = ts.tiles_z;
-  pl.ntiles = ts.tiles_y * ts.tiles_x * ts.tiles_z;
-  pl.groups = g.num;  // atlases_per_group = 1; only group 0 (atlas_base) is run
+  pl.ntiles = ntiles;
+  pl.groups = 2;  // partial slots (the pair of each item), not a plan's atlas groups
   TmaParams p{};
-  p.sv = subject_view(g, in, nullptr, div, nullptr, pl);
-  p.sv.atlas_base = atlas;
-  p.sv.acc_p = acc_p;
-  p.sv.acc_w = acc_w;
+  p.sv = subject_view(g, in, nullptr, div, partial, pl);
+  p.sv.atlas_base = atlas_base;
+  p.sv.atlas_mask = masks;
   p.err = err;
   p.timeout_ns = 2000000000ull;
   p.withhold_cta = -1;
-  kern<<<sm_count() * per_sm, kThreads, C::SMEM, stream>>>(tmA, tmL, p, tiles, count);
+  kern<<<sm_count() * per_sm, kThreads, C::SMEM, stream>>>(tmA, tmL, p, items, count);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  masked_combine_kernel<<<sm_count() * 8, 256, 0, stream>>>(masks, ts, g.nx, g.ny, g.nz, g.lo,
+                                                            g.nvox(), partial, acc_p, acc_w);
   return cudaGetLastError();
 }
 
@@ -1084,7 +1160,7 @@ int fuse_tma_planes_read(const Geometry &g, const FusePlanInfo &info, int ztiles
 }
 
 cudaError_t launch_fuse_tma(const Geometry &g, const SlabInputs &in, float *out, double div,
-                            float *partial, int *err, const WaitTest &wt, int set,
+                            float *partial, int *err, const LaunchHooks &wt, int set,
                             cudaStream_t stream) {
   if (g.ix <= 0 || g.iy <= 0 || g.iz <= 0) return cudaSuccess;
   switch (set) {
@@ -1102,7 +1178,7 @@ cudaError_t launch_fuse_tma_items(const Geometry &g, const SlabInputs &in, doubl
                                   cudaStream_t stream) {
   if (g.ix <= 0 || g.iy <= 0 || g.iz <= 0) return cudaSuccess;
   if (item_begin < 0) return cudaErrorInvalidValue;
-  const WaitTest wt{0};
+  const LaunchHooks wt{0, nullptr, nullptr};
   switch (set) {
     case 0: return launch_set<0>(g, in, nullptr, div, partial, err, wt, item_begin, item_end, stream);
     case 1: return launch_set<1>(g, in, nullptr, div, partial, err, wt, item_begin, item_end, stream);

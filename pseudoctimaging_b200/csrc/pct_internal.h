@@ -36,10 +36,13 @@ struct SlabInputs {
 // non-zero code if a bounded wait gave up; the caller zeroes it beforehand. When the planner
 // splits the atlases into groups (to fill the persistent grid), `partial` must point to
 // fuse_tma_partial_bytes(g) bytes of device scratch; otherwise it may be null.
-// Testing hook for the bounded waits: when timeout_ns != 0, the first CTA withholds its first
-// copies, so its wait runs out after timeout_ns and the launch reports a timeout.
-struct WaitTest {
+// Hooks of one fusion launch. Testing hook for the bounded waits: when timeout_ns != 0, the first
+// CTA withholds its first copies, so its wait runs out after timeout_ns and the launch reports a
+// timeout. Timing hook: non-null start / stop events are recorded on the stream right before and
+// after the fusion kernel (not the group combine).
+struct LaunchHooks {
   unsigned long long timeout_ns;
+  cudaEvent_t start, stop;
 };
 
 // Tile-shape sets compiled into the library (chosen per handle, see pct_autotune).
@@ -52,7 +55,7 @@ struct FusePlanInfo {
 };
 cudaError_t fuse_tma_plan(const Geometry &g, int set, FusePlanInfo *info);
 cudaError_t launch_fuse_tma(const Geometry &g, const SlabInputs &in, float *out, double div,
-                            float *partial, int *err, const WaitTest &wt, int set,
+                            float *partial, int *err, const LaunchHooks &wt, int set,
                             cudaStream_t stream);
 // Pipelined form of the same (plans with 2 or more atlas groups only): the work items
 // [item_begin, item_end) into the partial sums (item = group * tiles + tile);
@@ -74,11 +77,14 @@ struct TileShape {
   int tiles_y, tiles_x, tiles_z;
 };
 TileShape fuse_tile_shape(const Geometry &g);
-// The plain full search of atlas `atlas` (NH = 11) over the *count tiles listed in `tiles` (both
-// on the device), adding every voxel's product and weight sums into acc_p / acc_w.
-cudaError_t launch_fuse_tiles(const Geometry &g, const SlabInputs &in, double div, int atlas,
-                              const int *tiles, const int *count, float *acc_p, float *acc_w,
-                              int *err, cudaStream_t stream);
+// The plain full search (NH = 11) of the flagged (tile, atlas) pairs of up to 32 atlases: bit i
+// of masks[t] flags atlas atlas_base + i for tile t. Lists one item per two flagged atlases of a
+// tile in `items` (room for 16 per tile; its length in *count), runs them into `partial` (slot
+// k of a tile holds its k-th pair's sums: 2 floats per voxel and slot, up to 16 slots), then adds
+// the slots of every interior voxel of a flagged tile into acc_p / acc_w in pair order.
+cudaError_t launch_fuse_masked(const Geometry &g, const SlabInputs &in, double div, int atlas_base,
+                               const uint32_t *masks, int *items, int *count, float *partial,
+                               float *acc_p, float *acc_w, int *err, cudaStream_t stream);
 
 // Batched form: many subjects (NH 7/9/11), one persistent launch.
 struct BatchSubjectIn {
@@ -149,10 +155,15 @@ struct LearnedStreams {
   cudaStream_t aux;
   cudaEvent_t ev[5];  // fork, proposal ready [2], rescoring done [2]
 };
+// A confidence threshold > 0 sends the low-confidence voxels' tiles of the plain kernel to its
+// full search (NH = 11, 16-byte aligned atlas rows) when `fb_partial` holds
+// fallback_partial_bytes(g) of device memory; otherwise (or with other windows) the rescoring
+// runs the whole window for low-confidence rows itself.
+size_t fallback_partial_bytes(const Geometry &g);
 cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInputs &in, float *out,
                            double div, float conf_thr, int block, int level, bool every_voxel,
-                           void *scratch, int *err, const LearnedStreams *streams,
-                           cudaStream_t s);
+                           void *scratch, float *fb_partial, int *err,
+                           const LearnedStreams *streams, cudaStream_t s);
 // The proposal baseline without a network (no convolutions, no proposal kernel): every voxel
 // rescores the k offsets of the window nearest its centre (1 <= k <= 125), with the same exact
 // FP32 rescoring as the learned form. Writes the interior of out.

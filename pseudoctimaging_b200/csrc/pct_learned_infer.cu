@@ -36,6 +36,7 @@ namespace learned {
 namespace {
 
 constexpr float kDblEpsilonF = 2.220446049250313080847e-16f;
+constexpr int kFallbackAtlases = 32;  // atlases per full-search launch of the fallback (mask bits)
 
 
 // ---------------------------------------------------------------- conv1 (tensor cores)
@@ -1353,15 +1354,15 @@ __global__ void __launch_bounds__(kRescoreWarps * 32, 4)
 }
 
 // The confidence fallback at the plain kernel's tile granularity (blocks of 4 x 4 rows share a
-// proposal and its per-voxel confidences): a tile falls back when any of its interior voxels has
-// a confidence below the threshold. Flagged tiles are listed (any order: each tile's result does
-// not depend on it) for the plain kernel, which runs the full search on them; the rescoring skips
-// them. Counts the fallback (voxel, atlas) pairs and the offsets evaluated by their rows.
+// proposal and its per-voxel confidences): a tile falls back for this atlas when any of its
+// interior voxels has a confidence below the threshold. The rescoring skips flagged tiles; bit
+// `bit` of the tile's mask records the atlas for the plain kernel's full search, which runs once
+// for a block of up to 32 atlases. Counts the fallback (voxel, atlas) pairs and the offsets
+// evaluated by their rows.
 __global__ void flag_tiles_kernel(const RowProp *__restrict__ props, int nx, int ny, int nz,
                                   float conf_thr, const TileShape ts,
-                                  unsigned char *__restrict__ flag, int *__restrict__ list,
-                                  int *__restrict__ count,
-                                  unsigned long long *__restrict__ fallbacks,
+                                  unsigned char *__restrict__ flag, uint32_t *__restrict__ masks,
+                                  int bit, unsigned long long *__restrict__ fallbacks,
                                   unsigned long long *__restrict__ evaluated) {
   const int lo = 6;  // NH = 11 only: the plain kernel's tiles of that window
   const int ix = nx - 2 * lo, iy = ny - 2 * lo, iz = nz - 2 * lo;
@@ -1385,7 +1386,7 @@ __global__ void flag_tiles_kernel(const RowProp *__restrict__ props, int nx, int
       }
     flag[t] = any ? 1 : 0;
     if (any) {
-      list[atomicAdd(count, 1)] = t;
+      masks[t] |= 1u << bit;  // one thread per tile; the atlases' launches are ordered
       const unsigned long long rows = (unsigned long long)(z1 - z0) * (x1 - x0);
       atomicAdd(fallbacks, rows * nyv);
       atomicAdd(evaluated, rows * kAxis * kAxis * kAxis);
@@ -1477,11 +1478,17 @@ size_t prop_table_bytes(const Geometry &g) {
   return (rows * sizeof(RowProp) + 255) / 256 * 256;
 }
 
-// The confidence fallback's tile flags, list and count (after the convolutions' lists).
+// The confidence fallback's item count, items (up to 16 per tile), atlas masks and per-atlas tile
+// flags (after the convolutions' lists).
 size_t fallback_bytes(const Geometry &g) {
   const TileShape ts = fuse_tile_shape(g);
   const size_t ntiles = (size_t)ts.tiles_y * ts.tiles_x * ts.tiles_z;
-  return 16 + ntiles * sizeof(int) + ntiles + 256;
+  return 16 + 16 * ntiles * sizeof(int) + ntiles * sizeof(uint32_t) + ntiles + 256;
+}
+
+size_t fallback_partial_bytes(const Geometry &g) {
+  const int slots = (std::min(g.num, kFallbackAtlases) + 1) / 2;
+  return (size_t)2 * slots * (size_t)g.nvox() * sizeof(float);
 }
 
 size_t infer_scratch_bytes(const Geometry &g) {
@@ -1776,8 +1783,8 @@ cudaError_t launch_rescore_prior(int blocks, const PriorList &pl, const float *i
 // input MRI contiguous). Writes the interior of `out`; the border is left untouched.
 cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInputs &in, float *out,
                            double div, float conf_thr, int block, int level, bool every_voxel,
-                           void *scratch, int *err, const LearnedStreams *streams,
-                           cudaStream_t s) {
+                           void *scratch, float *fb_partial, int *err,
+                           const LearnedStreams *streams, cudaStream_t s) {
   if (block < 1 || level < 2 || level > 4) return cudaErrorInvalidValue;
   // work items pack x and z coordinates in 16 bits
   if (g.nx >= 65536 || g.nz >= 65536) return cudaErrorInvalidValue;
@@ -1806,13 +1813,14 @@ cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInp
   const TileShape ts = fuse_tile_shape(g);
   const int ntiles = ts.tiles_y * ts.tiles_x * ts.tiles_z;
   const bool tile_fallback =
-      conf_thr > 0.f && block == kRows && g.hw == 5 && ntiles > 0 && in.pitch % 4 == 0 &&
-      reinterpret_cast<uintptr_t>(in.atlas) % 16 == 0 &&
+      conf_thr > 0.f && fb_partial && block == kRows && g.hw == 5 && ntiles > 0 &&
+      in.pitch % 4 == 0 && reinterpret_cast<uintptr_t>(in.atlas) % 16 == 0 &&
       reinterpret_cast<uintptr_t>(in.label) % 16 == 0;
   unsigned char *fb_region = reinterpret_cast<unsigned char *>(sc.lists) + conv_list_bytes(g);
   int *fb_count = reinterpret_cast<int *>(fb_region);
-  int *fb_list = reinterpret_cast<int *>(fb_region + 16);
-  unsigned char *fb_flag = fb_region + 16 + (size_t)ntiles * sizeof(int);
+  int *fb_items = reinterpret_cast<int *>(fb_region + 16);
+  uint32_t *fb_masks = reinterpret_cast<uint32_t *>(fb_items + 16 * (size_t)ntiles);
+  unsigned char *fb_flag = reinterpret_cast<unsigned char *>(fb_masks + ntiles);
   if ((e = cudaMemsetAsync(sc.pacc, 0, (size_t)nvox * 4 * 2, s)) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(sc.fallbacks, 0, 2 * sizeof(unsigned long long), s)) != cudaSuccess)
     return e;
@@ -1871,10 +1879,13 @@ cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInp
     if (block == kRows && g.ix >= kRows &&
         (long long)g.nz * g.nx * in.pitch < (1LL << 31) - 1) {
       if (tile_fallback) {
-        if ((e = cudaMemsetAsync(fb_count, 0, sizeof(int), s)) != cudaSuccess) return join(e);
+        // atlases in blocks of 32 (the mask bits); a block's full search runs after its last
+        if (a % kFallbackAtlases == 0 &&
+            (e = cudaMemsetAsync(fb_masks, 0, (size_t)ntiles * sizeof(uint32_t), s)) != cudaSuccess)
+          return join(e);
         flag_tiles_kernel<<<(ntiles + 255) / 256, 256, 0, s>>>(
-            props, g.nx, g.ny, g.nz, conf_thr, ts, fb_flag, fb_list, fb_count, sc.fallbacks,
-            sc.evaluated);
+            props, g.nx, g.ny, g.nz, conf_thr, ts, fb_flag, fb_masks, a % kFallbackAtlases,
+            sc.fallbacks, sc.evaluated);
         if ((e = cudaGetLastError()) != cudaSuccess) return join(e);
       }
       if ((e = launch_rescore4(level, rescore_blocks, props, in.img, A, L, g.nx, g.ny, g.nz,
@@ -1883,8 +1894,9 @@ cudaError_t launch_learned(const Geometry &g, const void *weights, const SlabInp
                                RescoreTiles{ts.zt, ts.xc, ts.tiles_x, ts.tiles_y}, g.hw, s)) !=
           cudaSuccess)
         return join(e);
-      if (tile_fallback) {
-        if ((e = launch_fuse_tiles(g, in, div, a, fb_list, fb_count, sc.pacc, sc.wacc, err, s)) !=
+      if (tile_fallback && (a % kFallbackAtlases == kFallbackAtlases - 1 || a == g.num - 1)) {
+        if ((e = launch_fuse_masked(g, in, div, a - a % kFallbackAtlases, fb_masks, fb_items,
+                                    fb_count, fb_partial, sc.pacc, sc.wacc, err, s)) !=
             cudaSuccess)
           return join(e);
       }

@@ -51,6 +51,9 @@ def test_null_handle_is_rejected():
     assert pct.lib.pct_synthesize(null, p, p, p, p, 2, 2, 2, 1, 7, 1.0, 3) == -1
     assert pct.lib.pct_synthesize_device(null, p, p, p, p, 2, 2, 2, 1, 7, 1.0, 3, None) == -1
     assert pct.lib.pct_last_error_message(null) == b""
+    assert pct.lib.pct_set_kernel_timing(null, 1) == -1
+    ms, n = ctypes.c_double(), ctypes.c_int()
+    assert pct.lib.pct_kernel_time(null, ctypes.byref(ms), ctypes.byref(n)) == -1
 
 
 def test_create_rejects_bad_device_index():

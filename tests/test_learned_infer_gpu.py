@@ -244,6 +244,77 @@ def test_partial_fallback_runs_whole_tiles_through_the_plain_kernel():
     assert fell * num == st["fallback_pairs"]
 
 
+def tiles_of(nx, ny, nz):
+    """Interior-relative slices of the plain kernel's tiles (30 y x 12 x x 8 z at NH = 11)."""
+    iz, ix, iy = nz - 2 * LO, nx - 2 * LO, ny - 2 * LO
+    return [(slice(tz, tz + 8), slice(tx, tx + 12), slice(ty, ty + 30))
+            for tz in range(0, iz, 8) for tx in range(0, ix, 12) for ty in range(0, iy, 30)]
+
+
+def test_full_fallback_over_blocks_of_atlases():
+    """A threshold above every confidence sends every (tile, atlas) pair to the plain kernel's full
+    search: 35 atlases run as a block of 32 (16 pairs) and a block of 3 (a pair and a single), and
+    the result is the full search of every atlas, within the plain gate of the FP64 oracle."""
+    nx, ny, nz, num = 30, 45, 30, 35
+    img, atl, lab = subject(nx, ny, nz, num, 61)
+    ref = oracle.fuse_port(img, atl, lab, NH, DIV)
+    core = (slice(LO, nz - LO), slice(LO, nx - LO), slice(LO, ny - LO))
+    with pct.Handle(0) as h, learned.LearnedModel(0, seed=9) as m:
+        h.attach_model(m, 2.0)
+        got = h.synthesize(img, atl, lab, NH, DIV, pct.EXEC_LEARNED)
+        st = h.learned_stats()
+    assert st["fallback_pairs"] == interior(nx, ny, nz) * num
+    g, r = got[core], ref[core]
+    assert np.array_equal(np.isnan(g), np.isnan(r))
+    fin = np.isfinite(r)
+    assert (np.abs(g[fin] - r[fin]) / np.abs(r[fin])).max() <= 1e-4
+
+
+def test_mixed_fallback_tiles_per_atlas():
+    """With several atlases each atlas flags its own tiles: a tile no atlas flags equals the run
+    without fallback bit for bit, a tile every atlas flags is the full search (FP64 oracle within
+    the plain gate), and the fallback count is the sum of the atlases' own counts (each atlas run
+    alone at the same threshold shows which tiles it flags)."""
+    nx, ny, nz, num = 40, 70, 36, 3
+    img, atl, lab = subject(nx, ny, nz, num, 53)
+    ref = oracle.fuse_port(img, atl, lab, NH, DIV)
+    core = (slice(LO, nz - LO), slice(LO, nx - LO), slice(LO, ny - LO))
+    tiles = tiles_of(nx, ny, nz)
+    with pct.Handle(0) as h, learned.LearnedModel(0, seed=9) as m:
+        h.attach_model(m, 0.0)
+        base = h.synthesize(img, atl, lab, NH, DIV, pct.EXEC_LEARNED)[core]
+        singles0 = [h.synthesize(img, atl[a:a + 1], lab[a:a + 1], NH, DIV,
+                                 pct.EXEC_LEARNED)[core] for a in range(num)]
+        found = None
+        for thr in np.geomspace(1e-3, 0.5, 40):
+            h.attach_model(m, float(thr))
+            got = h.synthesize(img, atl, lab, NH, DIV, pct.EXEC_LEARNED)[core]
+            st = h.learned_stats()
+            if 0 < st["fallback_pairs"] < interior(nx, ny, nz) * num:
+                flagged, count = [], 0
+                for a in range(num):
+                    one = h.synthesize(img, atl[a:a + 1], lab[a:a + 1], NH, DIV,
+                                       pct.EXEC_LEARNED)[core]
+                    count += h.learned_stats()["fallback_pairs"]
+                    flagged.append({i for i, t in enumerate(tiles) if not np.array_equal(
+                        one[t].view(np.uint32), singles0[a][t].view(np.uint32))})
+                found = (got, st, flagged, count)
+                break
+    assert found is not None, "no threshold gave a partial fallback"
+    got, st, flagged, count = found
+    assert st["fallback_pairs"] == count
+    assert sum(len(f) for f in flagged) > 0
+    r = ref[core]
+    for i, t in enumerate(tiles):
+        hit = sum(i in f for f in flagged)
+        if hit == 0:
+            assert np.array_equal(got[t].view(np.uint32), base[t].view(np.uint32))
+        elif hit == num:
+            fin = np.isfinite(r[t])
+            assert np.array_equal(np.isnan(got[t]), np.isnan(r[t]))
+            assert (np.abs(got[t][fin] - r[t][fin]) / np.abs(r[t][fin])).max() <= 1e-4
+
+
 def test_probe_matches_float64_network():
     nx, ny, nz = 38, 45, 31
     img, atl, _ = subject(nx, ny, nz, 1, 41)

@@ -155,6 +155,40 @@ def test_device_api_writes_interior_only(handle):
     assert np.array_equal(o[sl].view(np.uint32), host[sl].view(np.uint32))
 
 
+def test_kernel_timing_counts_fusion_launches():
+    """The fusion kernel's own device time, as the benchmark's roofline reads it: one timed
+    launch per plain call while timing is on, each inside the call's own span on the stream,
+    none while it is off, and a read starts the count over."""
+    g = load_golden("nh9_3atlas")
+    nh, div = 9, float(g["div"])
+    dev = torch.device("cuda:0")
+    img, atl, lab = (torch.from_numpy(g[k]).to(dev) for k in ("img", "atlas_mri", "label"))
+    out = torch.zeros_like(img)
+    nz, nx, ny = img.shape
+    stream = torch.cuda.current_stream()
+    with pct.Handle(0) as h:
+        def call():
+            h.synthesize_device(img.data_ptr(), atl.data_ptr(), lab.data_ptr(), out.data_ptr(),
+                                nx, ny, nz, atl.shape[0], nh, div, pct.EXEC_B200_FP32,
+                                stream.cuda_stream)
+        call()
+        assert h.kernel_time() == (0.0, 0)
+        h.set_kernel_timing(True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(3):
+            call()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms, n = h.kernel_time()
+        assert n == 3 and 0.0 < ms <= e0.elapsed_time(e1)
+        assert h.kernel_time() == (0.0, 0)
+        h.set_kernel_timing(False)
+        call()
+        torch.cuda.synchronize()
+        assert h.kernel_time() == (0.0, 0)
+
+
 @pytest.fixture(scope="module")
 def full_subject():
     """Config 1 inputs: 222x222x112, 60 blobs, 10 atlases (seed 1)."""
