@@ -1745,6 +1745,26 @@ cudaError_t launch_rescore4(int level, int blocks, const RowProp *props, const f
                             unsigned long long *fallbacks, unsigned long long *evaluated,
                             const unsigned char *tile_flag, RescoreTiles ts, int hw,
                             cudaStream_t s) {
+  // z-pair items (two planes of a block per warp) where there are two or more interior planes
+  // and 32 offsets per item (at 10 and 20 the one-plane items' higher occupancy wins: learned
+  // step k = 10 4.02 ms against 4.10, k = 20 4.61 against 4.65, k = 32 5.34 against 5.24)
+  const int lo = hw + 1, ix = nx - 2 * lo, iy = ny - 2 * lo, iz = nz - 2 * lo;
+  const char *pairs_env = getenv("PCT_RS_PAIRS");
+  if (level == 4 && iz >= 2 && ix >= kRows && iy > 0 && !(pairs_env && pairs_env[0] == '0')) {
+    void *f8 = rescore_jit(level == 2 ? "pct_rescore8_l2" : level == 3 ? "pct_rescore8_l3"
+                                                                       : "pct_rescore8_l4",
+                           nx, apitch, hw, s);
+    if (f8) {
+      const long long items = (long long)((iz + kRows - 1) / kRows) * 2 * ((ix + kRows - 1) / kRows) *
+                              ((iy + kRowOut - 1) / kRowOut);
+      const long long b8 = (items + kRescoreWarps - 1) / kRescoreWarps;
+      int blocks8 = (int)(b8 > 64LL * sms() ? 64LL * sms() : b8);
+      void *args[] = {&props, &img,     &atl,  &lab,  &nx,        &ny,        &nz,        &apitch,
+                      &scale, &conf_thr, &pacc, &wacc, &fallbacks, &evaluated, &tile_flag, &ts,
+                      &hw};
+      return jit::launch(f8, blocks8, kRescoreWarps * 32, s, args);
+    }
+  }
   void *fn = rescore_jit(level == 2 ? "pct_rescore4_l2" : level == 3 ? "pct_rescore4_l3"
                                                                       : "pct_rescore4_l4",
                          nx, apitch, hw, s);
@@ -1765,6 +1785,23 @@ cudaError_t launch_rescore_prior(int blocks, const PriorList &pl, const float *i
                                  const float *atl, const float *lab, int nx, int ny, int nz,
                                  int apitch, float scale, float *pacc, float *wacc,
                                  unsigned long long *evaluated, int hw, cudaStream_t s) {
+  // z-pair items from 32 offsets on, as for the proposals (prior k = 81: 4.54 ms against 4.85,
+  // k = 123 6.59 against 7.20)
+  const int lo = hw + 1, ix = nx - 2 * lo, iy = ny - 2 * lo, iz = nz - 2 * lo;
+  const char *pairs_env = getenv("PCT_RS_PAIRS");
+  if (pl.n >= 32 && iz >= 2 && ix >= kRows && iy > 0 && !(pairs_env && pairs_env[0] == '0')) {
+    void *f8 = rescore_jit("pct_rescore_prior8", nx, apitch, hw, s);
+    if (f8) {
+      const long long items = (long long)((iz + kRows - 1) / kRows) * 2 * ((ix + kRows - 1) / kRows) *
+                              ((iy + kRowOut - 1) / kRowOut);
+      const long long b8 = (items + kRescoreWarps - 1) / kRescoreWarps;
+      int blocks8 = (int)(b8 > 64LL * sms() ? 64LL * sms() : b8);
+      PriorList copy = pl;
+      void *args[] = {&copy, &img, &atl, &lab, &nx, &ny, &nz, &apitch, &scale, &pacc, &wacc,
+                      &evaluated, &hw};
+      return jit::launch(f8, blocks8, kRescoreWarps * 32, s, args);
+    }
+  }
   void *fn = rescore_jit("pct_rescore_prior", nx, apitch, hw, s);
   if (fn) {
     PriorList copy = pl;

@@ -16,7 +16,11 @@
 // 4 x 4 (z, x) block, which share a proposal and most of their atlas footprint in L1. The last
 // item of an x band is shifted back to end at the last interior row, the rows the previous item
 // owns left out, so no load needs a clamp. Needs at least 4 interior x-rows and an atlas volume
-// below 2^31 elements (32-bit offsets).
+// below 2^31 elements (32-bit offsets). The z-pair entry points (pct_rescore8_*, 2 or more
+// interior planes) give a warp the same 4 x-rows in two consecutive planes of a block: the two
+// patches share two of their three atlas planes, so an offset takes 24 tap loads for 8 rows
+// instead of 36 (learned step at 222x222x112, 10 atlases, k = 32: 5.19 ms against 5.31 with the
+// one-plane items; 96 registers at 5 CTAs per SM; 4 CTAs 5.33 ms, 6 CTAs 5.24 with spills).
 //
 // Per offset the 3 z x 6 x tap rows the 4 rows need are loaded once, D = (s A - s I)^2 (the
 // weight scale s folded into the differences, x-rows in pairs on packed FP32 FMAs), z summed in
@@ -34,6 +38,9 @@
 #endif
 #ifndef PCT_RS_MIN_CTAS
 #define PCT_RS_MIN_CTAS 7  // of the run-time compiled entry points
+#endif
+#ifndef PCT_RS_MIN_CTAS8
+#define PCT_RS_MIN_CTAS8 5  // of the run-time compiled z-pair entry points (measured above)
 #endif
 
 constexpr int kRsAxis = 11;       // offsets per axis of the NH = 11 window
@@ -279,6 +286,212 @@ __device__ __forceinline__ void rescore4_body(
   if (lane == 0 && my_evals) atomicAdd(evaluated, my_evals);
 }
 
+// ---- z-pair items: one warp = the same 4 x-rows in two consecutive z planes of one block
+
+// One offset for the 8 rows of a z-pair item: rows r (plane z0) and 4 + r (plane z0 + 1). `a`
+// points at the atlas voxel (z0 - 1 + dw, x0 - 1 + du, yc + dv), `l` at the label voxel (z0 + dw,
+// x0 + du, yc + dv). The two planes' patches share their middle two atlas planes, so an offset
+// loads 4 x 6 tap rows instead of 2 x 3 x 6; each row's arithmetic is eval_offset4's, in the same
+// order, so a row's sums are the same bits either way.
+template <bool MASKED>
+__device__ __forceinline__ void eval_offset8(const float *__restrict__ a,
+                                             const float *__restrict__ l,
+                                             const float2 (&in)[4][(kRows + 2) / 2], int axy,
+                                             int apitch, unsigned take, float2 s2,
+                                             float (&P)[2 * kRows], float (&W)[2 * kRows]) {
+  float Z[2][kRows + 2];
+#pragma unroll
+  for (int xp = 0; xp < (kRows + 2) / 2; ++xp) {
+    const int ro = 2 * xp * apitch;
+    float2 t[4];
+#pragma unroll
+    for (int dz = 0; dz < 4; ++dz) {
+      const float2 av = make_float2(__ldg(a + (ro + dz * axy)), __ldg(a + (ro + apitch + dz * axy)));
+      t[dz] = __ffma2_rn(av, s2, in[dz][xp]);
+    }
+#pragma unroll
+    for (int pz = 0; pz < 2; ++pz) {
+      float2 z = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int dz = 0; dz < 3; ++dz) z = __ffma2_rn(t[pz + dz], t[pz + dz], z);
+      Z[pz][2 * xp] = z.x;
+      Z[pz][2 * xp + 1] = z.y;
+    }
+  }
+#pragma unroll
+  for (int pz = 0; pz < 2; ++pz)
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) {
+      const float x = Z[pz][r] + Z[pz][r + 1] + Z[pz][r + 2];
+      const float e =
+          __shfl_up_sync(0xffffffffu, x, 1) + x + __shfl_down_sync(0xffffffffu, x, 1);
+      if (!MASKED || ((take >> (pz * kRows + r)) & 1u)) {
+        const float w = rs_ex2(-e);
+        P[pz * kRows + r] = fmaf(w, __ldg(l + (pz * axy + r * apitch)), P[pz * kRows + r]);
+        W[pz * kRows + r] += w;
+      }
+    }
+}
+
+// Item `it` = ((z block * nbx + bx) * segs + seg) * 2 + pair of the interior grid: planes zq, zq + 1
+// with zq = lo + 4 z block + 2 pair; a pair whose second plane lies past the interior is shifted
+// back by one plane and owns only its second plane (needs 2 or more interior planes). Bits r and
+// 4 + r of `owned` / `take` are row r of the first and the second plane.
+__device__ __forceinline__ bool rs_place2(long long it, int nx, int ny, int nz, int lo, int segs,
+                                          int nbx, int lane, RsItem &t, int &zq) {
+  const long long r0 = it / 2;
+  t.seg = (int)(r0 % segs);
+  const long long r1 = r0 / segs;
+  t.bx = (int)(r1 % nbx);
+  zq = (int)(r1 / nbx) * kRows + 2 * (int)(it % 2) + lo;
+  if (zq >= nz - lo) return false;
+  t.z = min(zq, nz - lo - 2);
+  t.xb = lo + t.bx * kRows;
+  t.x0 = min(t.xb, nx - lo - kRows);
+  t.y = lo + t.seg * kRowOut - 1 + lane;
+  t.out = lane >= 1 && lane <= kRowOut && t.y < ny - lo;
+  t.owned = 0;
+#pragma unroll
+  for (int r = 0; r < kRows; ++r)
+    if (t.x0 + r >= t.xb) t.owned |= (t.z == zq ? 1u : 0u) << r | 1u << (kRows + r);
+  t.take = t.out ? t.owned : 0u;
+  return true;
+}
+
+// Input taps I(z0 + dz - 1, x0 - 1 + xr, yc) of a z-pair item (4 planes), negated and scaled.
+__device__ __forceinline__ void rs_inputs2(const float *__restrict__ img, int nx, int ny,
+                                           const RsItem &t, int yc, float scale,
+                                           float2 (&in)[4][(kRows + 2) / 2]) {
+  const long long nxy = (long long)nx * ny;
+#pragma unroll
+  for (int dz = 0; dz < 4; ++dz)
+#pragma unroll
+    for (int xp = 0; xp < (kRows + 2) / 2; ++xp) {
+      const float *pi = img + (long long)(t.z + dz - 1) * nxy + (long long)(t.x0 - 1 + 2 * xp) * ny + yc;
+      in[dz][xp] = make_float2(-__ldg(pi) * scale, -__ldg(pi + ny) * scale);
+    }
+}
+
+__device__ __forceinline__ void rs_store2(const RsItem &t, int nx, int ny,
+                                          const float (&P)[2 * kRows],
+                                          const float (&W)[2 * kRows], float *__restrict__ pacc,
+                                          float *__restrict__ wacc) {
+  const long long nxy = (long long)nx * ny;
+#pragma unroll
+  for (int pz = 0; pz < 2; ++pz)
+#pragma unroll
+    for (int r = 0; r < kRows; ++r)
+      if ((t.take >> (pz * kRows + r)) & 1u) {
+        const long long v = (long long)(t.z + pz) * nxy + (long long)(t.x0 + r) * ny + t.y;
+        pacc[v] += P[pz * kRows + r];
+        wacc[v] += W[pz * kRows + r];
+      }
+}
+
+// rescore4_body over z-pair items (2 or more interior planes): the same proposals, offsets,
+// fallback rule and per-row arithmetic, 8 rows per warp.
+template <int LEVEL>
+__device__ __forceinline__ void rescore8_body(
+    const RowProp *__restrict__ props, const float *__restrict__ img, const float *__restrict__ atl,
+    const float *__restrict__ lab, int nx, int ny, int nz, int apitch, float scale, float conf_thr,
+    float *__restrict__ pacc, float *__restrict__ wacc, unsigned long long *__restrict__ fallbacks,
+    unsigned long long *__restrict__ evaluated, const unsigned char *__restrict__ tile_flag,
+    const RescoreTiles ts, int hw) {
+  __shared__ int s_off[kRescoreWarps][kRsTopK];
+#ifdef PCT_RS_NX
+  nx = PCT_RS_NX;
+#endif
+#ifdef PCT_RS_PITCH
+  apitch = PCT_RS_PITCH;
+#endif
+#ifdef PCT_RS_HW
+  hw = PCT_RS_HW;
+#endif
+  const int lane = threadIdx.x & 31;
+  int *w_off = s_off[threadIdx.x >> 5];
+  const int lo = hw + 1;
+  const int ix = nx - 2 * lo, iz = nz - 2 * lo, iy = ny - 2 * lo;
+  if (ix < kRows || iy <= 0 || iz < 2) return;
+  const int segs = (iy + kRowOut - 1) / kRowOut;
+  const int nbx = (ix + kRows - 1) / kRows;
+  const long long items = (long long)((iz + kRows - 1) / kRows) * 2 * nbx * segs;
+  const int axy = nx * apitch;
+  unsigned long long my_fallbacks = 0, my_evals = 0;
+  for (long long it = (long long)blockIdx.x * kRescoreWarps + (threadIdx.x >> 5); it < items;
+       it += (long long)gridDim.x * kRescoreWarps) {
+    RsItem t;
+    int zq;
+    if (!rs_place2(it, nx, ny, nz, lo, segs, nbx, lane, t, zq)) continue;
+    // both planes lie in one tile of the plain kernel (tiles start at even planes from lo), or
+    // only the second is owned
+    if (tile_flag &&
+        tile_flag[((zq - lo) / ts.zt * ts.tiles_x + (t.xb - lo) / ts.xc) * ts.tiles_y + t.seg])
+      continue;
+    const int yc = min(t.y, ny - lo);
+    const RowProp &rp = props[((long long)((zq - lo) / kRows) * nbx + t.bx) * segs + t.seg];
+    int top[3][4];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) top[a][r] = rp.top[a * 4 + r];
+    {
+      const int code = kRankTriples[lane];
+      const int dw = pick4(top[0], code & 3) - 5, du = pick4(top[1], (code >> 2) & 3) - 5,
+                dv = pick4(top[2], code >> 4) - 5;
+      __syncwarp();
+      w_off[lane] = dw * axy + du * apitch + dv;
+      __syncwarp();
+    }
+    const bool full = t.out && conf_thr > 0.f && rp.conf[lane - 1] < conf_thr;
+    const unsigned any_full = __ballot_sync(0xffffffffu, full);
+    if (full) my_fallbacks += __popc(t.take);
+    float2 in[4][(kRows + 2) / 2];
+    rs_inputs2(img, nx, ny, t, yc, scale, in);
+    const float2 s2 = make_float2(scale, scale);
+    const float *ab = atl + ((long long)(t.z - 1) * axy + (long long)(t.x0 - 1) * apitch + yc);
+    const float *lb = lab + ((long long)t.z * axy + (long long)t.x0 * apitch + yc);
+    float P[2 * kRows], W[2 * kRows];
+#pragma unroll
+    for (int r = 0; r < 2 * kRows; ++r) P[r] = W[r] = 0.f;
+    if (!any_full) {
+      constexpr int kept = LEVEL <= 2 ? 10 : LEVEL == 3 ? 20 : 32;
+#pragma unroll kRsUnroll
+      for (int c = 0; c < kept; ++c) {
+        const int off = w_off[c];
+        eval_offset8<false>(ab + off, lb + off, in, axy, apitch, t.take, s2, P, W);
+      }
+      my_evals += (unsigned long long)kept * __popc(t.owned);
+    } else {
+      unsigned long long rank[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        rank[a] = 0x77777777777ULL;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          rank[a] &= ~(0xFULL << (4 * top[a][r]));
+          rank[a] |= (unsigned long long)r << (4 * top[a][r]);
+        }
+      }
+      for (int jw = 5 - hw; jw <= 5 + hw; ++jw) {
+        const int rw = (int)((rank[0] >> (4 * jw)) & 0xF);
+        for (int ju = 5 - hw; ju <= 5 + hw; ++ju) {
+          const int ru = rw + (int)((rank[1] >> (4 * ju)) & 0xF);
+          for (int jv = 5 - hw; jv <= 5 + hw; ++jv) {
+            const bool mine = full || (ru + (int)((rank[2] >> (4 * jv)) & 0xF) <= LEVEL);
+            const int off = (jw - 5) * axy + (ju - 5) * apitch + (jv - 5);
+            eval_offset8<true>(ab + off, lb + off, in, axy, apitch, mine ? t.take : 0u, s2, P, W);
+          }
+        }
+      }
+      const unsigned long long nw = 2 * hw + 1;
+      my_evals += nw * nw * nw * __popc(t.owned);
+    }
+    rs_store2(t, nx, ny, P, W, pacc, wacc);
+  }
+  if (my_fallbacks) atomicAdd(fallbacks, my_fallbacks);
+  if (lane == 0 && my_evals) atomicAdd(evaluated, my_evals);
+}
+
 // The proposal baseline without a network: every voxel rescores the same k offsets, the ones of
 // the window nearest its centre. Same items, taps and arithmetic as the proposal rescoring.
 __device__ __forceinline__ void rescore_prior_body(
@@ -328,6 +541,55 @@ __device__ __forceinline__ void rescore_prior_body(
   if (lane == 0 && my_evals) atomicAdd(evaluated, my_evals);
 }
 
+// rescore_prior_body over z-pair items (2 or more interior planes).
+__device__ __forceinline__ void rescore_prior8_body(
+    const PriorList &pl, const float *__restrict__ img, const float *__restrict__ atl,
+    const float *__restrict__ lab, int nx, int ny, int nz, int apitch, float scale,
+    float *__restrict__ pacc, float *__restrict__ wacc, unsigned long long *__restrict__ evaluated,
+    int hw) {
+#ifdef PCT_RS_NX
+  nx = PCT_RS_NX;
+#endif
+#ifdef PCT_RS_PITCH
+  apitch = PCT_RS_PITCH;
+#endif
+#ifdef PCT_RS_HW
+  hw = PCT_RS_HW;
+#endif
+  const int lane = threadIdx.x & 31;
+  const int lo = hw + 1;
+  const int ix = nx - 2 * lo, iz = nz - 2 * lo, iy = ny - 2 * lo;
+  if (ix < kRows || iy <= 0 || iz < 2) return;
+  const int segs = (iy + kRowOut - 1) / kRowOut;
+  const int nbx = (ix + kRows - 1) / kRows;
+  const long long items = (long long)((iz + kRows - 1) / kRows) * 2 * nbx * segs;
+  const int axy = nx * apitch;
+  unsigned long long my_evals = 0;
+  for (long long it = (long long)blockIdx.x * kRescoreWarps + (threadIdx.x >> 5); it < items;
+       it += (long long)gridDim.x * kRescoreWarps) {
+    RsItem t;
+    int zq;
+    if (!rs_place2(it, nx, ny, nz, lo, segs, nbx, lane, t, zq)) continue;
+    const int yc = min(t.y, ny - lo);
+    float2 in[4][(kRows + 2) / 2];
+    rs_inputs2(img, nx, ny, t, yc, scale, in);
+    const float2 s2 = make_float2(scale, scale);
+    const float *ab = atl + ((long long)(t.z - 1) * axy + (long long)(t.x0 - 1) * apitch + yc);
+    const float *lb = lab + ((long long)t.z * axy + (long long)t.x0 * apitch + yc);
+    float P[2 * kRows], W[2 * kRows];
+#pragma unroll
+    for (int r = 0; r < 2 * kRows; ++r) P[r] = W[r] = 0.f;
+#pragma unroll kRsUnroll
+    for (int c = 0; c < pl.n; ++c) {
+      const int off = pl.off[c];
+      eval_offset8<false>(ab + off, lb + off, in, axy, apitch, t.take, s2, P, W);
+    }
+    my_evals += (unsigned long long)pl.n * __popc(t.owned);
+    rs_store2(t, nx, ny, P, W, pacc, wacc);
+  }
+  if (lane == 0 && my_evals) atomicAdd(evaluated, my_evals);
+}
+
 #ifdef PCT_RS_JIT
 // Entry points of the run-time compiled module (same parameters as the library's kernels).
 #define PCT_RS_ENTRY(NAME, LEVEL)                                                                 \
@@ -345,6 +607,21 @@ PCT_RS_ENTRY(pct_rescore4_l2, 2)
 PCT_RS_ENTRY(pct_rescore4_l3, 3)
 PCT_RS_ENTRY(pct_rescore4_l4, 4)
 #undef PCT_RS_ENTRY
+#define PCT_RS_ENTRY8(NAME, LEVEL)                                                                \
+  extern "C" __global__ void __launch_bounds__(kRescoreWarps * 32, PCT_RS_MIN_CTAS8) NAME(        \
+      const RowProp *__restrict__ props, const float *__restrict__ img,                           \
+      const float *__restrict__ atl, const float *__restrict__ lab, int nx, int ny, int nz,       \
+      int apitch, float scale, float conf_thr, float *__restrict__ pacc,                          \
+      float *__restrict__ wacc, unsigned long long *__restrict__ fallbacks,                       \
+      unsigned long long *__restrict__ evaluated, const unsigned char *__restrict__ tile_flag,    \
+      const RescoreTiles ts, int hw) {                                                            \
+    rescore8_body<LEVEL>(props, img, atl, lab, nx, ny, nz, apitch, scale, conf_thr, pacc, wacc,   \
+                         fallbacks, evaluated, tile_flag, ts, hw);                                \
+  }
+PCT_RS_ENTRY8(pct_rescore8_l2, 2)
+PCT_RS_ENTRY8(pct_rescore8_l3, 3)
+PCT_RS_ENTRY8(pct_rescore8_l4, 4)
+#undef PCT_RS_ENTRY8
 
 extern "C" __global__ void __launch_bounds__(kRescoreWarps * 32, PCT_RS_MIN_CTAS)
     pct_rescore_prior(const __grid_constant__ PriorList pl, const float *__restrict__ img,
@@ -352,5 +629,14 @@ extern "C" __global__ void __launch_bounds__(kRescoreWarps * 32, PCT_RS_MIN_CTAS
                       int nz, int apitch, float scale, float *__restrict__ pacc,
                       float *__restrict__ wacc, unsigned long long *__restrict__ evaluated, int hw) {
   rescore_prior_body(pl, img, atl, lab, nx, ny, nz, apitch, scale, pacc, wacc, evaluated, hw);
+}
+
+extern "C" __global__ void __launch_bounds__(kRescoreWarps * 32, PCT_RS_MIN_CTAS8)
+    pct_rescore_prior8(const __grid_constant__ PriorList pl, const float *__restrict__ img,
+                       const float *__restrict__ atl, const float *__restrict__ lab, int nx, int ny,
+                       int nz, int apitch, float scale, float *__restrict__ pacc,
+                       float *__restrict__ wacc, unsigned long long *__restrict__ evaluated,
+                       int hw) {
+  rescore_prior8_body(pl, img, atl, lab, nx, ny, nz, apitch, scale, pacc, wacc, evaluated, hw);
 }
 #endif

@@ -487,6 +487,29 @@ def test_runtime_compiled_rescoring_matches_library_build(mode, nh, monkeypatch)
 
 
 
+@pytest.mark.parametrize("mode", ["network", "prior"])
+@pytest.mark.parametrize("nz", [13, 14, 15, 17])
+def test_pair_items_on_thin_volumes(nz, mode, monkeypatch):
+    """The rescoring's z-pair items (two planes of a proposal block per warp) against the one-plane
+    items, bit for bit, on 1 to 5 interior planes: one plane keeps the one-plane items, an odd
+    count shifts the last pair back by a plane that it does not own."""
+    nx, ny, num = 20, 37, 2
+    img, atl, lab = subject(nx, ny, nz, num, 70 + nz)
+    outs = []
+    for pairs in ("1", "0"):
+        monkeypatch.setenv("PCT_RS_PAIRS", pairs)
+        with pct.Handle(0) as h, learned.LearnedModel(0, seed=5) as m:
+            if mode == "prior":
+                h.set_learned_prior(32)
+            else:
+                h.attach_model(m, 0.0)
+            outs.append((h.synthesize(img, atl, lab, NH, DIV, pct.EXEC_LEARNED), h.learned_stats()))
+    (a, sa), (b, sb) = outs
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert sa == sb
+    assert sa["row_offsets"] == rows_of(nx, ny, nz) * 32 * num
+
+
 def window_proposal(nh, k, scales=(0.7, 0.5, 0.3)):
     """The prior network's proposal for an NH window: per axis the softmax of its biases over the
     window's offsets, the 4 most probable (ties: lower offset first), the kept rank triples and
