@@ -158,7 +158,8 @@ int launch_fusion(pct_handle *h, const pct::Geometry &g, const pct::SlabInputs &
   PCT_CUDA(h, cudaMemsetAsync(err, 0, sizeof(int), s));
   pct::LaunchHooks wt{h->wait_test_ns, nullptr, nullptr};
   h->wait_test_ns = 0;
-  if (h->time_kernels && h->kt_used < kMaxTimedLaunches) {
+  // (an empty interior launches nothing, so it records no pair)
+  if (h->time_kernels && h->kt_used < kMaxTimedLaunches && g.ix > 0 && g.iy > 0 && g.iz > 0) {
     while (h->kt_ev.size() < 2 * (h->kt_used + 1)) {
       cudaEvent_t e = nullptr;
       PCT_CUDA(h, cudaEventCreate(&e));
@@ -166,14 +167,13 @@ int launch_fusion(pct_handle *h, const pct::Geometry &g, const pct::SlabInputs &
     }
     wt.start = h->kt_ev[2 * h->kt_used];
     wt.stop = h->kt_ev[2 * h->kt_used + 1];
-    ++h->kt_used;
   }
   PCT_CUDA(h, pct::launch_fuse_tma(g, in, d_out, div, static_cast<float *>(h->partial.ptr), err, wt,
                                    h->tile_set, s));
+  if (wt.stop) ++h->kt_used;  // a pair is read only once the launch between its events was enqueued
   return PCT_OK;
 }
 
-// Reads (and clears) the device status word after `s` has drained.
 // Marks the end of a learned run on `s`, so that pct_learned_stats can read its counters later
 // without touching the caller's stream (which may be gone by then).
 int learned_ran(pct_handle *h, const pct::Geometry &g, cudaStream_t s) {
@@ -288,6 +288,7 @@ int launch_path(pct_handle *h, const pct::Geometry &g, const pct::SlabInputs &in
   return launch_fusion(h, g, in, d_out, div, s);
 }
 
+// Reads (and clears) the device status word after `s` has drained.
 int read_device_status(pct_handle *h, cudaStream_t s) {
   if (!h->err.ptr) return PCT_OK;
   int v = 0;

@@ -183,6 +183,10 @@ def test_kernel_timing_counts_fusion_launches():
         ms, n = h.kernel_time()
         assert n == 3 and 0.0 < ms <= e0.elapsed_time(e1)
         assert h.kernel_time() == (0.0, 0)
+        # a volume with no interior voxel launches no fusion kernel and times nothing
+        flat = np.zeros((2 * 5, 12, 12), np.float32)
+        h.synthesize(flat, flat[None], flat[None], nh, div)
+        assert h.kernel_time() == (0.0, 0)
         h.set_kernel_timing(False)
         call()
         torch.cuda.synchronize()
