@@ -42,6 +42,11 @@
 #ifndef PCT_RS_MIN_CTAS8
 #define PCT_RS_MIN_CTAS8 5  // of the run-time compiled z-pair entry points (measured above)
 #endif
+#ifndef PCT_RS_UNROLL8
+#define PCT_RS_UNROLL8 1  // offsets in flight per warp of the z-pair items
+#endif
+// z-pair entry points, offsets in flight / CTAs per SM (learned step, same workload): 1/5 5.20
+// ms, 2/4 5.29, 2/5 5.60, 1/6 5.24 (spills).
 
 constexpr int kRsAxis = 11;       // offsets per axis of the NH = 11 window
 constexpr int kRsTopK = 32;       // the largest kept set (level 4)
@@ -50,6 +55,7 @@ constexpr int kRescoreWarps = 4;  // warps per CTA
 constexpr int kRows = 4;          // x-rows per warp item (the block edge)
 constexpr int kMaxPrior = 125;    // offsets of the no-network prior (5 x 5 x 5 around the centre)
 constexpr int kRsUnroll = PCT_RS_UNROLL;
+constexpr int kRsUnroll8 = PCT_RS_UNROLL8;
 static_assert(kRescoreWarps == kRows, "a CTA's warps cover the z planes of one block");
 
 // The proposal of one row segment (30 voxels along y) of a block anchor row: the 4 most probable
@@ -455,7 +461,7 @@ __device__ __forceinline__ void rescore8_body(
     for (int r = 0; r < 2 * kRows; ++r) P[r] = W[r] = 0.f;
     if (!any_full) {
       constexpr int kept = LEVEL <= 2 ? 10 : LEVEL == 3 ? 20 : 32;
-#pragma unroll kRsUnroll
+#pragma unroll kRsUnroll8
       for (int c = 0; c < kept; ++c) {
         const int off = w_off[c];
         eval_offset8<false>(ab + off, lb + off, in, axy, apitch, t.take, s2, P, W);
@@ -579,7 +585,7 @@ __device__ __forceinline__ void rescore_prior8_body(
     float P[2 * kRows], W[2 * kRows];
 #pragma unroll
     for (int r = 0; r < 2 * kRows; ++r) P[r] = W[r] = 0.f;
-#pragma unroll kRsUnroll
+#pragma unroll kRsUnroll8
     for (int c = 0; c < pl.n; ++c) {
       const int off = pl.off[c];
       eval_offset8<false>(ab + off, lb + off, in, axy, apitch, t.take, s2, P, W);
