@@ -48,6 +48,7 @@ struct pct_handle {
   cudaEvent_t learned_done = nullptr;   // recorded after the last learned run's kernels
   cudaStream_t copy_stream = nullptr;     // uploads of the pipelined host path
   cudaStream_t compute_stream = nullptr;  // its second compute stream
+  cudaStream_t output_stream = nullptr;   // its combine and download by plane ranges
   std::vector<cudaEvent_t> pipe_ev;       // its fork, one per uploaded part, two joins
   bool time_kernels = false;              // pct_set_kernel_timing
   std::vector<cudaEvent_t> kt_ev;         // start / stop pairs around timed fusion launches
@@ -351,19 +352,23 @@ int stage_pitched_slice(pct_handle *h, DevBuf &buf, float *stage_base, const flo
 }
 
 // The host-pointer path with uploads overlapped with the fusion. The handle's copy stream
-// uploads (and repacks) the subject in parts, each part's fusion items starting as soon as it has
-// landed: the first atlas group with the input MRI in up to three plane ranges (the first holds
+// uploads (and repacks) the subject in parts, each part's work items starting as soon as it has
+// landed: the input MRI and the first atlas group in up to three plane ranges (the first holds
 // the planes read by just enough z-tiles to give every CTA of the grid an item, the second as
 // many z-tiles again, the third the rest), then one part per further group. The launches
 // alternate between `s` and the handle's second compute stream, so that the last round of one
-// launch overlaps the first round of the next; both streams join `s` before the group sums are
-// combined into d_out. Used when the plan has two or more atlas groups; returns
+// launch overlaps the first round of the next. With `host_out`, the last group runs in up to
+// three z-tile ranges as well (the last two as small as the first group's first), and the
+// handle's output stream combines and downloads each range's planes once its items and every
+// earlier launch are done, so that only the last range's combine and download follow the
+// fusion; without it, the group sums are combined into d_out on `s` at the end. Every stream
+// joins `s` before the call returns. Used when the plan has two or more atlas groups; returns
 // PCT_ERR_UNSUPPORTED (nothing enqueued) otherwise. `normalize` applies the label normalisation
 // to the CT stack on the device (the pipeline entry point). The items and the combine's group
 // order are those of the one-launch path, so the result is the same bit for bit.
 int fuse_pipelined(pct_handle *h, const pct::Geometry &g, const float *img, const float *atlas,
                    const float *atlas_ct, float *d_out, double div, bool normalize,
-                   cudaStream_t s) {
+                   float *host_out, cudaStream_t s) {
   pct::FusePlanInfo pl;
   PCT_CUDA(h, pct::fuse_tma_plan(g, h->tile_set, &pl));
   if (pl.groups < 2 || h->wait_test_ns) return PCT_ERR_UNSUPPORTED;
@@ -380,47 +385,74 @@ int fuse_pipelined(pct_handle *h, const pct::Geometry &g, const float *img, cons
   }
   struct Part {
     bool with_img;
-    int a0, a1, z0, z1;  // atlases [a0, a1), planes [z0, z1)
+    int a0, a1, z0, z1;  // upload atlases [a0, a1), planes [z0, z1) (none when z0 == z1)
     int i0, i1;          // work items that may run once it has landed
+    int o0, o1;          // output planes to combine and download after it (none when o0 == o1)
   };
   std::vector<Part> parts;
   const int per = g.num / pl.groups;
+  // z-tile tz holds the output planes [lo + 2 tz TZ, lo + 2 tz TZ + 2 TZ)
+  auto out_plane = [&](int tz) { return tz >= pl.tiles_z ? g.nz : g.lo + 2 * pl.tz * tz; };
+  const int first = std::min(pl.tiles_z, (pl.ctas + pl.tiles_xy - 1) / pl.tiles_xy);
   {
     // z-tile ends of the first group's leading parts; part k reads planes [0, planes_read(end))
-    const int a = std::min(pl.tiles_z, (pl.ctas + pl.tiles_xy - 1) / pl.tiles_xy);
-    const int ends[2] = {a, std::min(pl.tiles_z, 2 * a)};
+    const int ends[2] = {first, std::min(pl.tiles_z, 2 * first)};
     int z0 = 0, t0 = 0;
     for (const int e : ends) {
       if (e <= t0 || e >= pl.tiles_z) continue;
       const int z1 = pct::fuse_tma_planes_read(g, pl, e);
       if (z1 >= g.nz) continue;
-      parts.push_back(Part{true, 0, per, z0, z1, t0 * pl.tiles_xy, e * pl.tiles_xy});
+      parts.push_back(Part{true, 0, per, z0, z1, t0 * pl.tiles_xy, e * pl.tiles_xy, 0, 0});
       z0 = z1;
       t0 = e;
     }
-    parts.push_back(Part{true, 0, per, z0, g.nz, t0 * pl.tiles_xy, pl.tiles});
-    for (int grp = 1; grp < pl.groups; ++grp)
+    parts.push_back(Part{true, 0, per, z0, g.nz, t0 * pl.tiles_xy, pl.tiles, 0, 0});
+    for (int grp = 1; grp < pl.groups - 1; ++grp)
       parts.push_back(Part{false, grp * per, (grp + 1) * per, 0, g.nz, grp * pl.tiles,
-                           (grp + 1) * pl.tiles});
+                           (grp + 1) * pl.tiles, 0, 0});
+    const int last = pl.groups - 1;
+    const int base = last * pl.tiles;
+    if (!host_out) {
+      parts.push_back(Part{false, last * per, g.num, 0, g.nz, base, base + pl.tiles, 0, 0});
+    } else {
+      // the last group uploads whole; its items run in z-tile ranges ending with two of `first`
+      // z-tiles, each range's planes combined and downloaded after it
+      const int starts[3] = {0, std::max(0, pl.tiles_z - 2 * first),
+                             std::max(0, pl.tiles_z - first)};
+      bool uploaded = false;
+      for (int k = 0; k < 3; ++k) {
+        const int t0 = starts[k], t1 = k < 2 ? starts[k + 1] : pl.tiles_z;
+        if (t1 <= t0) continue;
+        parts.push_back(Part{false, last * per, g.num, 0, uploaded ? 0 : g.nz,
+                             base + t0 * pl.tiles_xy, base + t1 * pl.tiles_xy,
+                             t0 == 0 ? 0 : out_plane(t0), out_plane(t1)});
+        uploaded = true;
+      }
+    }
   }
   if (!h->copy_stream)
     PCT_CUDA(h, cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
   if (!h->compute_stream)
     PCT_CUDA(h, cudaStreamCreateWithFlags(&h->compute_stream, cudaStreamNonBlocking));
-  // events: the fork, one per part, two joins
-  while (h->pipe_ev.size() < parts.size() + 3) {
+  if (host_out && !h->output_stream)
+    PCT_CUDA(h, cudaStreamCreateWithFlags(&h->output_stream, cudaStreamNonBlocking));
+  // events: the fork, per part its upload and its launch's completion, three joins
+  const size_t nev = 1 + 2 * parts.size() + 3;
+  while (h->pipe_ev.size() < nev) {
     cudaEvent_t e = nullptr;
     PCT_CUDA(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     h->pipe_ev.push_back(e);
   }
-  const cudaStream_t cs = h->copy_stream;
+  const cudaStream_t cs = h->copy_stream, os = host_out ? h->output_stream : nullptr;
   const cudaStream_t lanes[2] = {s, h->compute_stream};
   int *err = static_cast<int *>(h->err.ptr);
   PCT_CUDA(h, cudaMemsetAsync(err, 0, sizeof(int), s));
-  // fork: the copy stream and the second compute stream follow the work already on s
+  // fork: the copy stream and the other streams follow the work already on s (the output's
+  // memset among it)
   PCT_CUDA(h, cudaEventRecord(h->pipe_ev[0], s));
   PCT_CUDA(h, cudaStreamWaitEvent(cs, h->pipe_ev[0], 0));
   PCT_CUDA(h, cudaStreamWaitEvent(lanes[1], h->pipe_ev[0], 0));
+  if (os) PCT_CUDA(h, cudaStreamWaitEvent(os, h->pipe_ev[0], 0));
   const size_t plane = (size_t)g.nx * g.ny;
   float *stage_mri = static_cast<float *>(h->stage.ptr);
   float *stage_ct = stage_mri ? stage_mri + rows * g.ny : nullptr;
@@ -428,34 +460,59 @@ int fuse_pipelined(pct_handle *h, const pct::Geometry &g, const float *img, cons
                            static_cast<const float *>(h->atlas.ptr),
                            static_cast<const float *>(h->label.ptr), pitch};
   float *partial = static_cast<float *>(h->partial.ptr);
-  // (config 1 end to end: 34.0 ms with the first group whole and the group launches on s alone;
+  // (config 1 end to end: 34.0 ms with the first group uploaded whole and the group launches on
+  // one stream, 29.99 ms with the parts on two streams and the download after the fusion;
   // pitched 2-D host copies of the 888-byte rows instead of the repack kernel made the uploads
   // several times slower: 82.9 ms)
+  auto landed = [&](size_t k) { return h->pipe_ev[1 + 2 * k]; };
+  auto done = [&](size_t k) { return h->pipe_ev[2 + 2 * k]; };
+  size_t last_upload = 0;
   auto run_part = [&](size_t k) -> int {
     const Part &p = parts[k];
-    if (p.with_img)
-      PCT_CUDA(h, cudaMemcpyAsync(static_cast<float *>(h->img.ptr) + p.z0 * plane,
-                                  img + p.z0 * plane, (size_t)(p.z1 - p.z0) * plane * sizeof(float),
-                                  cudaMemcpyHostToDevice, cs));
-    int r = stage_pitched_slice(h, h->atlas, stage_mri, atlas, g, p.a0, p.a1, p.z0, p.z1, false,
-                                cs);
-    if (!r)
-      r = stage_pitched_slice(h, h->label, stage_ct, atlas_ct, g, p.a0, p.a1, p.z0, p.z1,
-                              normalize, cs);
-    if (r) return r;
+    if (p.z1 > p.z0) {
+      if (p.with_img)
+        PCT_CUDA(h, cudaMemcpyAsync(static_cast<float *>(h->img.ptr) + p.z0 * plane,
+                                    img + p.z0 * plane,
+                                    (size_t)(p.z1 - p.z0) * plane * sizeof(float),
+                                    cudaMemcpyHostToDevice, cs));
+      int r = stage_pitched_slice(h, h->atlas, stage_mri, atlas, g, p.a0, p.a1, p.z0, p.z1, false,
+                                  cs);
+      if (!r)
+        r = stage_pitched_slice(h, h->label, stage_ct, atlas_ct, g, p.a0, p.a1, p.z0, p.z1,
+                                normalize, cs);
+      if (r) return r;
+      PCT_CUDA(h, cudaEventRecord(landed(k), cs));
+      last_upload = k;
+    }
     const cudaStream_t ls = lanes[k & 1];
-    PCT_CUDA(h, cudaEventRecord(h->pipe_ev[1 + k], cs));
-    PCT_CUDA(h, cudaStreamWaitEvent(ls, h->pipe_ev[1 + k], 0));
+    PCT_CUDA(h, cudaStreamWaitEvent(ls, landed(last_upload), 0));
     PCT_CUDA(h, pct::launch_fuse_tma_items(g, in, div, partial, err, h->tile_set, p.i0, p.i1, ls));
+    PCT_CUDA(h, cudaEventRecord(done(k), ls));
+    return PCT_OK;
+  };
+  // A range's planes are complete once its launch and the other stream's launch before it are
+  // (each stream runs its launches in order). Every launch is enqueued before the first download:
+  // a download into pageable memory returns only when it has run.
+  auto run_output = [&](size_t k) -> int {
+    const Part &p = parts[k];
+    PCT_CUDA(h, cudaStreamWaitEvent(os, done(k), 0));
+    PCT_CUDA(h, cudaStreamWaitEvent(os, done(k - 1), 0));
+    PCT_CUDA(h, pct::launch_fuse_tma_combine(g, partial, h->tile_set, d_out, p.o0, p.o1, os));
+    PCT_CUDA(h, cudaMemcpyAsync(host_out + p.o0 * plane, d_out + p.o0 * plane,
+                                (size_t)(p.o1 - p.o0) * plane * sizeof(float),
+                                cudaMemcpyDeviceToHost, os));
     return PCT_OK;
   };
   st = PCT_OK;
   for (size_t k = 0; k < parts.size() && !st; ++k) st = run_part(k);
+  for (size_t k = 1; k < parts.size() && !st; ++k)
+    if (parts[k].o1 > parts[k].o0) st = run_output(k);
   // join (on failure too, so that nothing of this call is still running on the other streams
   // when the caller's next call reuses the buffers)
-  const cudaStream_t others[2] = {lanes[1], cs};
-  for (int k = 0; k < 2; ++k) {
-    const cudaEvent_t joined = h->pipe_ev[1 + parts.size() + k];
+  const cudaStream_t others[3] = {lanes[1], cs, os};
+  for (int k = 0; k < 3; ++k) {
+    if (!others[k]) continue;
+    const cudaEvent_t joined = h->pipe_ev[1 + 2 * parts.size() + k];
     if (st) {  // best effort: the call already failed
       if (cudaEventRecord(joined, others[k]) == cudaSuccess) cudaStreamWaitEvent(s, joined, 0);
       continue;
@@ -464,7 +521,8 @@ int fuse_pipelined(pct_handle *h, const pct::Geometry &g, const float *img, cons
     PCT_CUDA(h, cudaStreamWaitEvent(s, joined, 0));
   }
   if (st) return st;
-  PCT_CUDA(h, pct::launch_fuse_tma_combine(g, partial, h->tile_set, d_out, s));
+  if (!host_out)
+    PCT_CUDA(h, pct::launch_fuse_tma_combine(g, partial, h->tile_set, d_out, 0, g.nz, s));
   return PCT_OK;
 }
 
@@ -637,6 +695,7 @@ int pct_destroy(pct_handle *h) {
     if (b->ptr) cudaFree(b->ptr);
   if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
   if (h->compute_stream) cudaStreamDestroy(h->compute_stream);
+  if (h->output_stream) cudaStreamDestroy(h->output_stream);
   if (h->learned_done) cudaEventDestroy(h->learned_done);
   if (h->learned_streams.aux) cudaStreamDestroy(h->learned_streams.aux);
   for (cudaEvent_t e : h->learned_streams.ev)
@@ -824,9 +883,8 @@ int pct_synthesize(pct_handle *h, const float *img, const float *atlas, const fl
   if (uses_tma_rows(exec_choice)) {
     // uploads overlapped with the fusion when the plan has two or more atlas groups
     st = fuse_pipelined(h, g, img, atlas, atlas_label, static_cast<float *>(h->out.ptr), div,
-                        false, s);
-    if (st == PCT_OK) {
-      PCT_CUDA(h, cudaMemcpyAsync(label_segmentation, h->out.ptr, vol, cudaMemcpyDeviceToHost, s));
+                        false, label_segmentation, s);
+    if (st == PCT_OK) {  // the download ran by plane ranges inside, joined into s
       PCT_CUDA(h, cudaStreamSynchronize(s));
       return read_device_status(h, s);
     }
@@ -972,7 +1030,7 @@ int pct_run_pipeline(pct_handle *h, const float *img, const float *atlas_mri,
   float *d_img = static_cast<float *>(h->img.ptr), *d_out = static_cast<float *>(h->out.ptr);
   PCT_CUDA(h, cudaMemsetAsync(d_out, 0, vol, s));
   st = uses_tma_rows(exec_choice)
-           ? fuse_pipelined(h, g, img, atlas_mri, atlas_ct_hu, d_out, div, true, s)
+           ? fuse_pipelined(h, g, img, atlas_mri, atlas_ct_hu, d_out, div, true, nullptr, s)
            : PCT_ERR_UNSUPPORTED;
   if (st == PCT_ERR_UNSUPPORTED) {  // one upload, then the path
     h->last_error.clear();

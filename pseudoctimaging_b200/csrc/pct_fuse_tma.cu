@@ -703,18 +703,20 @@ cudaError_t make_slab_map(CUtensorMap *map, const float *base, int nx, int ny, i
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
-// Sums the per-group partial (product, sum_weight) of every interior voxel in group order and
-// applies the output rule, so the result does not depend on which CTA ran which group.
+// Sums the per-group partial (product, sum_weight) of every interior voxel of planes [z0, z1) in
+// group order and applies the output rule, so the result does not depend on which CTA ran which
+// group.
 __global__ void combine_groups_kernel(const float *__restrict__ partial, int groups, int nx, int ny,
-                                      int nz, int lo, long long nvox, float *__restrict__ out) {
-  const int ix = nx - 2 * lo, iy = ny - 2 * lo, iz = nz - 2 * lo;
-  const long long total = (long long)ix * iy * iz;
+                                      int z0, int z1, int lo, long long nvox,
+                                      float *__restrict__ out) {
+  const int ix = nx - 2 * lo, iy = ny - 2 * lo;
+  const long long total = (long long)ix * iy * (z1 - z0);
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
        i += (long long)gridDim.x * blockDim.x) {
     const int y = (int)(i % iy) + lo;
     const long long r = i / iy;
     const int x = (int)(r % ix) + lo;
-    const int z = (int)(r / ix) + lo;
+    const int z = (int)(r / ix) + z0;
     const long long v = (long long)z * nx * ny + (long long)x * ny + y;
     float pr = 0.f, sw = 0.f;
     for (int g = 0; g < groups; ++g) {
@@ -725,14 +727,23 @@ __global__ void combine_groups_kernel(const float *__restrict__ partial, int gro
   }
 }
 
+// The combine over the interior planes [z0, z1) (clipped to the interior).
 cudaError_t launch_combine_groups(const Geometry &g, const float *partial, int groups, float *out,
-                                  cudaStream_t stream) {
+                                  int z0, int z1, cudaStream_t stream) {
+  z0 = std::max(z0, g.lo);
+  z1 = std::min(z1, g.nz - g.lo);
+  if (z1 <= z0 || g.ix <= 0 || g.iy <= 0) return cudaSuccess;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  combine_groups_kernel<<<sms * 8, 256, 0, stream>>>(partial, groups, g.nx, g.ny, g.nz, g.lo,
+  combine_groups_kernel<<<sms * 8, 256, 0, stream>>>(partial, groups, g.nx, g.ny, z0, z1, g.lo,
                                                      g.nvox(), out);
   return cudaGetLastError();
+}
+
+cudaError_t launch_combine_groups(const Geometry &g, const float *partial, int groups, float *out,
+                                  cudaStream_t stream) {
+  return launch_combine_groups(g, partial, groups, out, 0, g.nz, stream);
 }
 
 // Picks the number of atlas groups (a divisor of num) so that the work items fill the
@@ -1190,13 +1201,13 @@ cudaError_t launch_fuse_tma_items(const Geometry &g, const SlabInputs &in, doubl
 }
 
 cudaError_t launch_fuse_tma_combine(const Geometry &g, const float *partial, int set, float *out,
-                                    cudaStream_t stream) {
+                                    int z_begin, int z_end, cudaStream_t stream) {
   if (g.ix <= 0 || g.iy <= 0 || g.iz <= 0) return cudaSuccess;
   Plan pl;
   cudaError_t e = plan_any(g, set, &pl);
   if (e != cudaSuccess) return e;
   if (pl.groups < 2) return cudaErrorInvalidValue;
-  return launch_combine_groups(g, partial, pl.groups, out, stream);
+  return launch_combine_groups(g, partial, pl.groups, out, z_begin, z_end, stream);
 }
 
 namespace {

@@ -66,8 +66,9 @@ cudaError_t launch_fuse_tma_items(const Geometry &g, const SlabInputs &in, doubl
                                   cudaStream_t stream);
 // Planes [0, n) of the input and atlas volumes that the items of z-tiles [0, ztiles) read.
 int fuse_tma_planes_read(const Geometry &g, const FusePlanInfo &info, int ztiles);
+// The combine of the output planes [z_begin, z_end) (clipped to the interior).
 cudaError_t launch_fuse_tma_combine(const Geometry &g, const float *partial, int set, float *out,
-                                    cudaStream_t stream);
+                                    int z_begin, int z_end, cudaStream_t stream);
 
 // Tiles of the plain kernel as the learned form's fallback sees them (NH = 11, tile set 0): tile
 // t = (tz * tiles_x + tx) * tiles_y + ty covers interior y [30 ty, 30 ty + 30), x rows
