@@ -1722,6 +1722,9 @@ cudaError_t pack_all(const __nv_bfloat16 *wbf, uint32_t *frag, cudaStream_t s) {
 #include "pct_rescore_src.inc"  // k_pct_rescore_source: the text of pct_rescore.cuh
 
 // Resident CTAs per SM of the run-time compiled z-pair rescoring (its launch bound, 96 registers).
+// Its launches are one wave of resident CTAs; the one-plane items keep one CTA per four items
+// (as one wave of 7 per SM they measured slower: k = 20 4.80 ms against 4.61, k = 10 4.35
+// against 4.02).
 constexpr int kRs8CtasPerSm = PCT_RS_MIN_CTAS8;
 
 // An entry point of the rescoring module compiled for this x extent and atlas row pitch, or
